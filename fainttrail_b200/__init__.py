@@ -1,0 +1,202 @@
+"""FaintTrail B200 search backend: Python host binding over the C ABI.
+
+The public C ABI is include/ft_b200.h, implemented by the in-tree CUDA library
+fainttrail_b200/libft_b200.so (built by fainttrail_b200/build.py). This module
+mirrors the reference's plugin interface for the stacking pass
+(FaintTrail include/fainttrail/backend.hpp:71-139): ``StackPass``,
+``StackResult``, ``SearchBackend.run``, ``make_backend``, ``validate_pass``.
+There is no CPU fallback: importing the binding without the built library, or
+running it without a B200, raises.
+"""
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libft_b200.so")
+
+FT_B200_OK, FT_B200_ERROR, FT_B200_CANCELLED = 0, 1, 2
+
+_lib = None
+_lock = threading.Lock()
+
+PROGRESS_FN = C.CFUNCTYPE(C.c_int, C.c_double, C.c_char_p, C.c_void_p)
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+class Cancelled(RuntimeError):
+    """A progress callback asked to stop (types.hpp:70-76)."""
+
+
+def lib():
+    """The loaded C ABI library (raises if it was not built)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"{LIB_PATH} is missing: build it with python -m fainttrail_b200.build")
+            L = C.CDLL(LIB_PATH)
+            _declare(L)
+            _lib = L
+    return _lib
+
+
+def _declare(L):
+    L.ft_b200_version.restype = C.c_char_p
+    L.ft_b200_open.argtypes = [C.c_int, C.c_double, C.POINTER(C.c_void_p)]
+    L.ft_b200_close.argtypes = [C.c_void_p]
+    L.ft_b200_last_error.argtypes = [C.c_void_p]
+    L.ft_b200_last_error.restype = C.c_char_p
+    L.ft_b200_device_info.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.ft_b200_stack.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _i32p, _i32p, C.c_int, C.c_int,
+                                _f32p, _i32p, PROGRESS_FN, C.c_void_p]
+    L.ft_b200_stack_linear.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_int, C.c_int,
+                                       _f32p, _i32p, PROGRESS_FN, C.c_void_p]
+
+
+def exported_symbols():
+    """Names of the entry points include/ft_b200.h declares."""
+    import re
+    with open(os.path.join(os.path.dirname(HERE), "include", "ft_b200.h")) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(ft_b200_[a-z0-9_]+)\s*\(", text)))
+
+
+class Device:
+    """An open B200 context (ft_b200_open). One per host thread."""
+
+    def __init__(self, device=-1, hbm_budget_bytes=0.0):
+        self.L = lib()
+        h = C.c_void_p()
+        if self.L.ft_b200_open(device, hbm_budget_bytes, C.byref(h)) != FT_B200_OK:
+            raise RuntimeError("ft_b200_open: " + self.L.ft_b200_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ft_b200_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def error(self):
+        return self.L.ft_b200_last_error(self.h).decode()
+
+    def check(self, rc, what):
+        if rc == FT_B200_CANCELLED:
+            raise Cancelled("cancelled")
+        if rc != FT_B200_OK:
+            raise RuntimeError(f"{what}: {self.error()}")
+
+    def info(self):
+        name = C.create_string_buffer(256)
+        sms, mem = C.c_int(), C.c_double()
+        self.check(self.L.ft_b200_device_info(self.h, name, 256, C.byref(sms), C.byref(mem)), "device_info")
+        return name.value.decode(), sms.value, mem.value
+
+
+def _progress(fn):
+    if fn is None:
+        return PROGRESS_FN()
+
+    def cb(f, stage, _user):
+        return 1 if fn(f, stage.decode() if stage else "") else 0
+    return PROGRESS_FN(cb)
+
+
+# ----------------------------------------------------------------------------- plugin mirror
+class StackPass:
+    """One stacking pass (backend.hpp:71-78): frames (n, h, w) float32, either
+    times t_h + velocities (m, 2) or an explicit shift table (dx, dy: (m, n))."""
+
+    def __init__(self, frames, t_h=None, velocities=None, shifts=None, min_count=3, threads=0):
+        self.frames = frames
+        self.t_h = t_h
+        self.velocities = velocities
+        self.shifts = shifts
+        self.min_count = min_count
+        self.threads = threads
+
+
+class StackResult:
+    """max_snr (h, w) float32, best_v (h, w) int32 (backend.hpp:99-105)."""
+
+    def __init__(self, max_snr, best_v, timings=None):
+        self.max_snr = max_snr
+        self.best_v = best_v
+        self.timings = timings or []
+
+
+def validate_pass(p):
+    """The checks of validate_pass (backend.cpp:89-108); raises RuntimeError."""
+    if p.frames is None:
+        raise RuntimeError("stack pass: missing frames")
+    f = np.asarray(p.frames)
+    if f.ndim != 3 or f.shape[0] == 0:
+        raise RuntimeError("stack pass: no frames")
+    n = f.shape[0]
+    if p.shifts is not None:
+        dx, dy = (np.asarray(a) for a in p.shifts)
+        if dx.ndim != 2 or dx.shape[1] != n:
+            raise RuntimeError("stack pass: shift table and frame counts differ")
+        if dx.shape[0] < 1 or dy.shape != dx.shape:
+            raise RuntimeError("stack pass: malformed shift table")
+        if p.velocities is not None and len(p.velocities) != dx.shape[0]:
+            raise RuntimeError("stack pass: shift table and velocity counts differ")
+    else:
+        if p.t_h is None or p.velocities is None:
+            raise RuntimeError("stack pass: missing times or velocities")
+        if len(p.t_h) != n:
+            raise RuntimeError("stack pass: frame and time counts differ")
+    if p.min_count < 1:
+        raise RuntimeError("stack pass: min_count must be at least 1")
+
+
+class SearchBackend:
+    """The "b200" stacking backend (SearchBackend, backend.hpp:107-117)."""
+
+    def __init__(self, device=None):
+        self.dev = device if device is not None else Device()
+
+    def name(self):
+        return "b200"
+
+    def description(self):
+        name, sms, mem = self.dev.info()
+        return f"B200 backend: {name}, {mem / 1073741824.0:.1f} GB, {sms} SMs, sm_100a kernels"
+
+    def run(self, p, progress=None):
+        validate_pass(p)
+        frames = np.ascontiguousarray(p.frames, dtype=np.float32)
+        n, h, w = frames.shape
+        ms = np.empty((h, w), np.float32)
+        bv = np.empty((h, w), np.int32)
+        cb = _progress(progress)
+        if p.shifts is not None:
+            dx = np.ascontiguousarray(p.shifts[0], dtype=np.int32)
+            dy = np.ascontiguousarray(p.shifts[1], dtype=np.int32)
+            rc = self.dev.L.ft_b200_stack(self.dev.h, frames, w, h, n, dx, dy, dx.shape[0], p.min_count, ms, bv, cb,
+                                          None)
+        else:
+            t = np.ascontiguousarray(p.t_h, dtype=np.float64)
+            v = np.ascontiguousarray(p.velocities, dtype=np.float64).reshape(-1, 2)
+            rc = self.dev.L.ft_b200_stack_linear(self.dev.h, frames, w, h, n, t, v, v.shape[0], p.min_count, ms, bv,
+                                                 cb, None)
+        self.dev.check(rc, "stack")
+        return StackResult(ms, bv)
+
+
+def make_backend(name="b200", device=None):
+    """make_backend (backend.hpp:139) for this package's one backend."""
+    if name != "b200":
+        raise RuntimeError(f"unknown or unavailable search backend '{name}' (available: b200)")
+    return SearchBackend(device)

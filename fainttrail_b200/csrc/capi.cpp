@@ -1,0 +1,126 @@
+// The C ABI of the B200 backend (include/ft_b200.h): argument checks, error
+// capture and status codes around the C++ engine.
+#include "ft_b200.h"
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+struct ft_b200_ctx {
+    std::unique_ptr<ftb::Context> c;
+};
+
+namespace {
+
+thread_local std::string g_open_error;
+
+ftb::Progress wrap(ft_b200_progress_fn fn, void* user) {
+    if (!fn) return {};
+    return [fn, user](double f, const char* stage) { return fn(f, stage, user) != 0; };
+}
+
+template <class F>
+int guarded(ft_b200_ctx* ctx, F&& f) {
+    if (!ctx || !ctx->c) return FT_B200_ERROR;
+    try {
+        ctx->c->bind();
+        f(*ctx->c);
+        return FT_B200_OK;
+    } catch (const ftb::Cancelled&) {
+        ctx->c->error = "cancelled";
+        return FT_B200_CANCELLED;
+    } catch (const std::exception& e) {
+        ctx->c->error = e.what();
+        return FT_B200_ERROR;
+    }
+}
+
+// validate_pass (backend.cpp:89-108) for the C form of a pass
+void check_pass(const float* frames, int w, int h, int n, int m, int min_count) {
+    if (!frames) throw std::runtime_error("stack pass: missing frames");
+    if (n < 1) throw std::runtime_error("stack pass: no frames");
+    if (w < 1 || h < 1) throw std::runtime_error("stack pass: frames differ in size");
+    if (m < 1) throw std::runtime_error("stack pass: malformed shift table");
+    if (min_count < 1) throw std::runtime_error("stack pass: min_count must be at least 1");
+}
+
+double max_abs(const double* t, int n) {
+    double m = 0;
+    for (int i = 0; i < n; ++i) m = std::max(m, std::fabs(t[i]));
+    return m;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ft_b200_version(void) { return "0.9.1-b200.1"; }
+
+int ft_b200_open(int device, double hbm_budget_bytes, ft_b200_ctx** out) {
+    if (!out) return FT_B200_ERROR;
+    *out = nullptr;
+    try {
+        auto* h = new ft_b200_ctx;
+        h->c = std::make_unique<ftb::Context>(device, hbm_budget_bytes);
+        *out = h;
+        return FT_B200_OK;
+    } catch (const std::exception& e) {
+        g_open_error = e.what();
+        return FT_B200_ERROR;
+    }
+}
+
+void ft_b200_close(ft_b200_ctx* ctx) { delete ctx; }
+
+const char* ft_b200_last_error(const ft_b200_ctx* ctx) {
+    if (!ctx || !ctx->c) return g_open_error.c_str();
+    return ctx->c->error.c_str();
+}
+
+int ft_b200_device_info(ft_b200_ctx* ctx, char* name, int name_len, int* sms, double* hbm_bytes) {
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (name && name_len > 0) {
+            std::strncpy(name, c.name().c_str(), static_cast<size_t>(name_len) - 1);
+            name[name_len - 1] = 0;
+        }
+        if (sms) *sms = c.sms();
+        if (hbm_bytes) *hbm_bytes = c.total_bytes();
+    });
+}
+
+int ft_b200_stack(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const int* dx,
+                  const int* dy, int motions, int min_count, float* max_snr, int* best_v,
+                  ft_b200_progress_fn progress, void* user) {
+    return guarded(ctx, [&](ftb::Context& c) {
+        check_pass(frames, width, height, nframes, motions, min_count);
+        if (!dx || !dy) throw std::runtime_error("stack pass: malformed shift table");
+        if (!max_snr || !best_v) throw std::runtime_error("stack pass: missing outputs");
+        ftb::stack_pass_host(c, frames, width, height, nframes, dx, dy, motions, min_count, nullptr, 0.0, max_snr,
+                             best_v, wrap(progress, user));
+    });
+}
+
+int ft_b200_stack_linear(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes,
+                         const double* t_h, const double* velocities, int motions, int min_count, float* max_snr,
+                         int* best_v, ft_b200_progress_fn progress, void* user) {
+    return guarded(ctx, [&](ftb::Context& c) {
+        check_pass(frames, width, height, nframes, motions, min_count);
+        if (!t_h || !velocities) throw std::runtime_error("stack pass: missing times or velocities");
+        if (!max_snr || !best_v) throw std::runtime_error("stack pass: missing outputs");
+        // round(v t), half away from zero, in double (pass_shift, backend.hpp:87-97)
+        std::vector<int> dx(static_cast<size_t>(motions) * nframes), dy(dx.size());
+        for (int j = 0; j < motions; ++j)
+            for (int i = 0; i < nframes; ++i) {
+                dx[static_cast<size_t>(j) * nframes + i] = static_cast<int>(std::lround(velocities[2 * j] * t_h[i]));
+                dy[static_cast<size_t>(j) * nframes + i] = static_cast<int>(std::lround(velocities[2 * j + 1] * t_h[i]));
+            }
+        ftb::stack_pass_host(c, frames, width, height, nframes, dx.data(), dy.data(), motions, min_count, velocities,
+                             max_abs(t_h, nframes), max_snr, best_v, wrap(progress, user));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+// Device context and the stacking-pass driver of the B200 backend.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+
+namespace ftb {
+
+// ------------------------------------------------------------------ memory
+
+DevBuf::DevBuf(Context* c, size_t bytes, const char* what) : ctx_(c), bytes_(bytes) {
+    c->charge(bytes, what);
+    const cudaError_t e = cudaMallocAsync(&p_, std::max<size_t>(bytes, 1), c->stream());
+    if (e != cudaSuccess) {
+        c->release(bytes);
+        p_ = nullptr;
+        cudaGetLastError();
+        throw CudaError(std::string("allocate ") + what + " (" + std::to_string(bytes) + " bytes): " +
+                        cudaGetErrorString(e));
+    }
+}
+
+void DevBuf::reset() {
+    if (p_) {
+        cudaFreeAsync(p_, ctx_->stream());
+        ctx_->release(bytes_);
+    }
+    p_ = nullptr;
+    bytes_ = 0;
+    ctx_ = nullptr;
+}
+
+Context::Context(int device, double budget_bytes) {
+    if (device < 0) {
+        const char* e = std::getenv("FAINTTRAIL_CUDA_DEVICE");
+        device = e ? std::atoi(e) : 0;
+    }
+    int count = 0;
+    FTB_CHECK(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count)
+        throw std::runtime_error("CUDA device " + std::to_string(device) + " not present (" + std::to_string(count) +
+                                 " found)");
+    device_ = device;
+    FTB_CHECK(cudaSetDevice(device_));
+    cudaDeviceProp prop{};
+    FTB_CHECK(cudaGetDeviceProperties(&prop, device_));
+    if (prop.major != 10) throw std::runtime_error(std::string("this backend is built for sm_100a (B200); device is ") + prop.name);
+    name_ = prop.name;
+    sms_ = prop.multiProcessorCount;
+    smem_optin_ = static_cast<int>(prop.sharedMemPerBlockOptin);
+    total_ = static_cast<double>(prop.totalGlobalMem);
+    size_t free_b = 0, total_b = 0;
+    FTB_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    budget_ = budget_bytes > 0 ? static_cast<size_t>(budget_bytes) : static_cast<size_t>(0.9 * free_b);
+    FTB_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    FTB_CHECK(cudaMalloc(&d_err_, sizeof(int)));
+    FTB_CHECK(cudaMemset(d_err_, 0, sizeof(int)));
+    // keep freed pool memory for reuse instead of returning it at every sync
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device_) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+}
+
+Context::~Context() {
+    cudaSetDevice(device_);
+    scratch_.clear();
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (d_err_) cudaFree(d_err_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Context::bind() const { FTB_CHECK(cudaSetDevice(device_)); }
+
+void Context::charge(size_t bytes, const char* what) {
+    if (used_ + bytes > budget_)
+        throw std::runtime_error(std::string("HBM budget exceeded allocating ") + what + ": " +
+                                 std::to_string((used_ + bytes) / 1048576) + " MiB needed, budget " +
+                                 std::to_string(budget_ / 1048576) + " MiB");
+    used_ += bytes;
+}
+
+void Context::check_kernel_error(const char* what) {
+    FTB_CHECK(cudaStreamSynchronize(stream_));
+    int e = 0;
+    FTB_CHECK(cudaMemcpy(&e, d_err_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e != 0) {
+        FTB_CHECK(cudaMemset(d_err_, 0, sizeof(int)));
+        throw std::runtime_error(std::string(what) + ": a device wait timed out (error " + std::to_string(e) + ")");
+    }
+}
+
+DevBuf& Context::scratch(int slot, size_t bytes, const char* what) {
+    if (static_cast<int>(scratch_.size()) <= slot) scratch_.resize(static_cast<size_t>(slot) + 1);
+    DevBuf& b = scratch_[static_cast<size_t>(slot)];
+    if (b.bytes() < bytes) {
+        b.reset();
+        b = DevBuf(this, bytes, what);
+    }
+    return b;
+}
+
+// ------------------------------------------------------------------ stacking
+
+namespace {
+
+enum Slot { kFrames = 0, kBest, kArg, kMax, kBestV };
+
+// Launch a planned pass in group ranges; between ranges the progress callback
+// is asked (fraction of groups done), as the reference CUDA backend does between
+// its launches (backend_cuda.cu:167-173).
+void run_plan(Context& c, const StackPlan& plan, const float* d_frames, float* d_max, int* d_bv,
+              const Progress& progress) {
+    StackPlanDev dev;
+    dev.upload(plan, c.stream());
+    const int ng = static_cast<int>(plan.groups.size());
+    const int chunks = progress ? std::min(ng, 16) : 1;
+    float* d_best = nullptr;
+    int* d_arg = nullptr;
+    if (chunks > 1) {
+        d_best = c.scratch(kBest, sizeof(float) * static_cast<size_t>(plan.w) * plan.h, "stack maxima").as<float>();
+        d_arg = c.scratch(kArg, sizeof(int) * static_cast<size_t>(plan.w) * plan.h, "stack argmax").as<int>();
+    }
+    try {
+        for (int q = 0; q < chunks; ++q) {
+            const int g0 = static_cast<int>(static_cast<long long>(ng) * q / chunks);
+            const int g1 = static_cast<int>(static_cast<long long>(ng) * (q + 1) / chunks);
+            stack_launch(plan, dev, d_frames, g0, g1, q == 0, q == chunks - 1, d_best, d_arg, d_max, d_bv,
+                         c.err_flag(), c.stream());
+            if (progress) {
+                c.check_kernel_error("stack kernel");
+                if (!progress(static_cast<double>(q + 1) / chunks, "stack")) throw Cancelled();
+            }
+        }
+        c.check_kernel_error("stack kernel");
+    } catch (...) {
+        cudaStreamSynchronize(c.stream());
+        dev.release();
+        throw;
+    }
+    dev.release();
+}
+
+}  // namespace
+
+void stack_pass_device(Context& c, const float* d_frames, int w, int h, int n, const int* dx, const int* dy, int m,
+                       int min_count, const double* vel, double tmax, float* d_max_snr, int* d_best_v,
+                       const Progress& progress) {
+    const StackConfig cfg = choose_stack_config(w, h, n, c.smem_optin());
+    const std::vector<int> order = motion_order(vel, m, tmax, 4.0, 4.0);
+    const StackPlan plan = make_stack_plan(w, h, n, dx, dy, m, min_count, order, cfg);
+    run_plan(c, plan, d_frames, d_max_snr, d_best_v, progress);
+}
+
+void stack_pass_host(Context& c, const float* frames, int w, int h, int n, const int* dx, const int* dy, int m,
+                     int min_count, const double* vel, double tmax, float* max_snr, int* best_v,
+                     const Progress& progress) {
+    c.bind();
+    const int pitch = frame_pitch(w);
+    const size_t plane = static_cast<size_t>(w) * h;
+    float* d_frames =
+        c.scratch(kFrames, sizeof(float) * static_cast<size_t>(pitch) * h * n, "frames").as<float>();
+    float* d_max = c.scratch(kMax, sizeof(float) * plane, "max_snr").as<float>();
+    int* d_bv = c.scratch(kBestV, sizeof(int) * plane, "best_v").as<int>();
+    FTB_CHECK(cudaMemcpy2DAsync(d_frames, sizeof(float) * pitch, frames, sizeof(float) * w, sizeof(float) * w,
+                                static_cast<size_t>(h) * n, cudaMemcpyHostToDevice, c.stream()));
+    stack_pass_device(c, d_frames, w, h, n, dx, dy, m, min_count, vel, tmax, d_max, d_bv, progress);
+    FTB_CHECK(cudaMemcpyAsync(max_snr, d_max, sizeof(float) * plane, cudaMemcpyDeviceToHost, c.stream()));
+    FTB_CHECK(cudaMemcpyAsync(best_v, d_bv, sizeof(int) * plane, cudaMemcpyDeviceToHost, c.stream()));
+    FTB_CHECK(cudaStreamSynchronize(c.stream()));
+}
+
+}  // namespace ftb

@@ -1,0 +1,102 @@
+// Host engine of the B200 backend: device context, memory budget, and the
+// search orchestration behind the C ABI (capi.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <functional>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ft_internal.h"
+
+namespace ftb {
+
+struct Cancelled : std::runtime_error {
+    Cancelled() : std::runtime_error("cancelled") {}
+};
+
+// Progress callback in the reference's form: fraction, stage; false cancels.
+using Progress = std::function<bool(double, const char*)>;
+
+class Context;
+
+// Device allocation charged against the context's HBM budget.
+class DevBuf {
+public:
+    DevBuf() = default;
+    DevBuf(Context* c, size_t bytes, const char* what);
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept { swap(o); }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        DevBuf t(std::move(o));
+        swap(t);
+        return *this;
+    }
+    ~DevBuf() { reset(); }
+    void reset();
+    void swap(DevBuf& o) noexcept {
+        std::swap(ctx_, o.ctx_);
+        std::swap(p_, o.p_);
+        std::swap(bytes_, o.bytes_);
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(p_); }
+    size_t bytes() const { return bytes_; }
+    explicit operator bool() const { return p_ != nullptr; }
+
+private:
+    Context* ctx_ = nullptr;
+    void* p_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+class Context {
+public:
+    Context(int device, double budget_bytes);
+    ~Context();
+    int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+    int sms() const { return sms_; }
+    int smem_optin() const { return smem_optin_; }
+    const std::string& name() const { return name_; }
+    double total_bytes() const { return total_; }
+    size_t budget() const { return budget_; }
+    size_t used() const { return used_; }
+    void charge(size_t bytes, const char* what);
+    void release(size_t bytes) { used_ -= bytes; }
+    int* err_flag() const { return d_err_; }
+    void check_kernel_error(const char* what);  // syncs the stream, reads the error flag
+    void bind() const;                          // make the device current on this thread
+
+    // reusable device buffers, grown on demand
+    DevBuf& scratch(int slot, size_t bytes, const char* what);
+
+    std::string error;
+
+private:
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+    int sms_ = 0, smem_optin_ = 0;
+    std::string name_;
+    double total_ = 0;
+    size_t budget_ = 0, used_ = 0;
+    int* d_err_ = nullptr;
+    std::vector<DevBuf> scratch_;
+};
+
+// One stacking pass over host frames (nframes x h x w) with a motion-major shift
+// table; vel (2 m doubles) only guides the planner's motion order (may be null).
+void stack_pass_host(Context& c, const float* frames, int w, int h, int n, const int* dx, const int* dy, int m,
+                     int min_count, const double* vel, double tmax, float* max_snr, int* best_v,
+                     const Progress& progress);
+
+// The same over frames already on the device (n x h x pitch), results on the
+// device; the split into launches follows the progress granularity.
+void stack_pass_device(Context& c, const float* d_frames, int w, int h, int n, const int* dx, const int* dy, int m,
+                       int min_count, const double* vel, double tmax, float* d_max_snr, int* d_best_v,
+                       const Progress& progress);
+
+}  // namespace ftb

@@ -1,0 +1,105 @@
+// Internal interfaces of the B200 search backend, shared by the CUDA kernel
+// files and the host engine. Everything here is C++; the public surface is the
+// C ABI in include/ft_b200.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace ftb {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void cuda_check(cudaError_t e, const char* what);
+#define FTB_CHECK(call) ::ftb::cuda_check((call), #call)
+
+// Device pixel layout of a frame stack: n frames of h rows, row pitch `pitch`
+// floats (a multiple of 32, so every row starts on a 128-byte boundary, as TMA
+// tensor maps require); columns [w, pitch) are never read as image data.
+inline int frame_pitch(int w) { return (w + 31) / 32 * 32; }
+
+// ------------------------------------------------------------------ stacking
+// A pass plan: the motions are cut into groups whose shifted frame windows fit
+// together in shared memory for one output tile (see stack.cu).
+struct StackGroup {
+    int slot0 = 0;           // first slot of the group in the slot arrays
+    int nslots = 0;          // slots (a multiple of the motion block; pads are -1)
+    int gdxmin = 0, gdxmax = 0, gdymin = 0, gdymax = 0;  // shift extremes over the group
+    int rows_total = 0;      // window rows in shared memory (sum over frames)
+    int win0 = 0;            // first per-frame window descriptor of the group
+};
+
+struct StackWin {            // one frame's window for a group
+    int dx0 = 0;             // window x origin relative to the tile (a multiple of 4)
+    int dy0 = 0;             // window y origin relative to the tile
+    int row0 = 0;            // first shared-memory row of the window
+    int rows = 0;            // rows (a multiple of the TMA box height)
+};
+
+struct StackConfig {         // one compiled kernel variant
+    int ty = 4;              // warps per CTA (rows of warps)
+    int p = 4;               // output rows per thread
+    int tile_w = 32;         // output columns per tile (one warp)
+    int tile_h() const { return ty * p; }
+    int threads() const { return 32 * ty; }
+    int wp = 40;             // window pitch in floats
+    int bh = 4;              // TMA box height (rows)
+    int mblock = 8;          // motions accumulated together in registers
+    int smem_bytes = 200 * 1024;
+};
+
+struct StackPlan {
+    int w = 0, h = 0, n = 0, m = 0, min_count = 1, pitch = 0;
+    StackConfig cfg;
+    std::vector<StackGroup> groups;
+    std::vector<StackWin> wins;               // groups x frames
+    std::vector<int> slot_motion;             // motion index per slot, -1 = pad
+    std::vector<uint16_t> slot_off;           // per group: [frame][slot] shared-memory offsets
+    std::vector<int> slot_off_base;           // per group: start in slot_off (elements)
+    std::vector<short2> slot_shift;           // [slot][frame] clamped (dx, dy), for coverage counts
+    std::vector<float> inv_sqrt;              // float(1 / sqrt(c)), c = 0..n
+    int max_rows = 0;                         // largest rows_total over the groups
+    long long max_group_bytes = 0;            // largest windows + offset table of one group
+    int max_slots = 0;
+    double adds = 0;                          // m * n * w * h
+};
+
+// Motion visiting order for the planner: motions close in velocity first.
+// vel may be null (explicit shift tables keep index order).
+std::vector<int> motion_order(const double* vel, int m, double tmax, double sx_px, double sy_px);
+
+// Build a plan for a pass; dx/dy are motion-major (j * n + i) host tables.
+StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int m, int min_count,
+                          const std::vector<int>& order, const StackConfig& cfg);
+
+StackConfig choose_stack_config(int w, int h, int n, int device_smem_optin);
+
+// Device copy of a plan.
+struct StackPlanDev {
+    StackGroup* groups = nullptr;
+    StackWin* wins = nullptr;
+    int* slot_motion = nullptr;
+    uint16_t* slot_off = nullptr;
+    int* slot_off_base = nullptr;
+    short2* slot_shift = nullptr;
+    float* inv_sqrt = nullptr;
+    int ngroups = 0;
+    void upload(const StackPlan& p, cudaStream_t s);
+    void release();
+    cudaStream_t stream_ = nullptr;
+};
+
+// Run a planned pass over device frames (n x h x pitch); writes max_snr / best_v
+// (h x w, dense). best/arg scratch carry the running maxima between launches
+// when the pass is split into group ranges [g0, g1).
+void stack_launch(const StackPlan& plan, const StackPlanDev& dev, const float* d_frames, int g0, int g1, bool first,
+                  bool last, float* d_best, int* d_arg, float* d_max_snr, int* d_best_v, int* d_err,
+                  cudaStream_t s);
+
+}  // namespace ftb

@@ -1,0 +1,546 @@
+// Shift-and-stack with per-pixel max-S/N and argmax, for sm_100a.
+//
+// Contract (FaintTrail backend.hpp:10-40, CPU reference backend_cpu.cpp:77-204):
+// for output pixel p and motion j, S_j(p) = (sum over covering frames i, in
+// ascending i, of g_i(p + d_ji)) * float(1/sqrt(c)); undefined if c < min_count;
+// max_snr = max_j S_j with ties to the lowest j, best_v = argmax or -1; non-finite
+// maxima become 0. Results are bit-identical to the CPU backend: every sum starts
+// at +0.0f and adds the frames in ascending order with round-to-nearest adds and
+// no fused multiply-add.
+//
+// Design (B200):
+//  * One CTA owns a 32 x TH output tile. The motions are cut (host planner) into
+//    groups whose shifted windows of all n frames fit in shared memory at once;
+//    the CTA walks every group for its tile, so the frames are read from HBM/L2
+//    once per group and every staged float feeds (motions in the group) adds.
+//  * Windows are staged by TMA (cp.async.bulk.tensor, no multicast) with zero
+//    fill outside the frame. A zero from outside the frame adds +0.0f, which is
+//    bit-identical to skipping the frame: the running sum starts at +0.0f and a
+//    round-to-nearest sum of anything but two -0.0f is never -0.0f. The coverage
+//    count c is therefore the only per-frame bookkeeping, and tiles whose group
+//    shifts stay inside the frame (almost all) use c = n without counting.
+//  * Each thread owns P rows of one column (lanes run along x, so every shared
+//    load of a warp is 32 consecutive words: no bank conflicts) and M motions in
+//    registers; the per-(motion, frame) window offset comes from a 16-bit table
+//    staged with the windows.
+//  * The running maximum uses the order-independent rule (larger S/N, or equal
+//    S/N and lower motion index), which equals the reference's ascending strict
+//    scan whatever order the groups are visited in.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <math_constants.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <mutex>
+#include <numeric>
+
+#include "ft_internal.h"
+
+namespace ftb {
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string("CUDA: ") + what + ": " + cudaGetErrorString(e));
+}
+
+// ------------------------------------------------------------------ host plan
+
+std::vector<int> motion_order(const double* vel, int m, double tmax, double sx_px, double sy_px) {
+    std::vector<int> order(static_cast<size_t>(m));
+    std::iota(order.begin(), order.end(), 0);
+    if (!vel || tmax <= 0.0) return order;
+    // patches of the velocity plane whose shifts spread by about sx x sy pixels at
+    // the extreme frame; row-major inside a patch (equal vy = equal dy per frame)
+    std::vector<long long> kx(static_cast<size_t>(m)), ky(static_cast<size_t>(m));
+    for (int j = 0; j < m; ++j) {
+        kx[static_cast<size_t>(j)] = static_cast<long long>(std::floor(vel[2 * j] * tmax / sx_px));
+        ky[static_cast<size_t>(j)] = static_cast<long long>(std::floor(vel[2 * j + 1] * tmax / sy_px));
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        if (ky[a] != ky[b]) return ky[a] < ky[b];
+        if (kx[a] != kx[b]) return kx[a] < kx[b];
+        if (vel[2 * a + 1] != vel[2 * b + 1]) return vel[2 * a + 1] < vel[2 * b + 1];
+        return vel[2 * a] < vel[2 * b];
+    });
+    return order;
+}
+
+namespace {
+inline int floor4(int v) { return (v >> 2) * 4; }  // arithmetic shift: floor for negatives too
+inline int roundup(int v, int q) { return (v + q - 1) / q * q; }
+}  // namespace
+
+StackConfig choose_stack_config(int w, int h, int n, int smem_optin) {
+    (void)w;
+    (void)h;
+    StackConfig c;
+    c.smem_bytes = std::min(smem_optin, 220 * 1024);
+    // tallest tile whose n windows (with 4 rows of vertical spread) fill at most
+    // 3/4 of shared memory, leaving room for the spread and the offset table
+    const int budget = c.smem_bytes * 3 / 4;
+    auto need = [&](int th) { return n * roundup(th + 4, c.bh) * c.wp * 4; };
+    if (need(32) <= budget) {
+        c.ty = 8;
+        c.p = 4;
+    } else if (need(16) <= budget) {
+        c.ty = 4;
+        c.p = 4;
+    } else {
+        c.ty = 4;
+        c.p = 2;
+    }
+    return c;
+}
+
+StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int m, int min_count,
+                          const std::vector<int>& order, const StackConfig& cfg) {
+    if (w <= 0 || h <= 0 || n <= 0 || m <= 0) throw std::runtime_error("stack pass: empty frames or motions");
+    if (min_count < 1) throw std::runtime_error("stack pass: min_count must be at least 1");
+    StackPlan P;
+    P.w = w;
+    P.h = h;
+    P.n = n;
+    P.m = m;
+    P.min_count = min_count;
+    P.pitch = frame_pitch(w);
+    P.cfg = cfg;
+    P.adds = static_cast<double>(m) * n * w * h;
+    const int TW = cfg.tile_w, TH = cfg.tile_h(), WP = cfg.wp, BH = cfg.bh, M = cfg.mblock;
+    // shared memory in floats after the barrier and alignment slack (256 bytes)
+    const long long budget = (cfg.smem_bytes - 256) / 4;
+
+    P.inv_sqrt.assign(static_cast<size_t>(n) + 1, 0.0f);
+    for (int c = 1; c <= n; ++c) P.inv_sqrt[static_cast<size_t>(c)] = static_cast<float>(1.0 / std::sqrt(static_cast<double>(c)));
+
+    // clamped shifts: beyond +-w / +-h a frame never covers, as within
+    auto cdx = [&](int j, int i) { return std::clamp(dx[static_cast<size_t>(j) * n + i], -w, w); };
+    auto cdy = [&](int j, int i) { return std::clamp(dy[static_cast<size_t>(j) * n + i], -h, h); };
+
+    std::vector<int> mnx(static_cast<size_t>(n)), mxx(static_cast<size_t>(n)), mny(static_cast<size_t>(n)),
+        mxy(static_cast<size_t>(n));
+    std::vector<int> tnx(mnx), txx(mxx), tny(mny), txy(mxy);
+    std::vector<int> members;
+
+    auto table_floats = [&](int count) { return static_cast<long long>(roundup(roundup(count, M) * n, 8)) / 2; };
+    auto flush = [&]() {
+        StackGroup g;
+        g.slot0 = static_cast<int>(P.slot_motion.size());
+        const int cnt = static_cast<int>(members.size());
+        g.nslots = roundup(cnt, M);
+        g.win0 = static_cast<int>(P.wins.size());
+        g.gdxmin = g.gdymin = std::numeric_limits<int>::max();
+        g.gdxmax = g.gdymax = std::numeric_limits<int>::min();
+        int row = 0;
+        for (int i = 0; i < n; ++i) {
+            StackWin wv;
+            wv.dx0 = floor4(mnx[static_cast<size_t>(i)]);
+            wv.dy0 = mny[static_cast<size_t>(i)];
+            wv.rows = roundup(TH + mxy[static_cast<size_t>(i)] - mny[static_cast<size_t>(i)], BH);
+            wv.row0 = row;
+            row += wv.rows;
+            P.wins.push_back(wv);
+            g.gdxmin = std::min(g.gdxmin, mnx[static_cast<size_t>(i)]);
+            g.gdxmax = std::max(g.gdxmax, mxx[static_cast<size_t>(i)]);
+            g.gdymin = std::min(g.gdymin, mny[static_cast<size_t>(i)]);
+            g.gdymax = std::max(g.gdymax, mxy[static_cast<size_t>(i)]);
+        }
+        g.rows_total = row;
+        P.max_rows = std::max(P.max_rows, row);
+        P.max_group_bytes = std::max(P.max_group_bytes, static_cast<long long>(row) * WP * 4 +
+                                                            static_cast<long long>(roundup(roundup(cnt, M) * n, 8)) * 2);
+        P.max_slots = std::max(P.max_slots, g.nslots);
+        P.slot_off_base.push_back(static_cast<int>(P.slot_off.size()));
+        const size_t tab = static_cast<size_t>(roundup(g.nslots * n, 8));
+        const size_t base = P.slot_off.size();
+        P.slot_off.resize(base + tab, 0);
+        for (int s = 0; s < g.nslots; ++s) {
+            const int j = members[static_cast<size_t>(std::min(s, cnt - 1))];  // pads repeat the last motion
+            P.slot_motion.push_back(s < cnt ? j : -1);
+            for (int i = 0; i < n; ++i) {
+                const StackWin& wv = P.wins[static_cast<size_t>(g.win0 + i)];
+                const int ddx = cdx(j, i), ddy = cdy(j, i);
+                const long long off = static_cast<long long>(wv.row0 + ddy - wv.dy0) * WP + (ddx - wv.dx0);
+                if (off < 0 || off > 65535) throw std::runtime_error("stack plan: window offset out of range");
+                P.slot_off[base + static_cast<size_t>(i) * g.nslots + static_cast<size_t>(s)] = static_cast<uint16_t>(off);
+                P.slot_shift.push_back(make_short2(static_cast<short>(ddx), static_cast<short>(ddy)));
+            }
+        }
+        P.groups.push_back(g);
+        members.clear();
+    };
+
+    auto start_group = [&](int j) {
+        for (int i = 0; i < n; ++i) {
+            const size_t k = static_cast<size_t>(i);
+            mnx[k] = mxx[k] = cdx(j, i);
+            mny[k] = mxy[k] = cdy(j, i);
+        }
+        if (TW + 3 > WP || static_cast<long long>(n) * roundup(TH, BH) * WP + table_floats(1) > budget)
+            throw std::runtime_error("stack plan: one motion's frame windows exceed shared memory");
+        members.push_back(j);
+    };
+    for (const int j : order) {
+        if (members.empty()) {
+            start_group(j);
+            continue;
+        }
+        bool fits = true;
+        long long rows = 0;
+        for (int i = 0; i < n && fits; ++i) {
+            const size_t k = static_cast<size_t>(i);
+            const int ddx = cdx(j, i), ddy = cdy(j, i);
+            tnx[k] = std::min(mnx[k], ddx);
+            txx[k] = std::max(mxx[k], ddx);
+            tny[k] = std::min(mny[k], ddy);
+            txy[k] = std::max(mxy[k], ddy);
+            if (txx[k] - floor4(tnx[k]) + TW > WP) fits = false;
+            rows += roundup(TH + txy[k] - tny[k], BH);
+        }
+        const int cnt = static_cast<int>(members.size()) + 1;
+        if (fits && rows * WP + table_floats(cnt) > budget) fits = false;
+        if (!fits) {
+            flush();
+            start_group(j);
+            continue;
+        }
+        mnx.swap(tnx);
+        mxx.swap(txx);
+        mny.swap(tny);
+        mxy.swap(txy);
+        members.push_back(j);
+    }
+    if (!members.empty()) flush();
+    return P;
+}
+
+void StackPlanDev::upload(const StackPlan& p, cudaStream_t s) {
+    release();
+    auto put = [&](auto*& dst, const auto& v) {
+        using T = std::remove_reference_t<decltype(v[0])>;
+        const size_t bytes = std::max<size_t>(1, v.size()) * sizeof(T);
+        FTB_CHECK(cudaMallocAsync(reinterpret_cast<void**>(&dst), bytes, s));
+        if (!v.empty()) FTB_CHECK(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    };
+    put(groups, p.groups);
+    put(wins, p.wins);
+    put(slot_motion, p.slot_motion);
+    put(slot_off, p.slot_off);
+    put(slot_off_base, p.slot_off_base);
+    put(slot_shift, p.slot_shift);
+    put(inv_sqrt, p.inv_sqrt);
+    ngroups = static_cast<int>(p.groups.size());
+    stream_ = s;
+}
+
+void StackPlanDev::release() {
+    for (void* q : {static_cast<void*>(groups), static_cast<void*>(wins), static_cast<void*>(slot_motion),
+                    static_cast<void*>(slot_off), static_cast<void*>(slot_off_base), static_cast<void*>(slot_shift),
+                    static_cast<void*>(inv_sqrt)})
+        if (q) cudaFreeAsync(q, stream_);
+    groups = nullptr;
+    wins = nullptr;
+    slot_motion = nullptr;
+    slot_off = nullptr;
+    slot_off_base = nullptr;
+    slot_shift = nullptr;
+    inv_sqrt = nullptr;
+    ngroups = 0;
+}
+
+// ------------------------------------------------------------------ device
+
+namespace {
+
+struct StackArgs {
+    int w, h, n, min_count;
+    int g0, g1, first, last;
+    const StackGroup* groups;
+    const StackWin* wins;
+    const int* slot_motion;
+    const uint16_t* slot_off;
+    const int* slot_off_base;
+    const short2* slot_shift;
+    const float* inv_sqrt;
+    float* best;
+    int* arg;
+    float* max_snr;
+    int* best_v;
+    int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Bounded wait on the staging barrier: about two seconds of clock, then the
+// kernel records an error and gives up (the host turns it into an exception).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > 4000000000LL) {
+            atomicExch(err, 1);
+            return false;
+        }
+    }
+    return true;
+}
+
+template <int TY, int P, int M, int WP, bool BORDER>
+__device__ __forceinline__ void stack_group(const StackArgs& a, const StackGroup& G, const float* __restrict__ win,
+                                            const uint16_t* __restrict__ offs, int x, int ybase, int tb, float inv_n,
+                                            float (&best)[P], int (&arg)[P]) {
+    const int n = a.n;
+    for (int s0 = 0; s0 < G.nslots; s0 += M) {
+        float acc[M][P];
+        int cnt[M][P];
+#pragma unroll
+        for (int k = 0; k < M; ++k)
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                acc[k][p] = 0.0f;
+                cnt[k][p] = 0;
+            }
+        for (int i = 0; i < n; ++i) {
+            const uint16_t* o = offs + i * G.nslots + s0;
+            uint16_t ov[M];
+            if constexpr (M == 8) {
+                const uint4 q = *reinterpret_cast<const uint4*>(o);
+                const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    ov[2 * k] = static_cast<uint16_t>(w4[k] & 0xffffu);
+                    ov[2 * k + 1] = static_cast<uint16_t>(w4[k] >> 16);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < M; ++k) ov[k] = o[k];
+            }
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                const float* src = win + ov[k] + tb;
+#pragma unroll
+                for (int p = 0; p < P; ++p) acc[k][p] = __fadd_rn(acc[k][p], src[p * WP]);
+                if constexpr (BORDER) {
+                    const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * n + i];
+                    const bool inx = static_cast<unsigned>(x + sh.x) < static_cast<unsigned>(a.w);
+#pragma unroll
+                    for (int p = 0; p < P; ++p)
+                        cnt[k][p] += (inx && static_cast<unsigned>(ybase + p + sh.y) < static_cast<unsigned>(a.h)) ? 1 : 0;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            const int j = a.slot_motion[G.slot0 + s0 + k];
+            if (j < 0) continue;
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                float f = inv_n;
+                if constexpr (BORDER) {
+                    if (cnt[k][p] < a.min_count) continue;
+                    f = a.inv_sqrt[cnt[k][p]];
+                }
+                const float s = __fmul_rn(acc[k][p], f);
+                if (s > best[p] || (s == best[p] && j < arg[p])) {
+                    best[p] = s;
+                    arg[p] = j;
+                }
+            }
+        }
+    }
+}
+
+template <int TY, int P, int M, int WP, int BH>
+__global__ void __launch_bounds__(32 * TY, 1) stack_kernel(const __grid_constant__ CUtensorMap tmap, const StackArgs a) {
+    constexpr int TH = TY * P;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // 128-byte aligned base (TMA destinations), the barrier in its first 8 bytes
+    unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base);
+    float* win = reinterpret_cast<float*>(base + 128);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TH;
+    const int x = x0 + lane, ybase = y0 + warp * P;
+    const int tb = warp * P * WP + lane;
+
+    float best[P];
+    int arg[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        best[p] = -CUDART_INF_F;
+        arg[p] = -1;
+        const int y = ybase + p;
+        if (!a.first && x < a.w && y < a.h) {
+            best[p] = a.best[static_cast<size_t>(y) * a.w + x];
+            arg[p] = a.arg[static_cast<size_t>(y) * a.w + x];
+        }
+    }
+    const bool full = x0 + 31 < a.w && y0 + TH - 1 < a.h;
+    const float inv_n = a.inv_sqrt[a.n];
+    if (tid == 0) mbar_init(bar, 1);
+    __syncthreads();
+
+    uint32_t phase = 0;
+    for (int g = a.g0; g < a.g1; ++g) {
+        const StackGroup G = a.groups[g];
+        uint16_t* offs = reinterpret_cast<uint16_t*>(win + G.rows_total * WP);
+        // the previous group's windows and offsets are no longer read, and this
+        // thread's generic-proxy stores are ordered before the TMA writes below
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            mbar_expect_tx(bar, static_cast<uint32_t>(G.rows_total * WP * 4));
+            for (int i = 0; i < a.n; ++i) {
+                const StackWin wv = a.wins[G.win0 + i];
+                for (int b = 0; b < wv.rows; b += BH)
+                    tma_load_3d(win + (wv.row0 + b) * WP, &tmap, x0 + wv.dx0, y0 + wv.dy0 + b, i, bar);
+            }
+        }
+        {
+            const int nvec = (G.nslots * a.n + 7) / 8;  // 16-byte chunks of the offset table
+            const uint4* src = reinterpret_cast<const uint4*>(a.slot_off + a.slot_off_base[g]);
+            uint4* dst = reinterpret_cast<uint4*>(offs);
+            for (int q = tid; q < nvec; q += blockDim.x) dst[q] = src[q];
+        }
+        __syncthreads();
+        const bool ok = mbar_wait_bounded(bar, phase, a.err);
+        if (__syncthreads_or(!ok)) return;  // staging did not complete: the host reports the error
+        phase ^= 1u;
+        const bool interior = full && x0 + G.gdxmin >= 0 && x0 + 31 + G.gdxmax < a.w && y0 + G.gdymin >= 0 &&
+                              y0 + TH - 1 + G.gdymax < a.h;
+        if (interior)
+            stack_group<TY, P, M, WP, false>(a, G, win, offs, x, ybase, tb, inv_n, best, arg);
+        else
+            stack_group<TY, P, M, WP, true>(a, G, win, offs, x, ybase, tb, inv_n, best, arg);
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const int y = ybase + p;
+        if (x >= a.w || y >= a.h) continue;
+        const size_t o = static_cast<size_t>(y) * a.w + x;
+        if (a.last) {
+            a.max_snr[o] = isfinite(best[p]) ? best[p] : 0.0f;
+            a.best_v[o] = arg[p];
+        } else {
+            a.best[o] = best[p];
+            a.arg[o] = arg[p];
+        }
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    if (!fn) throw CudaError("cuTensorMapEncodeTiled is not available from the driver");
+    return fn;
+}
+
+template <int TY, int P, int M, int WP, int BH>
+void launch_variant(const StackPlan& plan, const StackPlanDev& dev, const float* d_frames, int g0, int g1, bool first,
+                    bool last, float* d_best, int* d_arg, float* d_max_snr, int* d_best_v, int* d_err,
+                    cudaStream_t s) {
+    constexpr int TH = TY * P;
+    CUtensorMap map;
+    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(plan.w), static_cast<cuuint64_t>(plan.h),
+                                static_cast<cuuint64_t>(plan.n)};
+    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(plan.pitch) * 4,
+                                   static_cast<cuuint64_t>(plan.pitch) * plan.h * 4};
+    const cuuint32_t box[3] = {WP, BH, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(d_frames), dims, strides,
+                                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed (" + std::to_string(static_cast<int>(r)) + ")");
+    StackArgs a;
+    a.w = plan.w;
+    a.h = plan.h;
+    a.n = plan.n;
+    a.min_count = plan.min_count;
+    a.g0 = g0;
+    a.g1 = g1;
+    a.first = first;
+    a.last = last;
+    a.groups = dev.groups;
+    a.wins = dev.wins;
+    a.slot_motion = dev.slot_motion;
+    a.slot_off = dev.slot_off;
+    a.slot_off_base = dev.slot_off_base;
+    a.slot_shift = dev.slot_shift;
+    a.inv_sqrt = dev.inv_sqrt;
+    a.best = d_best;
+    a.arg = d_arg;
+    a.max_snr = d_max_snr;
+    a.best_v = d_best_v;
+    a.err = d_err;
+    const size_t smem = 256 + static_cast<size_t>(plan.max_group_bytes);
+    if (smem > static_cast<size_t>(plan.cfg.smem_bytes)) throw std::runtime_error("stack plan exceeds shared memory");
+    auto kern = stack_kernel<TY, P, M, WP, BH>;
+    FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    const dim3 grid((plan.w + 31) / 32, (plan.h + TH - 1) / TH);
+    kern<<<grid, 32 * TY, smem, s>>>(map, a);
+    FTB_CHECK(cudaGetLastError());
+}
+
+}  // namespace
+
+void stack_launch(const StackPlan& plan, const StackPlanDev& dev, const float* d_frames, int g0, int g1, bool first,
+                  bool last, float* d_best, int* d_arg, float* d_max_snr, int* d_best_v, int* d_err,
+                  cudaStream_t s) {
+    const StackConfig& c = plan.cfg;
+    if (c.wp != 40 || c.bh != 4 || c.mblock != 8) throw std::runtime_error("stack: unsupported kernel configuration");
+    if (c.ty == 8 && c.p == 4)
+        launch_variant<8, 4, 8, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
+                                       d_err, s);
+    else if (c.ty == 4 && c.p == 4)
+        launch_variant<4, 4, 8, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
+                                       d_err, s);
+    else if (c.ty == 4 && c.p == 2)
+        launch_variant<4, 2, 8, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
+                                       d_err, s);
+    else
+        throw std::runtime_error("stack: unsupported tile shape");
+}
+
+}  // namespace ftb

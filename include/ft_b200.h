@@ -1,0 +1,66 @@
+/* FaintTrail B200 search backend: plain C ABI.
+ *
+ * A drop-in for the stacking backend and the time-order-dependent preprocessing
+ * of FaintTrail 0.9.1 (jkobierczynski/FaintTrail), running on one NVIDIA B200
+ * (sm_100a). Plain pointers and sizes only; host buffers are caller-owned and
+ * never retained past the call. Images are row-major float32, a frame stack is
+ * n consecutive w x h images. Every result is bit-identical to the reference CPU
+ * backend on the same inputs.
+ *
+ * Status codes follow the reference C API (include/fainttrail/fainttrail.h:26-28):
+ * FT_B200_OK, FT_B200_ERROR (message in ft_b200_last_error), FT_B200_CANCELLED
+ * (a progress callback returned 0). A context is not thread-safe: one context
+ * per host thread, like ft_context.
+ */
+#ifndef FT_B200_H
+#define FT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FT_B200_OK 0
+#define FT_B200_ERROR 1
+#define FT_B200_CANCELLED 2
+
+typedef struct ft_b200_ctx ft_b200_ctx;
+
+/* Progress: fraction done in [0,1] and a stage name; return 0 to cancel.
+ * Same shape as ft_progress_fn (fainttrail.h:72). */
+typedef int (*ft_b200_progress_fn)(double fraction, const char* stage, void* user);
+
+const char* ft_b200_version(void);
+
+/* Open device `device` (-1: FAINTTRAIL_CUDA_DEVICE or 0, as the reference CUDA
+ * backend resolves it, backend_cuda.cu:74-78). hbm_budget_bytes caps the device
+ * memory the context allocates (0 = 90 % of the free memory). */
+int ft_b200_open(int device, double hbm_budget_bytes, ft_b200_ctx** out);
+void ft_b200_close(ft_b200_ctx* ctx);
+/* Last error message of the context (ft_last_error, fainttrail.h:106); with a
+ * NULL context, the last error of ft_b200_open on this thread. */
+const char* ft_b200_last_error(const ft_b200_ctx* ctx);
+/* Device name, SM count and memory; replaces SearchBackend::description()
+ * (backend.hpp:113). name_len bytes are written to name, NUL-terminated. */
+int ft_b200_device_info(ft_b200_ctx* ctx, char* name, int name_len, int* sms, double* hbm_bytes);
+
+/* One stacking pass: SearchBackend::run (backend.hpp:107-117; CPU reference
+ * backend_cpu.cpp:77-204) with an explicit shift table (ShiftTable,
+ * backend.hpp:56-69): motion j, frame i at dx[j * nframes + i]. frames: host,
+ * nframes x height x width. Outputs max_snr and best_v (height x width, host),
+ * exactly StackResult (backend.hpp:99-105). Malformed passes are refused as
+ * validate_pass does (backend.cpp:89-108). progress may be NULL. */
+int ft_b200_stack(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const int* dx,
+                  const int* dy, int motions, int min_count, float* max_snr, int* best_v,
+                  ft_b200_progress_fn progress, void* user);
+
+/* The same with straight-line shifts round(v t) (pass_shift, backend.hpp:87-97):
+ * t_h[nframes] in hours, velocities[2 * motions] as (vx, vy) pairs in px/hour. */
+int ft_b200_stack_linear(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes,
+                         const double* t_h, const double* velocities, int motions, int min_count, float* max_snr,
+                         int* best_v, ft_b200_progress_fn progress, void* user);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FT_B200_H */

@@ -1,0 +1,105 @@
+"""Regenerate the golden fixtures in this directory from the reference itself.
+
+Runs FaintTrail 0.9.1 built from its own sources (oracle/Makefile ->
+oracle/_ref/) through oracle/ref_driver.cpp and stores small input/output
+vectors as compressed .npz files. Needs the reference build (only where the
+reference tree is present); the fixtures it writes are committed, so the tests
+that read them run anywhere.
+
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+from ftoracle import Reference  # noqa: E402
+
+
+def contract_case(R, constant, seed):
+    """The awkward pass of the reference's backend contract test
+    (tests/test_main.cpp:389-470): 37x23x7, symmetric times with x.5 shifts,
+    a 13x13 velocity lattice plus a far-out motion, min_count 5."""
+    rng = np.random.default_rng(seed)
+    w, h, n = 37, 23, 7
+    t = (np.arange(n) - (n - 1) / 2.0) * 0.25
+    frames = np.ones((n, h, w), np.float32) if constant else rng.standard_normal((n, h, w)).astype(np.float32)
+    vel = [(j * 2.0, k * 2.0) for j in range(-6, 7) for k in range(-6, 7)] + [(400.0, 0.0)]
+    vel = np.array(vel)
+    ms, bv = R.stack(frames, t_h=t, vel=vel, min_count=5, which=0)
+    return dict(frames=frames, t_h=t, vel=vel, min_count=np.int32(5), max_snr=ms, best_v=bv)
+
+
+def nan_table_case(R, seed):
+    """The CUDA-algorithm test pass (tests/test_main.cpp:553-622): 37x23x7 with a
+    NaN pixel, 171 motions (far shifts +-400 px) and a curved 150-motion table
+    with jumps of +500 / -900 px."""
+    rng = np.random.default_rng(seed)
+    w, h, n = 37, 23, 7
+    t = (np.arange(n) - 3) * 0.25
+    frames = rng.standard_normal((n, h, w)).astype(np.float32)
+    frames[2].flat[100] = np.nan
+    vel = np.array([(j * 2.0, k * 2.0) for j in range(-6, 7) for k in range(-6, 7)] + [(400.0, 0.0), (0.0, -400.0)])
+    ms, bv = R.stack(frames, t_h=t, vel=vel, min_count=5, which=0)
+    m = 150
+    dx = np.zeros((m, n), np.int32)
+    dy = np.zeros((m, n), np.int32)
+    for j in range(m):
+        for i in range(n):
+            ti = t[i]
+            # np.round is half-to-even; the table uses half away from zero like std::lround
+            fx = (j % 13 - 6) * ti + ((j % 7) - 3.0) * ti * ti
+            fy = (j % 11 - 5) * ti + ((j % 5) - 2.0) * ti * ti
+            dx[j, i] = int(np.sign(fx) * np.floor(abs(fx) + 0.5)) + (500 if j == 77 else 0)
+            dy[j, i] = int(np.sign(fy) * np.floor(abs(fy) + 0.5)) - (900 if j == 91 else 0)
+    ms2, bv2 = R.stack(frames, dx=dx, dy=dy, min_count=5, which=0)
+    return dict(frames=frames, t_h=t, vel=vel, min_count=np.int32(5), max_snr=ms, best_v=bv, dx=dx, dy=dy,
+                table_max_snr=ms2, table_best_v=bv2)
+
+
+def stage_case(R):
+    """prepare() on a small simulated sequence: background, blank-border growth,
+    static sky, noise, scatter mask, CR rejection, matched filter. Blank (NaN)
+    left columns exercise the coverage rule and the grown border."""
+    frames, mjd, exp = R.simulate(width=72, height=52, nframes=12, nstars=40, nmovers=2, hot_pixels=6,
+                                  cosmic_rays_per_frame=3.0, seed=17)
+    frames[:, :, :5] = np.nan
+    frames[3, 10:13, 30:33] = np.nan
+    prep = R.prepare(frames, mjd, exp, fwhm_px=2.5)
+    v, im = prep.vectors(), prep.images()
+    return dict(raw=frames, mjd=mjd, exptime=exp, fwhm=np.float64(prep.fwhm), span_h=np.float64(prep.span_h),
+                t_h=v["t_h"], sigma=v["sigma"], background=v["background"], cr=v["cr"], sub=im["sub"],
+                filtered=im["filtered"], static_sky=im["static_sky"], mask=im["mask"])
+
+
+def search_case(R):
+    """A whole search() with null calibration (2 null runs) on a small sequence:
+    threshold, pooled null peaks, detection map and candidates."""
+    frames, mjd, exp = R.simulate(width=96, height=80, nframes=12, nstars=60, nmovers=2, seed=5)
+    prep = R.prepare(frames, mjd, exp, fwhm_px=2.5, null_runs=2)
+    res = prep.search(fwhm_px=2.5, null_runs=2, backend="cpu")
+    cands = np.array([c[0] for c in res["candidates"]]).reshape(-1, 17)
+    grid, dv = R.velocity_grid(prep.span_h)
+    return dict(raw=frames, mjd=mjd, exptime=exp, threshold=np.float64(res["threshold"]),
+                method=np.array(res["method"]), null_peaks=res["null_peaks"], max_snr=res["max_snr"],
+                n_velocities=np.int32(res["n_velocities"]), dv=np.float64(res["dv"]), candidates=cands,
+                null_a=np.float64(res["null_a"]), null_k=np.float64(res["null_k"]),
+                null_inv_s2=np.float64(res["null_inv_s2"]), grid=grid)
+
+
+def main():
+    R = Reference()
+    np.savez_compressed(os.path.join(HERE, "stack_contract.npz"), **contract_case(R, False, 4242))
+    np.savez_compressed(os.path.join(HERE, "stack_constant.npz"), **contract_case(R, True, 4242))
+    np.savez_compressed(os.path.join(HERE, "stack_nan_table.npz"), **nan_table_case(R, 99))
+    np.savez_compressed(os.path.join(HERE, "stage_small.npz"), **stage_case(R))
+    np.savez_compressed(os.path.join(HERE, "search_small.npz"), **search_case(R))
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,48 @@
+"""The C-ABI library loads and exports every entry point include/ft_b200.h
+declares; host-side argument checks. No GPU needed."""
+import ctypes as C
+import numpy as np
+import pytest
+
+import fainttrail_b200 as ftb
+
+
+def test_library_exports_every_declared_symbol():
+    L = ftb.lib()
+    names = ftb.exported_symbols()
+    assert "ft_b200_stack" in names and "ft_b200_open" in names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_open_without_gpu_reports_an_error():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    assert ftb.lib().ft_b200_open(0, 0.0, C.byref(h)) == ftb.FT_B200_ERROR
+    assert ftb.lib().ft_b200_last_error(None)
+
+
+def test_null_context_is_an_error():
+    L = ftb.lib()
+    f = np.zeros((1, 4, 4), np.float32)
+    d = np.zeros((1, 1), np.int32)
+    out = np.zeros((4, 4), np.float32)
+    bv = np.zeros((4, 4), np.int32)
+    assert L.ft_b200_stack(None, f, 4, 4, 1, d, d, 1, 1, out, bv, ftb.PROGRESS_FN(), None) == ftb.FT_B200_ERROR
+
+
+def test_validate_pass_mirrors_reference():
+    f = np.zeros((3, 5, 6), np.float32)
+    with pytest.raises(RuntimeError, match="missing times"):
+        ftb.validate_pass(ftb.StackPass(f, min_count=1))
+    with pytest.raises(RuntimeError, match="frame and time counts"):
+        ftb.validate_pass(ftb.StackPass(f, t_h=[0.0, 1.0], velocities=[(1.0, 0.0)]))
+    with pytest.raises(RuntimeError, match="shift table and frame counts"):
+        ftb.validate_pass(ftb.StackPass(f, shifts=(np.zeros((4, 2)), np.zeros((4, 2)))))
+    with pytest.raises(RuntimeError, match="min_count"):
+        ftb.validate_pass(ftb.StackPass(f, t_h=[0, 1, 2], velocities=[(1.0, 0.0)], min_count=0))
+    ftb.validate_pass(ftb.StackPass(f, t_h=[0, 1, 2], velocities=[(1.0, 0.0)]))
+    with pytest.raises(RuntimeError, match="unknown or unavailable"):
+        ftb.make_backend("cuda")
