@@ -57,6 +57,9 @@ def _declare(L):
                                 _f32p, _i32p, PROGRESS_FN, C.c_void_p]
     L.ft_b200_stack_linear.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_int, C.c_int,
                                        _f32p, _i32p, PROGRESS_FN, C.c_void_p]
+    L.ft_b200_stack_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, C.c_int,
+                                    C.c_int, C.c_void_p, C.c_void_p]
+    L.ft_b200_timings.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_void_p, C.c_int]
 
 
 def exported_symbols():
@@ -96,6 +99,21 @@ class Device:
             raise Cancelled("cancelled")
         if rc != FT_B200_OK:
             raise RuntimeError(f"{what}: {self.error()}")
+
+    def timings(self):
+        """[(stage, seconds)] of the last call (CUDA events on the context stream)."""
+        names = C.create_string_buffer(4096)
+        vals = np.zeros(64)
+        k = self.L.ft_b200_timings(self.h, names, 4096, vals.ctypes.data_as(C.c_void_p), 64)
+        return list(zip(names.value.decode().split(";"), vals[:k].tolist())) if k else []
+
+    def stack_dev(self, d_frames, width, height, pitch, nframes, dx, dy, min_count, d_max_snr, d_best_v):
+        """ft_b200_stack_dev on device pointers (ints), host shift tables."""
+        dx = np.ascontiguousarray(dx, dtype=np.int32)
+        dy = np.ascontiguousarray(dy, dtype=np.int32)
+        rc = self.L.ft_b200_stack_dev(self.h, C.c_void_p(d_frames), width, height, pitch, nframes, dx, dy,
+                                      dx.shape[0], min_count, C.c_void_p(d_max_snr), C.c_void_p(d_best_v))
+        self.check(rc, "stack_dev")
 
     def info(self):
         name = C.create_string_buffer(256)

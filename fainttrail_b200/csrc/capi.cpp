@@ -3,6 +3,7 @@
 #include "ft_b200.h"
 
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -121,6 +122,36 @@ int ft_b200_stack_linear(ft_b200_ctx* ctx, const float* frames, int width, int h
         ftb::stack_pass_host(c, frames, width, height, nframes, dx.data(), dy.data(), motions, min_count, velocities,
                              max_abs(t_h, nframes), max_snr, best_v, wrap(progress, user));
     });
+}
+
+int ft_b200_stack_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
+                      const int* dx, const int* dy, int motions, int min_count, float* d_max_snr, int* d_best_v) {
+    return guarded(ctx, [&](ftb::Context& c) {
+        check_pass(d_frames, width, height, nframes, motions, min_count);
+        if (!dx || !dy) throw std::runtime_error("stack pass: malformed shift table");
+        if (!d_max_snr || !d_best_v) throw std::runtime_error("stack pass: missing outputs");
+        if (pitch < width || (pitch * 4) % 16 != 0 || reinterpret_cast<uintptr_t>(d_frames) % 16 != 0)
+            throw std::runtime_error("stack pass: device frames need a 16-byte aligned base and row pitch");
+        c.timing_reset();
+        ftb::stack_pass_device(c, d_frames, pitch, width, height, nframes, dx, dy, motions, min_count, nullptr, 0.0,
+                               d_max_snr, d_best_v, {});
+        c.timing_resolve();
+    });
+}
+
+int ft_b200_timings(const ft_b200_ctx* ctx, char* names, int names_len, double* seconds, int cap) {
+    if (!ctx || !ctx->c) return 0;
+    const auto& t = ctx->c->timings;
+    std::string joined;
+    for (size_t k = 0; k < t.size(); ++k) {
+        if (seconds && static_cast<int>(k) < cap) seconds[k] = t[k].second;
+        joined += (k ? ";" : "") + t[k].first;
+    }
+    if (names && names_len > 0) {
+        std::strncpy(names, joined.c_str(), static_cast<size_t>(names_len) - 1);
+        names[names_len - 1] = 0;
+    }
+    return static_cast<int>(t.size());
 }
 
 }  // extern "C"

@@ -2,6 +2,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 
@@ -64,9 +65,70 @@ Context::Context(int device, double budget_bytes) {
     }
 }
 
+double wall_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int Context::event() {
+    if (next_event_ >= static_cast<int>(events_.size())) {
+        cudaEvent_t e;
+        FTB_CHECK(cudaEventCreate(&e));
+        events_.push_back(e);
+    }
+    return next_event_++;
+}
+
+void Context::timing_reset() {
+    spans_.clear();
+    timings.clear();
+    next_event_ = 0;
+}
+
+int Context::span_begin(const std::string& name) {
+    Span s;
+    s.name = name;
+    s.a = event();
+    FTB_CHECK(cudaEventRecord(events_[static_cast<size_t>(s.a)], stream_));
+    spans_.push_back(s);
+    return static_cast<int>(spans_.size()) - 1;
+}
+
+void Context::span_end(int span) {
+    Span& s = spans_[static_cast<size_t>(span)];
+    s.b = event();
+    FTB_CHECK(cudaEventRecord(events_[static_cast<size_t>(s.b)], stream_));
+}
+
+void Context::host_time(const std::string& name, double seconds) {
+    Span s;
+    s.name = name;
+    s.host = seconds;
+    spans_.push_back(s);
+}
+
+void Context::timing_resolve() {
+    timings.clear();
+    for (const Span& s : spans_) {
+        double sec = s.host;
+        if (s.a >= 0 && s.b >= 0) {
+            float ms = 0;
+            FTB_CHECK(cudaEventElapsedTime(&ms, events_[static_cast<size_t>(s.a)], events_[static_cast<size_t>(s.b)]));
+            sec = ms * 1e-3;
+        }
+        bool merged = false;
+        for (auto& t : timings)
+            if (t.first == s.name) {
+                t.second += sec;
+                merged = true;
+            }
+        if (!merged) timings.emplace_back(s.name, sec);
+    }
+}
+
 Context::~Context() {
     cudaSetDevice(device_);
     scratch_.clear();
+    for (cudaEvent_t e : events_) cudaEventDestroy(e);
     if (stream_) cudaStreamSynchronize(stream_);
     if (d_err_) cudaFree(d_err_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -124,6 +186,7 @@ void run_plan(Context& c, const StackPlan& plan, const float* d_frames, float* d
         d_arg = c.scratch(kArg, sizeof(int) * static_cast<size_t>(plan.w) * plan.h, "stack argmax").as<int>();
     }
     try {
+        const int span = c.span_begin("kernel");
         for (int q = 0; q < chunks; ++q) {
             const int g0 = static_cast<int>(static_cast<long long>(ng) * q / chunks);
             const int g1 = static_cast<int>(static_cast<long long>(ng) * (q + 1) / chunks);
@@ -134,6 +197,7 @@ void run_plan(Context& c, const StackPlan& plan, const float* d_frames, float* d
                 if (!progress(static_cast<double>(q + 1) / chunks, "stack")) throw Cancelled();
             }
         }
+        c.span_end(span);
         c.check_kernel_error("stack kernel");
     } catch (...) {
         cudaStreamSynchronize(c.stream());
@@ -145,12 +209,17 @@ void run_plan(Context& c, const StackPlan& plan, const float* d_frames, float* d
 
 }  // namespace
 
-void stack_pass_device(Context& c, const float* d_frames, int w, int h, int n, const int* dx, const int* dy, int m,
-                       int min_count, const double* vel, double tmax, float* d_max_snr, int* d_best_v,
-                       const Progress& progress) {
+void stack_pass_device(Context& c, const float* d_frames, int pitch, int w, int h, int n, const int* dx,
+                       const int* dy, int m, int min_count, const double* vel, double tmax, float* d_max_snr,
+                       int* d_best_v, const Progress& progress) {
+    const double t0 = wall_seconds();
     const StackConfig cfg = choose_stack_config(w, h, n, c.smem_optin());
-    const std::vector<int> order = motion_order(vel, m, tmax, 4.0, 4.0);
-    const StackPlan plan = make_stack_plan(w, h, n, dx, dy, m, min_count, order, cfg);
+    const std::vector<int> order = motion_order(dx, dy, m, n, 4.0, 4.0);
+    (void)vel;
+    (void)tmax;
+    StackPlan plan = make_stack_plan(w, h, n, dx, dy, m, min_count, order, cfg);
+    plan.pitch = pitch;
+    c.host_time("setup", wall_seconds() - t0);
     run_plan(c, plan, d_frames, d_max_snr, d_best_v, progress);
 }
 
@@ -164,12 +233,18 @@ void stack_pass_host(Context& c, const float* frames, int w, int h, int n, const
         c.scratch(kFrames, sizeof(float) * static_cast<size_t>(pitch) * h * n, "frames").as<float>();
     float* d_max = c.scratch(kMax, sizeof(float) * plane, "max_snr").as<float>();
     int* d_bv = c.scratch(kBestV, sizeof(int) * plane, "best_v").as<int>();
+    c.timing_reset();
+    const int up = c.span_begin("upload");
     FTB_CHECK(cudaMemcpy2DAsync(d_frames, sizeof(float) * pitch, frames, sizeof(float) * w, sizeof(float) * w,
                                 static_cast<size_t>(h) * n, cudaMemcpyHostToDevice, c.stream()));
-    stack_pass_device(c, d_frames, w, h, n, dx, dy, m, min_count, vel, tmax, d_max, d_bv, progress);
+    c.span_end(up);
+    stack_pass_device(c, d_frames, pitch, w, h, n, dx, dy, m, min_count, vel, tmax, d_max, d_bv, progress);
+    const int down = c.span_begin("download");
     FTB_CHECK(cudaMemcpyAsync(max_snr, d_max, sizeof(float) * plane, cudaMemcpyDeviceToHost, c.stream()));
     FTB_CHECK(cudaMemcpyAsync(best_v, d_bv, sizeof(int) * plane, cudaMemcpyDeviceToHost, c.stream()));
+    c.span_end(down);
     FTB_CHECK(cudaStreamSynchronize(c.stream()));
+    c.timing_resolve();
 }
 
 }  // namespace ftb

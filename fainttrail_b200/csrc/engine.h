@@ -74,6 +74,14 @@ public:
     // reusable device buffers, grown on demand
     DevBuf& scratch(int slot, size_t bytes, const char* what);
 
+    // stage timings of the last call: CUDA-event spans on the stream, or host time
+    void timing_reset();
+    int span_begin(const std::string& name);   // records a start event
+    void span_end(int span);                    // records its end event
+    void host_time(const std::string& name, double seconds);
+    void timing_resolve();                      // after a stream sync: event spans -> seconds
+    std::vector<std::pair<std::string, double>> timings;
+
     std::string error;
 
 private:
@@ -85,7 +93,19 @@ private:
     size_t budget_ = 0, used_ = 0;
     int* d_err_ = nullptr;
     std::vector<DevBuf> scratch_;
+    struct Span {
+        std::string name;
+        int a = -1, b = -1;
+        double host = -1;
+    };
+    std::vector<Span> spans_;
+    std::vector<cudaEvent_t> events_;
+    int next_event_ = 0;
+    int event();
 };
+
+// Wall-clock seconds since an arbitrary epoch (host stages).
+double wall_seconds();
 
 // One stacking pass over host frames (nframes x h x w) with a motion-major shift
 // table; vel (2 m doubles) only guides the planner's motion order (may be null).
@@ -95,8 +115,8 @@ void stack_pass_host(Context& c, const float* frames, int w, int h, int n, const
 
 // The same over frames already on the device (n x h x pitch), results on the
 // device; the split into launches follows the progress granularity.
-void stack_pass_device(Context& c, const float* d_frames, int w, int h, int n, const int* dx, const int* dy, int m,
-                       int min_count, const double* vel, double tmax, float* d_max_snr, int* d_best_v,
-                       const Progress& progress);
+void stack_pass_device(Context& c, const float* d_frames, int pitch, int w, int h, int n, const int* dx,
+                       const int* dy, int m, int min_count, const double* vel, double tmax, float* d_max_snr,
+                       int* d_best_v, const Progress& progress);
 
 }  // namespace ftb

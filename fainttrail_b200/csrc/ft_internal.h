@@ -43,14 +43,14 @@ struct StackWin {            // one frame's window for a group
 };
 
 struct StackConfig {         // one compiled kernel variant
-    int ty = 4;              // warps per CTA (rows of warps)
-    int p = 4;               // output rows per thread
+    int ty = 12;             // warps per CTA; they share the tile and split the motions
+    int p = 16;              // output rows per tile (and per thread)
     int tile_w = 32;         // output columns per tile (one warp)
-    int tile_h() const { return ty * p; }
+    int tile_h() const { return p; }
     int threads() const { return 32 * ty; }
     int wp = 40;             // window pitch in floats
     int bh = 4;              // TMA box height (rows)
-    int mblock = 8;          // motions accumulated together in registers
+    int mblock = 4;          // motions accumulated together in registers
     int smem_bytes = 200 * 1024;
 };
 
@@ -70,9 +70,9 @@ struct StackPlan {
     double adds = 0;                          // m * n * w * h
 };
 
-// Motion visiting order for the planner: motions close in velocity first.
-// vel may be null (explicit shift tables keep index order).
-std::vector<int> motion_order(const double* vel, int m, double tmax, double sx_px, double sy_px);
+// Motion visiting order for the planner: motions whose shifts are close come
+// together (patches of about sx x sy pixels at the frame of widest spread).
+std::vector<int> motion_order(const int* dx, const int* dy, int m, int n, double sx_px, double sy_px);
 
 // Build a plan for a pass; dx/dy are motion-major (j * n + i) host tables.
 StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int m, int min_count,

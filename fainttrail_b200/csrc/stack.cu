@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <limits>
 #include <mutex>
 #include <numeric>
@@ -47,22 +48,41 @@ void cuda_check(cudaError_t e, const char* what) {
 
 // ------------------------------------------------------------------ host plan
 
-std::vector<int> motion_order(const double* vel, int m, double tmax, double sx_px, double sy_px) {
+std::vector<int> motion_order(const int* dx, const int* dy, int m, int n, double sx_px, double sy_px) {
     std::vector<int> order(static_cast<size_t>(m));
     std::iota(order.begin(), order.end(), 0);
-    if (!vel || tmax <= 0.0) return order;
-    // patches of the velocity plane whose shifts spread by about sx x sy pixels at
-    // the extreme frame; row-major inside a patch (equal vy = equal dy per frame)
-    std::vector<long long> kx(static_cast<size_t>(m)), ky(static_cast<size_t>(m));
-    for (int j = 0; j < m; ++j) {
-        kx[static_cast<size_t>(j)] = static_cast<long long>(std::floor(vel[2 * j] * tmax / sx_px));
-        ky[static_cast<size_t>(j)] = static_cast<long long>(std::floor(vel[2 * j + 1] * tmax / sy_px));
+    if (m < 2) return order;
+    // the frame whose shifts spread most (for straight tracks: the frame furthest
+    // from the reference epoch) decides the grouping: motions are bucketed into
+    // patches of about sx x sy pixels of shift there, row-major inside a patch
+    // (equal dy first), so that the planner's groups are compact in both axes
+    int ie = 0;
+    long long best = -1;
+    for (int i = 0; i < n; ++i) {
+        int lo = INT32_MAX, hi = INT32_MIN;
+        for (int j = 0; j < m; ++j) {
+            lo = std::min(lo, dx[static_cast<size_t>(j) * n + i]);
+            hi = std::max(hi, dx[static_cast<size_t>(j) * n + i]);
+            lo = std::min(lo, dy[static_cast<size_t>(j) * n + i]);
+            hi = std::max(hi, dy[static_cast<size_t>(j) * n + i]);
+        }
+        if (static_cast<long long>(hi) - lo > best) {
+            best = static_cast<long long>(hi) - lo;
+            ie = i;
+        }
     }
+    auto ex = [&](int j) { return dx[static_cast<size_t>(j) * n + ie]; };
+    auto ey = [&](int j) { return dy[static_cast<size_t>(j) * n + ie]; };
+    auto kx = [&](int j) { return static_cast<long long>(std::floor(ex(j) / sx_px)); };
+    auto ky = [&](int j) { return static_cast<long long>(std::floor(ey(j) / sy_px)); };
+    // patches are visited column by column: a group then grows in dy (more
+    // window rows, limited only by shared memory) while its dx spread stays
+    // within the window pitch
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        if (ky[a] != ky[b]) return ky[a] < ky[b];
-        if (kx[a] != kx[b]) return kx[a] < kx[b];
-        if (vel[2 * a + 1] != vel[2 * b + 1]) return vel[2 * a + 1] < vel[2 * b + 1];
-        return vel[2 * a] < vel[2 * b];
+        if (kx(a) != kx(b)) return kx(a) < kx(b);
+        if (ky(a) != ky(b)) return ky(a) < ky(b);
+        if (ey(a) != ey(b)) return ey(a) < ey(b);
+        return ex(a) < ex(b);
     });
     return order;
 }
@@ -76,21 +96,14 @@ StackConfig choose_stack_config(int w, int h, int n, int smem_optin) {
     (void)w;
     (void)h;
     StackConfig c;
-    c.smem_bytes = std::min(smem_optin, 220 * 1024);
-    // tallest tile whose n windows (with 4 rows of vertical spread) fill at most
-    // 3/4 of shared memory, leaving room for the spread and the offset table
-    const int budget = c.smem_bytes * 3 / 4;
-    auto need = [&](int th) { return n * roundup(th + 4, c.bh) * c.wp * 4; };
-    if (need(32) <= budget) {
-        c.ty = 8;
-        c.p = 4;
-    } else if (need(16) <= budget) {
-        c.ty = 4;
-        c.p = 4;
-    } else {
-        c.ty = 4;
-        c.p = 2;
-    }
+    c.ty = 12;     // warps per CTA, sharing one tile
+    c.mblock = 4;  // motions per register block
+    c.smem_bytes = std::min(smem_optin - 1024, 224 * 1024);
+    // the tallest tile (16, 8 or 4 rows) whose windows, with 4 rows of vertical
+    // spread, use at most 70 % of shared memory (the rest: spread and offsets)
+    auto need = [&](int p) { return static_cast<long long>(n) * roundup(p + 4, c.bh) * c.wp * 4; };
+    const long long cap = static_cast<long long>(c.smem_bytes) * 7 / 10;
+    c.p = need(16) <= cap ? 16 : need(8) <= cap ? 8 : 4;
     return c;
 }
 
@@ -108,7 +121,7 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
     P.cfg = cfg;
     P.adds = static_cast<double>(m) * n * w * h;
     const int TW = cfg.tile_w, TH = cfg.tile_h(), WP = cfg.wp, BH = cfg.bh, M = cfg.mblock;
-    // shared memory in floats after the barrier and alignment slack (256 bytes)
+    // shared memory in floats after the barrier and alignment slack
     const long long budget = (cfg.smem_bytes - 256) / 4;
 
     P.inv_sqrt.assign(static_cast<size_t>(n) + 1, 0.0f);
@@ -123,6 +136,7 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
     std::vector<int> tnx(mnx), txx(mxx), tny(mny), txy(mxy);
     std::vector<int> members;
 
+    // offset table of a group of `count` motions, in floats
     auto table_floats = [&](int count) { return static_cast<long long>(roundup(roundup(count, M) * n, 8)) / 2; };
     auto flush = [&]() {
         StackGroup g;
@@ -148,10 +162,10 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
         }
         g.rows_total = row;
         P.max_rows = std::max(P.max_rows, row);
-        P.max_group_bytes = std::max(P.max_group_bytes, static_cast<long long>(row) * WP * 4 +
-                                                            static_cast<long long>(roundup(roundup(cnt, M) * n, 8)) * 2);
+        P.max_group_bytes = std::max(P.max_group_bytes, static_cast<long long>(row) * WP * 4 + table_floats(cnt) * 4);
         P.max_slots = std::max(P.max_slots, g.nslots);
         P.slot_off_base.push_back(static_cast<int>(P.slot_off.size()));
+        // [frame][slot] 16-bit offsets, padded to a multiple of 16 bytes
         const size_t tab = static_cast<size_t>(roundup(g.nslots * n, 8));
         const size_t base = P.slot_off.size();
         P.slot_off.resize(base + tab, 0);
@@ -181,6 +195,54 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
             throw std::runtime_error("stack plan: one motion's frame windows exceed shared memory");
         members.push_back(j);
     };
+    // bounds of a member list, recomputed after a cut
+    auto recompute = [&](const std::vector<int>& mem) {
+        for (int i = 0; i < n; ++i) {
+            const size_t k = static_cast<size_t>(i);
+            mnx[k] = mny[k] = std::numeric_limits<int>::max();
+            mxx[k] = mxy[k] = std::numeric_limits<int>::min();
+            for (int jj : mem) {
+                mnx[k] = std::min(mnx[k], cdx(jj, i));
+                mxx[k] = std::max(mxx[k], cdx(jj, i));
+                mny[k] = std::min(mny[k], cdy(jj, i));
+                mxy[k] = std::max(mxy[k], cdy(jj, i));
+            }
+        }
+    };
+    // try to add motion j to the open group; returns false (and changes nothing)
+    // when its windows would not fit
+    auto try_add = [&](int j) {
+        if (members.empty()) {
+            start_group(j);
+            return true;
+        }
+        bool fits = true;
+        long long rows = 0;
+        for (int i = 0; i < n && fits; ++i) {
+            const size_t k = static_cast<size_t>(i);
+            const int ddx = cdx(j, i), ddy = cdy(j, i);
+            tnx[k] = std::min(mnx[k], ddx);
+            txx[k] = std::max(mxx[k], ddx);
+            tny[k] = std::min(mny[k], ddy);
+            txy[k] = std::max(mxy[k], ddy);
+            if (txx[k] - floor4(tnx[k]) + TW > WP) fits = false;
+            rows += roundup(TH + txy[k] - tny[k], BH);
+        }
+        const int cnt = static_cast<int>(members.size()) + 1;
+        if (fits && rows * WP + table_floats(cnt) > budget) fits = false;
+        if (!fits) return false;
+        mnx.swap(tnx);
+        mxx.swap(txx);
+        mny.swap(tny);
+        mxy.swap(txy);
+        members.push_back(j);
+        return true;
+    };
+    std::function<void(int)> add_or_flush = [&](int j) {
+        if (try_add(j)) return;
+        flush();
+        start_group(j);
+    };
     for (const int j : order) {
         if (members.empty()) {
             start_group(j);
@@ -201,8 +263,17 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
         const int cnt = static_cast<int>(members.size()) + 1;
         if (fits && rows * WP + table_floats(cnt) > budget) fits = false;
         if (!fits) {
+            const int share = cfg.ty * M;  // one block for every warp
+            const int keep = static_cast<int>(members.size()) / share * share;
+            std::vector<int> carry;
+            if (keep > 0 && keep < static_cast<int>(members.size())) {
+                carry.assign(members.begin() + keep, members.end());
+                members.resize(static_cast<size_t>(keep));
+                recompute(members);
+            }
             flush();
-            start_group(j);
+            for (int c : carry) add_or_flush(c);
+            add_or_flush(j);
             continue;
         }
         mnx.swap(tnx);
@@ -319,74 +390,104 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return true;
 }
 
-template <int TY, int P, int M, int WP, bool BORDER>
-__device__ __forceinline__ void stack_group(const StackArgs& a, const StackGroup& G, const float* __restrict__ win,
-                                            const uint16_t* __restrict__ offs, int x, int ybase, int tb, float inv_n,
-                                            float (&best)[P], int (&arg)[P]) {
-    const int n = a.n;
-    for (int s0 = 0; s0 < G.nslots; s0 += M) {
-        float acc[M][P];
-        int cnt[M][P];
+__device__ __forceinline__ uint32_t half16(const uint4& q, int k) {
+    const uint32_t w = k < 2 ? q.x : k < 4 ? q.y : k < 6 ? q.z : q.w;
+    return (k & 1) ? (w >> 16) : (w & 0xffffu);
+}
+
+template <int P, int WP>
+__device__ __forceinline__ void load_column(float (&v)[P], const float* __restrict__ src) {
 #pragma unroll
-        for (int k = 0; k < M; ++k)
+    for (int p = 0; p < P; ++p) v[p] = src[p * WP];
+}
+
+template <int P>
+__device__ __forceinline__ void add_column(float (&acc)[P], const float (&v)[P]) {
 #pragma unroll
-            for (int p = 0; p < P; ++p) {
-                acc[k][p] = 0.0f;
-                cnt[k][p] = 0;
-            }
-        for (int i = 0; i < n; ++i) {
-            const uint16_t* o = offs + i * G.nslots + s0;
-            uint16_t ov[M];
-            if constexpr (M == 8) {
-                const uint4 q = *reinterpret_cast<const uint4*>(o);
-                const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+    for (int p = 0; p < P; ++p) acc[p] = __fadd_rn(acc[p], v[p]);
+}
+
+// One block of 4 consecutive motions of a group for this thread's P pixels
+// (one column, P rows), frames in ascending order. A motion whose window offset
+// for frame i equals the previous motion's adds the P values already in
+// registers instead of loading them again; the offsets are the same for the
+// whole CTA, so these branches are warp-uniform.
+// BORDER: coverage counts. A frame that covers the whole tile for a motion (the
+// common case; a warp-uniform test) adds 1 to the motion's count, a frame that
+// covers part of it is counted per pixel (8-bit counters, 4 per register).
+template <int P, int WP, bool BORDER>
+__device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup& G, int s0,
+                                            const float* __restrict__ win, const uint16_t* __restrict__ offs, int tb,
+                                            int x, int x0, int y0, float inv_n, float (&best)[P], int (&arg)[P]) {
+    constexpr int M = 4;
+    constexpr int PW = (P + 3) / 4;
+    float acc[M][P];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    ov[2 * k] = static_cast<uint16_t>(w4[k] & 0xffffu);
-                    ov[2 * k + 1] = static_cast<uint16_t>(w4[k] >> 16);
-                }
-            } else {
+    for (int k = 0; k < M; ++k)
 #pragma unroll
-                for (int k = 0; k < M; ++k) ov[k] = o[k];
-            }
+        for (int p = 0; p < P; ++p) acc[k][p] = 0.0f;
+    int cfull[M] = {0, 0, 0, 0};
+    uint32_t cpart[M][PW];
+#pragma unroll
+    for (int k = 0; k < M; ++k)
+#pragma unroll
+        for (int w = 0; w < PW; ++w) cpart[k][w] = 0;
+    for (int i = 0; i < a.n; ++i) {
+        const uint2 q = *reinterpret_cast<const uint2*>(offs + i * G.nslots + s0);
+        const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
+        float v[P];
+        load_column<P, WP>(v, win + o0 + tb);
+        add_column<P>(acc[0], v);
+        if (o1 != o0) load_column<P, WP>(v, win + o1 + tb);
+        add_column<P>(acc[1], v);
+        if (o2 != o1) load_column<P, WP>(v, win + o2 + tb);
+        add_column<P>(acc[2], v);
+        if (o3 != o2) load_column<P, WP>(v, win + o3 + tb);
+        add_column<P>(acc[3], v);
+        if constexpr (BORDER) {
 #pragma unroll
             for (int k = 0; k < M; ++k) {
-                const float* src = win + ov[k] + tb;
-#pragma unroll
-                for (int p = 0; p < P; ++p) acc[k][p] = __fadd_rn(acc[k][p], src[p * WP]);
-                if constexpr (BORDER) {
-                    const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * n + i];
+                const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * a.n + i];
+                const bool whole = x0 + sh.x >= 0 && x0 + 31 + sh.x < a.w && y0 + sh.y >= 0 && y0 + P - 1 + sh.y < a.h;
+                if (whole) {
+                    ++cfull[k];
+                } else {
                     const bool inx = static_cast<unsigned>(x + sh.x) < static_cast<unsigned>(a.w);
 #pragma unroll
                     for (int p = 0; p < P; ++p)
-                        cnt[k][p] += (inx && static_cast<unsigned>(ybase + p + sh.y) < static_cast<unsigned>(a.h)) ? 1 : 0;
+                        if (inx && static_cast<unsigned>(y0 + p + sh.y) < static_cast<unsigned>(a.h))
+                            cpart[k][p / 4] += 1u << (8 * (p % 4));
                 }
             }
         }
+    }
 #pragma unroll
-        for (int k = 0; k < M; ++k) {
-            const int j = a.slot_motion[G.slot0 + s0 + k];
-            if (j < 0) continue;
+    for (int k = 0; k < M; ++k) {
+        const int j = a.slot_motion[G.slot0 + s0 + k];
+        if (j < 0) continue;
 #pragma unroll
-            for (int p = 0; p < P; ++p) {
-                float f = inv_n;
-                if constexpr (BORDER) {
-                    if (cnt[k][p] < a.min_count) continue;
-                    f = a.inv_sqrt[cnt[k][p]];
-                }
-                const float s = __fmul_rn(acc[k][p], f);
-                if (s > best[p] || (s == best[p] && j < arg[p])) {
-                    best[p] = s;
-                    arg[p] = j;
-                }
+        for (int p = 0; p < P; ++p) {
+            float f = inv_n;
+            if constexpr (BORDER) {
+                const int c = cfull[k] + static_cast<int>((cpart[k][p / 4] >> (8 * (p % 4))) & 0xffu);
+                if (c < a.min_count) continue;
+                f = a.inv_sqrt[c];
+            }
+            const float s = __fmul_rn(acc[k][p], f);
+            if (s > best[p] || (s == best[p] && j < arg[p])) {
+                best[p] = s;
+                arg[p] = j;
             }
         }
     }
 }
 
-template <int TY, int P, int M, int WP, int BH>
-__global__ void __launch_bounds__(32 * TY, 1) stack_kernel(const __grid_constant__ CUtensorMap tmap, const StackArgs a) {
-    constexpr int TH = TY * P;
+// One CTA = one 32 x P output tile, one CTA per SM; its NW warps share the tile
+// and split each group's 4-motion blocks; per-warp maxima merge through shared
+// memory at the end.
+template <int NW, int P, int WP, int BH>
+__global__ void __launch_bounds__(32 * NW, 1) stack_kernel(const __grid_constant__ CUtensorMap tmap, const StackArgs a) {
+    constexpr int M = 4;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // 128-byte aligned base (TMA destinations), the barrier in its first 8 bytes
     unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
@@ -394,9 +495,9 @@ __global__ void __launch_bounds__(32 * TY, 1) stack_kernel(const __grid_constant
     float* win = reinterpret_cast<float*>(base + 128);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TH;
-    const int x = x0 + lane, ybase = y0 + warp * P;
-    const int tb = warp * P * WP + lane;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * P;
+    const int x = x0 + lane;
+    const int tb = lane;  // thread's first window element relative to a motion's offset
 
     float best[P];
     int arg[P];
@@ -404,13 +505,8 @@ __global__ void __launch_bounds__(32 * TY, 1) stack_kernel(const __grid_constant
     for (int p = 0; p < P; ++p) {
         best[p] = -CUDART_INF_F;
         arg[p] = -1;
-        const int y = ybase + p;
-        if (!a.first && x < a.w && y < a.h) {
-            best[p] = a.best[static_cast<size_t>(y) * a.w + x];
-            arg[p] = a.arg[static_cast<size_t>(y) * a.w + x];
-        }
     }
-    const bool full = x0 + 31 < a.w && y0 + TH - 1 < a.h;
+    const bool full = x0 + 31 < a.w && y0 + P - 1 < a.h;
     const float inv_n = a.inv_sqrt[a.n];
     if (tid == 0) mbar_init(bar, 1);
     __syncthreads();
@@ -442,23 +538,50 @@ __global__ void __launch_bounds__(32 * TY, 1) stack_kernel(const __grid_constant
         if (__syncthreads_or(!ok)) return;  // staging did not complete: the host reports the error
         phase ^= 1u;
         const bool interior = full && x0 + G.gdxmin >= 0 && x0 + 31 + G.gdxmax < a.w && y0 + G.gdymin >= 0 &&
-                              y0 + TH - 1 + G.gdymax < a.h;
-        if (interior)
-            stack_group<TY, P, M, WP, false>(a, G, win, offs, x, ybase, tb, inv_n, best, arg);
-        else
-            stack_group<TY, P, M, WP, true>(a, G, win, offs, x, ybase, tb, inv_n, best, arg);
+                              y0 + P - 1 + G.gdymax < a.h;
+        if (interior) {
+            for (int s0 = warp * M; s0 < G.nslots; s0 += NW * M)
+                motion_quad<P, WP, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+        } else {
+            for (int s0 = warp * M; s0 < G.nslots; s0 += NW * M)
+                motion_quad<P, WP, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+        }
     }
+    // merge the warps' maxima (and, for a continued pass, the stored running ones)
+    __syncthreads();
+    float* mb = win;
+    int* ma = reinterpret_cast<int*>(win + NW * 32 * P);
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-        const int y = ybase + p;
-        if (x >= a.w || y >= a.h) continue;
-        const size_t o = static_cast<size_t>(y) * a.w + x;
+        mb[(warp * P + p) * 32 + lane] = best[p];
+        ma[(warp * P + p) * 32 + lane] = arg[p];
+    }
+    __syncthreads();
+    for (int q = tid; q < 32 * P; q += 32 * NW) {
+        const int p = q >> 5, l = q & 31;
+        const int xx = x0 + l, yy = y0 + p;
+        if (xx >= a.w || yy >= a.h) continue;
+        const size_t o = static_cast<size_t>(yy) * a.w + xx;
+        float b = -CUDART_INF_F;
+        int ar = -1;
+        if (!a.first) {
+            b = a.best[o];
+            ar = a.arg[o];
+        }
+        for (int w = 0; w < NW; ++w) {
+            const float s = mb[(w * P + p) * 32 + l];
+            const int j = ma[(w * P + p) * 32 + l];
+            if (j >= 0 && (s > b || (s == b && (ar < 0 || j < ar)))) {
+                b = s;
+                ar = j;
+            }
+        }
         if (a.last) {
-            a.max_snr[o] = isfinite(best[p]) ? best[p] : 0.0f;
-            a.best_v[o] = arg[p];
+            a.max_snr[o] = isfinite(b) ? b : 0.0f;
+            a.best_v[o] = ar;
         } else {
-            a.best[o] = best[p];
-            a.arg[o] = arg[p];
+            a.best[o] = b;
+            a.arg[o] = ar;
         }
     }
 }
@@ -477,11 +600,10 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-template <int TY, int P, int M, int WP, int BH>
+template <int NW, int P, int WP, int BH>
 void launch_variant(const StackPlan& plan, const StackPlanDev& dev, const float* d_frames, int g0, int g1, bool first,
                     bool last, float* d_best, int* d_arg, float* d_max_snr, int* d_best_v, int* d_err,
                     cudaStream_t s) {
-    constexpr int TH = TY * P;
     CUtensorMap map;
     const cuuint64_t dims[3] = {static_cast<cuuint64_t>(plan.w), static_cast<cuuint64_t>(plan.h),
                                 static_cast<cuuint64_t>(plan.n)};
@@ -514,12 +636,13 @@ void launch_variant(const StackPlan& plan, const StackPlanDev& dev, const float*
     a.max_snr = d_max_snr;
     a.best_v = d_best_v;
     a.err = d_err;
-    const size_t smem = 256 + static_cast<size_t>(plan.max_group_bytes);
-    if (smem > static_cast<size_t>(plan.cfg.smem_bytes)) throw std::runtime_error("stack plan exceeds shared memory");
-    auto kern = stack_kernel<TY, P, M, WP, BH>;
+    const size_t merge = static_cast<size_t>(NW) * 32 * P * 8;
+    const size_t smem = 256 + std::max(merge, static_cast<size_t>(plan.max_group_bytes));
+    if (smem > static_cast<size_t>(plan.cfg.smem_bytes) + 256) throw std::runtime_error("stack plan exceeds shared memory");
+    auto kern = stack_kernel<NW, P, WP, BH>;
     FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    const dim3 grid((plan.w + 31) / 32, (plan.h + TH - 1) / TH);
-    kern<<<grid, 32 * TY, smem, s>>>(map, a);
+    const dim3 grid((plan.w + 31) / 32, (plan.h + P - 1) / P);
+    kern<<<grid, 32 * NW, smem, s>>>(map, a);
     FTB_CHECK(cudaGetLastError());
 }
 
@@ -529,16 +652,16 @@ void stack_launch(const StackPlan& plan, const StackPlanDev& dev, const float* d
                   bool last, float* d_best, int* d_arg, float* d_max_snr, int* d_best_v, int* d_err,
                   cudaStream_t s) {
     const StackConfig& c = plan.cfg;
-    if (c.wp != 40 || c.bh != 4 || c.mblock != 8) throw std::runtime_error("stack: unsupported kernel configuration");
-    if (c.ty == 8 && c.p == 4)
-        launch_variant<8, 4, 8, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
-                                       d_err, s);
-    else if (c.ty == 4 && c.p == 4)
-        launch_variant<4, 4, 8, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
-                                       d_err, s);
-    else if (c.ty == 4 && c.p == 2)
-        launch_variant<4, 2, 8, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
-                                       d_err, s);
+    if (c.wp != 40 || c.bh != 4 || c.mblock != 4 || c.ty != 12) throw std::runtime_error("stack: unsupported kernel configuration");
+    if (c.p == 16)
+        launch_variant<12, 16, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
+                                      d_err, s);
+    else if (c.p == 8)
+        launch_variant<12, 8, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
+                                     d_err, s);
+    else if (c.p == 4)
+        launch_variant<12, 4, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
+                                     d_err, s);
     else
         throw std::runtime_error("stack: unsupported tile shape");
 }

@@ -59,6 +59,20 @@ int ft_b200_stack_linear(ft_b200_ctx* ctx, const float* frames, int width, int h
                          const double* t_h, const double* velocities, int motions, int min_count, float* max_snr,
                          int* best_v, ft_b200_progress_fn progress, void* user);
 
+/* Device-resident pass for callers that keep frames in HBM: d_frames is a device
+ * pointer to nframes x height rows of `pitch` floats (pitch >= width, pitch * 4 a
+ * multiple of 16, base 16-byte aligned); dx/dy are host tables as above;
+ * d_max_snr / d_best_v are device outputs (height x width, dense). Runs on the
+ * context's stream and returns when the pass is complete. */
+int ft_b200_stack_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
+                      const int* dx, const int* dy, int motions, int min_count, float* d_max_snr, int* d_best_v);
+
+/* Stage timings of the last call on the context, measured with CUDA events on the
+ * context's stream (the reference's StackResult::timings, backend.hpp:99-105, and
+ * Prepared::timings, search.hpp:118): names as one ';'-separated string in
+ * `names` (names_len bytes), seconds[k] for each; returns the number of stages. */
+int ft_b200_timings(const ft_b200_ctx* ctx, char* names, int names_len, double* seconds, int cap);
+
 #ifdef __cplusplus
 }
 #endif
