@@ -29,6 +29,12 @@ _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 
 
+class StageParams(C.Structure):
+    """ft_b200_stage_params: the stage's SearchParams fields (search.hpp:18-90)."""
+    _fields_ = [("fwhm_px", C.c_double), ("static_exclude", C.c_int), ("clip_sigma", C.c_double),
+                ("cr_sigma", C.c_double), ("mask_scatter", C.c_double), ("weight_scatter", C.c_double)]
+
+
 class Cancelled(RuntimeError):
     """A progress callback asked to stop (types.hpp:70-76)."""
 
@@ -60,6 +66,9 @@ def _declare(L):
     L.ft_b200_stack_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, C.c_int,
                                     C.c_int, C.c_void_p, C.c_void_p]
     L.ft_b200_timings.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_void_p, C.c_int]
+    L.ft_b200_stage_params_default.argtypes = [C.POINTER(StageParams)]
+    L.ft_b200_stage.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, C.POINTER(StageParams),
+                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
 
 
 def exported_symbols():
@@ -114,6 +123,27 @@ class Device:
         rc = self.L.ft_b200_stack_dev(self.h, C.c_void_p(d_frames), width, height, pitch, nframes, dx, dy,
                                       dx.shape[0], min_count, C.c_void_p(d_max_snr), C.c_void_p(d_best_v))
         self.check(rc, "stack_dev")
+
+    def stage(self, sub, t_h, fwhm_px, **kw):
+        """build_stage on host frames (ft_b200_stage). Returns a dict with
+        filtered, static_sky, mask, sigma, cr (the reference's Prepared fields)."""
+        sub = np.ascontiguousarray(sub, dtype=np.float32)
+        n, h, w = sub.shape
+        p = StageParams()
+        self.L.ft_b200_stage_params_default(C.byref(p))
+        p.fwhm_px = fwhm_px
+        for k, v in kw.items():
+            setattr(p, k, v)
+        filt = np.empty_like(sub)
+        sky = np.empty((h, w), np.float32)
+        mask = np.empty((h, w), np.float32)
+        sigma = np.empty(n, np.float64)
+        cr = np.empty(n, np.int32)
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        rc = self.L.ft_b200_stage(self.h, sub, w, h, n, np.ascontiguousarray(t_h, dtype=np.float64), C.byref(p),
+                                  ptr(filt), ptr(sky), ptr(mask), ptr(sigma), ptr(cr))
+        self.check(rc, "stage")
+        return dict(filtered=filt, static_sky=sky, mask=mask, sigma=sigma, cr=cr)
 
     def info(self):
         name = C.create_string_buffer(256)

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "stage.h"
 
 struct ft_b200_ctx {
     std::unique_ptr<ftb::Context> c;
@@ -136,6 +137,35 @@ int ft_b200_stack_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int he
         ftb::stack_pass_device(c, d_frames, pitch, width, height, nframes, dx, dy, motions, min_count, nullptr, 0.0,
                                d_max_snr, d_best_v, {});
         c.timing_resolve();
+    });
+}
+
+void ft_b200_stage_params_default(ft_b200_stage_params* p) {
+    if (!p) return;
+    const ftb::StageParams d;
+    p->fwhm_px = 0.0;
+    p->static_exclude = d.static_exclude;
+    p->clip_sigma = d.clip_sigma;
+    p->cr_sigma = d.cr_sigma;
+    p->mask_scatter = d.mask_scatter;
+    p->weight_scatter = d.weight_scatter;
+}
+
+int ft_b200_stage(ft_b200_ctx* ctx, const float* sub, int width, int height, int nframes, const double* t_h,
+                  const ft_b200_stage_params* params, float* filtered, float* static_sky, float* mask, double* sigma,
+                  int* cr_pixels) {
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (!sub || !t_h || !params) throw std::runtime_error("stage: missing frames, times or parameters");
+        if (nframes < 1 || width < 1 || height < 1) throw std::runtime_error("stage: empty frames");
+        if (!(params->fwhm_px > 0.0)) throw std::runtime_error("stage: the PSF FWHM must be positive");
+        ftb::StageParams sp;
+        sp.fwhm_px = params->fwhm_px;
+        sp.static_exclude = params->static_exclude;
+        sp.clip_sigma = params->clip_sigma;
+        sp.cr_sigma = params->cr_sigma;
+        sp.mask_scatter = params->mask_scatter;
+        sp.weight_scatter = params->weight_scatter;
+        ftb::stage_host(c, sub, width, height, nframes, t_h, sp, filtered, static_sky, mask, sigma, cr_pixels);
     });
 }
 

@@ -1,6 +1,8 @@
 // Device context and the stacking-pass driver of the B200 backend.
 #include "engine.h"
 
+#include "stage.h"
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -166,9 +168,9 @@ DevBuf& Context::scratch(int slot, size_t bytes, const char* what) {
 
 // ------------------------------------------------------------------ stacking
 
-namespace {
+enum Slot { kFrames = 0, kBest, kArg, kMax, kBestV, kStageOut, kSky, kMask };
 
-enum Slot { kFrames = 0, kBest, kArg, kMax, kBestV };
+namespace {
 
 // Launch a planned pass in group ranges; between ranges the progress callback
 // is asked (fraction of groups done), as the reference CUDA backend does between
@@ -245,6 +247,43 @@ void stack_pass_host(Context& c, const float* frames, int w, int h, int n, const
     c.span_end(down);
     FTB_CHECK(cudaStreamSynchronize(c.stream()));
     c.timing_resolve();
+}
+
+// ------------------------------------------------------------------ stage
+
+void stage_host(Context& c, const float* sub, int w, int h, int n, const double* t_h, const StageParams& sp,
+                float* filtered, float* static_sky, float* mask, double* sigma, int* cr) {
+    c.bind();
+    const int pitch = frame_pitch(w);
+    const size_t plane = static_cast<size_t>(pitch) * h;
+    c.timing_reset();
+    float* d_sub = c.scratch(kFrames, sizeof(float) * plane * n, "frames").as<float>();
+    float* d_filt = c.scratch(kStageOut, sizeof(float) * plane * n, "filtered frames").as<float>();
+    float* d_sky = c.scratch(kSky, sizeof(float) * plane, "static sky").as<float>();
+    float* d_mask = c.scratch(kMask, sizeof(float) * plane, "mask").as<float>();
+    StageScratch sc(c, w, h, n, sp.fwhm_px);
+    const int up = c.span_begin("upload");
+    FTB_CHECK(cudaMemcpy2DAsync(d_sub, sizeof(float) * pitch, sub, sizeof(float) * w, sizeof(float) * w,
+                                static_cast<size_t>(h) * n, cudaMemcpyHostToDevice, c.stream()));
+    c.span_end(up);
+    std::vector<double> sg(static_cast<size_t>(n));
+    std::vector<int> crv(static_cast<size_t>(n));
+    stage_run(c, sc, d_sub, w, h, n, t_h, sp, d_filt, d_sky, d_mask, sg.data(), crv.data());
+    const int down = c.span_begin("download");
+    if (filtered)
+        FTB_CHECK(cudaMemcpy2DAsync(filtered, sizeof(float) * w, d_filt, sizeof(float) * pitch, sizeof(float) * w,
+                                    static_cast<size_t>(h) * n, cudaMemcpyDeviceToHost, c.stream()));
+    if (static_sky)
+        FTB_CHECK(cudaMemcpy2DAsync(static_sky, sizeof(float) * w, d_sky, sizeof(float) * pitch, sizeof(float) * w,
+                                    static_cast<size_t>(h), cudaMemcpyDeviceToHost, c.stream()));
+    if (mask)
+        FTB_CHECK(cudaMemcpy2DAsync(mask, sizeof(float) * w, d_mask, sizeof(float) * pitch, sizeof(float) * w,
+                                    static_cast<size_t>(h), cudaMemcpyDeviceToHost, c.stream()));
+    c.span_end(down);
+    FTB_CHECK(cudaStreamSynchronize(c.stream()));
+    c.timing_resolve();
+    if (sigma) std::copy(sg.begin(), sg.end(), sigma);
+    if (cr) std::copy(crv.begin(), crv.end(), cr);
 }
 
 }  // namespace ftb

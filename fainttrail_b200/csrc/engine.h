@@ -119,4 +119,10 @@ void stack_pass_device(Context& c, const float* d_frames, int pitch, int w, int 
                        const int* dy, int m, int min_count, const double* vel, double tmax, float* d_max_snr,
                        int* d_best_v, const Progress& progress);
 
+struct StageParams;
+
+// build_stage over host buffers (the C ABI's ft_b200_stage).
+void stage_host(Context& c, const float* sub, int w, int h, int n, const double* t_h, const StageParams& sp,
+                float* filtered, float* static_sky, float* mask, double* sigma, int* cr);
+
 }  // namespace ftb

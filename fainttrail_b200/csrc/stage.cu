@@ -1,0 +1,596 @@
+// The time-order-dependent preprocessing stage on the B200: FaintTrail's
+// build_stage (preprocess.cpp:286-486) for a whole image with a fixed PSF width,
+// bit-identical to the reference CPU code.
+//
+//  sky_kernel      static sky + leave-out residuals (preprocess.cpp:154-204)
+//  sample + select per-frame residual noise: regular sample grid, exact medians
+//                  by radix select (common.hpp:64-100, preprocess.cpp:356-365)
+//  scatter_kernel  temporal scatter (preprocess.cpp:373-391)
+//  mask_kernel     dilated scatter mask (preprocess.cpp:392-400)
+//  filter_kernel   normalise + weight, cosmic-ray rejection, clip, separable
+//                  matched filter, fused per tile (preprocess.cpp:414-451, 116-148)
+//  sample + select robust sigma of the filter output, then rescale
+//                  (preprocess.cpp:454-471)
+//
+// Arithmetic follows the reference operation by operation: float adds and
+// multiplies with round-to-nearest and no contraction, double where the
+// reference promotes to double, the same summation orders, NaN rules and casts.
+#include <math_constants.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "engine.h"
+#include "stage.h"
+
+namespace ftb {
+
+namespace {
+
+constexpr double kFwhmToSigma = 1.0 / 2.354820045030949;  // psf.hpp:16
+
+__device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
+
+// ------------------------------------------------------------------ static sky
+
+struct SkyArgs {
+    const float* sub;
+    float* residual;
+    float* sky;
+    const unsigned char* rank;         // time rank of each frame
+    const unsigned char* frame_of;     // frame of each time rank
+    int w, h, pitch, n, exclude, need;
+};
+
+// One thread per pixel. The finite (value, rank) pairs of the pixel's column are
+// placed in sorted order by counting, for each, the pairs that sort before it
+// (the pairs are distinct because the ranks are); the leave-out median of frame
+// i is then the lo-th / hi-th sorted pair outside the exclusion window, found by
+// selecting zero bits of a bitmask of the excluded sorted positions.
+__global__ void __launch_bounds__(64) sky_kernel(const SkyArgs a) {
+    extern __shared__ unsigned char sm[];
+    const int T = blockDim.x, t = threadIdx.x;
+    float* V = reinterpret_cast<float*>(sm);                  // [n][T] values by frame
+    float* S = V + a.n * T;                                             // [n][T] sorted values
+    unsigned char* PF = reinterpret_cast<unsigned char*>(S + a.n * T);  // [n][T] sorted position of each frame
+    const long long q = static_cast<long long>(blockIdx.x) * T + t;
+    const int x = static_cast<int>(q % a.w), y = static_cast<int>(q / a.w);
+    if (y >= a.h) return;
+    const size_t plane = static_cast<size_t>(a.pitch) * a.h;
+    const size_t pix = static_cast<size_t>(y) * a.pitch + x;
+    int m_all = 0;
+    for (int i = 0; i < a.n; ++i) {
+        const float v = a.sub[i * plane + pix];
+        V[i * T + t] = v;
+        m_all += finitef(v);
+    }
+    if (m_all < a.need) {
+        a.sky[pix] = CUDART_NAN_F;
+        for (int i = 0; i < a.n; ++i) a.residual[i * plane + pix] = CUDART_NAN_F;
+        return;
+    }
+    for (int e = 0; e < a.n; ++e) {
+        const float ve = V[e * T + t];
+        if (!finitef(ve)) {
+            PF[e * T + t] = 255;
+            continue;
+        }
+        const int re = a.rank[e];
+        int pos = 0;
+        for (int f = 0; f < a.n; ++f) {
+            const float vf = V[f * T + t];
+            pos += finitef(vf) && (vf < ve || (vf == ve && a.rank[f] < re));
+        }
+        S[pos * T + t] = ve;
+        PF[e * T + t] = static_cast<unsigned char>(pos);
+    }
+    // global median: the two middle floats are added in float (preprocess.cpp:171)
+    const float mid_sum = __fadd_rn(S[((m_all - 1) / 2) * T + t], S[(m_all / 2) * T + t]);
+    const double global = 0.5 * static_cast<double>(mid_sum);
+    a.sky[pix] = __double2float_rn(global);
+    const int words = (m_all + 31) / 32;
+    for (int i = 0; i < a.n; ++i) {
+        const float v = V[i * T + t];
+        if (!finitef(v)) {
+            a.residual[i * plane + pix] = CUDART_NAN_F;
+            continue;
+        }
+        double st = global;
+        if (a.exclude > 0) {
+            uint32_t ex[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            const int ri = a.rank[i];
+            int excluded = 0;
+            const int r0 = max(0, ri - a.exclude), r1 = min(a.n - 1, ri + a.exclude);
+            for (int r = r0; r <= r1; ++r) {
+                const int p = PF[a.frame_of[r] * T + t];
+                if (p == 255) continue;
+                ex[p >> 5] |= 1u << (p & 31);
+                ++excluded;
+            }
+            const int m = m_all - excluded;
+            if (m >= 5) {
+                const int lo = (m - 1) / 2, hi = m / 2;
+                // positions of the lo-th and hi-th kept (zero) bits below m_all
+                int plo = -1, phi = -1, seen = 0;
+                for (int wd = 0; wd < words && phi < 0; ++wd) {
+                    const int nb = min(32, m_all - wd * 32);
+                    const uint32_t valid = nb == 32 ? 0xffffffffu : ((1u << nb) - 1u);
+                    const uint32_t keep = ~ex[wd] & valid;
+                    const int c = __popc(keep);
+                    if (plo < 0 && lo < seen + c) plo = wd * 32 + static_cast<int>(__fns(keep, 0, lo - seen + 1));
+                    if (hi < seen + c) phi = wd * 32 + static_cast<int>(__fns(keep, 0, hi - seen + 1));
+                    seen += c;
+                }
+                // double add of the two middle values (preprocess.cpp:198)
+                st = 0.5 * (static_cast<double>(S[plo * T + t]) + static_cast<double>(S[phi * T + t]));
+            }
+        }
+        a.residual[i * plane + pix] = __double2float_rn(static_cast<double>(v) - st);
+    }
+}
+
+// ------------------------------------------------------------------ samples + exact medians
+
+// The regular sample grid of sample_pixels (common.hpp:85-100): every step-th
+// column and row from `border`, finite values only, optionally masked. Order is
+// irrelevant (only order statistics are taken); the count is exact.
+__global__ void sample_kernel(const float* img, size_t plane, int w, int h, int pitch, int n, int border, int step,
+                              int gw, int gh, const float* mask, float* out, int cap, int* counts) {
+    const int f = blockIdx.y;
+    const long long g = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= static_cast<long long>(gw) * gh) return;
+    const int x = border + static_cast<int>(g % gw) * step, y = border + static_cast<int>(g / gw) * step;
+    const size_t pix = static_cast<size_t>(y) * pitch + x;
+    if (mask && mask[pix] == 0.0f) return;
+    const float v = img[f * plane + pix];
+    if (!finitef(v)) return;
+    const int k = atomicAdd(&counts[f], 1);
+    if (k < cap) out[static_cast<size_t>(f) * cap + k] = v;
+}
+
+__device__ __forceinline__ uint32_t order_key(float v) {
+    const uint32_t b = __float_as_uint(v);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key_value(uint32_t k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// k-th smallest key (0-based) of the CTA's values, by four 8-bit radix passes.
+// MODE 0: keys of x; MODE 1: keys of float(|x - med|) (the MAD deviations,
+// common.hpp:80). Needs >= 256 threads.
+template <int MODE>
+__device__ uint32_t cta_select(const float* x, int cnt, int k, double med, uint32_t* hist, uint32_t* shared_out) {
+    uint32_t prefix = 0, pmask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+        __syncthreads();
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+            float v = x[e];
+            if (MODE == 1) v = __double2float_rn(fabs(static_cast<double>(v) - med));
+            const uint32_t key = order_key(v);
+            if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            int d = 0;
+            for (; d < 255; ++d) {
+                if (acc + hist[d] > static_cast<uint32_t>(k)) break;
+                acc += hist[d];
+            }
+            shared_out[0] = static_cast<uint32_t>(d);
+            shared_out[1] = acc;
+        }
+        __syncthreads();
+        const uint32_t d = shared_out[0];
+        k -= static_cast<int>(shared_out[1]);
+        prefix |= d << shift;
+        pmask |= 255u << shift;
+        __syncthreads();
+    }
+    return prefix;
+}
+
+// median_inplace (common.hpp:64-74) of the CTA's values: the mid-th smallest,
+// averaged (in double) with the (mid-1)-th for an even count; 0 when empty.
+template <int MODE>
+__device__ double cta_median(const float* x, int cnt, double med, uint32_t* hist, uint32_t* sh) {
+    if (cnt == 0) return 0.0;
+    const int mid = cnt / 2;
+    double m = key_value(cta_select<MODE>(x, cnt, mid, med, hist, sh));
+    if (cnt % 2 == 0) {
+        const float lower = key_value(cta_select<MODE>(x, cnt, mid - 1, med, hist, sh));
+        m = 0.5 * (m + lower);
+    }
+    return m;
+}
+
+// robust_sigma (common.hpp:77-82) per frame, one CTA per frame.
+// out_sigma: sigma_from_samples (1 if not positive, preprocess.cpp:265-268) when
+// `unit_if_zero`, else the raw value.
+__global__ void __launch_bounds__(1024) robust_sigma_kernel(const float* samples, int cap, const int* counts,
+                                                            double* out, int unit_if_zero) {
+    __shared__ uint32_t hist[256];
+    __shared__ uint32_t sh[2];
+    const int f = blockIdx.x;
+    const int cnt = min(counts[f], cap);
+    const float* x = samples + static_cast<size_t>(f) * cap;
+    double sg = 0.0;
+    if (cnt >= 3) {
+        const double med = cta_median<0>(x, cnt, 0.0, hist, sh);
+        sg = 1.4826 * cta_median<1>(x, cnt, med, hist, sh);
+    }
+    if (threadIdx.x == 0) out[f] = (unit_if_zero && !(sg > 0.0)) ? 1.0 : sg;
+}
+
+// ------------------------------------------------------------------ scatter + mask
+
+struct ScatterArgs {
+    const float* residual;
+    const double* sigma;
+    float* scatter;
+    int w, h, pitch, n;
+};
+
+// scatter = 1.4826 * median_i float(|r_i| / sigma_i) over finite residuals, or
+// 1e9 with fewer than n/2 of them (preprocess.cpp:380-389). The median's order
+// statistics are found by counting (the values are >= 0, so their bit patterns
+// order like the values).
+__global__ void __launch_bounds__(128) scatter_kernel(const ScatterArgs a) {
+    extern __shared__ unsigned char sm[];
+    const int T = blockDim.x, t = threadIdx.x;
+    uint32_t* C = reinterpret_cast<uint32_t*>(sm);
+    const long long q = static_cast<long long>(blockIdx.x) * T + t;
+    const int x = static_cast<int>(q % a.w), y = static_cast<int>(q / a.w);
+    if (y >= a.h) return;
+    const size_t plane = static_cast<size_t>(a.pitch) * a.h;
+    const size_t pix = static_cast<size_t>(y) * a.pitch + x;
+    int c = 0;
+    for (int i = 0; i < a.n; ++i) {
+        const float v = a.residual[i * plane + pix];
+        if (!finitef(v)) continue;
+        const float d = __double2float_rn(__ddiv_rn(static_cast<double>(fabsf(v)), a.sigma[i]));
+        C[c * T + t] = __float_as_uint(d);
+        ++c;
+    }
+    if (c < a.n / 2) {
+        a.scatter[pix] = 1e9f;
+        return;
+    }
+    const int mid = c / 2;
+    uint32_t vmid = 0, vlow = 0;
+    for (int e = 0; e < c; ++e) {
+        const uint32_t ve = C[e * T + t];
+        int less = 0, leq = 0;
+        for (int f = 0; f < c; ++f) {
+            const uint32_t vf = C[f * T + t];
+            less += vf < ve;
+            leq += vf <= ve;
+        }
+        if (less <= mid && mid < leq) vmid = ve;
+        if (less <= mid - 1 && mid - 1 < leq) vlow = ve;
+    }
+    double m = __uint_as_float(vmid);
+    if (c % 2 == 0) m = 0.5 * (m + __uint_as_float(vlow));
+    a.scatter[pix] = __double2float_rn(1.4826 * m);
+}
+
+__global__ void mask_kernel(const float* scatter, float* mask, int w, int h, int pitch, int dil, double limit) {
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int x = static_cast<int>(q % w), y = static_cast<int>(q / w);
+    if (y >= h) return;
+    float out = 1.0f;
+    for (int yy = max(0, y - dil); yy <= min(h - 1, y + dil) && out != 0.0f; ++yy)
+        for (int xx = max(0, x - dil); xx <= min(w - 1, x + dil); ++xx)
+            if (static_cast<double>(scatter[static_cast<size_t>(yy) * pitch + xx]) > limit) {
+                out = 0.0f;
+                break;
+            }
+    mask[static_cast<size_t>(y) * pitch + x] = out;
+}
+
+// ------------------------------------------------------------------ matched filter
+
+constexpr int kFTW = 32, kFTH = 16;  // output tile of the filter kernel
+
+struct FilterArgs {
+    const float* residual;
+    const float* mask;
+    const float* scatter;
+    const double* sigma;   // per-frame residual noise
+    float* out;            // unnormalised filter output
+    int* cr;               // cosmic-ray hits per frame
+    const float* k;        // 2R+1 taps, float(exp(-i^2 / 2 s^2))
+    float norm;            // float(1 / sum k^2)
+    float wscat, hit, ratio, clip;
+    int w, h, pitch, R;
+};
+
+// One CTA per (frame, 32 x 16 tile). z (normalised, weighted) over the tile plus
+// a halo of R + 2; cosmic-ray centres over the tile plus R + 1; cleaned and
+// clipped z over the tile plus R; then the horizontal pass over the tile's
+// columns and the vertical pass. Pixels outside the image hold 0: a product with
+// 0 adds +0.0f to a sum that starts at +0.0f, which equals the reference's
+// truncated sums at the borders (preprocess.cpp:133-135, 140-145).
+__global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
+    extern __shared__ float fs[];
+    const int R = a.R, H = R + 2;
+    const int ZW = kFTW + 2 * H, ZH = kFTH + 2 * H;
+    float* Z = fs;                                    // ZH x ZW  z, then cleaned z
+    unsigned char* F = reinterpret_cast<unsigned char*>(Z + ZW * ZH);  // ZH x ZW cosmic-ray centre flags
+    float* Tt = reinterpret_cast<float*>(F + ((ZW * ZH + 15) / 16) * 16);  // (kFTH + 2R) x kFTW horizontal pass
+    __shared__ int cr_tile;
+    const int f = blockIdx.z;
+    const int x0 = blockIdx.x * kFTW, y0 = blockIdx.y * kFTH;
+    const size_t plane = static_cast<size_t>(a.pitch) * a.h;
+    const float inv = __double2float_rn(__ddiv_rn(1.0, a.sigma[f]));
+    if (threadIdx.x == 0) cr_tile = 0;
+    for (int e = threadIdx.x; e < ZW * ZH; e += blockDim.x) {
+        const int gx = x0 - H + e % ZW, gy = y0 - H + e / ZW;
+        float z = 0.0f;
+        if (gx >= 0 && gy >= 0 && gx < a.w && gy < a.h) {
+            const size_t pix = static_cast<size_t>(gy) * a.pitch + gx;
+            const float v = a.residual[f * plane + pix];
+            if (a.mask[pix] != 0.0f && finitef(v)) {
+                const float s = a.scatter[pix];
+                const float ew = s > a.wscat ? s : 1.0f;
+                z = __fdiv_rn(__fmul_rn(v, inv), ew);
+            }
+        }
+        Z[e] = z;
+    }
+    __syncthreads();
+    // cosmic-ray centres (preprocess.cpp:433-447): inside [1, w-2] x [1, h-2]
+    for (int e = threadIdx.x; e < ZW * ZH; e += blockDim.x) {
+        const int lx = e % ZW, ly = e / ZW;
+        const int gx = x0 - H + lx, gy = y0 - H + ly;
+        unsigned char flag = 0;
+        if (lx >= 1 && ly >= 1 && lx < ZW - 1 && ly < ZH - 1 && gx >= 1 && gy >= 1 && gx < a.w - 1 && gy < a.h - 1) {
+            const float v = Z[e];
+            if (v >= a.hit) {
+                const float s4 = __fadd_rn(__fadd_rn(__fadd_rn(Z[e - 1], Z[e + 1]), Z[e - ZW]), Z[e + ZW]);
+                const float n4 = __fmul_rn(0.25f, s4);
+                if (!(n4 >= __fmul_rn(a.ratio, v))) {
+                    flag = 1;
+                    if (gx >= x0 && gx < x0 + kFTW && gy >= y0 && gy < y0 + kFTH) atomicAdd(&cr_tile, 1);
+                }
+            }
+        }
+        F[e] = flag;
+    }
+    __syncthreads();
+    // cleaned, clipped z over the tile plus R (kills applied after the scan)
+    float* Zc = Z;  // in place: the kill test reads the original z of the same pixel only
+    for (int e = threadIdx.x; e < ZW * ZH; e += blockDim.x) {
+        const int lx = e % ZW, ly = e / ZW;
+        if (lx < 2 || ly < 2 || lx >= ZW - 2 || ly >= ZH - 2) continue;
+        const float v = Z[e];
+        bool kill = F[e] != 0;
+        if (!kill && v > 2.5f)
+            for (int dy = -1; dy <= 1 && !kill; ++dy)
+                for (int dx = -1; dx <= 1; ++dx)
+                    if (F[e + dy * ZW + dx]) {
+                        kill = true;
+                        break;
+                    }
+        const float zc = kill ? 0.0f : v;
+        Zc[e] = zc < -a.clip ? -a.clip : (a.clip < zc ? a.clip : zc);
+    }
+    __syncthreads();
+    // horizontal pass over rows y0-R .. y0+kFTH+R-1, the tile's columns
+    const int TR = kFTH + 2 * R;
+    for (int e = threadIdx.x; e < TR * kFTW; e += blockDim.x) {
+        const int c = e % kFTW, r = e / kFTW;
+        const float* row = Zc + (r + 2) * ZW + (c + 2);  // centre column at H + c, row at 2 + r (= H - R + r)
+        float acc = 0.0f;
+        for (int j = 0; j <= 2 * R; ++j) acc = __fadd_rn(acc, __fmul_rn(row[j], a.k[j]));
+        const int gy = y0 - R + r;
+        Tt[e] = (gy >= 0 && gy < a.h) ? acc : 0.0f;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kFTW * kFTH; e += blockDim.x) {
+        const int c = e % kFTW, r = e / kFTW;
+        const int gx = x0 + c, gy = y0 + r;
+        if (gx >= a.w || gy >= a.h) continue;
+        float acc = 0.0f;
+        for (int j = 0; j <= 2 * R; ++j) acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(a.k[j], a.norm), Tt[(r + j) * kFTW + c]));
+        a.out[f * plane + static_cast<size_t>(gy) * a.pitch + gx] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && cr_tile) atomicAdd(&a.cr[f], cr_tile);
+}
+
+__global__ void rescale_kernel(float* g, size_t plane, int w, int h, int pitch, const double* sg) {
+    const int f = blockIdx.y;
+    const double s = sg[f];
+    if (!(s > 0.0)) return;
+    const float ig = __double2float_rn(__ddiv_rn(1.0, s));
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int x = static_cast<int>(q % w), y = static_cast<int>(q / w);
+    if (y >= h) return;
+    float* p = g + f * plane + static_cast<size_t>(y) * pitch + x;
+    *p = __fmul_rn(*p, ig);
+}
+
+inline int grid_step(int w, int h, int border, size_t max_samples) {
+    const size_t usable = static_cast<size_t>(std::max(0, w - 2 * border)) * static_cast<size_t>(std::max(0, h - 2 * border));
+    if (usable == 0) return 0;
+    return std::max(1, static_cast<int>(std::sqrt(static_cast<double>(usable) / static_cast<double>(max_samples))));
+}
+
+inline int grid_count(int lo, int hi, int step) { return hi <= lo ? 0 : (hi - lo + step - 1) / step; }
+
+}  // namespace
+
+// ------------------------------------------------------------------ host driver
+
+void stage_time_ranks(const double* t_h, int n, std::vector<int>& rank) {
+    // stable sort of the frame indices by time (preprocess.cpp:323-331)
+    std::vector<int> order(static_cast<size_t>(n));
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return t_h[a] < t_h[b]; });
+    rank.assign(static_cast<size_t>(n), 0);
+    for (int r = 0; r < n; ++r) rank[static_cast<size_t>(order[static_cast<size_t>(r)])] = r;
+}
+
+int sample_grid_points(int w, int h, int border) {
+    const int st = grid_step(w, h, border, 200000);
+    return st > 0 ? grid_count(border, w - border, st) * grid_count(border, h - border, st) : 0;
+}
+
+namespace {
+int filter_border(double fwhm_px) { return static_cast<int>(std::ceil(3 * fwhm_px * kFwhmToSigma)) + 1; }
+}  // namespace
+
+StageScratch::StageScratch(Context& c, int w, int h, int n, double fwhm_px) : w_(w), h_(h), n_(n) {
+    const int pitch = frame_pitch(w);
+    const size_t plane = static_cast<size_t>(pitch) * h;
+    residual = DevBuf(&c, sizeof(float) * plane * n, "residuals");
+    scatter = DevBuf(&c, sizeof(float) * plane, "scatter map");
+    cap = std::max({1, sample_grid_points(w, h, 2), sample_grid_points(w, h, filter_border(fwhm_px))});
+    samples = DevBuf(&c, sizeof(float) * static_cast<size_t>(cap) * n, "noise samples");
+    small = DevBuf(&c, 4096 + sizeof(double) * 2 * n + sizeof(int) * 2 * n + 2 * static_cast<size_t>(n), "stage tables");
+}
+
+bool StageScratch::fits(int w, int h, int n, double fwhm_px) const {
+    return w == w_ && h == h_ && n == n_ && sample_grid_points(w, h, filter_border(fwhm_px)) <= cap;
+}
+
+void stage_run(Context& c, StageScratch& sc, const float* d_sub, int w, int h, int n, const double* t_h,
+               const StageParams& sp, float* d_filtered, float* d_sky, float* d_mask, double* h_sigma, int* h_cr) {
+    if (n < 1 || n > 255) throw std::runtime_error("stage: between 1 and 255 frames are supported");
+    if (!sc.fits(w, h, n, sp.fwhm_px)) throw std::runtime_error("stage: scratch sized for another shape");
+    const int pitch = frame_pitch(w);
+    const size_t plane = static_cast<size_t>(pitch) * h;
+    const long long npix = static_cast<long long>(w) * h;
+    cudaStream_t s = c.stream();
+
+    // host tables: time ranks, the frame of each rank, the filter taps
+    std::vector<int> rank;
+    stage_time_ranks(t_h, n, rank);
+    const int exclude = sp.static_exclude >= 0 ? sp.static_exclude : std::max(1, static_cast<int>(std::lround(n / 8.0)));
+    std::vector<unsigned char> tab(2 * static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) {
+        tab[static_cast<size_t>(i)] = static_cast<unsigned char>(rank[static_cast<size_t>(i)]);
+        tab[static_cast<size_t>(n + rank[static_cast<size_t>(i)])] = static_cast<unsigned char>(i);
+    }
+    const double psf_sigma = sp.fwhm_px * kFwhmToSigma;
+    const int R = std::max(1, static_cast<int>(std::ceil(3.0 * psf_sigma)));
+    std::vector<float> taps(static_cast<size_t>(2 * R + 1));
+    double k2 = 0.0;
+    for (int i = -R; i <= R; ++i) {
+        const double v = std::exp(-0.5 * i * i / (psf_sigma * psf_sigma));
+        taps[static_cast<size_t>(i + R)] = static_cast<float>(v);
+        k2 += v * v;
+    }
+    if (taps.size() > 512) throw std::runtime_error("stage: PSF too wide");
+    unsigned char* base = sc.small.as<unsigned char>();
+    float* d_taps = reinterpret_cast<float*>(base);                     // up to 512 floats
+    double* d_sigma = reinterpret_cast<double*>(base + 2048);
+    double* d_sg = d_sigma + n;
+    int* d_counts = reinterpret_cast<int*>(d_sg + n);
+    int* d_cr = d_counts + n;
+    unsigned char* d_tab = reinterpret_cast<unsigned char*>(d_cr + n);
+    FTB_CHECK(cudaMemcpyAsync(d_taps, taps.data(), sizeof(float) * taps.size(), cudaMemcpyHostToDevice, s));
+    FTB_CHECK(cudaMemcpyAsync(d_tab, tab.data(), tab.size(), cudaMemcpyHostToDevice, s));
+    FTB_CHECK(cudaMemsetAsync(d_counts, 0, sizeof(int) * 2 * n, s));  // counts and cosmic-ray tallies
+
+    // 1. static sky + residuals
+    {
+        const int span = c.span_begin("static sky + residuals");
+        SkyArgs a{d_sub, sc.residual.as<float>(), d_sky, d_tab, d_tab + n, w, h, pitch, n, exclude,
+                  std::max(5, static_cast<int>(0.6 * n))};
+        const int T = 64;
+        const size_t smem = static_cast<size_t>(T) * n * 9;
+        FTB_CHECK(cudaFuncSetAttribute(sky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        sky_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
+        FTB_CHECK(cudaGetLastError());
+        c.span_end(span);
+    }
+    // 2. per-frame noise from the residual samples (border 2)
+    {
+        const int span = c.span_begin("noise");
+        const int st = grid_step(w, h, 2, 200000);
+        if (st > 0) {
+            const int gw = grid_count(2, w - 2, st), gh = grid_count(2, h - 2, st);
+            const long long g = static_cast<long long>(gw) * gh;
+            sample_kernel<<<dim3(static_cast<unsigned>((g + 255) / 256), n), 256, 0, s>>>(
+                sc.residual.as<float>(), plane, w, h, pitch, n, 2, st, gw, gh, nullptr, sc.samples.as<float>(), sc.cap,
+                d_counts);
+            FTB_CHECK(cudaGetLastError());
+        }
+        robust_sigma_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, d_counts, d_sigma, 1);
+        FTB_CHECK(cudaGetLastError());
+        c.span_end(span);
+    }
+    // 3. scatter map and mask
+    {
+        const int span = c.span_begin("scatter mask");
+        ScatterArgs a{sc.residual.as<float>(), d_sigma, sc.scatter.as<float>(), w, h, pitch, n};
+        const int T = 128;
+        const size_t smem = static_cast<size_t>(T) * n * 4;
+        FTB_CHECK(cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        scatter_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
+        FTB_CHECK(cudaGetLastError());
+        const int dil = std::max(1, static_cast<int>(std::lround(0.5 * sp.fwhm_px)));
+        mask_kernel<<<static_cast<unsigned>((npix + 255) / 256), 256, 0, s>>>(sc.scatter.as<float>(), d_mask, w, h,
+                                                                              pitch, dil, sp.mask_scatter);
+        FTB_CHECK(cudaGetLastError());
+        c.span_end(span);
+    }
+    // 4. normalise, cosmic rays, clip, matched filter
+    {
+        const int span = c.span_begin("matched filter");
+        FilterArgs a;
+        a.residual = sc.residual.as<float>();
+        a.mask = d_mask;
+        a.scatter = sc.scatter.as<float>();
+        a.sigma = d_sigma;
+        a.out = d_filtered;
+        a.cr = d_cr;
+        a.k = d_taps;
+        a.norm = static_cast<float>(1.0 / k2);
+        a.wscat = static_cast<float>(sp.weight_scatter);
+        a.hit = static_cast<float>(sp.cr_sigma);
+        a.ratio = static_cast<float>(0.5 * std::exp(-0.5 / (psf_sigma * psf_sigma)));
+        a.clip = static_cast<float>(sp.clip_sigma);
+        a.w = w;
+        a.h = h;
+        a.pitch = pitch;
+        a.R = R;
+        const int H = R + 2, ZW = kFTW + 2 * H, ZH = kFTH + 2 * H;
+        const size_t smem = sizeof(float) * ZW * ZH + ((ZW * ZH + 15) / 16) * 16 + sizeof(float) * (kFTH + 2 * R) * kFTW;
+        FTB_CHECK(cudaFuncSetAttribute(filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        filter_kernel<<<dim3((w + kFTW - 1) / kFTW, (h + kFTH - 1) / kFTH, n), 256, smem, s>>>(a);
+        FTB_CHECK(cudaGetLastError());
+        c.span_end(span);
+    }
+    // 5. robust sigma of the masked filter output (border ceil(3 s) + 1), rescale
+    {
+        const int span = c.span_begin("filter normalisation");
+        const int fb = static_cast<int>(std::ceil(3 * psf_sigma)) + 1;
+        FTB_CHECK(cudaMemsetAsync(d_counts, 0, sizeof(int) * n, s));
+        const int st = grid_step(w, h, fb, 200000);
+        if (st > 0) {
+            const int gw = grid_count(fb, w - fb, st), gh = grid_count(fb, h - fb, st);
+            const long long g = static_cast<long long>(gw) * gh;
+            if (static_cast<long long>(gw) * gh > sc.cap) throw std::runtime_error("stage: sample buffer too small");
+            sample_kernel<<<dim3(static_cast<unsigned>((g + 255) / 256), n), 256, 0, s>>>(
+                d_filtered, plane, w, h, pitch, n, fb, st, gw, gh, d_mask, sc.samples.as<float>(), sc.cap, d_counts);
+            FTB_CHECK(cudaGetLastError());
+        }
+        robust_sigma_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, d_counts, d_sg, 0);
+        FTB_CHECK(cudaGetLastError());
+        rescale_kernel<<<dim3(static_cast<unsigned>((npix + 255) / 256), n), 256, 0, s>>>(d_filtered, plane, w, h, pitch,
+                                                                                       d_sg);
+        FTB_CHECK(cudaGetLastError());
+        c.span_end(span);
+    }
+    if (h_sigma) FTB_CHECK(cudaMemcpyAsync(h_sigma, d_sigma, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    if (h_cr) FTB_CHECK(cudaMemcpyAsync(h_cr, d_cr, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+}
+
+}  // namespace ftb

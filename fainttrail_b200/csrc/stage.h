@@ -1,0 +1,40 @@
+// The preprocessing stage (FaintTrail build_stage) on the device.
+#pragma once
+
+#include <vector>
+
+#include "engine.h"
+
+namespace ftb {
+
+struct StageParams {
+    double fwhm_px = 0.0;         // PSF FWHM (fixed)
+    int static_exclude = -1;      // -1: max(1, lround(n / 8))
+    double clip_sigma = 8.0;
+    double cr_sigma = 5.0;
+    double mask_scatter = 2.5;
+    double weight_scatter = 1.5;
+};
+
+// Device scratch of one stage: residuals, scatter map, sample buffers, tables.
+struct StageScratch {
+    StageScratch(Context& c, int w, int h, int n, double fwhm_px);
+    bool fits(int w, int h, int n, double fwhm_px) const;
+    DevBuf residual, scatter, samples, small;
+    int cap = 0;  // samples per frame
+    int w_ = 0, h_ = 0, n_ = 0;
+};
+
+// Maximum sample-grid points of sample_pixels(…, 200000, …, border) on w x h.
+int sample_grid_points(int w, int h, int border);
+
+void stage_time_ranks(const double* t_h, int n, std::vector<int>& rank);
+
+// build_stage on device frames d_sub (n x h x pitch, pitch = frame_pitch(w)):
+// d_filtered (same layout), d_sky and d_mask (h x pitch); h_sigma / h_cr (host,
+// may be null) receive the per-frame noise and cosmic-ray counts after the
+// stream is synchronised by the caller.
+void stage_run(Context& c, StageScratch& sc, const float* d_sub, int w, int h, int n, const double* t_h,
+               const StageParams& sp, float* d_filtered, float* d_sky, float* d_mask, double* h_sigma, int* h_cr);
+
+}  // namespace ftb

@@ -67,6 +67,33 @@ int ft_b200_stack_linear(ft_b200_ctx* ctx, const float* frames, int width, int h
 int ft_b200_stack_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
                       const int* dx, const int* dy, int motions, int min_count, float* d_max_snr, int* d_best_v);
 
+/* Parameters of the preprocessing stage; the defaults are SearchParams'
+ * (include/fainttrail/search.hpp:18-90): static_exclude -1 (= max(1, lround(n/8))),
+ * clip 8, cosmic-ray level 5, mask scatter 2.5, weight scatter 1.5. fwhm_px is the
+ * PSF FWHM in pixels and must be > 0 (the stage does not estimate it). */
+typedef struct ft_b200_stage_params {
+    double fwhm_px;
+    int static_exclude;
+    double clip_sigma;
+    double cr_sigma;
+    double mask_scatter;
+    double weight_scatter;
+} ft_b200_stage_params;
+
+void ft_b200_stage_params_default(ft_b200_stage_params* p);
+
+/* The time-order-dependent preprocessing: detail::build_stage (internal.hpp:55-58,
+ * preprocess.cpp:286-486) on background-subtracted frames `sub` (host,
+ * nframes x height x width, NaN = blank) observed at t_h[nframes] hours, with a
+ * fixed PSF width (the form every null run uses, preprocess.cpp:488-521).
+ * Outputs (host, any may be NULL): filtered (nframes x height x width, the
+ * unit-variance matched-filtered frames), static_sky and mask (height x width),
+ * sigma[nframes] (residual noise) and cr_pixels[nframes] (cosmic-ray hits).
+ * At most 255 frames. */
+int ft_b200_stage(ft_b200_ctx* ctx, const float* sub, int width, int height, int nframes, const double* t_h,
+                  const ft_b200_stage_params* params, float* filtered, float* static_sky, float* mask, double* sigma,
+                  int* cr_pixels);
+
 /* Stage timings of the last call on the context, measured with CUDA events on the
  * context's stream (the reference's StackResult::timings, backend.hpp:99-105, and
  * Prepared::timings, search.hpp:118): names as one ';'-separated string in
