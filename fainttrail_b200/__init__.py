@@ -35,6 +35,20 @@ class StageParams(C.Structure):
                 ("cr_sigma", C.c_double), ("mask_scatter", C.c_double), ("weight_scatter", C.c_double)]
 
 
+class SearchParams(C.Structure):
+    """ft_b200_search_params: ft_params (fainttrail.h:32-54) + null-model fields."""
+    _fields_ = [(n, C.c_double) for n in (
+        "vmin_pxh", "vmax_pxh", "grid_tol_px", "fwhm_px", "clip_sigma", "cr_sigma", "mask_scatter",
+        "weight_scatter", "min_coverage", "threshold_snr", "min_snr_floor", "target_false_per_run",
+        "max_frame_fraction", "half_tolerance")] + [
+        ("static_exclude", C.c_int), ("null_runs", C.c_int), ("max_candidates", C.c_int), ("edge_px", C.c_int),
+        ("threads", C.c_int), ("seed", C.c_ulonglong), ("null_tested", C.c_int), ("null_model_gauss", C.c_int)]
+
+
+class Peak(C.Structure):
+    _fields_ = [("x", C.c_int), ("y", C.c_int), ("snr", C.c_float), ("vidx", C.c_int)]
+
+
 class Cancelled(RuntimeError):
     """A progress callback asked to stop (types.hpp:70-76)."""
 
@@ -67,6 +81,17 @@ def _declare(L):
                                     C.c_int, C.c_void_p, C.c_void_p]
     L.ft_b200_timings.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_void_p, C.c_int]
     L.ft_b200_stage_params_default.argtypes = [C.POINTER(StageParams)]
+    L.ft_b200_search_params_default.argtypes = [C.POINTER(SearchParams)]
+    L.ft_b200_search.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.POINTER(SearchParams),
+                                 PROGRESS_FN, C.c_void_p, C.POINTER(C.c_void_p)]
+    L.ft_b200_result_free.argtypes = [C.c_void_p]
+    L.ft_b200_result_threshold.argtypes = [C.c_void_p, C.c_char_p, C.c_int] + [C.POINTER(C.c_double)] * 4
+    L.ft_b200_result_threshold.restype = C.c_double
+    L.ft_b200_result_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 3 + [C.POINTER(C.c_int)]
+    L.ft_b200_result_peaks.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int]
+    L.ft_b200_result_null_peaks.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    L.ft_b200_result_maps.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ft_b200_result_velocity.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.ft_b200_stage.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, C.POINTER(StageParams),
                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
 
@@ -144,6 +169,49 @@ class Device:
                                   ptr(filt), ptr(sky), ptr(mask), ptr(sigma), ptr(cr))
         self.check(rc, "stage")
         return dict(filtered=filt, static_sky=sky, mask=mask, sigma=sigma, cr=cr)
+
+    def search(self, frames, mjd, exptime, progress=None, **kw):
+        """A whole search (ft_b200_search) from raw frames; returns a dict."""
+        frames = np.ascontiguousarray(frames, dtype=np.float32)
+        n, h, w = frames.shape
+        p = SearchParams()
+        self.L.ft_b200_search_params_default(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        r = C.c_void_p()
+        rc = self.L.ft_b200_search(self.h, frames, w, h, n, np.ascontiguousarray(mjd, dtype=np.float64),
+                                   np.ascontiguousarray(exptime, dtype=np.float64), C.byref(p), _progress(progress),
+                                   None, C.byref(r))
+        self.check(rc, "search")
+        L = self.L
+        try:
+            meth = C.create_string_buffer(32)
+            a, b, k, s2 = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+            thr = L.ft_b200_result_threshold(r, meth, 32, C.byref(a), C.byref(b), C.byref(k), C.byref(s2))
+            fw, dv, tref, nv = C.c_double(), C.c_double(), C.c_double(), C.c_int()
+            L.ft_b200_result_info(r, C.byref(fw), C.byref(dv), C.byref(tref), C.byref(nv))
+
+            def peaks(which):
+                cnt = L.ft_b200_result_peaks(r, which, None, 0)
+                arr = (Peak * max(cnt, 1))()
+                L.ft_b200_result_peaks(r, which, arr, cnt)
+                return [(q.x, q.y, q.snr, q.vidx) for q in arr[:cnt]]
+            cnt = L.ft_b200_result_null_peaks(r, None, 0)
+            nulls = np.empty(cnt)
+            L.ft_b200_result_null_peaks(r, nulls.ctypes.data_as(C.c_void_p), cnt)
+            ms = np.empty((h, w), np.float32)
+            bv = np.empty((h, w), np.int32)
+            L.ft_b200_result_maps(r, ms.ctypes.data_as(C.c_void_p), bv.ctypes.data_as(C.c_void_p))
+            grid = np.empty((nv.value, 2))
+            vx, vy = C.c_double(), C.c_double()
+            for j in range(nv.value):
+                L.ft_b200_result_velocity(r, j, C.byref(vx), C.byref(vy))
+                grid[j] = (vx.value, vy.value)
+            return dict(threshold=thr, method=meth.value.decode(), null_a=a.value, null_b=b.value, null_k=k.value,
+                        null_inv_s2=s2.value, fwhm=fw.value, dv=dv.value, t_ref=tref.value, n_velocities=nv.value,
+                        peaks=peaks(0), selected=peaks(1), null_peaks=nulls, max_snr=ms, best_v=bv, grid=grid)
+        finally:
+            L.ft_b200_result_free(r)
 
     def info(self):
         name = C.create_string_buffer(256)

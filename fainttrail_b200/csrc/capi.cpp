@@ -10,10 +10,15 @@
 #include <vector>
 
 #include "engine.h"
+#include "search.h"
 #include "stage.h"
 
 struct ft_b200_ctx {
     std::unique_ptr<ftb::Context> c;
+};
+
+struct ft_b200_result {
+    ftb::SearchOut o;
 };
 
 namespace {
@@ -167,6 +172,126 @@ int ft_b200_stage(ft_b200_ctx* ctx, const float* sub, int width, int height, int
         sp.weight_scatter = params->weight_scatter;
         ftb::stage_host(c, sub, width, height, nframes, t_h, sp, filtered, static_sky, mask, sigma, cr_pixels);
     });
+}
+
+void ft_b200_search_params_default(ft_b200_search_params* p) {
+    if (!p) return;
+    const ftb::SearchParams d;
+    std::memset(p, 0, sizeof *p);
+    p->vmin_pxh = d.vmin_pxh;
+    p->vmax_pxh = d.vmax_pxh;
+    p->grid_tol_px = d.grid_tol_px;
+    p->fwhm_px = d.fwhm_px;
+    p->clip_sigma = d.clip_sigma;
+    p->cr_sigma = d.cr_sigma;
+    p->mask_scatter = d.mask_scatter;
+    p->weight_scatter = d.weight_scatter;
+    p->min_coverage = d.min_coverage;
+    p->threshold_snr = d.threshold_snr;
+    p->min_snr_floor = d.min_snr_floor;
+    p->target_false_per_run = d.target_false_per_run;
+    p->max_frame_fraction = d.max_frame_fraction;
+    p->half_tolerance = 3.0;
+    p->static_exclude = d.static_exclude;
+    p->null_runs = d.null_runs;
+    p->max_candidates = d.max_candidates;
+    p->edge_px = d.edge_px;
+    p->threads = 0;
+    p->seed = d.seed;
+    p->null_tested = d.null_tested;
+    p->null_model_gauss = d.gauss_model ? 1 : 0;
+}
+
+int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
+                   const double* exptime, const ft_b200_search_params* params, ft_b200_progress_fn progress,
+                   void* user, ft_b200_result** out) {
+    if (out) *out = nullptr;
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (!frames || !mjd || !out) throw std::runtime_error("search: missing frames, times or result pointer");
+        ft_b200_search_params d;
+        ft_b200_search_params_default(&d);
+        const ft_b200_search_params& q = params ? *params : d;
+        ftb::SearchParams p;
+        p.vmin_pxh = q.vmin_pxh;
+        p.vmax_pxh = q.vmax_pxh;
+        p.grid_tol_px = q.grid_tol_px;
+        p.fwhm_px = q.fwhm_px;
+        p.clip_sigma = q.clip_sigma;
+        p.cr_sigma = q.cr_sigma;
+        p.mask_scatter = q.mask_scatter;
+        p.weight_scatter = q.weight_scatter;
+        p.min_coverage = q.min_coverage;
+        p.threshold_snr = q.threshold_snr;
+        p.min_snr_floor = q.min_snr_floor;
+        p.target_false_per_run = q.target_false_per_run;
+        p.max_frame_fraction = q.max_frame_fraction;
+        p.static_exclude = q.static_exclude;
+        p.null_runs = q.null_runs;
+        p.null_tested = q.null_tested;
+        p.max_candidates = q.max_candidates;
+        p.edge_px = q.edge_px;
+        p.gauss_model = q.null_model_gauss != 0;
+        p.seed = q.seed;
+        auto r = std::make_unique<ft_b200_result>();
+        r->o = ftb::search_host(c, frames, width, height, nframes, mjd, exptime, p, wrap(progress, user));
+        *out = r.release();
+    });
+}
+
+void ft_b200_result_free(ft_b200_result* r) { delete r; }
+
+double ft_b200_result_threshold(const ft_b200_result* r, char* method, int method_len, double* null_a,
+                                double* null_b, double* null_k, double* null_inv_s2) {
+    if (!r) return 0.0;
+    const ftb::Threshold& t = r->o.thr;
+    if (method && method_len > 0) {
+        std::strncpy(method, t.method.c_str(), static_cast<size_t>(method_len) - 1);
+        method[method_len - 1] = 0;
+    }
+    if (null_a) *null_a = t.a;
+    if (null_b) *null_b = t.b;
+    if (null_k) *null_k = t.k;
+    if (null_inv_s2) *null_inv_s2 = t.inv_s2;
+    return t.snr;
+}
+
+int ft_b200_result_info(const ft_b200_result* r, double* fwhm_px, double* dv_pxh, double* t_ref_mjd,
+                        int* n_velocities) {
+    if (!r) return FT_B200_ERROR;
+    if (fwhm_px) *fwhm_px = r->o.fwhm_px;
+    if (dv_pxh) *dv_pxh = r->o.dv;
+    if (t_ref_mjd) *t_ref_mjd = r->o.t_ref_mjd;
+    if (n_velocities) *n_velocities = static_cast<int>(r->o.grid.size());
+    return FT_B200_OK;
+}
+
+int ft_b200_result_peaks(const ft_b200_result* r, int which, ft_b200_peak* out, int cap) {
+    if (!r) return 0;
+    const auto& v = which == 1 ? r->o.selected : r->o.peaks;
+    for (size_t k = 0; out && k < v.size() && static_cast<int>(k) < cap; ++k)
+        out[k] = {v[k].x, v[k].y, v[k].snr, v[k].vidx};
+    return static_cast<int>(v.size());
+}
+
+int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap) {
+    if (!r) return 0;
+    const auto& v = r->o.null_peaks;
+    for (size_t k = 0; out && k < v.size() && static_cast<int>(k) < cap; ++k) out[k] = v[k];
+    return static_cast<int>(v.size());
+}
+
+int ft_b200_result_maps(const ft_b200_result* r, float* max_snr, int* best_v) {
+    if (!r) return FT_B200_ERROR;
+    if (max_snr) std::memcpy(max_snr, r->o.max_snr.data(), sizeof(float) * r->o.max_snr.size());
+    if (best_v) std::memcpy(best_v, r->o.best_v.data(), sizeof(int) * r->o.best_v.size());
+    return FT_B200_OK;
+}
+
+int ft_b200_result_velocity(const ft_b200_result* r, int vidx, double* vx_pxh, double* vy_pxh) {
+    if (!r || vidx < 0 || vidx >= static_cast<int>(r->o.grid.size())) return FT_B200_ERROR;
+    if (vx_pxh) *vx_pxh = r->o.grid[static_cast<size_t>(vidx)].first;
+    if (vy_pxh) *vy_pxh = r->o.grid[static_cast<size_t>(vidx)].second;
+    return FT_B200_OK;
 }
 
 int ft_b200_timings(const ft_b200_ctx* ctx, char* names, int names_len, double* seconds, int cap) {

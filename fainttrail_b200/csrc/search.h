@@ -1,0 +1,90 @@
+// The search around the stacking passes: motion grid, time-shuffled null runs,
+// null-peak screening, the tail fit and threshold (FaintTrail search.cpp), with
+// the per-pixel work on the device and the small sequential steps on the host.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "engine.h"
+#include "stage.h"
+
+namespace ftb {
+
+// SearchParams fields used by the search path (search.hpp:18-90).
+struct SearchParams {
+    double vmin_pxh = 4.0, vmax_pxh = 40.0, grid_tol_px = 0.5, fwhm_px = 0.0;
+    double clip_sigma = 8.0, cr_sigma = 5.0, mask_scatter = 2.5, weight_scatter = 1.5;
+    double min_coverage = 0.7, threshold_snr = 0.0, min_snr_floor = 5.0, target_false_per_run = 0.02;
+    double max_frame_fraction = 0.25;
+    int static_exclude = -1, null_runs = 3, null_tested = 3000, max_candidates = 300, edge_px = 4;
+    bool gauss_model = true;  // null_model "gauss" (else "linear")
+    uint64_t seed = 12345;
+};
+
+struct Peak {
+    int x = 0, y = 0;
+    float snr = 0.0f;
+    int vidx = -1;
+};
+
+// ---- host steps (bit-identical restatements of the reference's host code)
+std::vector<std::pair<double, double>> velocity_grid(double span_h, const SearchParams& p, double* dv_out);
+std::vector<std::vector<double>> null_time_orders(const std::vector<double>& t_h, int runs, uint64_t seed);
+void shift_table(const std::vector<double>& t_h, const std::vector<std::pair<double, double>>& grid,
+                 std::vector<int>& dx, std::vector<int>& dy);
+int pass_min_count(double min_coverage, int n);
+// find_peaks' order: raster-ordered candidates sorted by std::sort on S/N
+// descending, then truncated (search.cpp:105-135)
+void order_peaks(std::vector<Peak>& raster_ordered, size_t max_peaks);
+struct Threshold {
+    double snr = 0.0;
+    std::string method;
+    double a = 0.0, b = 0.0, k = 0.0, inv_s2 = 0.0;
+};
+// set_threshold with null runs, or fixed (search.cpp:573-598); the Gaussian
+// trial-count rule for runs == 0 without a fixed threshold (search.cpp:599-611)
+Threshold set_threshold(const SearchParams& p, const std::vector<float>& pooled, int runs, double fwhm_px, int w,
+                        int h, size_t n_motions);
+double estimate_fwhm(const std::vector<float>& img, int w, int h, double noise_sigma);
+double estimate_psf_fwhm(const std::vector<float>& static_sky, int w, int h, std::vector<double> sigma,
+                         const SearchParams& p);
+double median_of(std::vector<float> v);  // median_inplace (common.hpp:64-74)
+
+// ---- device steps
+// prepare_core's background and blank-border growth (preprocess.cpp:572-580,
+// 233-254): d_raw (overwritten) -> d_sub; per-frame backgrounds to h_bg.
+void prepare_sub(Context& c, StageScratch& sc, float* d_raw, float* d_sub, int w, int h, int n, double* h_bg);
+// local maxima of a detection map above `floor` (search.cpp:105-131), in
+// raster order
+std::vector<Peak> device_peaks(Context& c, const float* d_max, const int* d_best_v, int w, int h, float floor,
+                               int radius, int edge);
+// artefact flags (single-frame share, field edge) of peaks at their grid motion
+// (is_artefact_peak, search.cpp:229-243, 142-190), on the device
+std::vector<char> device_artefacts(Context& c, const std::vector<Peak>& peaks, size_t count,
+                                   const std::vector<std::pair<double, double>>& grid, const float* d_filtered,
+                                   const float* d_sub, const float* d_sky, const std::vector<double>& t_h, int w,
+                                   int h, int n, double fwhm_px, double max_frame_fraction);
+
+// One whole search from raw frames (ft_search's prepare + search, without the
+// candidate refinement).
+struct SearchOut {
+    int w = 0, h = 0, n = 0;
+    double fwhm_px = 0, span_h = 0, t_ref_mjd = 0, dv = 0;
+    std::vector<double> t_h, background, sigma;
+    std::vector<std::pair<double, double>> grid;
+    Threshold thr;
+    std::vector<double> null_peaks;      // pooled S/N of the null runs (search.hpp:177)
+    std::vector<Peak> peaks;             // real-run peaks above the floor (find_peaks)
+    std::vector<Peak> selected;          // select_peaks (search.cpp:614-620)
+    std::vector<float> max_snr;          // real detection map
+    std::vector<int> best_v;
+    double adds = 0;                     // pixel x frame x motion additions of all passes
+};
+
+SearchOut search_host(Context& c, const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
+                      const SearchParams& p, const Progress& progress);
+
+}  // namespace ftb

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "search.h"
 #include "stage.h"
 
 namespace ftb {
@@ -415,6 +416,45 @@ __global__ void rescale_kernel(float* g, size_t plane, int w, int h, int pitch, 
     *p = __fmul_rn(*p, ig);
 }
 
+// median_inplace of each frame's samples (the background, preprocess.cpp:574-575)
+__global__ void __launch_bounds__(1024) median_kernel(const float* samples, int cap, const int* counts, double* out) {
+    __shared__ uint32_t hist[256];
+    __shared__ uint32_t sh[2];
+    const int f = blockIdx.x;
+    const int cnt = min(counts[f], cap);
+    const double m = cta_median<0>(samples + static_cast<size_t>(f) * cap, cnt, 0.0, hist, sh);
+    if (threadIdx.x == 0) out[f] = m;
+}
+
+// v -> float(v - bg), NaN stays NaN (preprocess.cpp:235), in place
+__global__ void subtract_kernel(float* img, size_t plane, int w, int h, int pitch, const double* bg) {
+    const int f = blockIdx.y;
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int x = static_cast<int>(q % w), y = static_cast<int>(q / w);
+    if (y >= h) return;
+    float* p = img + f * plane + static_cast<size_t>(y) * pitch + x;
+    const float v = *p;
+    *p = finitef(v) ? __double2float_rn(static_cast<double>(v) - bg[f]) : CUDART_NAN_F;
+}
+
+// blank areas grown by `grow` pixels: NaN wherever a non-finite pixel lies within
+// +-grow in x and y (preprocess.cpp:240-253)
+__global__ void grow_kernel(const float* in, float* out, size_t plane, int w, int h, int pitch, int grow) {
+    const int f = blockIdx.y;
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int x = static_cast<int>(q % w), y = static_cast<int>(q / w);
+    if (y >= h) return;
+    const float* src = in + f * plane;
+    bool bad = false;
+    for (int yy = max(0, y - grow); yy <= min(h - 1, y + grow) && !bad; ++yy)
+        for (int xx = max(0, x - grow); xx <= min(w - 1, x + grow); ++xx)
+            if (!finitef(src[static_cast<size_t>(yy) * pitch + xx])) {
+                bad = true;
+                break;
+            }
+    out[f * plane + static_cast<size_t>(y) * pitch + x] = bad ? CUDART_NAN_F : src[static_cast<size_t>(y) * pitch + x];
+}
+
 inline int grid_step(int w, int h, int border, size_t max_samples) {
     const size_t usable = static_cast<size_t>(std::max(0, w - 2 * border)) * static_cast<size_t>(std::max(0, h - 2 * border));
     if (usable == 0) return 0;
@@ -450,7 +490,9 @@ StageScratch::StageScratch(Context& c, int w, int h, int n, double fwhm_px) : w_
     const size_t plane = static_cast<size_t>(pitch) * h;
     residual = DevBuf(&c, sizeof(float) * plane * n, "residuals");
     scatter = DevBuf(&c, sizeof(float) * plane, "scatter map");
-    cap = std::max({1, sample_grid_points(w, h, 2), sample_grid_points(w, h, filter_border(fwhm_px))});
+    // room for any sample grid this stage can use (borders 0 .. 64, and the PSF's)
+    cap = std::max(1, sample_grid_points(w, h, filter_border(fwhm_px)));
+    for (int b = 0; b <= 64; ++b) cap = std::max(cap, sample_grid_points(w, h, b));
     samples = DevBuf(&c, sizeof(float) * static_cast<size_t>(cap) * n, "noise samples");
     small = DevBuf(&c, 4096 + sizeof(double) * 2 * n + sizeof(int) * 2 * n + 2 * static_cast<size_t>(n), "stage tables");
 }
@@ -459,49 +501,54 @@ bool StageScratch::fits(int w, int h, int n, double fwhm_px) const {
     return w == w_ && h == h_ && n == n_ && sample_grid_points(w, h, filter_border(fwhm_px)) <= cap;
 }
 
-void stage_run(Context& c, StageScratch& sc, const float* d_sub, int w, int h, int n, const double* t_h,
-               const StageParams& sp, float* d_filtered, float* d_sky, float* d_mask, double* h_sigma, int* h_cr) {
+// The device tables of a stage in StageScratch::small: filter taps, per-frame
+// sigma, filter sigma, sample counts, cosmic-ray tallies, rank tables.
+struct StageTables {
+    float* taps;
+    double* sigma;
+    double* sg;
+    int* counts;
+    int* cr;
+    unsigned char* tab;
+};
+
+static StageTables stage_tables(StageScratch& sc, int n) {
+    unsigned char* base = sc.small.as<unsigned char>();
+    StageTables t;
+    t.taps = reinterpret_cast<float*>(base);  // up to 512 floats
+    t.sigma = reinterpret_cast<double*>(base + 2048);
+    t.sg = t.sigma + n;
+    t.counts = reinterpret_cast<int*>(t.sg + n);
+    t.cr = t.counts + n;
+    t.tab = reinterpret_cast<unsigned char*>(t.cr + n);
+    return t;
+}
+
+void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h, int n, const double* t_h,
+                 int static_exclude, float* d_sky) {
     if (n < 1 || n > 255) throw std::runtime_error("stage: between 1 and 255 frames are supported");
-    if (!sc.fits(w, h, n, sp.fwhm_px)) throw std::runtime_error("stage: scratch sized for another shape");
+    if (w != sc.w_ || h != sc.h_ || n != sc.n_) throw std::runtime_error("stage: scratch sized for another shape");
     const int pitch = frame_pitch(w);
     const size_t plane = static_cast<size_t>(pitch) * h;
     const long long npix = static_cast<long long>(w) * h;
     cudaStream_t s = c.stream();
+    const StageTables tb = stage_tables(sc, n);
 
-    // host tables: time ranks, the frame of each rank, the filter taps
+    // host tables: time ranks and the frame of each rank
     std::vector<int> rank;
     stage_time_ranks(t_h, n, rank);
-    const int exclude = sp.static_exclude >= 0 ? sp.static_exclude : std::max(1, static_cast<int>(std::lround(n / 8.0)));
+    const int exclude = static_exclude >= 0 ? static_exclude : std::max(1, static_cast<int>(std::lround(n / 8.0)));
     std::vector<unsigned char> tab(2 * static_cast<size_t>(n));
     for (int i = 0; i < n; ++i) {
         tab[static_cast<size_t>(i)] = static_cast<unsigned char>(rank[static_cast<size_t>(i)]);
         tab[static_cast<size_t>(n + rank[static_cast<size_t>(i)])] = static_cast<unsigned char>(i);
     }
-    const double psf_sigma = sp.fwhm_px * kFwhmToSigma;
-    const int R = std::max(1, static_cast<int>(std::ceil(3.0 * psf_sigma)));
-    std::vector<float> taps(static_cast<size_t>(2 * R + 1));
-    double k2 = 0.0;
-    for (int i = -R; i <= R; ++i) {
-        const double v = std::exp(-0.5 * i * i / (psf_sigma * psf_sigma));
-        taps[static_cast<size_t>(i + R)] = static_cast<float>(v);
-        k2 += v * v;
-    }
-    if (taps.size() > 512) throw std::runtime_error("stage: PSF too wide");
-    unsigned char* base = sc.small.as<unsigned char>();
-    float* d_taps = reinterpret_cast<float*>(base);                     // up to 512 floats
-    double* d_sigma = reinterpret_cast<double*>(base + 2048);
-    double* d_sg = d_sigma + n;
-    int* d_counts = reinterpret_cast<int*>(d_sg + n);
-    int* d_cr = d_counts + n;
-    unsigned char* d_tab = reinterpret_cast<unsigned char*>(d_cr + n);
-    FTB_CHECK(cudaMemcpyAsync(d_taps, taps.data(), sizeof(float) * taps.size(), cudaMemcpyHostToDevice, s));
-    FTB_CHECK(cudaMemcpyAsync(d_tab, tab.data(), tab.size(), cudaMemcpyHostToDevice, s));
-    FTB_CHECK(cudaMemsetAsync(d_counts, 0, sizeof(int) * 2 * n, s));  // counts and cosmic-ray tallies
-
+    FTB_CHECK(cudaMemcpyAsync(tb.tab, tab.data(), tab.size(), cudaMemcpyHostToDevice, s));
+    FTB_CHECK(cudaMemsetAsync(tb.counts, 0, sizeof(int) * 2 * n, s));  // counts and cosmic-ray tallies
     // 1. static sky + residuals
     {
         const int span = c.span_begin("static sky + residuals");
-        SkyArgs a{d_sub, sc.residual.as<float>(), d_sky, d_tab, d_tab + n, w, h, pitch, n, exclude,
+        SkyArgs a{d_sub, sc.residual.as<float>(), d_sky, tb.tab, tb.tab + n, w, h, pitch, n, exclude,
                   std::max(5, static_cast<int>(0.6 * n))};
         const int T = 64;
         const size_t smem = static_cast<size_t>(T) * n * 9;
@@ -519,13 +566,40 @@ void stage_run(Context& c, StageScratch& sc, const float* d_sub, int w, int h, i
             const long long g = static_cast<long long>(gw) * gh;
             sample_kernel<<<dim3(static_cast<unsigned>((g + 255) / 256), n), 256, 0, s>>>(
                 sc.residual.as<float>(), plane, w, h, pitch, n, 2, st, gw, gh, nullptr, sc.samples.as<float>(), sc.cap,
-                d_counts);
+                tb.counts);
             FTB_CHECK(cudaGetLastError());
         }
-        robust_sigma_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, d_counts, d_sigma, 1);
+        robust_sigma_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, tb.counts, tb.sigma, 1);
         FTB_CHECK(cudaGetLastError());
         c.span_end(span);
     }
+}
+
+void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const StageParams& sp, float* d_filtered,
+                  float* d_mask, double* h_sigma, int* h_cr) {
+    if (!sc.fits(w, h, n, sp.fwhm_px)) throw std::runtime_error("stage: scratch sized for another shape");
+    const int pitch = frame_pitch(w);
+    const size_t plane = static_cast<size_t>(pitch) * h;
+    const long long npix = static_cast<long long>(w) * h;
+    cudaStream_t s = c.stream();
+    const StageTables tb = stage_tables(sc, n);
+    // the separable filter taps (preprocess.cpp:118-126)
+    const double psf_sigma = sp.fwhm_px * kFwhmToSigma;
+    const int R = std::max(1, static_cast<int>(std::ceil(3.0 * psf_sigma)));
+    std::vector<float> taps(static_cast<size_t>(2 * R + 1));
+    double k2 = 0.0;
+    for (int i = -R; i <= R; ++i) {
+        const double v = std::exp(-0.5 * i * i / (psf_sigma * psf_sigma));
+        taps[static_cast<size_t>(i + R)] = static_cast<float>(v);
+        k2 += v * v;
+    }
+    if (taps.size() > 512) throw std::runtime_error("stage: PSF too wide");
+    FTB_CHECK(cudaMemcpyAsync(tb.taps, taps.data(), sizeof(float) * taps.size(), cudaMemcpyHostToDevice, s));
+    float* d_taps = tb.taps;
+    double* d_sigma = tb.sigma;
+    double* d_sg = tb.sg;
+    int* d_counts = tb.counts;
+    int* d_cr = tb.cr;
     // 3. scatter map and mask
     {
         const int span = c.span_begin("scatter mask");
@@ -591,6 +665,44 @@ void stage_run(Context& c, StageScratch& sc, const float* d_sub, int w, int h, i
     }
     if (h_sigma) FTB_CHECK(cudaMemcpyAsync(h_sigma, d_sigma, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
     if (h_cr) FTB_CHECK(cudaMemcpyAsync(h_cr, d_cr, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+}
+
+void stage_run(Context& c, StageScratch& sc, const float* d_sub, int w, int h, int n, const double* t_h,
+               const StageParams& sp, float* d_filtered, float* d_sky, float* d_mask, double* h_sigma, int* h_cr) {
+    stage_noise(c, sc, d_sub, w, h, n, t_h, sp.static_exclude, d_sky);
+    stage_filter(c, sc, w, h, n, sp, d_filtered, d_mask, h_sigma, h_cr);
+}
+
+void stage_sigma_to_host(Context& c, StageScratch& sc, int n, double* h_sigma) {
+    FTB_CHECK(cudaMemcpyAsync(h_sigma, stage_tables(sc, n).sigma, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                              c.stream()));
+}
+
+void prepare_sub(Context& c, StageScratch& sc, float* d_raw, float* d_sub, int w, int h, int n, double* h_bg) {
+    const int pitch = frame_pitch(w);
+    const size_t plane = static_cast<size_t>(pitch) * h;
+    const long long npix = static_cast<long long>(w) * h;
+    cudaStream_t s = c.stream();
+    const StageTables tb = stage_tables(sc, n);
+    const int span = c.span_begin("background + borders");
+    FTB_CHECK(cudaMemsetAsync(tb.counts, 0, sizeof(int) * n, s));
+    const int st = grid_step(w, h, 0, 200000);
+    if (st > 0) {
+        const int gw = grid_count(0, w, st), gh = grid_count(0, h, st);
+        const long long g = static_cast<long long>(gw) * gh;
+        sample_kernel<<<dim3(static_cast<unsigned>((g + 255) / 256), n), 256, 0, s>>>(
+            d_raw, plane, w, h, pitch, n, 0, st, gw, gh, nullptr, sc.samples.as<float>(), sc.cap, tb.counts);
+        FTB_CHECK(cudaGetLastError());
+    }
+    median_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, tb.counts, tb.sg);
+    FTB_CHECK(cudaGetLastError());
+    const dim3 grid(static_cast<unsigned>((npix + 255) / 256), n);
+    subtract_kernel<<<grid, 256, 0, s>>>(d_raw, plane, w, h, pitch, tb.sg);
+    FTB_CHECK(cudaGetLastError());
+    grow_kernel<<<grid, 256, 0, s>>>(d_raw, d_sub, plane, w, h, pitch, 3);
+    FTB_CHECK(cudaGetLastError());
+    c.span_end(span);
+    if (h_bg) FTB_CHECK(cudaMemcpyAsync(h_bg, tb.sg, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
 }
 
 }  // namespace ftb

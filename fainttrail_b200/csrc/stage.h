@@ -30,6 +30,15 @@ int sample_grid_points(int w, int h, int border);
 
 void stage_time_ranks(const double* t_h, int n, std::vector<int>& rank);
 
+// The two halves of build_stage, so that a PSF estimate can sit between them as
+// in the reference (preprocess.cpp:368): static sky, residuals and per-frame
+// noise; then scatter, mask, matched filter and its normalisation.
+void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h, int n, const double* t_h,
+                 int static_exclude, float* d_sky);
+void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const StageParams& sp, float* d_filtered,
+                  float* d_mask, double* h_sigma, int* h_cr);
+void stage_sigma_to_host(Context& c, StageScratch& sc, int n, double* h_sigma);
+
 // build_stage on device frames d_sub (n x h x pitch, pitch = frame_pitch(w)):
 // d_filtered (same layout), d_sky and d_mask (h x pitch); h_sigma / h_cr (host,
 // may be null) receive the per-frame noise and cosmic-ray counts after the

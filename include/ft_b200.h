@@ -94,6 +94,63 @@ int ft_b200_stage(ft_b200_ctx* ctx, const float* sub, int width, int height, int
                   const ft_b200_stage_params* params, float* filtered, float* static_sky, float* mask, double* sigma,
                   int* cr_pixels);
 
+/* Parameters of a search: ft_params (fainttrail.h:32-54) plus the null-model
+ * fields of SearchParams (search.hpp:58-68). Defaults: ft_b200_search_params_default,
+ * equal to the reference's SearchParams defaults. `threads` is accepted and
+ * ignored (the reference's CPU thread count). */
+typedef struct ft_b200_search_params {
+    double vmin_pxh, vmax_pxh, grid_tol_px, fwhm_px;
+    double clip_sigma, cr_sigma, mask_scatter, weight_scatter, min_coverage;
+    double threshold_snr, min_snr_floor, target_false_per_run, max_frame_fraction, half_tolerance;
+    int static_exclude, null_runs, max_candidates, edge_px, threads;
+    unsigned long long seed;
+    int null_tested;      /* strongest null peaks per run screened for artefacts (3000) */
+    int null_model_gauss; /* 1: "gauss" tail model (default), 0: "linear" */
+} ft_b200_search_params;
+
+void ft_b200_search_params_default(ft_b200_search_params* p);
+
+/* A detection-map peak (detail::Peak, internal.hpp:88-92): 0-based pixel,
+ * coarse S/N, index of the trial motion. */
+typedef struct ft_b200_peak {
+    int x, y;
+    float snr;
+    int vidx;
+} ft_b200_peak;
+
+typedef struct ft_b200_result ft_b200_result;
+
+/* A whole search from raw registered frames, as ft_search does (c_api.cpp:172-204:
+ * frames stable-sorted by mid-exposure time, prepare, then search): background
+ * and blank-border growth, preprocessing, the real stacking pass and its peaks,
+ * params->null_runs time-shuffled null runs (preprocessing rebuilt, stacked,
+ * peaks screened for artefacts), the null-tail fit and threshold, and the peaks
+ * selected for refinement (search.cpp:716-788). Candidate refinement is left to
+ * the caller. frames: host, nframes x height x width; mjd/exptime per frame.
+ * On success *out receives a result to release with ft_b200_result_free. */
+int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
+                   const double* exptime, const ft_b200_search_params* params, ft_b200_progress_fn progress,
+                   void* user, ft_b200_result** out);
+void ft_b200_result_free(ft_b200_result* r);
+/* threshold_snr and the tail model (SearchResult, search.hpp:163-172); method
+ * receives "fixed", "null-fit gauss", "null-fit linear", "null-quantile" or
+ * "gaussian". Any pointer may be NULL. */
+double ft_b200_result_threshold(const ft_b200_result* r, char* method, int method_len, double* null_a,
+                                double* null_b, double* null_k, double* null_inv_s2);
+/* fwhm_px, dv_pxh, t_ref_mjd and the number of trial motions of the search. */
+int ft_b200_result_info(const ft_b200_result* r, double* fwhm_px, double* dv_pxh, double* t_ref_mjd,
+                        int* n_velocities);
+/* which = 0: all real-run peaks above the floor, S/N descending (find_peaks);
+ * which = 1: the peaks selected for refinement (select_peaks). Returns the
+ * count; writes at most cap. */
+int ft_b200_result_peaks(const ft_b200_result* r, int which, ft_b200_peak* out, int cap);
+/* The pooled null-peak S/N values (SearchResult::null_peaks). Returns the count. */
+int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap);
+/* The real run's detection map: max_snr and best_v, height x width each. */
+int ft_b200_result_maps(const ft_b200_result* r, float* max_snr, int* best_v);
+/* The trial motion vidx of the grid (velocity_grid, search.cpp:39-58), px/hour. */
+int ft_b200_result_velocity(const ft_b200_result* r, int vidx, double* vx_pxh, double* vy_pxh);
+
 /* Stage timings of the last call on the context, measured with CUDA events on the
  * context's stream (the reference's StackResult::timings, backend.hpp:99-105, and
  * Prepared::timings, search.hpp:118): names as one ';'-separated string in
