@@ -1,0 +1,323 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 search backend.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload NAME]
+
+A step is one whole search (FaintTrail ft_search without candidate refinement:
+background, preprocessing, the real stacking pass and its peaks, the null runs
+with their rebuilt preprocessing, stacks, peaks and artefact screen, and the
+tail-fit threshold) over one synthetic sequence resident in HBM. The metric is
+the reference's stacking throughput, pixel x frame x motion per second
+(io.cpp:316-319), here over the whole search time, not the stacking time alone.
+
+Default workload: the full-frame plain search on one B200 -- 40 float32 frames
+of 4096 x 4096, 30 s cadence, rates 0.1-2 px/min on a half-pixel grid (19,328
+trial motions), 3 time-shuffled null runs (4 passes). Under torchrun each rank
+runs its own sequence (a different sky field, seed 7 + rank): weak scaling, no
+collective in the data path; the per-step device time is the maximum over ranks.
+
+--impl reference times the reference's own CPU implementation (FaintTrail
+0.9.1 built from its sources, oracle/_ref) on the host's cores with all
+threads, each step a bounded crop of the same workload (all frames, the full
+motion grid, null runs), same metric and unit. Under torchrun only rank 0 runs it.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "pixel·frame·motion/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="fullframe-4k")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms (reads only)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.lines, self.proc = gpu, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def workload_desc(wl, m):
+    return (f"{wl.name}: {wl.nframes} x {wl.width} x {wl.height} float32 frames, {wl.cadence_s:g} s cadence, "
+            f"rates {wl.rate_px_min[0]:g}-{wl.rate_px_min[1]:g} px/min ({m} trial motions), "
+            f"{wl.null_runs} null runs ({wl.null_runs + 1} passes)")
+
+
+# --------------------------------------------------------------------------- reference CPU timing
+def reference_search_rate(wl, frames_np, mjd, exptime, target_s=15.0, steps=1):
+    """The reference CPU search (prepare + search, all host threads) on a crop of
+    the workload sized to about target_s seconds. Returns adds/s and a note."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from ftoracle import Reference
+    R = Reference()
+    params = dict(wl.search_params())
+    grid, _ = R.velocity_grid((mjd[-1] - mjd[0]) * 24.0, vmin_pxh=params["vmin_pxh"], vmax_pxh=params["vmax_pxh"],
+                              grid_tol_px=params["grid_tol_px"])
+    m = grid.shape[0]
+
+    def run(side):
+        crop = np.ascontiguousarray(frames_np[:, :side, :side])
+        t0 = time.perf_counter()
+        prep = R.prepare(crop, mjd, exptime, fwhm_px=params["fwhm_px"], null_runs=params["null_runs"])
+        prep.search(backend="cpu", **params)
+        dt = time.perf_counter() - t0
+        return m * wl.nframes * side * side * (1 + params["null_runs"]) / dt, dt
+    side = 128
+    rate, dt = run(side)
+    # grow the crop until a step takes a few seconds, within the frame
+    while dt * 4 < target_s and side * 2 <= min(wl.width, wl.height):
+        side *= 2
+        rate, dt = run(side)
+    rates = [rate] + [run(side)[0] for _ in range(steps - 1)]
+    return statistics.median(rates), side, dt
+
+
+# --------------------------------------------------------------------------- arms
+def reference_arm(args):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return
+    from fainttrail_b200 import synthetic
+    wl = synthetic.WORKLOADS[args.workload]
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    frames, mjd, exptime, _ = synthetic.generate(wl, seed=7, device=dev)
+    side_max = min(1024, wl.width, wl.height)
+    frames_np = frames[:, :side_max, :side_max].cpu().numpy()
+    del frames
+    t0 = time.perf_counter()
+    rate, side, dt = reference_search_rate(wl, frames_np, mjd, exptime, steps=max(1, args.steps))
+    cores = os.cpu_count()
+    sample = (f"reference search() (prepare + real pass + {wl.null_runs} null runs, backend cpu) on a "
+              f"{side} x {side} crop of all {wl.nframes} frames, full motion grid; {dt:.1f} s per step")
+    out = {"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1000.0, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+           "config": {"workload": args.workload, "crop": f"{side}x{side}"},
+           "cpu_baseline": {"value": rate, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample},
+           "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "wall_s": time.perf_counter() - t0}
+    print(json.dumps(out), flush=True)
+
+
+def b200_arm(args):
+    import torch
+    import fainttrail_b200 as ftb
+    from fainttrail_b200 import synthetic
+    rank, local_rank, world = env_rank()
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local_rank)
+    wl = synthetic.WORKLOADS[args.workload]
+    params = wl.search_params()
+    frames, mjd, exptime, truth = synthetic.generate(wl, seed=7 + rank, device=f"cuda:{local_rank}")
+    torch.cuda.synchronize()
+    n, h, w = frames.shape
+    dev = ftb.Device(local_rank)
+
+    def step():
+        r = dev.search_dev(frames.data_ptr(), w, h, w, n, mjd, exptime, maps=False, **params)
+        return r, dict(dev.timings()), dev.launches()
+
+    for _ in range(max(3, args.warmup)):
+        r, tm, _ = step()
+    m = r["n_velocities"]
+    adds_step = float(m) * n * w * h * (1 + wl.null_runs)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    totals, kernels, launches = [], [], 0
+    stage = {}
+    for _ in range(args.steps):
+        r, tm, nl = step()
+        totals.append(tm["total"])
+        kernels.append(tm["kernel"])
+        launches += nl
+        for k, v in tm.items():
+            stage[k] = stage.get(k, 0.0) + v
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    total = sum(totals)
+    if dist:
+        t = torch.tensor([total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    value = world * args.steps * adds_step / total
+    peaks, peak_kind = measured_peaks()
+    sms = dev.info()[1]
+    fp32_peak = sms * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12  # non-FMA adds, TFLOP/s
+    passes = 1 + wl.null_runs
+    per_launch_adds = float(m) * n * w * h
+    kernel_avg = sum(kernels) / (args.steps * passes)
+    achieved = per_launch_adds / kernel_avg / 1e12
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    # the HBM-bound stage kernels: algorithmic bytes per launch over their event time
+    sky_bytes = (8.0 * n + 4.0) * w * h
+    filt_bytes = (8.0 * n + 8.0) * w * h
+    stage_roof = {}
+    for name, b in (("static sky + residuals", sky_bytes), ("matched filter", filt_bytes)):
+        if name in stage:
+            gbs = b * passes * args.steps / stage[name] / 1e9
+            stage_roof[name] = {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                                "bytes_per_launch": b}
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "stack_traffic.json")) as f:
+            tr = json.load(f)
+        if tr.get("workload") == args.workload:
+            traffic = tr["bytes_per_launch"]
+    except (OSError, ValueError, KeyError):
+        pass
+
+    # end to end through the C ABI with host buffers: pinned frames in, maps out
+    e2e = None
+    if args.e2e_steps > 0:
+        host = torch.empty((n, h, w), dtype=torch.float32, pin_memory=True)
+        host.copy_(frames)
+        host_np = host.numpy()
+        dev.search(host_np, mjd, exptime, maps=True, **params)  # first call allocates
+        if dist:
+            dist.barrier()
+        walls = []
+        for _ in range(args.e2e_steps):
+            t0 = time.perf_counter()
+            dev.search(host_np, mjd, exptime, maps=True, **params)
+            walls.append(time.perf_counter() - t0)
+        wall = sum(walls)
+        if dist:
+            t = torch.tensor([wall], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        e2e = {"value": world * args.e2e_steps * adds_step / wall, "unit": METRIC,
+               "h2d_bytes_per_step": 4 * n * h * w, "d2h_bytes_per_step": 8 * h * w,
+               "ms_per_step": 1000.0 * wall / args.e2e_steps}
+        del host, host_np
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            frames_np = frames[:, :1024, :1024].cpu().numpy()
+            rate, side, dt = reference_search_rate(wl, frames_np, mjd, exptime)
+            cpu = {"value": rate, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"reference search() with backend cpu on a {side} x {side} crop of all {n} frames, "
+                             f"full motion grid, {wl.null_runs} null runs ({dt:.1f} s)"}
+        except Exception as e:  # the reference build is test infrastructure; report, do not fail the bench
+            cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+               "warmup": max(3, args.warmup), "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded sky/read/photon noise, log-uniform stars, movers at target S/N)",
+               "config": {"workload": workload_desc(wl, m), "parallelism": f"independent searches x{world}",
+                          "l2": f"inputs ({4 * n * h * w / 1e9:.1f} GB of frames) exceed the {L2_BYTES >> 20} MB L2"},
+               "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                            "frac": achieved / fp32_peak, "traffic": traffic,
+                            "kernel": "stack_kernel (one launch per pass)",
+                            "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x sm_max_mhz "
+                                           f"{peaks.get('sm_max_mhz', 1965.0):g} MHz ({peak_kind} peaks file has no "
+                                           f"FP32 figure); adds are non-FMA, one per lane per clock"},
+               "stage_roofline": stage_roof,
+               "stage_seconds_per_step": {k: v / args.steps for k, v in stage.items()},
+               "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
+               "threshold_snr": r["threshold"], "threshold_method": r["method"]}
+        print(json.dumps(out), flush=True)
+    dev.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

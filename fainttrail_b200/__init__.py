@@ -84,6 +84,9 @@ def _declare(L):
     L.ft_b200_search_params_default.argtypes = [C.POINTER(SearchParams)]
     L.ft_b200_search.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.POINTER(SearchParams),
                                  PROGRESS_FN, C.c_void_p, C.POINTER(C.c_void_p)]
+    L.ft_b200_search_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
+                                     C.POINTER(SearchParams), C.POINTER(C.c_void_p)]
+    L.ft_b200_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
     L.ft_b200_result_free.argtypes = [C.c_void_p]
     L.ft_b200_result_threshold.argtypes = [C.c_void_p, C.c_char_p, C.c_int] + [C.POINTER(C.c_double)] * 4
     L.ft_b200_result_threshold.restype = C.c_double
@@ -170,19 +173,43 @@ class Device:
         self.check(rc, "stage")
         return dict(filtered=filt, static_sky=sky, mask=mask, sigma=sigma, cr=cr)
 
-    def search(self, frames, mjd, exptime, progress=None, **kw):
+    def launches(self):
+        """Kernels launched by the last call (ft_b200_stats)."""
+        k = C.c_longlong()
+        self.L.ft_b200_stats(self.h, C.byref(k), None)
+        return k.value
+
+    @staticmethod
+    def _search_params(L, kw):
+        p = SearchParams()
+        L.ft_b200_search_params_default(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+    def search_dev(self, d_frames, width, height, pitch, nframes, mjd, exptime, maps=True, **kw):
+        """ft_b200_search_dev on a device pointer; returns the result dict."""
+        p = self._search_params(self.L, kw)
+        r = C.c_void_p()
+        rc = self.L.ft_b200_search_dev(self.h, C.c_void_p(d_frames), width, height, pitch, nframes,
+                                       np.ascontiguousarray(mjd, dtype=np.float64),
+                                       np.ascontiguousarray(exptime, dtype=np.float64), C.byref(p), C.byref(r))
+        self.check(rc, "search_dev")
+        return self._result(r, width, height, maps)
+
+    def search(self, frames, mjd, exptime, progress=None, maps=True, **kw):
         """A whole search (ft_b200_search) from raw frames; returns a dict."""
         frames = np.ascontiguousarray(frames, dtype=np.float32)
         n, h, w = frames.shape
-        p = SearchParams()
-        self.L.ft_b200_search_params_default(C.byref(p))
-        for k, v in kw.items():
-            setattr(p, k, v)
+        p = self._search_params(self.L, kw)
         r = C.c_void_p()
         rc = self.L.ft_b200_search(self.h, frames, w, h, n, np.ascontiguousarray(mjd, dtype=np.float64),
                                    np.ascontiguousarray(exptime, dtype=np.float64), C.byref(p), _progress(progress),
                                    None, C.byref(r))
         self.check(rc, "search")
+        return self._result(r, w, h, maps)
+
+    def _result(self, r, w, h, maps):
         L = self.L
         try:
             meth = C.create_string_buffer(32)
@@ -199,9 +226,11 @@ class Device:
             cnt = L.ft_b200_result_null_peaks(r, None, 0)
             nulls = np.empty(cnt)
             L.ft_b200_result_null_peaks(r, nulls.ctypes.data_as(C.c_void_p), cnt)
-            ms = np.empty((h, w), np.float32)
-            bv = np.empty((h, w), np.int32)
-            L.ft_b200_result_maps(r, ms.ctypes.data_as(C.c_void_p), bv.ctypes.data_as(C.c_void_p))
+            ms = bv = None
+            if maps:
+                ms = np.empty((h, w), np.float32)
+                bv = np.empty((h, w), np.int32)
+                L.ft_b200_result_maps(r, ms.ctypes.data_as(C.c_void_p), bv.ctypes.data_as(C.c_void_p))
             grid = np.empty((nv.value, 2))
             vx, vy = C.c_double(), C.c_double()
             for j in range(nv.value):

@@ -202,40 +202,68 @@ void ft_b200_search_params_default(ft_b200_search_params* p) {
     p->null_model_gauss = d.gauss_model ? 1 : 0;
 }
 
+namespace {
+ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
+    ft_b200_search_params d;
+    ft_b200_search_params_default(&d);
+    const ft_b200_search_params& q = params ? *params : d;
+    ftb::SearchParams p;
+    p.vmin_pxh = q.vmin_pxh;
+    p.vmax_pxh = q.vmax_pxh;
+    p.grid_tol_px = q.grid_tol_px;
+    p.fwhm_px = q.fwhm_px;
+    p.clip_sigma = q.clip_sigma;
+    p.cr_sigma = q.cr_sigma;
+    p.mask_scatter = q.mask_scatter;
+    p.weight_scatter = q.weight_scatter;
+    p.min_coverage = q.min_coverage;
+    p.threshold_snr = q.threshold_snr;
+    p.min_snr_floor = q.min_snr_floor;
+    p.target_false_per_run = q.target_false_per_run;
+    p.max_frame_fraction = q.max_frame_fraction;
+    p.static_exclude = q.static_exclude;
+    p.null_runs = q.null_runs;
+    p.null_tested = q.null_tested;
+    p.max_candidates = q.max_candidates;
+    p.edge_px = q.edge_px;
+    p.gauss_model = q.null_model_gauss != 0;
+    p.seed = q.seed;
+    return p;
+}
+}  // namespace
+
 int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
                    const double* exptime, const ft_b200_search_params* params, ft_b200_progress_fn progress,
                    void* user, ft_b200_result** out) {
     if (out) *out = nullptr;
     return guarded(ctx, [&](ftb::Context& c) {
         if (!frames || !mjd || !out) throw std::runtime_error("search: missing frames, times or result pointer");
-        ft_b200_search_params d;
-        ft_b200_search_params_default(&d);
-        const ft_b200_search_params& q = params ? *params : d;
-        ftb::SearchParams p;
-        p.vmin_pxh = q.vmin_pxh;
-        p.vmax_pxh = q.vmax_pxh;
-        p.grid_tol_px = q.grid_tol_px;
-        p.fwhm_px = q.fwhm_px;
-        p.clip_sigma = q.clip_sigma;
-        p.cr_sigma = q.cr_sigma;
-        p.mask_scatter = q.mask_scatter;
-        p.weight_scatter = q.weight_scatter;
-        p.min_coverage = q.min_coverage;
-        p.threshold_snr = q.threshold_snr;
-        p.min_snr_floor = q.min_snr_floor;
-        p.target_false_per_run = q.target_false_per_run;
-        p.max_frame_fraction = q.max_frame_fraction;
-        p.static_exclude = q.static_exclude;
-        p.null_runs = q.null_runs;
-        p.null_tested = q.null_tested;
-        p.max_candidates = q.max_candidates;
-        p.edge_px = q.edge_px;
-        p.gauss_model = q.null_model_gauss != 0;
-        p.seed = q.seed;
         auto r = std::make_unique<ft_b200_result>();
-        r->o = ftb::search_host(c, frames, width, height, nframes, mjd, exptime, p, wrap(progress, user));
+        r->o = ftb::search_host(c, frames, width, height, nframes, mjd, exptime, to_search_params(params),
+                                wrap(progress, user));
         *out = r.release();
     });
+}
+
+int ft_b200_search_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
+                       const double* mjd, const double* exptime, const ft_b200_search_params* params,
+                       ft_b200_result** out) {
+    if (out) *out = nullptr;
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (!d_frames || !mjd || !out) throw std::runtime_error("search: missing frames, times or result pointer");
+        if (pitch < width) throw std::runtime_error("search: row pitch below the width");
+        auto r = std::make_unique<ft_b200_result>();
+        r->o = ftb::search_host(c, d_frames, width, height, nframes, mjd, exptime, to_search_params(params), {}, true,
+                                pitch);
+        *out = r.release();
+    });
+}
+
+int ft_b200_stats(const ft_b200_ctx* ctx, long long* kernel_launches, double* pixel_adds) {
+    if (!ctx || !ctx->c) return FT_B200_ERROR;
+    if (kernel_launches) *kernel_launches = ctx->c->launches;
+    (void)pixel_adds;
+    return FT_B200_OK;
 }
 
 void ft_b200_result_free(ft_b200_result* r) { delete r; }

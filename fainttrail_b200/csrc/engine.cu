@@ -84,6 +84,7 @@ void Context::timing_reset() {
     spans_.clear();
     timings.clear();
     next_event_ = 0;
+    launches = 0;
 }
 
 int Context::span_begin(const std::string& name) {
@@ -194,6 +195,7 @@ void run_plan(Context& c, const StackPlan& plan, const float* d_frames, float* d
             const int g1 = static_cast<int>(static_cast<long long>(ng) * (q + 1) / chunks);
             stack_launch(plan, dev, d_frames, g0, g1, q == 0, q == chunks - 1, d_best, d_arg, d_max, d_bv,
                          c.err_flag(), c.stream());
+            ++c.launches;
             if (progress) {
                 c.check_kernel_error("stack kernel");
                 if (!progress(static_cast<double>(q + 1) / chunks, "stack")) throw Cancelled();

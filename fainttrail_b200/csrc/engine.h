@@ -81,6 +81,7 @@ public:
     void host_time(const std::string& name, double seconds);
     void timing_resolve();                      // after a stream sync: event spans -> seconds
     std::vector<std::pair<std::string, double>> timings;
+    long long launches = 0;  // kernels launched by the last call (reset with the timings)
 
     std::string error;
 

@@ -139,6 +139,7 @@ std::vector<Peak> device_peaks(Context& c, const float* d_max, const int* d_best
         peak_kernel<<<static_cast<unsigned>((npix + 255) / 256), 256, 0, s>>>(d_max, d_best_v, w, h, floor, radius,
                                                                              edge, d_count, d_out, cap);
         FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         int count = 0;
         FTB_CHECK(cudaMemcpyAsync(&count, d_count, sizeof(int), cudaMemcpyDeviceToHost, s));
         FTB_CHECK(cudaStreamSynchronize(s));
@@ -181,6 +182,7 @@ std::vector<char> device_artefacts(Context& c, const std::vector<Peak>& peaks, s
               static_cast<int>(std::ceil(2.0 * fwhm_px)) + 1, max_frame_fraction, d_out};
     artefact_kernel<<<static_cast<unsigned>((count + 127) / 128), 128, 0, s>>>(a);
     FTB_CHECK(cudaGetLastError());
+    ++c.launches;
     FTB_CHECK(cudaMemcpyAsync(art.data(), d_out, count, cudaMemcpyDeviceToHost, s));
     FTB_CHECK(cudaStreamSynchronize(s));
     return art;
@@ -193,7 +195,7 @@ enum SearchSlot { kRaw = 30, kSub, kFiltReal, kFiltNull, kSkyReal, kSkyNull, kMa
 }  // namespace
 
 SearchOut search_host(Context& c, const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
-                      const SearchParams& p, const Progress& progress) {
+                      const SearchParams& p, const Progress& progress, bool frames_on_device, int in_pitch) {
     (void)exptime;
     c.bind();
     if (n < 5) throw std::runtime_error("synthetic tracking needs at least 5 frames");
@@ -206,6 +208,7 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
     o.h = h;
     o.n = n;
     c.timing_reset();
+    const int total = c.span_begin("total");
     const double t_setup = wall_seconds();
     // frames in time order (the C API stable-sorts by mid-exposure, c_api.cpp:177-179)
     std::vector<int> order(static_cast<size_t>(n));
@@ -232,12 +235,15 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
     int* d_bv = c.scratch(kBestMap, sizeof(int) * static_cast<size_t>(w) * h, "best_v").as<int>();
     c.host_time("setup", wall_seconds() - t_setup);
 
-    const int up = c.span_begin("upload");
+    const int up = c.span_begin(frames_on_device ? "copy in" : "upload");
+    const size_t in_plane = frames_on_device ? static_cast<size_t>(in_pitch) * h : static_cast<size_t>(w) * h;
     for (int i = 0; i < n; ++i)
         FTB_CHECK(cudaMemcpy2DAsync(d_raw + static_cast<size_t>(i) * plane, sizeof(float) * pitch,
-                                    frames + static_cast<size_t>(order[static_cast<size_t>(i)]) * w * h,
-                                    sizeof(float) * w, sizeof(float) * w, static_cast<size_t>(h),
-                                    cudaMemcpyHostToDevice, c.stream()));
+                                    frames + static_cast<size_t>(order[static_cast<size_t>(i)]) * in_plane,
+                                    sizeof(float) * (frames_on_device ? in_pitch : w), sizeof(float) * w,
+                                    static_cast<size_t>(h),
+                                    frames_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    c.stream()));
     c.span_end(up);
     report(0.0, "background");
 
@@ -335,6 +341,7 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
     for (const Peak& pk : o.peaks)
         if (pk.snr >= o.thr.snr && pk.vidx >= 0) o.selected.push_back(pk);
     if (static_cast<int>(o.selected.size()) > p.max_candidates) o.selected.resize(static_cast<size_t>(p.max_candidates));
+    c.span_end(total);
     FTB_CHECK(cudaStreamSynchronize(c.stream()));
     c.timing_resolve();
     report(1.0, "done");

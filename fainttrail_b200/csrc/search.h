@@ -84,7 +84,10 @@ struct SearchOut {
     double adds = 0;                     // pixel x frame x motion additions of all passes
 };
 
+// frames: host (n x h x w) or, with frames_on_device, device rows of in_pitch
+// floats (left untouched; copied in time order).
 SearchOut search_host(Context& c, const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
-                      const SearchParams& p, const Progress& progress);
+                      const SearchParams& p, const Progress& progress, bool frames_on_device = false,
+                      int in_pitch = 0);
 
 }  // namespace ftb

@@ -555,6 +555,7 @@ void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h,
         FTB_CHECK(cudaFuncSetAttribute(sky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         sky_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
         FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         c.span_end(span);
     }
     // 2. per-frame noise from the residual samples (border 2)
@@ -568,9 +569,11 @@ void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h,
                 sc.residual.as<float>(), plane, w, h, pitch, n, 2, st, gw, gh, nullptr, sc.samples.as<float>(), sc.cap,
                 tb.counts);
             FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         }
         robust_sigma_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, tb.counts, tb.sigma, 1);
         FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         c.span_end(span);
     }
 }
@@ -609,10 +612,12 @@ void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const Stage
         FTB_CHECK(cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         scatter_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
         FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         const int dil = std::max(1, static_cast<int>(std::lround(0.5 * sp.fwhm_px)));
         mask_kernel<<<static_cast<unsigned>((npix + 255) / 256), 256, 0, s>>>(sc.scatter.as<float>(), d_mask, w, h,
                                                                               pitch, dil, sp.mask_scatter);
         FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         c.span_end(span);
     }
     // 4. normalise, cosmic rays, clip, matched filter
@@ -640,6 +645,7 @@ void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const Stage
         FTB_CHECK(cudaFuncSetAttribute(filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         filter_kernel<<<dim3((w + kFTW - 1) / kFTW, (h + kFTH - 1) / kFTH, n), 256, smem, s>>>(a);
         FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         c.span_end(span);
     }
     // 5. robust sigma of the masked filter output (border ceil(3 s) + 1), rescale
@@ -655,12 +661,15 @@ void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const Stage
             sample_kernel<<<dim3(static_cast<unsigned>((g + 255) / 256), n), 256, 0, s>>>(
                 d_filtered, plane, w, h, pitch, n, fb, st, gw, gh, d_mask, sc.samples.as<float>(), sc.cap, d_counts);
             FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         }
         robust_sigma_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, d_counts, d_sg, 0);
         FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         rescale_kernel<<<dim3(static_cast<unsigned>((npix + 255) / 256), n), 256, 0, s>>>(d_filtered, plane, w, h, pitch,
                                                                                        d_sg);
         FTB_CHECK(cudaGetLastError());
+        ++c.launches;
         c.span_end(span);
     }
     if (h_sigma) FTB_CHECK(cudaMemcpyAsync(h_sigma, d_sigma, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
@@ -693,14 +702,18 @@ void prepare_sub(Context& c, StageScratch& sc, float* d_raw, float* d_sub, int w
         sample_kernel<<<dim3(static_cast<unsigned>((g + 255) / 256), n), 256, 0, s>>>(
             d_raw, plane, w, h, pitch, n, 0, st, gw, gh, nullptr, sc.samples.as<float>(), sc.cap, tb.counts);
         FTB_CHECK(cudaGetLastError());
+        ++c.launches;
     }
     median_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, tb.counts, tb.sg);
     FTB_CHECK(cudaGetLastError());
+        ++c.launches;
     const dim3 grid(static_cast<unsigned>((npix + 255) / 256), n);
     subtract_kernel<<<grid, 256, 0, s>>>(d_raw, plane, w, h, pitch, tb.sg);
     FTB_CHECK(cudaGetLastError());
+        ++c.launches;
     grow_kernel<<<grid, 256, 0, s>>>(d_raw, d_sub, plane, w, h, pitch, 3);
     FTB_CHECK(cudaGetLastError());
+        ++c.launches;
     c.span_end(span);
     if (h_bg) FTB_CHECK(cudaMemcpyAsync(h_bg, tb.sg, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
 }

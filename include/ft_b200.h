@@ -131,6 +131,12 @@ typedef struct ft_b200_result ft_b200_result;
 int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
                    const double* exptime, const ft_b200_search_params* params, ft_b200_progress_fn progress,
                    void* user, ft_b200_result** out);
+/* The same over frames already in device memory: d_frames holds nframes x height
+ * rows of `pitch` floats (pitch >= width), is read only, and is copied in time
+ * order. Synchronous; no progress callback. */
+int ft_b200_search_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
+                       const double* mjd, const double* exptime, const ft_b200_search_params* params,
+                       ft_b200_result** out);
 void ft_b200_result_free(ft_b200_result* r);
 /* threshold_snr and the tail model (SearchResult, search.hpp:163-172); method
  * receives "fixed", "null-fit gauss", "null-fit linear", "null-quantile" or
@@ -150,6 +156,10 @@ int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap);
 int ft_b200_result_maps(const ft_b200_result* r, float* max_snr, int* best_v);
 /* The trial motion vidx of the grid (velocity_grid, search.cpp:39-58), px/hour. */
 int ft_b200_result_velocity(const ft_b200_result* r, int vidx, double* vx_pxh, double* vy_pxh);
+
+/* Kernels launched by the last call on the context (its stacking passes, stage,
+ * peak and screening kernels). pixel_adds is reserved (left unchanged). */
+int ft_b200_stats(const ft_b200_ctx* ctx, long long* kernel_launches, double* pixel_adds);
 
 /* Stage timings of the last call on the context, measured with CUDA events on the
  * context's stream (the reference's StackResult::timings, backend.hpp:99-105, and
