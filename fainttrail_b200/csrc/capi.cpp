@@ -63,6 +63,10 @@ double max_abs(const double* t, int n) {
 
 }  // namespace
 
+namespace ftb {
+void set_thread_error(const std::string& msg) { g_open_error = msg; }
+}  // namespace ftb
+
 extern "C" {
 
 const char* ft_b200_version(void) { return "0.9.1-b200.1"; }
