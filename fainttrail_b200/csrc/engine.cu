@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstdlib>
 
@@ -169,7 +170,7 @@ DevBuf& Context::scratch(int slot, size_t bytes, const char* what) {
 
 // ------------------------------------------------------------------ stacking
 
-enum Slot { kFrames = 0, kBest, kArg, kMax, kBestV, kStageOut, kSky, kMask };
+enum Slot { kFrames = 0, kBest, kArg, kMax, kBestV, kStageOut, kSky, kMask, kDesc };
 
 namespace {
 
@@ -193,8 +194,20 @@ void run_plan(Context& c, const StackPlan& plan, const float* d_frames, float* d
         for (int q = 0; q < chunks; ++q) {
             const int g0 = static_cast<int>(static_cast<long long>(ng) * q / chunks);
             const int g1 = static_cast<int>(static_cast<long long>(ng) * (q + 1) / chunks);
-            stack_launch(plan, dev, d_frames, g0, g1, q == 0, q == chunks - 1, d_best, d_arg, d_max, d_bv,
-                         c.err_flag(), c.stream());
+            BatchPass bp;
+            bp.plan = &plan;
+            bp.dev = &dev;
+            bp.frames = d_frames;
+            bp.g0 = g0;
+            bp.g1 = g1;
+            bp.first = q == 0;
+            bp.last = q == chunks - 1;
+            bp.best = d_best;
+            bp.arg = d_arg;
+            bp.max_snr = d_max;
+            bp.best_v = d_bv;
+            DevBuf& desc = c.scratch(kDesc, batch_desc_bytes(1), "stack descriptors");
+            stack_launch_batch({bp}, desc.as<unsigned char>(), desc.bytes(), c.err_flag(), c.sms(), c.stream());
             ++c.launches;
             if (progress) {
                 c.check_kernel_error("stack kernel");
@@ -286,6 +299,72 @@ void stage_host(Context& c, const float* sub, int w, int h, int n, const double*
     c.timing_resolve();
     if (sigma) std::copy(sg.begin(), sg.end(), sigma);
     if (cr) std::copy(crv.begin(), crv.end(), cr);
+}
+
+// ------------------------------------------------------------------ batched passes
+
+void stack_passes_device(Context& c, std::vector<PassJob>& jobs) {
+    if (jobs.empty()) return;
+    const double t0 = wall_seconds();
+    // plans on host threads (the GPU keeps running whatever was queued before)
+    std::vector<StackPlan> plans(jobs.size());
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t workers = std::min<size_t>(hw, jobs.size());
+    std::vector<std::thread> pool;
+    std::vector<std::exception_ptr> errs(workers);
+    for (size_t wkr = 0; wkr < workers; ++wkr)
+        pool.emplace_back([&, wkr] {
+            try {
+                for (size_t k = wkr; k < jobs.size(); k += workers) {
+                    const PassJob& j = jobs[k];
+                    const StackConfig cfg = choose_stack_config(j.w, j.h, j.n, c.smem_optin());
+                    plans[k] = make_stack_plan(j.w, j.h, j.n, j.dx.data(), j.dy.data(), j.m, j.min_count,
+                                               motion_order(j.dx.data(), j.dy.data(), j.m, j.n, 4.0, 4.0), cfg);
+                    plans[k].pitch = j.pitch;
+                }
+            } catch (...) {
+                errs[wkr] = std::current_exception();
+            }
+        });
+    for (auto& t : pool) t.join();
+    for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
+    c.host_time("setup", wall_seconds() - t0);
+    std::vector<StackPlanDev> devs(jobs.size());
+    try {
+        for (size_t k = 0; k < jobs.size(); ++k) devs[k].upload(plans[k], c.stream());
+        // one persistent launch per kernel shape
+        std::vector<std::pair<int, int>> shapes;
+        for (const auto& p : plans)
+            if (std::find(shapes.begin(), shapes.end(), std::make_pair(p.cfg.ty, p.cfg.p)) == shapes.end())
+                shapes.emplace_back(p.cfg.ty, p.cfg.p);
+        const int span = c.span_begin("kernel");
+        for (const auto& sh : shapes) {
+            std::vector<BatchPass> batch;
+            for (size_t k = 0; k < jobs.size(); ++k) {
+                if (plans[k].cfg.ty != sh.first || plans[k].cfg.p != sh.second) continue;
+                BatchPass bp;
+                bp.plan = &plans[k];
+                bp.dev = &devs[k];
+                bp.frames = jobs[k].d_frames;
+                bp.g0 = 0;
+                bp.g1 = static_cast<int>(plans[k].groups.size());
+                bp.max_snr = jobs[k].d_max;
+                bp.best_v = jobs[k].d_bv;
+                batch.push_back(bp);
+            }
+            DevBuf& desc = c.scratch(kDesc, batch_desc_bytes(static_cast<int>(batch.size())), "stack descriptors");
+            stack_launch_batch(batch, desc.as<unsigned char>(), desc.bytes(), c.err_flag(), c.sms(), c.stream());
+            ++c.launches;
+        }
+        c.span_end(span);
+        c.check_kernel_error("stack kernel");
+    } catch (...) {
+        cudaStreamSynchronize(c.stream());
+        for (auto& d : devs) d.release();
+        throw;
+    }
+    for (auto& d : devs) d.release();
 }
 
 }  // namespace ftb

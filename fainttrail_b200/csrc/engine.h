@@ -120,6 +120,21 @@ void stack_pass_device(Context& c, const float* d_frames, int pitch, int w, int 
                        const int* dy, int m, int min_count, const double* vel, double tmax, float* d_max_snr,
                        int* d_best_v, const Progress& progress);
 
+// One stacking pass of a batch: device frames (n x h x pitch), a motion-major
+// shift table, device outputs (h x w).
+struct PassJob {
+    const float* d_frames = nullptr;
+    int pitch = 0, w = 0, h = 0, n = 0;
+    std::vector<int> dx, dy;
+    int m = 0, min_count = 3;
+    float* d_max = nullptr;
+    int* d_bv = nullptr;
+};
+
+// Several passes, possibly of different shapes: plans built on host threads,
+// then one persistent launch per kernel shape; returns when all are complete.
+void stack_passes_device(Context& c, std::vector<PassJob>& jobs);
+
 struct StageParams;
 
 // build_stage over host buffers (the C ABI's ft_b200_stage).

@@ -95,11 +95,29 @@ struct StackPlanDev {
     cudaStream_t stream_ = nullptr;
 };
 
-// Run a planned pass over device frames (n x h x pitch); writes max_snr / best_v
-// (h x w, dense). best/arg scratch carry the running maxima between launches
-// when the pass is split into group ranges [g0, g1).
-void stack_launch(const StackPlan& plan, const StackPlanDev& dev, const float* d_frames, int g0, int g1, bool first,
-                  bool last, float* d_best, int* d_arg, float* d_max_snr, int* d_best_v, int* d_err,
-                  cudaStream_t s);
+// One planned pass of a batch over device frames (n x h x pitch), writing
+// max_snr / best_v (h x w, dense). best/arg carry the running maxima between
+// launches when a pass is split into group ranges [g0, g1).
+struct BatchPass {
+    const StackPlan* plan = nullptr;
+    const StackPlanDev* dev = nullptr;
+    const float* frames = nullptr;
+    int g0 = 0, g1 = 0;
+    bool first = true, last = true;
+    float* best = nullptr;
+    int* arg = nullptr;
+    float* max_snr = nullptr;
+    int* best_v = nullptr;
+};
+
+// Device bytes of the descriptors of a batch (a work-queue counter, one tensor
+// map and one argument block per pass).
+size_t batch_desc_bytes(int npasses);
+
+// All passes of a batch in one persistent launch (one CTA per SM taking
+// (pass, tile) items from a queue). The passes must share a kernel shape
+// (cfg.ty, cfg.p). d_desc: device buffer of at least batch_desc_bytes bytes.
+void stack_launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, size_t desc_bytes, int* d_err,
+                        int sms, cudaStream_t s);
 
 }  // namespace ftb

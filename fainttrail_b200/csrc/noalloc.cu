@@ -32,6 +32,7 @@ struct DeviceScratch {
     unsigned char* tables = nullptr;  // device address of g_plan_scratch on this device
     int* err = nullptr;               // device address of g_wait_error
     int smem_optin = 0;
+    int sms = 0;
 };
 
 std::mutex g_mu;
@@ -49,6 +50,7 @@ DeviceScratch& device_scratch() {
         FTB_CHECK(cudaGetSymbolAddress(reinterpret_cast<void**>(&d.tables), g_plan_scratch));
         FTB_CHECK(cudaGetSymbolAddress(reinterpret_cast<void**>(&d.err), g_wait_error));
         FTB_CHECK(cudaDeviceGetAttribute(&d.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        FTB_CHECK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
         d.ready = true;
     }
     return d;
@@ -95,6 +97,8 @@ extern "C" int ft_b200_stack_dev_noalloc(const float* d_frames, int width, int h
             p.off = used;
             used += align256(p.bytes);
         }
+        const size_t desc_off = used;  // the launch descriptors follow the tables
+        used += align256(batch_desc_bytes(1));
         if (used > kScratchBytes)
             throw std::runtime_error("stack pass: its plan tables need " + std::to_string((used + 1048575) >> 20) +
                                      " MiB; the allocation-free entry point holds at most " +
@@ -112,8 +116,15 @@ extern "C" int ft_b200_stack_dev_noalloc(const float* d_frames, int width, int h
         view.slot_shift = reinterpret_cast<short2*>(d.tables + parts[5].off);
         view.inv_sqrt = reinterpret_cast<float*>(d.tables + parts[6].off);
         view.ngroups = static_cast<int>(plan.groups.size());
-        stack_launch(plan, view, d_frames, 0, view.ngroups, true, true, nullptr, nullptr, d_max_snr, d_best_v, d.err,
-                     s);
+        BatchPass bp;
+        bp.plan = &plan;
+        bp.dev = &view;
+        bp.frames = d_frames;
+        bp.g0 = 0;
+        bp.g1 = view.ngroups;
+        bp.max_snr = d_max_snr;
+        bp.best_v = d_best_v;
+        stack_launch_batch({bp}, d.tables + desc_off, kScratchBytes - desc_off, d.err, d.sms, s);
         int err = 0;
         FTB_CHECK(cudaMemcpyAsync(&err, d.err, sizeof(int), cudaMemcpyDeviceToHost, s));
         FTB_CHECK(cudaStreamSynchronize(s));

@@ -284,22 +284,86 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
     const int nms = std::max(2, static_cast<int>(std::lround(o.fwhm_px)));
     const int edge = std::max(p.edge_px, 1);
     const int min_count = pass_min_count(p.min_coverage, n);
-    std::vector<int> dx, dy;
-    auto pass_progress = [&](double f0, double f1, const char* stage) -> Progress {
-        if (!progress) return {};
-        return [&, f0, f1, stage](double f, const char*) { return progress(f0 + (f1 - f0) * f, stage); };
-    };
 
-    shift_table(o.t_h, o.grid, dx, dy);
-    stack_pass_device(c, d_filt, pitch, w, h, n, dx.data(), dy.data(), static_cast<int>(m), min_count, nullptr, 0.0,
-                      d_max, d_bv, pass_progress(0.1, 0.1 + 0.9 * share, "search"));
-    o.adds += static_cast<double>(m) * n * w * h;
+    // the real pass and the null runs (preprocessing rebuilt with permuted times
+    // on the same sub frames) as batches of passes, each batch stacked in one
+    // persistent launch; a batch holds as many null runs as the HBM budget allows
+    const std::vector<std::vector<double>> orders = null_time_orders(o.t_h, runs, p.seed);
+    const size_t map_bytes = sizeof(float) * static_cast<size_t>(w) * h;
+    const size_t per_null = sizeof(float) * (plane * n + 2 * plane) + 2 * map_bytes;
+    const size_t reserve = size_t{256} << 20;  // plans, peaks, descriptors
+    const size_t avail = c.budget() > c.used() + reserve ? c.budget() - c.used() - reserve : 0;
+    const int per_batch = static_cast<int>(std::max<size_t>(1, std::min<size_t>(std::max(runs, 1), avail / per_null)));
+    std::vector<float> pooled;
     const float floor = static_cast<float>(auto_thr ? p.min_snr_floor : p.threshold_snr);
-    {
-        const int sp_ = c.span_begin("peaks");
-        o.peaks = device_peaks(c, d_max, d_bv, w, h, floor, nms, edge);
-        order_peaks(o.peaks, 100000);
-        c.span_end(sp_);
+    bool real_done = false;
+    for (int k0 = 0; k0 < std::max(runs, 1); k0 += per_batch) {
+        const int k1 = std::min(runs, k0 + per_batch);
+        struct NullBufs {
+            DevBuf filt, sky, mask, max, bv;
+        };
+        std::vector<NullBufs> nb(static_cast<size_t>(std::max(0, k1 - k0)));
+        std::vector<PassJob> jobs;
+        if (!real_done) {
+            PassJob j;
+            j.d_frames = d_filt;
+            j.pitch = pitch;
+            j.w = w;
+            j.h = h;
+            j.n = n;
+            shift_table(o.t_h, o.grid, j.dx, j.dy);
+            j.m = static_cast<int>(m);
+            j.min_count = min_count;
+            j.d_max = d_max;
+            j.d_bv = d_bv;
+            jobs.push_back(std::move(j));
+        }
+        for (int k = k0; k < k1; ++k) {
+            NullBufs& b = nb[static_cast<size_t>(k - k0)];
+            b.filt = DevBuf(&c, sizeof(float) * plane * n, "null filtered frames");
+            b.sky = DevBuf(&c, sizeof(float) * plane, "null static sky");
+            b.mask = DevBuf(&c, sizeof(float) * plane, "null mask");
+            b.max = DevBuf(&c, map_bytes, "null max_snr");
+            b.bv = DevBuf(&c, map_bytes, "null best_v");
+            report(0.1 + 0.9 * share * (k + 1), "null");
+            stage_run(c, sc, d_sub, w, h, n, orders[static_cast<size_t>(k)].data(), sp, b.filt.as<float>(),
+                      b.sky.as<float>(), b.mask.as<float>(), nullptr, nullptr);
+            PassJob j;
+            j.d_frames = b.filt.as<float>();
+            j.pitch = pitch;
+            j.w = w;
+            j.h = h;
+            j.n = n;
+            shift_table(orders[static_cast<size_t>(k)], o.grid, j.dx, j.dy);
+            j.m = static_cast<int>(m);
+            j.min_count = min_count;
+            j.d_max = b.max.as<float>();
+            j.d_bv = b.bv.as<int>();
+            jobs.push_back(std::move(j));
+        }
+        stack_passes_device(c, jobs);
+        o.adds += static_cast<double>(m) * n * w * h * static_cast<double>(jobs.size());
+        report(0.1 + 0.9 * share * (k1 + 1), "null");
+        const int pk_span = c.span_begin("peaks");
+        if (!real_done) {
+            o.peaks = device_peaks(c, d_max, d_bv, w, h, floor, nms, edge);
+            order_peaks(o.peaks, 100000);
+            real_done = true;
+        }
+        for (int k = k0; k < k1; ++k) {
+            NullBufs& b = nb[static_cast<size_t>(k - k0)];
+            std::vector<Peak> npk = device_peaks(c, b.max.as<float>(), b.bv.as<int>(), w, h, 3.0f, nms, edge);
+            order_peaks(npk, 20000);
+            const size_t tested = (p.gauss_model && p.null_tested > 0)
+                                      ? std::min(npk.size(), static_cast<size_t>(p.null_tested))
+                                      : 0;
+            const std::vector<char> art =
+                device_artefacts(c, npk, tested, o.grid, b.filt.as<float>(), d_sub, b.sky.as<float>(),
+                                 orders[static_cast<size_t>(k)], w, h, n, o.fwhm_px, p.max_frame_fraction);
+            for (size_t q = 0; q < npk.size(); ++q)
+                if (q >= art.size() || !art[q]) pooled.push_back(npk[q].snr);
+        }
+        c.span_end(pk_span);
     }
     o.max_snr.resize(static_cast<size_t>(w) * h);
     o.best_v.resize(static_cast<size_t>(w) * h);
@@ -307,35 +371,6 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
                               c.stream()));
     FTB_CHECK(cudaMemcpyAsync(o.best_v.data(), d_bv, sizeof(int) * o.best_v.size(), cudaMemcpyDeviceToHost,
                               c.stream()));
-
-    // null runs: the stage again with permuted times on the same sub frames
-    std::vector<float> pooled;
-    if (runs > 0) {
-        float* d_fn = c.scratch(kFiltNull, sizeof(float) * plane * n, "null filtered frames").as<float>();
-        float* d_skn = c.scratch(kSkyNull, sizeof(float) * plane, "null static sky").as<float>();
-        float* d_mkn = c.scratch(kMaskNull, sizeof(float) * plane, "null mask").as<float>();
-        const auto orders = null_time_orders(o.t_h, runs, p.seed);
-        for (int k = 0; k < runs; ++k) {
-            const std::vector<double>& t = orders[static_cast<size_t>(k)];
-            report(0.1 + 0.9 * share * (k + 1), "null");
-            stage_run(c, sc, d_sub, w, h, n, t.data(), sp, d_fn, d_skn, d_mkn, nullptr, nullptr);
-            shift_table(t, o.grid, dx, dy);
-            stack_pass_device(c, d_fn, pitch, w, h, n, dx.data(), dy.data(), static_cast<int>(m), min_count, nullptr,
-                              0.0, d_max, d_bv, pass_progress(0.1 + 0.9 * share * (k + 1), 0.1 + 0.9 * share * (k + 2), "null"));
-            o.adds += static_cast<double>(m) * n * w * h;
-            const int sp_ = c.span_begin("peaks");
-            std::vector<Peak> npk = device_peaks(c, d_max, d_bv, w, h, 3.0f, nms, edge);
-            order_peaks(npk, 20000);
-            const size_t tested = (p.gauss_model && p.null_tested > 0)
-                                      ? std::min(npk.size(), static_cast<size_t>(p.null_tested))
-                                      : 0;
-            const std::vector<char> art = device_artefacts(c, npk, tested, o.grid, d_fn, d_sub, d_skn, t, w, h, n,
-                                                           o.fwhm_px, p.max_frame_fraction);
-            for (size_t q = 0; q < npk.size(); ++q)
-                if (q >= art.size() || !art[q]) pooled.push_back(npk[q].snr);
-            c.span_end(sp_);
-        }
-    }
     o.thr = set_threshold(p, pooled, runs, o.fwhm_px, w, h, m);
     if (runs > 0 && auto_thr) o.null_peaks.assign(pooled.begin(), pooled.end());
     for (const Peak& pk : o.peaks)

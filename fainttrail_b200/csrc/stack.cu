@@ -104,6 +104,9 @@ StackConfig choose_stack_config(int w, int h, int n, int smem_optin) {
     auto need = [&](int p) { return static_cast<long long>(n) * roundup(p + 4, c.bh) * c.wp * 4; };
     const long long cap = static_cast<long long>(c.smem_bytes) * 7 / 10;
     c.p = need(16) <= cap ? 16 : need(8) <= cap ? 8 : 4;
+    // 16-row tiles hold 64 accumulators per thread: 12 warps fit the register
+    // file; shorter tiles run 16 warps for latency hiding
+    if (c.p < 16) c.ty = 16;
     return c;
 }
 
@@ -327,6 +330,8 @@ namespace {
 struct StackArgs {
     int w, h, n, min_count;
     int g0, g1, first, last;
+    int tiles_x, tiles_y;  // tile grid of this pass
+    long long item0;       // its first work item in the batch
     const StackGroup* groups;
     const StackWin* wins;
     const int* slot_motion;
@@ -432,8 +437,23 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
     for (int k = 0; k < M; ++k)
 #pragma unroll
         for (int w = 0; w < PW; ++w) cpart[k][w] = 0;
+#ifndef FTB_STACK_PIPE
+#define FTB_STACK_PIPE 1
+#endif
+    // the next frame's four offsets are loaded one frame ahead, so the reuse
+    // tests below do not wait on a shared-memory load
+    const uint16_t* op = offs + s0;
+    uint2 qn = *reinterpret_cast<const uint2*>(op);
+#if FTB_STACK_PIPE == 2
+#pragma unroll 2
+#endif
     for (int i = 0; i < a.n; ++i) {
+#if FTB_STACK_PIPE >= 1
+        const uint2 q = qn;
+        if (i + 1 < a.n) qn = *reinterpret_cast<const uint2*>(op + (i + 1) * G.nslots);
+#else
         const uint2 q = *reinterpret_cast<const uint2*>(offs + i * G.nslots + s0);
+#endif
         const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
         float v[P];
         load_column<P, WP>(v, win + o0 + tb);
@@ -482,20 +502,14 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
     }
 }
 
-// One CTA = one 32 x P output tile, one CTA per SM; its NW warps share the tile
-// and split each group's 4-motion blocks; per-warp maxima merge through shared
-// memory at the end.
+// One 32 x P output tile of one pass: the CTA's NW warps share the tile and
+// split each group's 4-motion blocks; per-warp maxima merge through shared memory
+// at the end. Returns false if a staging wait timed out.
 template <int NW, int P, int WP, int BH>
-__global__ void __launch_bounds__(32 * NW, 1) stack_kernel(const __grid_constant__ CUtensorMap tmap, const StackArgs a) {
+__device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, int y0, uint64_t* bar, float* win,
+                           int* err, uint32_t& phase) {
     constexpr int M = 4;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    // 128-byte aligned base (TMA destinations), the barrier in its first 8 bytes
-    unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(base);
-    float* win = reinterpret_cast<float*>(base + 128);
-
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * P;
     const int x = x0 + lane;
     const int tb = lane;  // thread's first window element relative to a motion's offset
 
@@ -508,10 +522,6 @@ __global__ void __launch_bounds__(32 * NW, 1) stack_kernel(const __grid_constant
     }
     const bool full = x0 + 31 < a.w && y0 + P - 1 < a.h;
     const float inv_n = a.inv_sqrt[a.n];
-    if (tid == 0) mbar_init(bar, 1);
-    __syncthreads();
-
-    uint32_t phase = 0;
     for (int g = a.g0; g < a.g1; ++g) {
         const StackGroup G = a.groups[g];
         uint16_t* offs = reinterpret_cast<uint16_t*>(win + G.rows_total * WP);
@@ -524,7 +534,7 @@ __global__ void __launch_bounds__(32 * NW, 1) stack_kernel(const __grid_constant
             for (int i = 0; i < a.n; ++i) {
                 const StackWin wv = a.wins[G.win0 + i];
                 for (int b = 0; b < wv.rows; b += BH)
-                    tma_load_3d(win + (wv.row0 + b) * WP, &tmap, x0 + wv.dx0, y0 + wv.dy0 + b, i, bar);
+                    tma_load_3d(win + (wv.row0 + b) * WP, tmap, x0 + wv.dx0, y0 + wv.dy0 + b, i, bar);
             }
         }
         {
@@ -534,8 +544,8 @@ __global__ void __launch_bounds__(32 * NW, 1) stack_kernel(const __grid_constant
             for (int q = tid; q < nvec; q += blockDim.x) dst[q] = src[q];
         }
         __syncthreads();
-        const bool ok = mbar_wait_bounded(bar, phase, a.err);
-        if (__syncthreads_or(!ok)) return;  // staging did not complete: the host reports the error
+        const bool ok = mbar_wait_bounded(bar, phase, err);
+        if (__syncthreads_or(!ok)) return false;  // staging did not complete: the host reports the error
         phase ^= 1u;
         const bool interior = full && x0 + G.gdxmin >= 0 && x0 + 31 + G.gdxmax < a.w && y0 + G.gdymin >= 0 &&
                               y0 + P - 1 + G.gdymax < a.h;
@@ -584,6 +594,39 @@ __global__ void __launch_bounds__(32 * NW, 1) stack_kernel(const __grid_constant
             a.arg[o] = ar;
         }
     }
+    __syncthreads();  // the merge area is reused by the next tile's windows
+    return true;
+}
+
+// Persistent: one CTA per SM takes (pass, tile) work items from a queue until the
+// batch is done, so passes of different shapes and sizes share one launch and
+// the SMs stay busy to the end.
+template <int NW, int P, int WP, int BH>
+__global__ void __launch_bounds__(32 * NW, 1)
+    stack_batch_kernel(const StackArgs* __restrict__ passes, const CUtensorMap* __restrict__ maps, int npasses,
+                       long long items, int* queue, int* err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // 128-byte aligned base (TMA destinations), the barrier in its first 8 bytes
+    unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(base);
+    long long* next = reinterpret_cast<long long*>(base + 8);
+    float* win = reinterpret_cast<float*>(base + 128);
+    if (threadIdx.x == 0) mbar_init(bar, 1);
+    __syncthreads();
+    uint32_t phase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) *next = atomicAdd(reinterpret_cast<unsigned long long*>(queue), 1ull);
+        __syncthreads();
+        const long long item = *next;
+        __syncthreads();
+        if (item >= items) break;
+        int p = 0;
+        while (p + 1 < npasses && passes[p + 1].item0 <= item) ++p;
+        const StackArgs& a = passes[p];
+        const long long t = item - a.item0;
+        const int tx = static_cast<int>(t % a.tiles_x), ty = static_cast<int>(t / a.tiles_x);
+        if (!stack_tile<NW, P, WP, BH>(a, maps + p, tx * 32, ty * P, bar, win, err, phase)) return;
+    }
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -601,67 +644,88 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 template <int NW, int P, int WP, int BH>
-void launch_variant(const StackPlan& plan, const StackPlanDev& dev, const float* d_frames, int g0, int g1, bool first,
-                    bool last, float* d_best, int* d_arg, float* d_max_snr, int* d_best_v, int* d_err,
-                    cudaStream_t s) {
-    CUtensorMap map;
-    const cuuint64_t dims[3] = {static_cast<cuuint64_t>(plan.w), static_cast<cuuint64_t>(plan.h),
-                                static_cast<cuuint64_t>(plan.n)};
-    const cuuint64_t strides[2] = {static_cast<cuuint64_t>(plan.pitch) * 4,
-                                   static_cast<cuuint64_t>(plan.pitch) * plan.h * 4};
-    const cuuint32_t box[3] = {WP, BH, 1};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(d_frames), dims, strides,
-                                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed (" + std::to_string(static_cast<int>(r)) + ")");
-    StackArgs a;
-    a.w = plan.w;
-    a.h = plan.h;
-    a.n = plan.n;
-    a.min_count = plan.min_count;
-    a.g0 = g0;
-    a.g1 = g1;
-    a.first = first;
-    a.last = last;
-    a.groups = dev.groups;
-    a.wins = dev.wins;
-    a.slot_motion = dev.slot_motion;
-    a.slot_off = dev.slot_off;
-    a.slot_off_base = dev.slot_off_base;
-    a.slot_shift = dev.slot_shift;
-    a.inv_sqrt = dev.inv_sqrt;
-    a.best = d_best;
-    a.arg = d_arg;
-    a.max_snr = d_max_snr;
-    a.best_v = d_best_v;
-    a.err = d_err;
-    const size_t merge = static_cast<size_t>(NW) * 32 * P * 8;
-    const size_t smem = 256 + std::max(merge, static_cast<size_t>(plan.max_group_bytes));
-    if (smem > static_cast<size_t>(plan.cfg.smem_bytes) + 256) throw std::runtime_error("stack plan exceeds shared memory");
-    auto kern = stack_kernel<NW, P, WP, BH>;
+void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, size_t desc_bytes, int* d_err,
+                  int sms, cudaStream_t s) {
+    const size_t np = batch.size();
+    std::vector<unsigned char> host(batch_desc_bytes(static_cast<int>(np)), 0);
+    if (host.size() > desc_bytes) throw std::runtime_error("stack batch: descriptor buffer too small");
+    CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(host.data() + 128);
+    StackArgs* args = reinterpret_cast<StackArgs*>(host.data() + 128 + 128 * np);
+    long long items = 0;
+    size_t smem = 256 + static_cast<size_t>(NW) * 32 * P * 8;
+    for (size_t k = 0; k < np; ++k) {
+        const BatchPass& bp = batch[k];
+        const StackPlan& plan = *bp.plan;
+        if (plan.cfg.ty != NW || plan.cfg.p != P) throw std::runtime_error("stack batch: passes of different kernel shapes");
+        const cuuint64_t dims[3] = {static_cast<cuuint64_t>(plan.w), static_cast<cuuint64_t>(plan.h),
+                                    static_cast<cuuint64_t>(plan.n)};
+        const cuuint64_t strides[2] = {static_cast<cuuint64_t>(plan.pitch) * 4,
+                                       static_cast<cuuint64_t>(plan.pitch) * plan.h * 4};
+        const cuuint32_t box[3] = {WP, BH, 1};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        const CUresult r = encode_fn()(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(bp.frames), dims,
+                                       strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                       CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS)
+            throw CudaError("cuTensorMapEncodeTiled failed (" + std::to_string(static_cast<int>(r)) + ")");
+        StackArgs& a = args[k];
+        a.w = plan.w;
+        a.h = plan.h;
+        a.n = plan.n;
+        a.min_count = plan.min_count;
+        a.g0 = bp.g0;
+        a.g1 = bp.g1;
+        a.first = bp.first;
+        a.last = bp.last;
+        a.tiles_x = (plan.w + 31) / 32;
+        a.tiles_y = (plan.h + P - 1) / P;
+        a.item0 = items;
+        items += static_cast<long long>(a.tiles_x) * a.tiles_y;
+        const StackPlanDev& dev = *bp.dev;
+        a.groups = dev.groups;
+        a.wins = dev.wins;
+        a.slot_motion = dev.slot_motion;
+        a.slot_off = dev.slot_off;
+        a.slot_off_base = dev.slot_off_base;
+        a.slot_shift = dev.slot_shift;
+        a.inv_sqrt = dev.inv_sqrt;
+        a.best = bp.best;
+        a.arg = bp.arg;
+        a.max_snr = bp.max_snr;
+        a.best_v = bp.best_v;
+        a.err = d_err;
+        smem = std::max(smem, 256 + static_cast<size_t>(plan.max_group_bytes));
+        if (smem > static_cast<size_t>(plan.cfg.smem_bytes) + 256)
+            throw std::runtime_error("stack plan exceeds shared memory");
+    }
+    if (items == 0) return;
+    FTB_CHECK(cudaMemcpyAsync(d_desc, host.data(), host.size(), cudaMemcpyHostToDevice, s));
+    auto kern = stack_batch_kernel<NW, P, WP, BH>;
     FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    const dim3 grid((plan.w + 31) / 32, (plan.h + P - 1) / P);
-    kern<<<grid, 32 * NW, smem, s>>>(map, a);
+    const int ctas = static_cast<int>(std::min<long long>(items, sms));
+    kern<<<ctas, 32 * NW, smem, s>>>(reinterpret_cast<const StackArgs*>(d_desc + 128 + 128 * np),
+                                     reinterpret_cast<const CUtensorMap*>(d_desc + 128), static_cast<int>(np), items,
+                                     reinterpret_cast<int*>(d_desc), d_err);
     FTB_CHECK(cudaGetLastError());
 }
 
 }  // namespace
 
-void stack_launch(const StackPlan& plan, const StackPlanDev& dev, const float* d_frames, int g0, int g1, bool first,
-                  bool last, float* d_best, int* d_arg, float* d_max_snr, int* d_best_v, int* d_err,
-                  cudaStream_t s) {
-    const StackConfig& c = plan.cfg;
-    if (c.wp != 40 || c.bh != 4 || c.mblock != 4 || c.ty != 12) throw std::runtime_error("stack: unsupported kernel configuration");
-    if (c.p == 16)
-        launch_variant<12, 16, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
-                                      d_err, s);
-    else if (c.p == 8)
-        launch_variant<12, 8, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
-                                     d_err, s);
-    else if (c.p == 4)
-        launch_variant<12, 4, 40, 4>(plan, dev, d_frames, g0, g1, first, last, d_best, d_arg, d_max_snr, d_best_v,
-                                     d_err, s);
+size_t batch_desc_bytes(int npasses) {
+    return 128 + 128 * static_cast<size_t>(npasses) + sizeof(StackArgs) * static_cast<size_t>(npasses);
+}
+
+void stack_launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, size_t desc_bytes, int* d_err,
+                        int sms, cudaStream_t s) {
+    if (batch.empty()) return;
+    const StackConfig& c = batch[0].plan->cfg;
+    if (c.wp != 40 || c.bh != 4 || c.mblock != 4) throw std::runtime_error("stack: unsupported kernel configuration");
+    if (c.ty == 12 && c.p == 16)
+        launch_batch<12, 16, 40, 4>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.ty == 16 && c.p == 8)
+        launch_batch<16, 8, 40, 4>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.ty == 16 && c.p == 4)
+        launch_batch<16, 4, 40, 4>(batch, d_desc, desc_bytes, d_err, sms, s);
     else
         throw std::runtime_error("stack: unsupported tile shape");
 }
