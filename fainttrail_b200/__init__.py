@@ -45,6 +45,11 @@ class SearchParams(C.Structure):
         ("threads", C.c_int), ("seed", C.c_ulonglong), ("null_tested", C.c_int), ("null_model_gauss", C.c_int)]
 
 
+class Injection(C.Structure):
+    """ft_b200_injection (Injection, validate.hpp:18-23)."""
+    _fields_ = [(n, C.c_double) for n in ("x_ref", "y_ref", "vx_pxh", "vy_pxh", "flux")]
+
+
 class Peak(C.Structure):
     _fields_ = [("x", C.c_int), ("y", C.c_int), ("snr", C.c_float), ("vidx", C.c_int)]
 
@@ -87,6 +92,9 @@ def _declare(L):
     L.ft_b200_search_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
                                      C.POINTER(SearchParams), C.POINTER(C.c_void_p)]
     L.ft_b200_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
+    L.ft_b200_search_batch.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
+                                       C.POINTER(SearchParams), C.c_int, C.c_void_p, C.c_void_p, PROGRESS_FN,
+                                       C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p]
     L.ft_b200_result_free.argtypes = [C.c_void_p]
     L.ft_b200_result_threshold.argtypes = [C.c_void_p, C.c_char_p, C.c_int] + [C.POINTER(C.c_double)] * 4
     L.ft_b200_result_threshold.restype = C.c_double
@@ -208,6 +216,25 @@ class Device:
                                    None, C.byref(r))
         self.check(rc, "search")
         return self._result(r, w, h, maps)
+
+    def search_batch(self, frames, mjd, exptime, copies, progress=None, maps=True, **kw):
+        """ft_b200_search_batch: the search plus injection copies. `copies` is a
+        list of lists of (x_ref, y_ref, vx_pxh, vy_pxh, flux). Returns (base
+        result dict, [copy result dicts])."""
+        frames = np.ascontiguousarray(frames, dtype=np.float32)
+        n, h, w = frames.shape
+        p = self._search_params(self.L, kw)
+        counts = (C.c_int * max(1, len(copies)))(*[len(c) for c in copies])
+        flat = [o for c in copies for o in c]
+        objs = (Injection * max(1, len(flat)))(*[Injection(*o) for o in flat])
+        base = C.c_void_p()
+        outs = (C.c_void_p * max(1, len(copies)))()
+        rc = self.L.ft_b200_search_batch(self.h, frames, w, h, n, np.ascontiguousarray(mjd, dtype=np.float64),
+                                         np.ascontiguousarray(exptime, dtype=np.float64), C.byref(p), len(copies),
+                                         counts, objs, _progress(progress), None, C.byref(base), outs)
+        self.check(rc, "search_batch")
+        res = self._result(base, w, h, maps)
+        return res, [self._result(C.c_void_p(outs[k]), w, h, maps) for k in range(len(copies))]
 
     def _result(self, r, w, h, maps):
         L = self.L

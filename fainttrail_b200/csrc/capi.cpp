@@ -249,6 +249,38 @@ int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height,
     });
 }
 
+int ft_b200_search_batch(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes,
+                         const double* mjd, const double* exptime, const ft_b200_search_params* params, int copies,
+                         const int* objects_per_copy, const ft_b200_injection* objects, ft_b200_progress_fn progress,
+                         void* user, ft_b200_result** base, ft_b200_result** copy_results) {
+    if (base) *base = nullptr;
+    for (int k = 0; copy_results && k < copies; ++k) copy_results[k] = nullptr;
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (!frames || !mjd || !exptime || !base) throw std::runtime_error("search: missing frames, times or result");
+        if (copies < 0 || (copies > 0 && (!objects_per_copy || !objects || !copy_results)))
+            throw std::runtime_error("search: malformed injection copies");
+        std::vector<std::vector<ftb::Injection>> sets(static_cast<size_t>(copies));
+        size_t at = 0;
+        for (int k = 0; k < copies; ++k) {
+            if (objects_per_copy[k] < 0) throw std::runtime_error("search: negative object count");
+            for (int q = 0; q < objects_per_copy[k]; ++q, ++at)
+                sets[static_cast<size_t>(k)].push_back(
+                    {objects[at].x_ref, objects[at].y_ref, objects[at].vx_pxh, objects[at].vy_pxh, objects[at].flux});
+        }
+        std::vector<ftb::SearchOut> outs;
+        auto r = std::make_unique<ft_b200_result>();
+        r->o = ftb::search_batch_host(c, frames, width, height, nframes, mjd, exptime, to_search_params(params), sets,
+                                      outs, wrap(progress, user));
+        std::vector<std::unique_ptr<ft_b200_result>> rs;
+        for (auto& o : outs) {
+            rs.push_back(std::make_unique<ft_b200_result>());
+            rs.back()->o = std::move(o);
+        }
+        *base = r.release();
+        for (int k = 0; k < copies; ++k) copy_results[k] = rs[static_cast<size_t>(k)].release();
+    });
+}
+
 int ft_b200_search_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
                        const double* mjd, const double* exptime, const ft_b200_search_params* params,
                        ft_b200_result** out) {

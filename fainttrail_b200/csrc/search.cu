@@ -124,7 +124,61 @@ __global__ void artefact_kernel(const ArtArgs a) {
     a.out[k] = (near_blank > max(1, a.n / 10)) ? 1 : 0;
 }
 
+// Injection increments added in order: one CTA per frame walks its patches in
+// sequence (patches may overlap; every pixel of one patch is touched once), so
+// each pixel receives its float additions in the reference's order.
+__global__ void patch_kernel(float* frames, size_t plane, int pitch, const int* pstart, const int* pframe_x0_y0_w_h,
+                             const unsigned long long* poff, const float* values) {
+    const int f = blockIdx.x;
+    float* img = frames + f * plane;
+    for (int q = pstart[f]; q < pstart[f + 1]; ++q) {
+        const int x0 = pframe_x0_y0_w_h[4 * q], y0 = pframe_x0_y0_w_h[4 * q + 1];
+        const int pw = pframe_x0_y0_w_h[4 * q + 2], ph = pframe_x0_y0_w_h[4 * q + 3];
+        const float* v = values + poff[q];
+        for (int e = threadIdx.x; e < pw * ph; e += blockDim.x) {
+            float* px = img + static_cast<size_t>(y0 + e / pw) * pitch + x0 + e % pw;
+            *px = __fadd_rn(*px, v[e]);
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+void apply_patches(Context& c, const InjectionPatches& ip, float* d_frames, int w, int h, int n) {
+    const size_t np = ip.frame.size();
+    if (np == 0) return;
+    const int pitch = frame_pitch(w);
+    std::vector<int> start(static_cast<size_t>(n) + 1, 0), geo(4 * np);
+    std::vector<unsigned long long> off(np);
+    for (size_t q = 0; q < np; ++q) {
+        if (q > 0 && ip.frame[q] < ip.frame[q - 1]) throw std::runtime_error("injection patches out of frame order");
+        ++start[static_cast<size_t>(ip.frame[q]) + 1];
+        geo[4 * q] = ip.x0[q];
+        geo[4 * q + 1] = ip.y0[q];
+        geo[4 * q + 2] = ip.pw[q];
+        geo[4 * q + 3] = ip.ph[q];
+        off[q] = ip.off[q];
+    }
+    for (int f = 0; f < n; ++f) start[static_cast<size_t>(f) + 1] += start[static_cast<size_t>(f)];
+    const size_t bytes = sizeof(int) * (start.size() + geo.size()) + sizeof(unsigned long long) * np +
+                         sizeof(float) * ip.values.size() + 1024;
+    DevBuf buf(&c, bytes, "injection patches");
+    unsigned char* b = buf.as<unsigned char>();
+    int* d_start = reinterpret_cast<int*>(b);
+    int* d_geo = d_start + start.size();
+    unsigned long long* d_off =
+        reinterpret_cast<unsigned long long*>(b + ((sizeof(int) * (start.size() + geo.size()) + 15) / 16) * 16);
+    float* d_val = reinterpret_cast<float*>(d_off + np);
+    cudaStream_t s = c.stream();
+    FTB_CHECK(cudaMemcpyAsync(d_start, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice, s));
+    FTB_CHECK(cudaMemcpyAsync(d_geo, geo.data(), sizeof(int) * geo.size(), cudaMemcpyHostToDevice, s));
+    FTB_CHECK(cudaMemcpyAsync(d_off, off.data(), sizeof(unsigned long long) * np, cudaMemcpyHostToDevice, s));
+    FTB_CHECK(cudaMemcpyAsync(d_val, ip.values.data(), sizeof(float) * ip.values.size(), cudaMemcpyHostToDevice, s));
+    patch_kernel<<<n, 256, 0, s>>>(d_frames, static_cast<size_t>(pitch) * h, pitch, d_start, d_geo, d_off, d_val);
+    FTB_CHECK(cudaGetLastError());
+    ++c.launches;
+}  // buf is released in stream order after the kernel
 
 std::vector<Peak> device_peaks(Context& c, const float* d_max, const int* d_best_v, int w, int h, float floor,
                                int radius, int edge) {
@@ -196,8 +250,16 @@ enum SearchSlot { kRaw = 30, kSub, kFiltReal, kFiltNull, kSkyReal, kSkyNull, kMa
 
 SearchOut search_host(Context& c, const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
                       const SearchParams& p, const Progress& progress, bool frames_on_device, int in_pitch) {
-    (void)exptime;
+    std::vector<SearchOut> none;
+    return search_batch_host(c, frames, w, h, n, mjd, exptime, p, {}, none, progress, frames_on_device, in_pitch);
+}
+
+SearchOut search_batch_host(Context& c, const float* frames, int w, int h, int n, const double* mjd,
+                            const double* exptime, const SearchParams& p,
+                            const std::vector<std::vector<Injection>>& copies, std::vector<SearchOut>& copies_out,
+                            const Progress& progress, bool frames_on_device, int in_pitch) {
     c.bind();
+    if (!copies.empty() && !exptime) throw std::runtime_error("injection copies need the exposure times");
     if (n < 5) throw std::runtime_error("synthetic tracking needs at least 5 frames");
     if (w < 16 || h < 16) throw std::runtime_error("frames are too small");
     auto report = [&](double f, const char* stage) {
@@ -246,6 +308,19 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
                                     c.stream()));
     c.span_end(up);
     report(0.0, "background");
+    // the raw frames stay available for the injection copies
+    const int ncopies = static_cast<int>(copies.size());
+    DevBuf raw0, sub2, copy_sky, copy_mask;
+    std::vector<double> exp_sorted;
+    if (ncopies > 0) {
+        raw0 = DevBuf(&c, sizeof(float) * plane * n, "raw frames (copies)");
+        sub2 = DevBuf(&c, sizeof(float) * plane * n, "copy sub frames");
+        copy_sky = DevBuf(&c, sizeof(float) * plane, "copy static sky");
+        copy_mask = DevBuf(&c, sizeof(float) * plane, "copy mask");
+        FTB_CHECK(cudaMemcpyAsync(raw0.as<float>(), d_raw, sizeof(float) * plane * n, cudaMemcpyDeviceToDevice,
+                                  c.stream()));
+        for (int i = 0; i < n; ++i) exp_sorted.push_back(exptime[order[static_cast<size_t>(i)]]);
+    }
 
     // prepare (preprocess.cpp:528-585)
     const double fwhm_guess = p.fwhm_px > 0.0 ? p.fwhm_px : 20.0;  // sizes the sample buffers
@@ -293,16 +368,23 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
     const size_t per_null = sizeof(float) * (plane * n + 2 * plane) + 2 * map_bytes;
     const size_t reserve = size_t{256} << 20;  // plans, peaks, descriptors
     const size_t avail = c.budget() > c.used() + reserve ? c.budget() - c.used() - reserve : 0;
-    const int per_batch = static_cast<int>(std::max<size_t>(1, std::min<size_t>(std::max(runs, 1), avail / per_null)));
+    const int per_batch = static_cast<int>(
+        std::max<size_t>(1, std::min<size_t>(std::max(runs + static_cast<int>(copies.size()), 1), avail / per_null)));
     std::vector<float> pooled;
     const float floor = static_cast<float>(auto_thr ? p.min_snr_floor : p.threshold_snr);
     bool real_done = false;
-    for (int k0 = 0; k0 < std::max(runs, 1); k0 += per_batch) {
+    // copies keep their maps to the end (their peaks need the calibrated threshold)
+    std::vector<DevBuf> copy_max(static_cast<size_t>(ncopies)), copy_bv(static_cast<size_t>(ncopies));
+    copies_out.assign(static_cast<size_t>(ncopies), SearchOut());
+    const int total_items = runs + ncopies;
+    for (int k0 = 0; k0 < std::max(total_items, 1); k0 += per_batch) {
         const int k1 = std::min(runs, k0 + per_batch);
+        const int c0 = std::max(0, k0 - runs), c1 = std::max(0, std::min(total_items, k0 + per_batch) - runs);
         struct NullBufs {
             DevBuf filt, sky, mask, max, bv;
         };
         std::vector<NullBufs> nb(static_cast<size_t>(std::max(0, k1 - k0)));
+        std::vector<DevBuf> copy_filt(static_cast<size_t>(std::max(0, c1 - c0)));
         std::vector<PassJob> jobs;
         if (!real_done) {
             PassJob j;
@@ -341,6 +423,35 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
             j.d_bv = b.bv.as<int>();
             jobs.push_back(std::move(j));
         }
+        for (int j = c0; j < c1; ++j) {
+            // the raw frames plus this copy's objects, prepared again (fixed PSF width)
+            DevBuf& f = copy_filt[static_cast<size_t>(j - c0)];
+            f = DevBuf(&c, sizeof(float) * plane * n, "copy filtered frames");
+            copy_max[static_cast<size_t>(j)] = DevBuf(&c, map_bytes, "copy max_snr");
+            copy_bv[static_cast<size_t>(j)] = DevBuf(&c, map_bytes, "copy best_v");
+            FTB_CHECK(cudaMemcpyAsync(d_raw, raw0.as<float>(), sizeof(float) * plane * n, cudaMemcpyDeviceToDevice,
+                                      c.stream()));
+            apply_patches(c, injection_patches(copies[static_cast<size_t>(j)], o.t_h, exp_sorted, o.fwhm_px, w, h),
+                          d_raw, w, h, n);
+            SearchOut& co = copies_out[static_cast<size_t>(j)];
+            co.background.resize(static_cast<size_t>(n));
+            prepare_sub(c, sc, d_raw, sub2.as<float>(), w, h, n, co.background.data());
+            co.sigma.resize(static_cast<size_t>(n));
+            stage_run(c, sc, sub2.as<float>(), w, h, n, o.t_h.data(), sp, f.as<float>(), copy_sky.as<float>(),
+                      copy_mask.as<float>(), co.sigma.data(), nullptr);
+            PassJob jb;
+            jb.d_frames = f.as<float>();
+            jb.pitch = pitch;
+            jb.w = w;
+            jb.h = h;
+            jb.n = n;
+            shift_table(o.t_h, o.grid, jb.dx, jb.dy);
+            jb.m = static_cast<int>(m);
+            jb.min_count = min_count;
+            jb.d_max = copy_max[static_cast<size_t>(j)].as<float>();
+            jb.d_bv = copy_bv[static_cast<size_t>(j)].as<int>();
+            jobs.push_back(std::move(jb));
+        }
         stack_passes_device(c, jobs);
         o.adds += static_cast<double>(m) * n * w * h * static_cast<double>(jobs.size());
         report(0.1 + 0.9 * share * (k1 + 1), "null");
@@ -372,6 +483,34 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
     FTB_CHECK(cudaMemcpyAsync(o.best_v.data(), d_bv, sizeof(int) * o.best_v.size(), cudaMemcpyDeviceToHost,
                               c.stream()));
     o.thr = set_threshold(p, pooled, runs, o.fwhm_px, w, h, m);
+    // the copies: peaks above the calibrated threshold, searched with it fixed
+    for (int j = 0; j < ncopies; ++j) {
+        SearchOut& co = copies_out[static_cast<size_t>(j)];
+        co.w = w;
+        co.h = h;
+        co.n = n;
+        co.fwhm_px = o.fwhm_px;
+        co.span_h = o.span_h;
+        co.t_ref_mjd = o.t_ref_mjd;
+        co.dv = o.dv;
+        co.t_h = o.t_h;
+        co.grid = o.grid;
+        co.thr.snr = o.thr.snr;
+        co.thr.method = "fixed";
+        co.adds = static_cast<double>(m) * n * w * h;
+        const float* dm = copy_max[static_cast<size_t>(j)].as<float>();
+        const int* db = copy_bv[static_cast<size_t>(j)].as<int>();
+        co.peaks = device_peaks(c, dm, db, w, h, static_cast<float>(o.thr.snr), nms, edge);
+        order_peaks(co.peaks, 100000);
+        for (const Peak& pk : co.peaks)
+            if (pk.snr >= co.thr.snr && pk.vidx >= 0) co.selected.push_back(pk);
+        if (static_cast<int>(co.selected.size()) > p.max_candidates)
+            co.selected.resize(static_cast<size_t>(p.max_candidates));
+        co.max_snr.resize(static_cast<size_t>(w) * h);
+        co.best_v.resize(static_cast<size_t>(w) * h);
+        FTB_CHECK(cudaMemcpyAsync(co.max_snr.data(), dm, map_bytes, cudaMemcpyDeviceToHost, c.stream()));
+        FTB_CHECK(cudaMemcpyAsync(co.best_v.data(), db, map_bytes, cudaMemcpyDeviceToHost, c.stream()));
+    }
     if (runs > 0 && auto_thr) o.null_peaks.assign(pooled.begin(), pooled.end());
     for (const Peak& pk : o.peaks)
         if (pk.snr >= o.thr.snr && pk.vidx >= 0) o.selected.push_back(pk);

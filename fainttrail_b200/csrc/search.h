@@ -68,6 +68,24 @@ std::vector<char> device_artefacts(Context& c, const std::vector<Peak>& peaks, s
                                    const float* d_sub, const float* d_sky, const std::vector<double>& t_h, int w,
                                    int h, int n, double fwhm_px, double max_frame_fraction);
 
+// An object injected into every frame of a copy (Injection, validate.hpp:18-23).
+struct Injection {
+    double x_ref = 0, y_ref = 0, vx_pxh = 0, vy_pxh = 0, flux = 0;
+};
+
+// The pixel increments inject() makes (validate.cpp:17-29 through add_trailed /
+// add_gaussian, psf.hpp:20-58), computed on the host with the reference's double
+// arithmetic, in the reference's order: one patch per Gaussian, frames in order.
+struct InjectionPatches {
+    std::vector<int> frame, x0, y0, pw, ph;  // per patch
+    std::vector<size_t> off;                 // into values
+    std::vector<float> values;               // the float increments, row-major per patch
+};
+InjectionPatches injection_patches(const std::vector<Injection>& objects, const std::vector<double>& t_mid_h,
+                                   const std::vector<double>& exptime_s, double fwhm_px, int w, int h);
+// Adds the patches to device frames (n x h x pitch) in order.
+void apply_patches(Context& c, const InjectionPatches& ip, float* d_frames, int w, int h, int n);
+
 // One whole search from raw frames (ft_search's prepare + search, without the
 // candidate refinement).
 struct SearchOut {
@@ -89,5 +107,16 @@ struct SearchOut {
 SearchOut search_host(Context& c, const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
                       const SearchParams& p, const Progress& progress, bool frames_on_device = false,
                       int in_pitch = 0);
+
+// The search plus injection-recovery copies (completeness's searches,
+// validate.cpp:88-126): each copy is the raw frames with its objects injected,
+// prepared again and searched with the threshold the null runs calibrated
+// (fixed, no null runs) and the same PSF width. The real pass, the null runs and
+// the copies are stacked together in persistent launches. copies_out receives
+// one result per copy (peaks above the threshold, selected peaks, maps).
+SearchOut search_batch_host(Context& c, const float* frames, int w, int h, int n, const double* mjd,
+                            const double* exptime, const SearchParams& p,
+                            const std::vector<std::vector<Injection>>& copies, std::vector<SearchOut>& copies_out,
+                            const Progress& progress, bool frames_on_device = false, int in_pitch = 0);
 
 }  // namespace ftb

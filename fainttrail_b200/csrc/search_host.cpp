@@ -337,4 +337,58 @@ double estimate_psf_fwhm(const std::vector<float>& static_sky, int w, int h, std
     return f;
 }
 
+// add_gaussian (psf.hpp:20-44) as a patch of float increments
+static void gaussian_patch(InjectionPatches& ip, int frame, int w, int h, double x0, double y0, double flux,
+                           double sigma) {
+    const int max_radius = 30;
+    if (flux <= 0.0 || sigma <= 0.0) return;
+    const double peak = flux / (2.0 * kPi * sigma * sigma);
+    int r = static_cast<int>(std::ceil(sigma * std::sqrt(2.0 * std::log(std::max(peak / 0.05, 2.0)))));
+    r = std::clamp(r, 2, max_radius);
+    const int xc = static_cast<int>(std::floor(x0 + 0.5));
+    const int yc = static_cast<int>(std::floor(y0 + 0.5));
+    const int x_lo = std::max(0, xc - r), x_hi = std::min(w - 1, xc + r);
+    const int y_lo = std::max(0, yc - r), y_hi = std::min(h - 1, yc + r);
+    if (x_lo > x_hi || y_lo > y_hi) return;
+    const double inv = 1.0 / (sigma * std::sqrt(2.0));
+    std::vector<double> wx(static_cast<size_t>(x_hi - x_lo + 1)), wy(static_cast<size_t>(y_hi - y_lo + 1));
+    for (int x = x_lo; x <= x_hi; ++x)
+        wx[static_cast<size_t>(x - x_lo)] = 0.5 * (std::erf((x + 0.5 - x0) * inv) - std::erf((x - 0.5 - x0) * inv));
+    for (int y = y_lo; y <= y_hi; ++y)
+        wy[static_cast<size_t>(y - y_lo)] = 0.5 * (std::erf((y + 0.5 - y0) * inv) - std::erf((y - 0.5 - y0) * inv));
+    ip.frame.push_back(frame);
+    ip.x0.push_back(x_lo);
+    ip.y0.push_back(y_lo);
+    ip.pw.push_back(x_hi - x_lo + 1);
+    ip.ph.push_back(y_hi - y_lo + 1);
+    ip.off.push_back(ip.values.size());
+    for (int y = y_lo; y <= y_hi; ++y) {
+        const double fy = flux * wy[static_cast<size_t>(y - y_lo)];
+        for (int x = x_lo; x <= x_hi; ++x) ip.values.push_back(static_cast<float>(fy * wx[static_cast<size_t>(x - x_lo)]));
+    }
+}
+
+InjectionPatches injection_patches(const std::vector<Injection>& objects, const std::vector<double>& t_mid_h,
+                                   const std::vector<double>& exptime_s, double fwhm_px, int w, int h) {
+    InjectionPatches ip;
+    const double s = fwhm_px * kFwhmToSigma;
+    for (size_t f = 0; f < t_mid_h.size(); ++f) {
+        const double t_mid = t_mid_h[f];
+        const double half = 0.5 * exptime_s[f] / 3600.0;
+        for (const Injection& o : objects) {
+            // add_trailed (psf.hpp:47-57)
+            const double x0 = o.x_ref + o.vx_pxh * (t_mid - half), y0 = o.y_ref + o.vy_pxh * (t_mid - half);
+            const double x1 = o.x_ref + o.vx_pxh * (t_mid + half), y1 = o.y_ref + o.vy_pxh * (t_mid + half);
+            const double len = std::hypot(x1 - x0, y1 - y0);
+            const int steps = std::max(1, static_cast<int>(std::ceil(len / 0.25)));
+            const double fl = o.flux / steps;
+            for (int k = 0; k < steps; ++k) {
+                const double u = (k + 0.5) / steps;
+                gaussian_patch(ip, static_cast<int>(f), w, h, x0 + u * (x1 - x0), y0 + u * (y1 - y0), fl, s);
+            }
+        }
+    }
+    return ip;
+}
+
 }  // namespace ftb

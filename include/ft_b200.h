@@ -162,6 +162,27 @@ int ft_b200_search_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int h
                        const double* mjd, const double* exptime, const ft_b200_search_params* params,
                        ft_b200_result** out);
 void ft_b200_result_free(ft_b200_result* r);
+
+/* An object to inject into every frame of a copy: Injection (validate.hpp:18-23),
+ * position at the reference epoch (0-based px), motion (px/hour), flux per frame. */
+typedef struct ft_b200_injection {
+    double x_ref, y_ref, vx_pxh, vy_pxh, flux;
+} ft_b200_injection;
+
+/* The search of ft_b200_search plus injection-recovery copies, all in one batch
+ * (completeness's searches, validate.cpp:62-126): copy k holds the raw frames
+ * with objects_per_copy[k] objects injected (ft_b200_injection, consecutive for
+ * all copies; the trailed Gaussians of inject(), validate.cpp:17-29, rendered
+ * with the reference's arithmetic), prepared again and searched with the
+ * threshold the null runs calibrated held fixed, no null runs, and the same PSF
+ * width. The real pass, the null runs and the copies are stacked together in
+ * persistent launches. *base receives the search's result; copy_results[k] (an
+ * array of `copies` pointers) each copy's result (peaks above the threshold,
+ * selected peaks, maps). Release every result with ft_b200_result_free. */
+int ft_b200_search_batch(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes,
+                         const double* mjd, const double* exptime, const ft_b200_search_params* params, int copies,
+                         const int* objects_per_copy, const ft_b200_injection* objects, ft_b200_progress_fn progress,
+                         void* user, ft_b200_result** base, ft_b200_result** copy_results);
 /* threshold_snr and the tail model (SearchResult, search.hpp:163-172); method
  * receives "fixed", "null-fit gauss", "null-fit linear", "null-quantile" or
  * "gaussian". Any pointer may be NULL. */

@@ -1,0 +1,40 @@
+"""Batched search with injection-recovery copies (ft_b200_search_batch) against
+the reference: each copy must equal the reference's inject() + prepare() +
+search() with the calibrated threshold held fixed and no null runs (the searches
+completeness() runs, validate.cpp:88-126); the batch's own search must equal a
+plain ft_b200_search."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def same(a, b):
+    return np.array_equal(np.asarray(a), np.asarray(b), equal_nan=True)
+
+
+def test_copies_match_reference_inject_and_search(device, reference, oracle):
+    R = reference
+    frames, mjd, exp = R.simulate(width=128, height=100, nframes=16, nstars=60, nmovers=1, seed=33,
+                                  rate_min_arcsec_min=0.3, rate_max_arcsec_min=0.8)
+    kw = dict(fwhm_px=2.5, null_runs=2, vmin_pxh=8.0, vmax_pxh=30.0)
+    copies = [[(40.0, 50.0, 20.0, -9.0, 900.0), (90.0, 30.0, -14.0, 12.0, 500.0)],
+              [(64.5, 70.25, 11.0, 15.0, 1200.0)],
+              []]
+    base, outs = device.search_batch(frames, mjd, exp, copies, **kw)
+    plain = device.search(frames, mjd, exp, **kw)
+    assert base["threshold"] == plain["threshold"] and same(base["null_peaks"], plain["null_peaks"])
+    assert same(base["max_snr"], plain["max_snr"]) and base["peaks"] == plain["peaks"]
+    prep = R.prepare(frames, mjd, exp, fwhm_px=2.5, null_runs=2)
+    ref = prep.search(backend="cpu", **kw)
+    assert base["threshold"] == ref["threshold"]
+    t_ref = 0.5 * (mjd[0] + mjd[-1])
+    for objs, got in zip(copies, outs):
+        injected = R.inject(frames, mjd, exp, np.array(objs, np.float64).reshape(-1, 5), t_ref, 2.5)
+        p2 = R.prepare(injected, mjd, exp, fwhm_px=2.5)
+        want = p2.search(backend="cpu", fwhm_px=2.5, vmin_pxh=8.0, vmax_pxh=30.0, null_runs=0,
+                         threshold_snr=ref["threshold"])
+        assert got["method"] == "fixed" and got["threshold"] == ref["threshold"]
+        assert same(got["max_snr"], want["max_snr"])
+        px, py, ps, pv = oracle.find_peaks(got["max_snr"], got["best_v"], np.float32(ref["threshold"]), 2, 4, 100000)
+        assert got["peaks"] == [(int(a), int(b), float(c), int(d)) for a, b, c, d in zip(px, py, ps, pv)]
