@@ -107,6 +107,80 @@ def _declare(L):
                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
 
 
+def _declare_server(L):
+    L.ft_b200_server_open.argtypes = [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]
+    L.ft_b200_server_close.argtypes = [C.c_void_p]
+    L.ft_b200_server_submit.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
+                                        C.POINTER(SearchParams), C.POINTER(C.c_longlong)]
+    L.ft_b200_server_poll.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.POINTER(C.c_void_p)]
+    L.ft_b200_server_error.argtypes = [C.c_void_p]
+    L.ft_b200_server_error.restype = C.c_char_p
+    L.ft_b200_server_pause.argtypes = [C.c_void_p, C.c_int]
+    L.ft_b200_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                                       C.POINTER(C.c_double)]
+
+
+FT_B200_PENDING = 3
+
+
+class Server:
+    """The serving loop (ft_b200_server_*): submit searches at any time, poll
+    results; requests admitted together share their stacking launches."""
+
+    def __init__(self, device=-1, hbm_budget_bytes=0.0, max_batch=16):
+        self.L = lib()
+        _declare_server(self.L)
+        h = C.c_void_p()
+        if self.L.ft_b200_server_open(device, hbm_budget_bytes, max_batch, C.byref(h)) != FT_B200_OK:
+            raise RuntimeError("ft_b200_server_open: " + self.L.ft_b200_last_error(None).decode())
+        self.h = h
+        self._dev = None
+
+    def submit(self, frames, mjd, exptime, **kw):
+        frames = np.ascontiguousarray(frames, dtype=np.float32)
+        n, h, w = frames.shape
+        p = Device._search_params(self.L, kw)
+        rid = C.c_longlong()
+        rc = self.L.ft_b200_server_submit(self.h, frames, w, h, n, np.ascontiguousarray(mjd, dtype=np.float64),
+                                          np.ascontiguousarray(exptime, dtype=np.float64), C.byref(p), C.byref(rid))
+        if rc != FT_B200_OK:
+            raise RuntimeError("submit: " + self.L.ft_b200_server_error(self.h).decode())
+        return rid.value, (w, h)
+
+    def poll(self, ticket, wait_ms=-1, maps=True):
+        rid, (w, h) = ticket
+        r = C.c_void_p()
+        rc = self.L.ft_b200_server_poll(self.h, rid, wait_ms, C.byref(r))
+        if rc == FT_B200_PENDING:
+            return None
+        if rc != FT_B200_OK:
+            raise RuntimeError("poll: " + self.L.ft_b200_server_error(self.h).decode())
+        return Device._result(self, r, w, h, maps)
+
+    def pause(self, paused=True):
+        self.L.ft_b200_server_pause(self.h, 1 if paused else 0)
+
+    def stats(self):
+        c, r = C.c_longlong(), C.c_longlong()
+        p50, p99, sps, mb = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        self.L.ft_b200_server_stats(self.h, C.byref(c), C.byref(p50), C.byref(p99), C.byref(sps), C.byref(r),
+                                    C.byref(mb))
+        return dict(completed=c.value, p50_s=p50.value, p99_s=p99.value, searches_per_s=sps.value, rounds=r.value,
+                    mean_batch=mb.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ft_b200_server_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def exported_symbols():
     """Names of the entry points include/ft_b200.h declares."""
     import re

@@ -11,6 +11,7 @@
 
 #include "engine.h"
 #include "search.h"
+#include "serve.h"
 #include "stage.h"
 
 struct ft_b200_ctx {
@@ -19,6 +20,11 @@ struct ft_b200_ctx {
 
 struct ft_b200_result {
     ftb::SearchOut o;
+};
+
+struct ft_b200_server {
+    std::unique_ptr<ftb::Server> s;
+    std::string error;
 };
 
 namespace {
@@ -293,6 +299,71 @@ int ft_b200_search_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int h
                                 pitch);
         *out = r.release();
     });
+}
+
+int ft_b200_server_open(int device, double hbm_budget_bytes, int max_batch, ft_b200_server** out) {
+    if (!out) return FT_B200_ERROR;
+    *out = nullptr;
+    try {
+        auto h = std::make_unique<ft_b200_server>();
+        h->s = std::make_unique<ftb::Server>(device, hbm_budget_bytes, max_batch);
+        *out = h.release();
+        return FT_B200_OK;
+    } catch (const std::exception& e) {
+        g_open_error = e.what();
+        return FT_B200_ERROR;
+    }
+}
+
+void ft_b200_server_close(ft_b200_server* s) { delete s; }
+
+int ft_b200_server_submit(ft_b200_server* s, const float* frames, int width, int height, int nframes,
+                          const double* mjd, const double* exptime, const ft_b200_search_params* params,
+                          long long* request_id) {
+    if (!s || !request_id) return FT_B200_ERROR;
+    try {
+        *request_id = s->s->submit(frames, width, height, nframes, mjd, exptime, to_search_params(params));
+        return FT_B200_OK;
+    } catch (const std::exception& e) {
+        s->error = e.what();
+        return FT_B200_ERROR;
+    }
+}
+
+int ft_b200_server_poll(ft_b200_server* s, long long request_id, int wait_ms, ft_b200_result** out) {
+    if (!s) return FT_B200_ERROR;
+    if (out) *out = nullptr;
+    auto r = std::make_unique<ft_b200_result>();
+    std::string err;
+    const int rc = s->s->poll(request_id, wait_ms, &r->o, &err);
+    if (rc == 3) return FT_B200_PENDING;
+    if (rc != 0) {
+        s->error = err;
+        return FT_B200_ERROR;
+    }
+    if (out) *out = r.release();
+    return FT_B200_OK;
+}
+
+const char* ft_b200_server_error(const ft_b200_server* s) { return s ? s->error.c_str() : g_open_error.c_str(); }
+
+int ft_b200_server_pause(ft_b200_server* s, int paused) {
+    if (!s) return FT_B200_ERROR;
+    s->s->pause(paused != 0);
+    return FT_B200_OK;
+}
+
+int ft_b200_server_stats(ft_b200_server* s, long long* completed, double* p50_s, double* p99_s,
+                         double* searches_per_s, long long* rounds, double* mean_batch) {
+    if (!s) return FT_B200_ERROR;
+    const ftb::ServerStats st = s->s->stats();
+    if (completed) *completed = st.completed;
+    if (p50_s) *p50_s = st.p50_s;
+    if (p99_s) *p99_s = st.p99_s;
+    if (searches_per_s) *searches_per_s = st.searches_per_s;
+    if (rounds) *rounds = st.rounds;
+    if (mean_batch) *mean_batch = st.mean_batch;
+    return FT_B200_OK;
 }
 
 int ft_b200_stats(const ft_b200_ctx* ctx, long long* kernel_launches, double* pixel_adds) {

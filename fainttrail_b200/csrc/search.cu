@@ -242,11 +242,256 @@ std::vector<char> device_artefacts(Context& c, const std::vector<Peak>& peaks, s
     return art;
 }
 
-namespace {
+// ------------------------------------------------------------------ a search request in phases
 
-enum SearchSlot { kRaw = 30, kSub, kFiltReal, kFiltNull, kSkyReal, kSkyNull, kMaskReal, kMaskNull, kMaxMap, kBestMap };
+SearchRequest::SearchRequest(Context& c, const SearchParams& p, int w, int h, int n) : c_(c), p_(p) {
+    if (n < 5) throw std::runtime_error("synthetic tracking needs at least 5 frames");
+    if (w < 16 || h < 16) throw std::runtime_error("frames are too small");
+    if (n > 255) throw std::runtime_error("at most 255 frames per search");
+    o_.w = w;
+    o_.h = h;
+    o_.n = n;
+    pitch_ = frame_pitch(w);
+    plane_ = static_cast<size_t>(pitch_) * h;
+    map_bytes_ = sizeof(float) * static_cast<size_t>(w) * h;
+}
 
-}  // namespace
+size_t SearchRequest::base_bytes(int w, int h, int n) {
+    const size_t plane = static_cast<size_t>(frame_pitch(w)) * h;
+    // raw, sub, filtered, residuals (stage scratch) + sky, mask, scatter + maps + samples
+    return sizeof(float) * (4 * plane * n + 3 * plane) + 2 * sizeof(float) * static_cast<size_t>(w) * h +
+           (size_t{64} << 20);
+}
+
+size_t SearchRequest::item_bytes() const {
+    return sizeof(float) * (plane_ * o_.n + 2 * plane_) + 2 * map_bytes_;
+}
+
+void SearchRequest::prepare(const float* frames, const double* mjd, const double* exptime, bool on_device,
+                            int in_pitch, bool keep_raw, const std::function<void(double, const char*)>& report) {
+    const int w = o_.w, h = o_.h, n = o_.n;
+    Context& c = c_;
+    const double t_setup = wall_seconds();
+    // frames in time order (the C API stable-sorts by mid-exposure, c_api.cpp:177-179)
+    std::vector<int> order(static_cast<size_t>(n));
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return mjd[a] < mjd[b]; });
+    double tmin = mjd[order[0]], tmax = tmin;
+    for (int i = 0; i < n; ++i) {
+        tmin = std::min(tmin, mjd[i]);
+        tmax = std::max(tmax, mjd[i]);
+    }
+    o_.t_ref_mjd = 0.5 * (tmin + tmax);
+    o_.span_h = (tmax - tmin) * 24.0;
+    if (o_.span_h <= 0.0) throw std::runtime_error("frames must span a non-zero time interval");
+    for (int i = 0; i < n; ++i) o_.t_h.push_back((mjd[order[static_cast<size_t>(i)]] - o_.t_ref_mjd) * 24.0);
+    if (exptime)
+        for (int i = 0; i < n; ++i) exp_sorted_.push_back(exptime[order[static_cast<size_t>(i)]]);
+
+    raw_ = DevBuf(&c, sizeof(float) * plane_ * n, "raw frames");
+    sub_ = DevBuf(&c, sizeof(float) * plane_ * n, "background-subtracted frames");
+    filt_ = DevBuf(&c, sizeof(float) * plane_ * n, "filtered frames");
+    sky_ = DevBuf(&c, sizeof(float) * plane_, "static sky");
+    mask_ = DevBuf(&c, sizeof(float) * plane_, "mask");
+    max_ = DevBuf(&c, map_bytes_, "max_snr");
+    bv_ = DevBuf(&c, map_bytes_, "best_v");
+    c.host_time("setup", wall_seconds() - t_setup);
+
+    const int up = c.span_begin(on_device ? "copy in" : "upload");
+    const size_t in_plane = on_device ? static_cast<size_t>(in_pitch) * h : static_cast<size_t>(w) * h;
+    for (int i = 0; i < n; ++i)
+        FTB_CHECK(cudaMemcpy2DAsync(raw_.as<float>() + static_cast<size_t>(i) * plane_, sizeof(float) * pitch_,
+                                    frames + static_cast<size_t>(order[static_cast<size_t>(i)]) * in_plane,
+                                    sizeof(float) * (on_device ? in_pitch : w), sizeof(float) * w,
+                                    static_cast<size_t>(h), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    c.stream()));
+    c.span_end(up);
+    if (report) report(0.0, "background");
+    if (keep_raw) {
+        raw0_ = DevBuf(&c, sizeof(float) * plane_ * n, "raw frames (copies)");
+        FTB_CHECK(cudaMemcpyAsync(raw0_.as<float>(), raw_.as<float>(), sizeof(float) * plane_ * n,
+                                  cudaMemcpyDeviceToDevice, c.stream()));
+    }
+    // prepare (preprocess.cpp:528-585)
+    sc_ = std::make_unique<StageScratch>(c, w, h, n, std::max(p_.fwhm_px > 0.0 ? p_.fwhm_px : 20.0, 20.0));
+    o_.background.resize(static_cast<size_t>(n));
+    prepare_sub(c, *sc_, raw_.as<float>(), sub_.as<float>(), w, h, n, o_.background.data());
+    sp_.static_exclude = p_.static_exclude;
+    sp_.clip_sigma = p_.clip_sigma;
+    sp_.cr_sigma = p_.cr_sigma;
+    sp_.mask_scatter = p_.mask_scatter;
+    sp_.weight_scatter = p_.weight_scatter;
+    stage_noise(c, *sc_, sub_.as<float>(), w, h, n, o_.t_h.data(), p_.static_exclude, sky_.as<float>());
+    o_.sigma.resize(static_cast<size_t>(n));
+    stage_sigma_to_host(c, *sc_, n, o_.sigma.data());
+    if (p_.fwhm_px > 0.0) {
+        o_.fwhm_px = p_.fwhm_px;
+    } else {
+        std::vector<float> sky(static_cast<size_t>(w) * h);
+        FTB_CHECK(cudaMemcpy2DAsync(sky.data(), sizeof(float) * w, sky_.as<float>(), sizeof(float) * pitch_,
+                                    sizeof(float) * w, h, cudaMemcpyDeviceToHost, c.stream()));
+        FTB_CHECK(cudaStreamSynchronize(c.stream()));
+        o_.fwhm_px = estimate_psf_fwhm(sky, w, h, o_.sigma, p_);
+    }
+    sp_.fwhm_px = o_.fwhm_px;
+    if (!sc_->fits(w, h, n, sp_.fwhm_px)) throw std::runtime_error("PSF too wide for the sample buffers");
+    stage_filter(c, *sc_, w, h, n, sp_, filt_.as<float>(), mask_.as<float>(), nullptr, nullptr);
+    if (report) report(0.1, "prepared");
+    // search setup (search.cpp:716-746)
+    o_.grid = velocity_grid(o_.span_h, p_, &o_.dv);
+    m_ = o_.grid.size();
+    auto_thr_ = p_.threshold_snr <= 0.0;
+    runs_ = auto_thr_ ? std::max(0, p_.null_runs) : 0;
+    nms_ = std::max(2, static_cast<int>(std::lround(o_.fwhm_px)));
+    edge_ = std::max(p_.edge_px, 1);
+    min_count_ = pass_min_count(p_.min_coverage, n);
+    floor_ = static_cast<float>(auto_thr_ ? p_.min_snr_floor : p_.threshold_snr);
+    orders_ = null_time_orders(o_.t_h, runs_, p_.seed);
+    raw_needed_ = keep_raw;
+    if (!keep_raw) raw_.reset();
+}
+
+PassJob SearchRequest::job(const float* frames, const std::vector<double>& t, float* d_max, int* d_bv) const {
+    PassJob j;
+    j.d_frames = frames;
+    j.pitch = pitch_;
+    j.w = o_.w;
+    j.h = o_.h;
+    j.n = o_.n;
+    shift_table(t, o_.grid, j.dx, j.dy);
+    j.m = static_cast<int>(m_);
+    j.min_count = min_count_;
+    j.d_max = d_max;
+    j.d_bv = d_bv;
+    return j;
+}
+
+void SearchRequest::stage_items(int k0, int k1, const std::vector<std::vector<Injection>>& copies,
+                                std::vector<PassJob>& jobs) {
+    Context& c = c_;
+    const int w = o_.w, h = o_.h, n = o_.n;
+    const bool add_real = !real_queued_;
+    if (add_real) {
+        jobs.push_back(job(filt_.as<float>(), o_.t_h, max_.as<float>(), bv_.as<int>()));
+        real_queued_ = true;
+    }
+    for (int k = k0; k < k1; ++k) {
+        Item it;
+        it.filt = DevBuf(&c, sizeof(float) * plane_ * n, "null filtered frames");
+        it.max = DevBuf(&c, map_bytes_, "null max_snr");
+        it.bv = DevBuf(&c, map_bytes_, "null best_v");
+        if (k < runs_) {
+            // preprocessing rebuilt with permuted times on the same sub frames (with_times, preprocess.cpp:488-521)
+            it.sky = DevBuf(&c, sizeof(float) * plane_, "null static sky");
+            it.mask = DevBuf(&c, sizeof(float) * plane_, "null mask");
+            stage_run(c, *sc_, sub_.as<float>(), w, h, n, orders_[static_cast<size_t>(k)].data(), sp_,
+                      it.filt.as<float>(), it.sky.as<float>(), it.mask.as<float>(), nullptr, nullptr);
+            jobs.push_back(job(it.filt.as<float>(), orders_[static_cast<size_t>(k)], it.max.as<float>(), it.bv.as<int>()));
+        } else {
+            // an injection copy: raw frames + objects, prepared again with the same PSF width
+            const int j = k - runs_;
+            if (!sub2_) {
+                sub2_ = DevBuf(&c, sizeof(float) * plane_ * n, "copy sub frames");
+                copy_sky_ = DevBuf(&c, sizeof(float) * plane_, "copy static sky");
+                copy_mask_ = DevBuf(&c, sizeof(float) * plane_, "copy mask");
+                if (!raw_) raw_ = DevBuf(&c, sizeof(float) * plane_ * n, "raw frames");
+            }
+            FTB_CHECK(cudaMemcpyAsync(raw_.as<float>(), raw0_.as<float>(), sizeof(float) * plane_ * n,
+                                      cudaMemcpyDeviceToDevice, c.stream()));
+            apply_patches(c, injection_patches(copies[static_cast<size_t>(j)], o_.t_h, exp_sorted_, o_.fwhm_px, w, h),
+                          raw_.as<float>(), w, h, n);
+            it.background.resize(static_cast<size_t>(n));
+            it.sigma.resize(static_cast<size_t>(n));
+            prepare_sub(c, *sc_, raw_.as<float>(), sub2_.as<float>(), w, h, n, it.background.data());
+            stage_run(c, *sc_, sub2_.as<float>(), w, h, n, o_.t_h.data(), sp_, it.filt.as<float>(),
+                      copy_sky_.as<float>(), copy_mask_.as<float>(), it.sigma.data(), nullptr);
+            jobs.push_back(job(it.filt.as<float>(), o_.t_h, it.max.as<float>(), it.bv.as<int>()));
+        }
+        items_.emplace(k, std::move(it));
+    }
+    o_.adds += static_cast<double>(m_) * n * w * h * static_cast<double>(std::max(0, k1 - k0) + (add_real ? 1 : 0));
+}
+
+void SearchRequest::finish_items(int k0, int k1) {
+    Context& c = c_;
+    const int w = o_.w, h = o_.h, n = o_.n;
+    if (!real_done_) {
+        o_.peaks = device_peaks(c, max_.as<float>(), bv_.as<int>(), w, h, floor_, nms_, edge_);
+        order_peaks(o_.peaks, 100000);
+        real_done_ = true;
+    }
+    for (int k = k0; k < std::min(k1, runs_); ++k) {
+        Item& it = items_.at(k);
+        std::vector<Peak> npk = device_peaks(c, it.max.as<float>(), it.bv.as<int>(), w, h, 3.0f, nms_, edge_);
+        order_peaks(npk, 20000);
+        const size_t tested =
+            (p_.gauss_model && p_.null_tested > 0) ? std::min(npk.size(), static_cast<size_t>(p_.null_tested)) : 0;
+        const std::vector<char> art = device_artefacts(c, npk, tested, o_.grid, it.filt.as<float>(), sub_.as<float>(),
+                                                       it.sky.as<float>(), orders_[static_cast<size_t>(k)], w, h, n,
+                                                       o_.fwhm_px, p_.max_frame_fraction);
+        for (size_t q = 0; q < npk.size(); ++q)
+            if (q >= art.size() || !art[q]) pooled_.push_back(npk[q].snr);
+        items_.erase(k);  // the null run's buffers are released in stream order
+    }
+    for (int k = std::max(k0, runs_); k < k1; ++k) {  // copies keep only their maps
+        Item& it = items_.at(k);
+        it.filt.reset();
+    }
+}
+
+SearchOut SearchRequest::finalize(std::vector<SearchOut>* copies_out) {
+    Context& c = c_;
+    const int w = o_.w, h = o_.h, n = o_.n;
+    o_.thr = set_threshold(p_, pooled_, runs_, o_.fwhm_px, w, h, m_);
+    if (runs_ > 0 && auto_thr_) o_.null_peaks.assign(pooled_.begin(), pooled_.end());
+    for (const Peak& pk : o_.peaks)
+        if (pk.snr >= o_.thr.snr && pk.vidx >= 0) o_.selected.push_back(pk);
+    if (static_cast<int>(o_.selected.size()) > p_.max_candidates) o_.selected.resize(static_cast<size_t>(p_.max_candidates));
+    o_.max_snr.resize(static_cast<size_t>(w) * h);
+    o_.best_v.resize(static_cast<size_t>(w) * h);
+    FTB_CHECK(cudaMemcpyAsync(o_.max_snr.data(), max_.as<float>(), map_bytes_, cudaMemcpyDeviceToHost, c.stream()));
+    FTB_CHECK(cudaMemcpyAsync(o_.best_v.data(), bv_.as<int>(), map_bytes_, cudaMemcpyDeviceToHost, c.stream()));
+    if (copies_out) {
+        // the copies: peaks above the calibrated threshold, which they were searched with
+        copies_out->clear();
+        for (auto& kv : items_) {
+            if (kv.first < runs_) continue;
+            Item& it = kv.second;
+            SearchOut co;
+            co.w = w;
+            co.h = h;
+            co.n = n;
+            co.fwhm_px = o_.fwhm_px;
+            co.span_h = o_.span_h;
+            co.t_ref_mjd = o_.t_ref_mjd;
+            co.dv = o_.dv;
+            co.t_h = o_.t_h;
+            co.grid = o_.grid;
+            co.background = it.background;
+            co.sigma = it.sigma;
+            co.thr.snr = o_.thr.snr;
+            co.thr.method = "fixed";
+            co.adds = static_cast<double>(m_) * n * w * h;
+            co.peaks = device_peaks(c, it.max.as<float>(), it.bv.as<int>(), w, h, static_cast<float>(o_.thr.snr), nms_,
+                                    edge_);
+            order_peaks(co.peaks, 100000);
+            for (const Peak& pk : co.peaks)
+                if (pk.snr >= co.thr.snr && pk.vidx >= 0) co.selected.push_back(pk);
+            if (static_cast<int>(co.selected.size()) > p_.max_candidates)
+                co.selected.resize(static_cast<size_t>(p_.max_candidates));
+            co.max_snr.resize(static_cast<size_t>(w) * h);
+            co.best_v.resize(static_cast<size_t>(w) * h);
+            FTB_CHECK(cudaMemcpyAsync(co.max_snr.data(), it.max.as<float>(), map_bytes_, cudaMemcpyDeviceToHost,
+                                      c.stream()));
+            FTB_CHECK(cudaMemcpyAsync(co.best_v.data(), it.bv.as<int>(), map_bytes_, cudaMemcpyDeviceToHost,
+                                      c.stream()));
+            copies_out->push_back(std::move(co));
+        }
+    }
+    FTB_CHECK(cudaStreamSynchronize(c.stream()));
+    items_.clear();
+    return std::move(o_);
+}
 
 SearchOut search_host(Context& c, const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
                       const SearchParams& p, const Progress& progress, bool frames_on_device, int in_pitch) {
@@ -260,261 +505,32 @@ SearchOut search_batch_host(Context& c, const float* frames, int w, int h, int n
                             const Progress& progress, bool frames_on_device, int in_pitch) {
     c.bind();
     if (!copies.empty() && !exptime) throw std::runtime_error("injection copies need the exposure times");
-    if (n < 5) throw std::runtime_error("synthetic tracking needs at least 5 frames");
-    if (w < 16 || h < 16) throw std::runtime_error("frames are too small");
     auto report = [&](double f, const char* stage) {
         if (progress && !progress(f, stage)) throw Cancelled();
     };
-    SearchOut o;
-    o.w = w;
-    o.h = h;
-    o.n = n;
     c.timing_reset();
     const int total = c.span_begin("total");
-    const double t_setup = wall_seconds();
-    // frames in time order (the C API stable-sorts by mid-exposure, c_api.cpp:177-179)
-    std::vector<int> order(static_cast<size_t>(n));
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return mjd[a] < mjd[b]; });
-    double tmin = mjd[order[0]], tmax = tmin;
-    for (int i = 0; i < n; ++i) {
-        tmin = std::min(tmin, mjd[i]);
-        tmax = std::max(tmax, mjd[i]);
-    }
-    o.t_ref_mjd = 0.5 * (tmin + tmax);
-    o.span_h = (tmax - tmin) * 24.0;
-    if (o.span_h <= 0.0) throw std::runtime_error("frames must span a non-zero time interval");
-    for (int i = 0; i < n; ++i) o.t_h.push_back((mjd[order[static_cast<size_t>(i)]] - o.t_ref_mjd) * 24.0);
-
-    const int pitch = frame_pitch(w);
-    const size_t plane = static_cast<size_t>(pitch) * h;
-    float* d_raw = c.scratch(kRaw, sizeof(float) * plane * n, "raw frames").as<float>();
-    float* d_sub = c.scratch(kSub, sizeof(float) * plane * n, "background-subtracted frames").as<float>();
-    float* d_filt = c.scratch(kFiltReal, sizeof(float) * plane * n, "filtered frames").as<float>();
-    float* d_sky = c.scratch(kSkyReal, sizeof(float) * plane, "static sky").as<float>();
-    float* d_mask = c.scratch(kMaskReal, sizeof(float) * plane, "mask").as<float>();
-    float* d_max = c.scratch(kMaxMap, sizeof(float) * static_cast<size_t>(w) * h, "max_snr").as<float>();
-    int* d_bv = c.scratch(kBestMap, sizeof(int) * static_cast<size_t>(w) * h, "best_v").as<int>();
-    c.host_time("setup", wall_seconds() - t_setup);
-
-    const int up = c.span_begin(frames_on_device ? "copy in" : "upload");
-    const size_t in_plane = frames_on_device ? static_cast<size_t>(in_pitch) * h : static_cast<size_t>(w) * h;
-    for (int i = 0; i < n; ++i)
-        FTB_CHECK(cudaMemcpy2DAsync(d_raw + static_cast<size_t>(i) * plane, sizeof(float) * pitch,
-                                    frames + static_cast<size_t>(order[static_cast<size_t>(i)]) * in_plane,
-                                    sizeof(float) * (frames_on_device ? in_pitch : w), sizeof(float) * w,
-                                    static_cast<size_t>(h),
-                                    frames_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                    c.stream()));
-    c.span_end(up);
-    report(0.0, "background");
-    // the raw frames stay available for the injection copies
-    const int ncopies = static_cast<int>(copies.size());
-    DevBuf raw0, sub2, copy_sky, copy_mask;
-    std::vector<double> exp_sorted;
-    if (ncopies > 0) {
-        raw0 = DevBuf(&c, sizeof(float) * plane * n, "raw frames (copies)");
-        sub2 = DevBuf(&c, sizeof(float) * plane * n, "copy sub frames");
-        copy_sky = DevBuf(&c, sizeof(float) * plane, "copy static sky");
-        copy_mask = DevBuf(&c, sizeof(float) * plane, "copy mask");
-        FTB_CHECK(cudaMemcpyAsync(raw0.as<float>(), d_raw, sizeof(float) * plane * n, cudaMemcpyDeviceToDevice,
-                                  c.stream()));
-        for (int i = 0; i < n; ++i) exp_sorted.push_back(exptime[order[static_cast<size_t>(i)]]);
-    }
-
-    // prepare (preprocess.cpp:528-585)
-    const double fwhm_guess = p.fwhm_px > 0.0 ? p.fwhm_px : 20.0;  // sizes the sample buffers
-    StageScratch sc(c, w, h, n, std::max(fwhm_guess, 20.0));
-    o.background.resize(static_cast<size_t>(n));
-    prepare_sub(c, sc, d_raw, d_sub, w, h, n, o.background.data());
-    StageParams sp;
-    sp.static_exclude = p.static_exclude;
-    sp.clip_sigma = p.clip_sigma;
-    sp.cr_sigma = p.cr_sigma;
-    sp.mask_scatter = p.mask_scatter;
-    sp.weight_scatter = p.weight_scatter;
-    stage_noise(c, sc, d_sub, w, h, n, o.t_h.data(), p.static_exclude, d_sky);
-    o.sigma.resize(static_cast<size_t>(n));
-    stage_sigma_to_host(c, sc, n, o.sigma.data());
-    if (p.fwhm_px > 0.0) {
-        o.fwhm_px = p.fwhm_px;
-    } else {
-        std::vector<float> sky(static_cast<size_t>(w) * h);
-        FTB_CHECK(cudaMemcpy2DAsync(sky.data(), sizeof(float) * w, d_sky, sizeof(float) * pitch, sizeof(float) * w, h,
-                                    cudaMemcpyDeviceToHost, c.stream()));
-        FTB_CHECK(cudaStreamSynchronize(c.stream()));
-        o.fwhm_px = estimate_psf_fwhm(sky, w, h, o.sigma, p);
-    }
-    sp.fwhm_px = o.fwhm_px;
-    if (!sc.fits(w, h, n, sp.fwhm_px)) throw std::runtime_error("PSF too wide for the sample buffers");
-    stage_filter(c, sc, w, h, n, sp, d_filt, d_mask, nullptr, nullptr);
-    report(0.1, "prepared");
-
-    // search (search.cpp:716-785)
-    o.grid = velocity_grid(o.span_h, p, &o.dv);
-    const size_t m = o.grid.size();
-    const bool auto_thr = p.threshold_snr <= 0.0;
-    const int runs = auto_thr ? std::max(0, p.null_runs) : 0;
-    const double share = 0.9 / (1 + runs);
-    const int nms = std::max(2, static_cast<int>(std::lround(o.fwhm_px)));
-    const int edge = std::max(p.edge_px, 1);
-    const int min_count = pass_min_count(p.min_coverage, n);
-
-    // the real pass and the null runs (preprocessing rebuilt with permuted times
-    // on the same sub frames) as batches of passes, each batch stacked in one
-    // persistent launch; a batch holds as many null runs as the HBM budget allows
-    const std::vector<std::vector<double>> orders = null_time_orders(o.t_h, runs, p.seed);
-    const size_t map_bytes = sizeof(float) * static_cast<size_t>(w) * h;
-    const size_t per_null = sizeof(float) * (plane * n + 2 * plane) + 2 * map_bytes;
+    SearchRequest r(c, p, w, h, n);
+    r.prepare(frames, mjd, exptime, frames_on_device, in_pitch, !copies.empty(), report);
+    // the real pass, the null runs and the copies as batches, each batch stacked
+    // in persistent launches; a batch holds as many items as the HBM budget allows
+    const int items = r.runs() + static_cast<int>(copies.size());
     const size_t reserve = size_t{256} << 20;  // plans, peaks, descriptors
     const size_t avail = c.budget() > c.used() + reserve ? c.budget() - c.used() - reserve : 0;
-    const int per_batch = static_cast<int>(
-        std::max<size_t>(1, std::min<size_t>(std::max(runs + static_cast<int>(copies.size()), 1), avail / per_null)));
-    std::vector<float> pooled;
-    const float floor = static_cast<float>(auto_thr ? p.min_snr_floor : p.threshold_snr);
-    bool real_done = false;
-    // copies keep their maps to the end (their peaks need the calibrated threshold)
-    std::vector<DevBuf> copy_max(static_cast<size_t>(ncopies)), copy_bv(static_cast<size_t>(ncopies));
-    copies_out.assign(static_cast<size_t>(ncopies), SearchOut());
-    const int total_items = runs + ncopies;
-    for (int k0 = 0; k0 < std::max(total_items, 1); k0 += per_batch) {
-        const int k1 = std::min(runs, k0 + per_batch);
-        const int c0 = std::max(0, k0 - runs), c1 = std::max(0, std::min(total_items, k0 + per_batch) - runs);
-        struct NullBufs {
-            DevBuf filt, sky, mask, max, bv;
-        };
-        std::vector<NullBufs> nb(static_cast<size_t>(std::max(0, k1 - k0)));
-        std::vector<DevBuf> copy_filt(static_cast<size_t>(std::max(0, c1 - c0)));
+    const int per_batch =
+        static_cast<int>(std::max<size_t>(1, std::min<size_t>(std::max(items, 1), avail / r.item_bytes())));
+    const double share = 0.9 / (1 + items);
+    for (int k0 = 0; k0 < std::max(items, 1); k0 += per_batch) {
+        const int k1 = std::min(items, k0 + per_batch);
+        report(0.1 + 0.9 * share * (k0 + 1), "null");
         std::vector<PassJob> jobs;
-        if (!real_done) {
-            PassJob j;
-            j.d_frames = d_filt;
-            j.pitch = pitch;
-            j.w = w;
-            j.h = h;
-            j.n = n;
-            shift_table(o.t_h, o.grid, j.dx, j.dy);
-            j.m = static_cast<int>(m);
-            j.min_count = min_count;
-            j.d_max = d_max;
-            j.d_bv = d_bv;
-            jobs.push_back(std::move(j));
-        }
-        for (int k = k0; k < k1; ++k) {
-            NullBufs& b = nb[static_cast<size_t>(k - k0)];
-            b.filt = DevBuf(&c, sizeof(float) * plane * n, "null filtered frames");
-            b.sky = DevBuf(&c, sizeof(float) * plane, "null static sky");
-            b.mask = DevBuf(&c, sizeof(float) * plane, "null mask");
-            b.max = DevBuf(&c, map_bytes, "null max_snr");
-            b.bv = DevBuf(&c, map_bytes, "null best_v");
-            report(0.1 + 0.9 * share * (k + 1), "null");
-            stage_run(c, sc, d_sub, w, h, n, orders[static_cast<size_t>(k)].data(), sp, b.filt.as<float>(),
-                      b.sky.as<float>(), b.mask.as<float>(), nullptr, nullptr);
-            PassJob j;
-            j.d_frames = b.filt.as<float>();
-            j.pitch = pitch;
-            j.w = w;
-            j.h = h;
-            j.n = n;
-            shift_table(orders[static_cast<size_t>(k)], o.grid, j.dx, j.dy);
-            j.m = static_cast<int>(m);
-            j.min_count = min_count;
-            j.d_max = b.max.as<float>();
-            j.d_bv = b.bv.as<int>();
-            jobs.push_back(std::move(j));
-        }
-        for (int j = c0; j < c1; ++j) {
-            // the raw frames plus this copy's objects, prepared again (fixed PSF width)
-            DevBuf& f = copy_filt[static_cast<size_t>(j - c0)];
-            f = DevBuf(&c, sizeof(float) * plane * n, "copy filtered frames");
-            copy_max[static_cast<size_t>(j)] = DevBuf(&c, map_bytes, "copy max_snr");
-            copy_bv[static_cast<size_t>(j)] = DevBuf(&c, map_bytes, "copy best_v");
-            FTB_CHECK(cudaMemcpyAsync(d_raw, raw0.as<float>(), sizeof(float) * plane * n, cudaMemcpyDeviceToDevice,
-                                      c.stream()));
-            apply_patches(c, injection_patches(copies[static_cast<size_t>(j)], o.t_h, exp_sorted, o.fwhm_px, w, h),
-                          d_raw, w, h, n);
-            SearchOut& co = copies_out[static_cast<size_t>(j)];
-            co.background.resize(static_cast<size_t>(n));
-            prepare_sub(c, sc, d_raw, sub2.as<float>(), w, h, n, co.background.data());
-            co.sigma.resize(static_cast<size_t>(n));
-            stage_run(c, sc, sub2.as<float>(), w, h, n, o.t_h.data(), sp, f.as<float>(), copy_sky.as<float>(),
-                      copy_mask.as<float>(), co.sigma.data(), nullptr);
-            PassJob jb;
-            jb.d_frames = f.as<float>();
-            jb.pitch = pitch;
-            jb.w = w;
-            jb.h = h;
-            jb.n = n;
-            shift_table(o.t_h, o.grid, jb.dx, jb.dy);
-            jb.m = static_cast<int>(m);
-            jb.min_count = min_count;
-            jb.d_max = copy_max[static_cast<size_t>(j)].as<float>();
-            jb.d_bv = copy_bv[static_cast<size_t>(j)].as<int>();
-            jobs.push_back(std::move(jb));
-        }
+        r.stage_items(k0, k1, copies, jobs);
         stack_passes_device(c, jobs);
-        o.adds += static_cast<double>(m) * n * w * h * static_cast<double>(jobs.size());
-        report(0.1 + 0.9 * share * (k1 + 1), "null");
-        const int pk_span = c.span_begin("peaks");
-        if (!real_done) {
-            o.peaks = device_peaks(c, d_max, d_bv, w, h, floor, nms, edge);
-            order_peaks(o.peaks, 100000);
-            real_done = true;
-        }
-        for (int k = k0; k < k1; ++k) {
-            NullBufs& b = nb[static_cast<size_t>(k - k0)];
-            std::vector<Peak> npk = device_peaks(c, b.max.as<float>(), b.bv.as<int>(), w, h, 3.0f, nms, edge);
-            order_peaks(npk, 20000);
-            const size_t tested = (p.gauss_model && p.null_tested > 0)
-                                      ? std::min(npk.size(), static_cast<size_t>(p.null_tested))
-                                      : 0;
-            const std::vector<char> art =
-                device_artefacts(c, npk, tested, o.grid, b.filt.as<float>(), d_sub, b.sky.as<float>(),
-                                 orders[static_cast<size_t>(k)], w, h, n, o.fwhm_px, p.max_frame_fraction);
-            for (size_t q = 0; q < npk.size(); ++q)
-                if (q >= art.size() || !art[q]) pooled.push_back(npk[q].snr);
-        }
-        c.span_end(pk_span);
+        const int pk = c.span_begin("peaks");
+        r.finish_items(k0, k1);
+        c.span_end(pk);
     }
-    o.max_snr.resize(static_cast<size_t>(w) * h);
-    o.best_v.resize(static_cast<size_t>(w) * h);
-    FTB_CHECK(cudaMemcpyAsync(o.max_snr.data(), d_max, sizeof(float) * o.max_snr.size(), cudaMemcpyDeviceToHost,
-                              c.stream()));
-    FTB_CHECK(cudaMemcpyAsync(o.best_v.data(), d_bv, sizeof(int) * o.best_v.size(), cudaMemcpyDeviceToHost,
-                              c.stream()));
-    o.thr = set_threshold(p, pooled, runs, o.fwhm_px, w, h, m);
-    // the copies: peaks above the calibrated threshold, searched with it fixed
-    for (int j = 0; j < ncopies; ++j) {
-        SearchOut& co = copies_out[static_cast<size_t>(j)];
-        co.w = w;
-        co.h = h;
-        co.n = n;
-        co.fwhm_px = o.fwhm_px;
-        co.span_h = o.span_h;
-        co.t_ref_mjd = o.t_ref_mjd;
-        co.dv = o.dv;
-        co.t_h = o.t_h;
-        co.grid = o.grid;
-        co.thr.snr = o.thr.snr;
-        co.thr.method = "fixed";
-        co.adds = static_cast<double>(m) * n * w * h;
-        const float* dm = copy_max[static_cast<size_t>(j)].as<float>();
-        const int* db = copy_bv[static_cast<size_t>(j)].as<int>();
-        co.peaks = device_peaks(c, dm, db, w, h, static_cast<float>(o.thr.snr), nms, edge);
-        order_peaks(co.peaks, 100000);
-        for (const Peak& pk : co.peaks)
-            if (pk.snr >= co.thr.snr && pk.vidx >= 0) co.selected.push_back(pk);
-        if (static_cast<int>(co.selected.size()) > p.max_candidates)
-            co.selected.resize(static_cast<size_t>(p.max_candidates));
-        co.max_snr.resize(static_cast<size_t>(w) * h);
-        co.best_v.resize(static_cast<size_t>(w) * h);
-        FTB_CHECK(cudaMemcpyAsync(co.max_snr.data(), dm, map_bytes, cudaMemcpyDeviceToHost, c.stream()));
-        FTB_CHECK(cudaMemcpyAsync(co.best_v.data(), db, map_bytes, cudaMemcpyDeviceToHost, c.stream()));
-    }
-    if (runs > 0 && auto_thr) o.null_peaks.assign(pooled.begin(), pooled.end());
-    for (const Peak& pk : o.peaks)
-        if (pk.snr >= o.thr.snr && pk.vidx >= 0) o.selected.push_back(pk);
-    if (static_cast<int>(o.selected.size()) > p.max_candidates) o.selected.resize(static_cast<size_t>(p.max_candidates));
+    SearchOut o = r.finalize(&copies_out);
     c.span_end(total);
     FTB_CHECK(cudaStreamSynchronize(c.stream()));
     c.timing_resolve();

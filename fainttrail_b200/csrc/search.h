@@ -4,6 +4,9 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
+#include <map>
+#include <memory>
 #include <string>
 #include <utility>
 #include <vector>
@@ -100,6 +103,47 @@ struct SearchOut {
     std::vector<float> max_snr;          // real detection map
     std::vector<int> best_v;
     double adds = 0;                     // pixel x frame x motion additions of all passes
+};
+
+// One search request in phases, so that the passes of several searches (or of
+// one search's null runs and copies) can be stacked in shared launches:
+// prepare (upload, background, the real stage, grid, time orders), stage a range
+// of items (null runs first, then injection copies) appending their pass jobs
+// (the real pass with the first call), finish those items after the jobs ran
+// (peaks, artefact screen, pooling), finalize (threshold, copies' peaks, maps).
+class SearchRequest {
+public:
+    SearchRequest(Context& c, const SearchParams& p, int w, int h, int n);
+    void prepare(const float* frames, const double* mjd, const double* exptime, bool on_device, int in_pitch,
+                 bool keep_raw, const std::function<void(double, const char*)>& report);
+    int runs() const { return runs_; }
+    size_t item_bytes() const;                        // device bytes one null run or copy holds in flight
+    static size_t base_bytes(int w, int h, int n);    // device bytes of a prepared request
+    void stage_items(int k0, int k1, const std::vector<std::vector<Injection>>& copies, std::vector<PassJob>& jobs);
+    void finish_items(int k0, int k1);
+    SearchOut finalize(std::vector<SearchOut>* copies_out);
+
+private:
+    struct Item {
+        DevBuf filt, sky, mask, max, bv;
+        std::vector<double> background, sigma;
+    };
+    PassJob job(const float* frames, const std::vector<double>& t, float* d_max, int* d_bv) const;
+    Context& c_;
+    SearchParams p_;
+    SearchOut o_;
+    StageParams sp_;
+    int pitch_ = 0;
+    size_t plane_ = 0, map_bytes_ = 0, m_ = 0;
+    bool auto_thr_ = true, real_queued_ = false, real_done_ = false, raw_needed_ = false;
+    int runs_ = 0, nms_ = 2, edge_ = 1, min_count_ = 3;
+    float floor_ = 0;
+    std::vector<std::vector<double>> orders_;
+    std::vector<double> exp_sorted_;
+    std::vector<float> pooled_;
+    DevBuf raw_, raw0_, sub_, filt_, sky_, mask_, max_, bv_, sub2_, copy_sky_, copy_mask_;
+    std::unique_ptr<StageScratch> sc_;
+    std::map<int, Item> items_;
 };
 
 // frames: host (n x h x w) or, with frames_on_device, device rows of in_pitch

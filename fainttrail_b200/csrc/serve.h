@@ -1,0 +1,53 @@
+// The serving loop (serve.cu): a request queue, admission by the HBM budget,
+// and rounds in which all admitted requests' passes share persistent launches.
+#pragma once
+
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "engine.h"
+#include "search.h"
+
+namespace ftb {
+
+struct ServerStats {
+    long long completed = 0, rounds = 0;
+    double p50_s = 0, p99_s = 0, searches_per_s = 0, mean_batch = 0;
+};
+
+class Server {
+public:
+    Server(int device, double budget_bytes, int max_batch);
+    ~Server();
+    // copies the request; returns its id
+    long long submit(const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
+                     const SearchParams& p);
+    // 0: done (out filled), 3: not done yet, 1: failed or unknown id (err filled).
+    // wait_ms: 0 = do not wait, < 0 = wait until done.
+    int poll(long long id, int wait_ms, SearchOut* out, std::string* err);
+    void pause(bool paused);  // hold admission (requests queue up) or resume
+    ServerStats stats();
+
+private:
+    struct Req;
+    void loop();
+    void run_round(std::vector<std::shared_ptr<Req>>& round);
+    std::unique_ptr<Context> ctx_;
+    int max_batch_ = 16;
+    std::thread worker_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    bool stop_ = false, paused_ = false;
+    long long next_id_ = 0, rounds_ = 0, batched_ = 0;
+    std::deque<std::shared_ptr<Req>> queue_;
+    std::unordered_map<long long, std::shared_ptr<Req>> reqs_;
+    std::vector<double> latencies_;
+    double first_submit_ = 0, last_done_ = 0;
+};
+
+}  // namespace ftb

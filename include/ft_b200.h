@@ -22,6 +22,7 @@ extern "C" {
 #define FT_B200_OK 0
 #define FT_B200_ERROR 1
 #define FT_B200_CANCELLED 2
+#define FT_B200_PENDING 3 /* ft_b200_server_poll: the request is not finished yet */
 
 typedef struct ft_b200_ctx ft_b200_ctx;
 
@@ -201,6 +202,37 @@ int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap);
 int ft_b200_result_maps(const ft_b200_result* r, float* max_snr, int* best_v);
 /* The trial motion vidx of the grid (velocity_grid, search.cpp:39-58), px/hour. */
 int ft_b200_result_velocity(const ft_b200_result* r, int vidx, double* vx_pxh, double* vy_pxh);
+
+/* The serving loop. A server owns a device context and a worker thread; requests
+ * (frames of any count and size, any motion range) are copied on submission,
+ * admitted in arrival order as the HBM budget allows, and run in rounds: every
+ * admitted request is prepared, its null runs rebuilt, and the real and null
+ * passes of all of them are stacked together in shared persistent launches; a
+ * request that arrives during a round joins the next one. Each result equals
+ * ft_b200_search on the same request. This has no counterpart in the reference,
+ * which runs one search at a time (search.cpp:716). max_batch caps the requests
+ * per round. */
+typedef struct ft_b200_server ft_b200_server;
+
+int ft_b200_server_open(int device, double hbm_budget_bytes, int max_batch, ft_b200_server** out);
+/* Finishes the queued requests, then stops the worker. */
+void ft_b200_server_close(ft_b200_server* s);
+int ft_b200_server_submit(ft_b200_server* s, const float* frames, int width, int height, int nframes,
+                          const double* mjd, const double* exptime, const ft_b200_search_params* params,
+                          long long* request_id);
+/* FT_B200_OK with *out set when the request is done; FT_B200_PENDING if not done
+ * within wait_ms (0: do not wait, < 0: wait until done); FT_B200_ERROR if it
+ * failed or the id is unknown (message: ft_b200_server_error). A finished
+ * request is handed out once. */
+int ft_b200_server_poll(ft_b200_server* s, long long request_id, int wait_ms, ft_b200_result** out);
+const char* ft_b200_server_error(const ft_b200_server* s);
+/* Hold (1) or resume (0) admission; held requests queue up and start together. */
+int ft_b200_server_pause(ft_b200_server* s, int paused);
+/* Completed requests, their p50 / p99 latency (submit to done, seconds),
+ * throughput (completed / time from first submit to last completion), rounds
+ * and mean requests per round. */
+int ft_b200_server_stats(ft_b200_server* s, long long* completed, double* p50_s, double* p99_s,
+                         double* searches_per_s, long long* rounds, double* mean_batch);
 
 /* Kernels launched by the last call on the context (its stacking passes, stage,
  * peak and screening kernels). pixel_adds is reserved (left unchanged). */

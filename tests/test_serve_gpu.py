@@ -1,0 +1,88 @@
+"""The serving loop (ft_b200_server_*): requests of different sizes, frame
+counts and null-model settings, admitted together, share their stacking
+launches; each result must equal the same search run alone (ft_b200_search),
+which the search tests pin to the reference's search()."""
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests():
+    g = golden("search_small.npz")
+    raw, mjd, exp = g["raw"], g["mjd"], g["exptime"]
+    n = raw.shape[0]
+    rng = np.random.default_rng(5)
+    reqs = [
+        (raw, mjd, exp, dict(fwhm_px=2.5, null_runs=2)),
+        (raw[:, 8:, 4:].copy(), mjd, exp, dict(fwhm_px=2.5, null_runs=3)),
+        (raw[: n - 3], mjd[: n - 3], exp[: n - 3], dict(fwhm_px=0.0, null_runs=1)),
+        (raw, mjd, exp, dict(fwhm_px=2.5, threshold_snr=4.5)),
+        (raw[:, :, ::-1].copy(), mjd, exp, dict(fwhm_px=2.0, null_runs=2, seed=99)),
+        ((raw + rng.normal(0, 3, raw.shape)).astype(np.float32), mjd, exp, dict(fwhm_px=2.5, null_runs=2)),
+    ]
+    return reqs
+
+
+def _same(a, b):
+    assert a["threshold"] == b["threshold"] and a["method"] == b["method"]
+    assert a["fwhm"] == b["fwhm"] and a["n_velocities"] == b["n_velocities"]
+    assert np.array_equal(a["null_peaks"], b["null_peaks"])
+    assert np.array_equal(a["max_snr"], b["max_snr"], equal_nan=True)
+    assert np.array_equal(a["best_v"], b["best_v"])
+    assert a["peaks"] == b["peaks"] and a["selected"] == b["selected"]
+
+
+def test_server_batch_matches_standalone(device):
+    import fainttrail_b200 as ftb
+    reqs = _requests()
+    alone = [device.search(f, m, e, **kw) for f, m, e, kw in reqs]
+    srv = ftb.Server(0, 0.0, max_batch=16)
+    try:
+        srv.pause(True)
+        tickets = [None] * len(reqs)
+
+        def submit(k):
+            f, m, e, kw = reqs[k]
+            tickets[k] = srv.submit(f, m, e, **kw)
+        th = [threading.Thread(target=submit, args=(k,)) for k in range(len(reqs))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        assert srv.poll(tickets[0], wait_ms=0) is None  # held while paused
+        srv.pause(False)
+        got = [srv.poll(t) for t in tickets]
+        st = srv.stats()
+    finally:
+        srv.close()
+    for a, b in zip(got, alone):
+        _same(a, b)
+    assert st["completed"] == len(reqs) and st["rounds"] == 1 and st["mean_batch"] == len(reqs)
+    assert 0 < st["p50_s"] <= st["p99_s"]
+
+
+def test_server_streaming_and_errors(device):
+    import fainttrail_b200 as ftb
+    reqs = _requests()[:3]
+    alone = [device.search(f, m, e, **kw) for f, m, e, kw in reqs]
+    srv = ftb.Server(0, 0.0, max_batch=2)
+    try:
+        g = golden("search_small.npz")
+        bad = srv.submit(g["raw"][:3], g["mjd"][:3], g["exptime"][:3], fwhm_px=2.5)  # too few frames
+        tickets = [srv.submit(f, m, e, **kw) for f, m, e, kw in reqs]
+        got = [srv.poll(t) for t in tickets]
+        with pytest.raises(RuntimeError, match="frames"):
+            srv.poll(bad)
+        with pytest.raises(RuntimeError, match="unknown"):
+            srv.poll(tickets[0])  # a finished request is handed out once
+        st = srv.stats()
+    finally:
+        srv.close()
+    for a, b in zip(got, alone):
+        _same(a, b)
+    assert st["completed"] == 3 and st["rounds"] >= 2
