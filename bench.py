@@ -16,6 +16,17 @@ trial motions), 3 time-shuffled null runs (4 passes). Under torchrun each rank
 runs its own sequence (a different sky field, seed 7 + rank): weak scaling, no
 collective in the data path; the per-step device time is the maximum over ranks.
 
+--workload batched-2k: a step is one search of 30 x 2048^2 frames with 64
+time-shuffled null runs plus 16 injection-recovery copies of 50 objects each,
+all 81 passes batched into persistent launches (ft_b200_search_batch_dev); the
+same work with one pass per launch (passes_per_launch 1) is timed beside it.
+
+--workload serving: 40 seeded search requests of uneven frame count, image size,
+rate range and null runs arrive as a Poisson stream at 20 per second into the
+serving loop (ft_b200_server_*); reports throughput, served searches/s and
+p50 / p99 latency, beside the same requests run one after another through
+ft_b200_search under the same arrival times.
+
 --impl reference times the reference's own CPU implementation (FaintTrail
 0.9.1 built from its sources, oracle/_ref) on the host's cores with all
 threads, each step a bounded crop of the same workload (all frames, the full
@@ -113,6 +124,22 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
+def profiled_traffic(workload):
+    """DRAM bytes (read + write) per stack_batch_kernel launch for a workload, from
+    the committed ncu summary (a line `traffic_bytes_per_launch[<workload>] = N`)."""
+    import re
+    path = os.path.join(ROOT, "profiles", "stack_batch_kernel_fullframe-2k.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                mt = re.match(r"\s*traffic_bytes_per_launch\[(\S+)\]\s*=\s*([0-9.eE+]+)", line)
+                if mt and mt.group(1) == workload:
+                    return float(mt.group(2))
+    except OSError:
+        pass
+    return None
+
+
 def workload_desc(wl, m):
     return (f"{wl.name}: {wl.nframes} x {wl.width} x {wl.height} float32 frames, {wl.cadence_s:g} s cadence, "
             f"rates {wl.rate_px_min[0]:g}-{wl.rate_px_min[1]:g} px/min ({m} trial motions), "
@@ -188,21 +215,30 @@ def b200_arm(args):
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local_rank)
+    if args.workload == "serving":
+        return serving_arm(args, rank, local_rank, world, dist)
     wl = synthetic.WORKLOADS[args.workload]
     params = wl.search_params()
     frames, mjd, exptime, truth = synthetic.generate(wl, seed=7 + rank, device=f"cuda:{local_rank}")
     torch.cuda.synchronize()
     n, h, w = frames.shape
     dev = ftb.Device(local_rank)
+    copies = synthetic.injection_copies(wl, frames.shape, seed=11 + rank)
+    batched = len(copies) > 0
 
-    def step():
-        r = dev.search_dev(frames.data_ptr(), w, h, w, n, mjd, exptime, maps=False, **params)
+    def step(**over):
+        kw = dict(params, **over)
+        if batched:
+            r, _ = dev.search_batch_dev(frames.data_ptr(), w, h, w, n, mjd, exptime, copies, maps=False, **kw)
+        else:
+            r = dev.search_dev(frames.data_ptr(), w, h, w, n, mjd, exptime, maps=False, **kw)
         return r, dict(dev.timings()), dev.launches()
 
     for _ in range(max(3, args.warmup)):
         r, tm, _ = step()
     m = r["n_velocities"]
-    adds_step = float(m) * n * w * h * (1 + wl.null_runs)
+    passes = 1 + wl.null_runs + len(copies)
+    adds_step = float(m) * n * w * h * passes
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -230,7 +266,6 @@ def b200_arm(args):
     peaks, peak_kind = measured_peaks()
     sms = dev.info()[1]
     fp32_peak = sms * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12  # non-FMA adds, TFLOP/s
-    passes = 1 + wl.null_runs
     per_launch_adds = float(m) * n * w * h
     kernel_avg = sum(kernels) / (args.steps * passes)
     achieved = per_launch_adds / kernel_avg / 1e12
@@ -244,14 +279,17 @@ def b200_arm(args):
             gbs = b * passes * args.steps / stage[name] / 1e9
             stage_roof[name] = {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
                                 "bytes_per_launch": b}
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "stack_traffic.json")) as f:
-            tr = json.load(f)
-        if tr.get("workload") == args.workload:
-            traffic = tr["bytes_per_launch"]
-    except (OSError, ValueError, KeyError):
-        pass
+    traffic = profiled_traffic(args.workload)
+
+    # the same search with one pass per launch (the plain one-search-per-launch path)
+    plain = None
+    if batched:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, tmp, nlp = step(passes_per_launch=1)
+        plain = {"ms_per_step": 1000.0 * tmp["total"], "value": adds_step / tmp["total"], "unit": METRIC,
+                 "passes_per_launch": 1, "gpu_launches": nlp,
+                 "searches_per_s": passes / tmp["total"], "wall_s": time.perf_counter() - t0}
 
     # end to end through the C ABI with host buffers: pinned frames in, maps out
     e2e = None
@@ -259,13 +297,19 @@ def b200_arm(args):
         host = torch.empty((n, h, w), dtype=torch.float32, pin_memory=True)
         host.copy_(frames)
         host_np = host.numpy()
-        dev.search(host_np, mjd, exptime, maps=True, **params)  # first call allocates
+
+        def e2e_step():
+            if batched:
+                dev.search_batch(host_np, mjd, exptime, copies, maps=True, **params)
+            else:
+                dev.search(host_np, mjd, exptime, maps=True, **params)
+        e2e_step()  # first call allocates
         if dist:
             dist.barrier()
         walls = []
         for _ in range(args.e2e_steps):
             t0 = time.perf_counter()
-            dev.search(host_np, mjd, exptime, maps=True, **params)
+            e2e_step()
             walls.append(time.perf_counter() - t0)
         wall = sum(walls)
         if dist:
@@ -273,7 +317,7 @@ def b200_arm(args):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             wall = float(t.item())
         e2e = {"value": world * args.e2e_steps * adds_step / wall, "unit": METRIC,
-               "h2d_bytes_per_step": 4 * n * h * w, "d2h_bytes_per_step": 8 * h * w,
+               "h2d_bytes_per_step": 4 * n * h * w, "d2h_bytes_per_step": 8 * h * w * (1 + len(copies)),
                "ms_per_step": 1000.0 * wall / args.e2e_steps}
         del host, host_np
 
@@ -297,7 +341,7 @@ def b200_arm(args):
                           "l2": f"inputs ({4 * n * h * w / 1e9:.1f} GB of frames) exceed the {L2_BYTES >> 20} MB L2"},
                "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                             "frac": achieved / fp32_peak, "traffic": traffic,
-                            "kernel": "stack_kernel (one launch per pass)",
+                            "kernel": "stack_batch_kernel (one persistent launch for all passes of a search)",
                             "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x sm_max_mhz "
                                            f"{peaks.get('sm_max_mhz', 1965.0):g} MHz ({peak_kind} peaks file has no "
                                            f"FP32 figure); adds are non-FMA, one per lane per clock"},
@@ -305,8 +349,124 @@ def b200_arm(args):
                "stage_seconds_per_step": {k: v / args.steps for k, v in stage.items()},
                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
                "threshold_snr": r["threshold"], "threshold_method": r["method"]}
+        if batched:
+            out["config"]["batch"] = (f"{wl.null_runs} null runs + {len(copies)} injection copies x "
+                                      f"{len(copies[0])} objects (S/N {wl.snr[0]:g}-{wl.snr[1]:g}); "
+                                      f"{passes} passes per step")
+            out["searches_per_s"] = passes * args.steps / total
+            out["plain"] = plain
+            out["speedup_vs_plain"] = plain["ms_per_step"] / out["ms_per_step"]
         print(json.dumps(out), flush=True)
     dev.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def result_digest(r):
+    """threshold, peaks and a hash of both maps: equal digests = equal results"""
+    import hashlib
+    hs = hashlib.sha256()
+    for a in (r["max_snr"], r["best_v"], r["null_peaks"]):
+        hs.update(np.ascontiguousarray(a).tobytes())
+    return (r["threshold"], r["method"], tuple(r["peaks"]), hs.hexdigest())
+
+
+def serving_arm(args, rank, local_rank, world, dist):
+    """The serving loop under a Poisson stream of uneven requests, beside the same
+    requests run one after another (first come, first served) through ft_b200_search."""
+    import torch
+    import fainttrail_b200 as ftb
+    from fainttrail_b200 import synthetic
+    reqs = synthetic.serving_requests(count=40, rate_per_s=20.0, seed=2024 + rank)
+    inputs = []
+    for k, (t_arr, wl) in enumerate(reqs):
+        f, mjd, exptime, _ = synthetic.generate(wl, seed=100 + k, device=f"cuda:{local_rank}")
+        inputs.append((t_arr, wl, f.cpu().numpy(), mjd, exptime))
+        del f
+    torch.cuda.synchronize()
+    dev = ftb.Device(local_rank)
+    # warm-up, then the plain sequential pass: each request alone, in arrival
+    # order; its latency under the same arrival times follows from the measured
+    # service times (one server, first come first served)
+    for t_arr, wl, f, mjd, exptime in inputs[:3]:
+        dev.search(f, mjd, exptime, maps=True, **wl.search_params())
+    service, alone, adds = [], [], []
+    for t_arr, wl, f, mjd, exptime in inputs:
+        t0 = time.perf_counter()
+        r = dev.search(f, mjd, exptime, maps=True, **wl.search_params())
+        service.append(time.perf_counter() - t0)
+        alone.append(result_digest(r))
+        n, h, w = f.shape
+        adds.append(float(r["n_velocities"]) * n * w * h * (1 + wl.null_runs))
+    dev.close()
+    finish, lat = 0.0, []
+    for (t_arr, *_), sv in zip(inputs, service):
+        finish = max(finish, t_arr) + sv
+        lat.append(finish - t_arr)
+    plain_makespan = finish  # from the stream's start, as the served run
+    srv = ftb.Server(local_rank, 0.0, max_batch=16)
+    tk = [srv.submit(f, mjd, exptime, **wl.search_params()) for _, wl, f, mjd, exptime in inputs[:3]]
+    for t in tk:  # warm-up round on the server's own context
+        srv.poll(t)
+    srv.close()
+    srv = ftb.Server(local_rank, 0.0, max_batch=16)
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    tickets = [None] * len(inputs)
+    t_start = time.perf_counter()
+
+    def submitter():
+        for k, (t_arr, wl, f, mjd, exptime) in enumerate(inputs):
+            d = t_arr - (time.perf_counter() - t_start)
+            if d > 0:
+                time.sleep(d)
+            tickets[k] = srv.submit(f, mjd, exptime, **wl.search_params())
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    results = [result_digest(srv.poll(t, maps=True)) for t in tickets]
+    t_end = time.perf_counter()
+    st = srv.stats()
+    srv.close()
+    clk = clocks.stop()
+    makespan = t_end - t_start
+    if dist:
+        t = torch.tensor([makespan], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        makespan = float(t.item())
+    total_adds = sum(adds)
+    h2d = sum(4 * f.size for _, _, f, _, _ in inputs)
+    d2h = sum(8 * f.shape[1] * f.shape[2] for _, _, f, _, _ in inputs)
+    lat_sorted = sorted(lat)
+
+    def pct(v, q):
+        k = max(1, int(np.ceil(q * len(v))))
+        return v[min(len(v), k) - 1]
+    if rank == 0:
+        out = {"metric": METRIC, "value": world * total_adds / makespan, "unit": METRIC, "n_gpus": world,
+               "steps": 1, "warmup": 3, "ms_per_step": 1000.0 * makespan, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded requests; sky/read/photon noise, stars, movers)",
+               "config": {"workload": (f"serving: {len(inputs)} requests, Poisson arrivals at 20/s, frames "
+                                       f"{min(i[1].nframes for i in inputs)}-{max(i[1].nframes for i in inputs)}, "
+                                       f"sizes up to {max(i[1].width for i in inputs)} x "
+                                       f"{max(i[1].height for i in inputs)}, rates 0.1-3 px/min, 8-32 null runs, "
+                                       f"each request at most 2e12 pixel-frame-motion adds"),
+                          "parallelism": f"independent request streams x{world}", "max_batch": 16},
+               "searches_per_s": world * len(inputs) / makespan,
+               "p50_s": st["p50_s"], "p99_s": st["p99_s"], "rounds": st["rounds"], "mean_batch": st["mean_batch"],
+               "plain": {"value": total_adds / plain_makespan, "unit": METRIC,
+                         "searches_per_s": len(inputs) / plain_makespan, "p50_s": pct(lat_sorted, 0.5),
+                         "p99_s": pct(lat_sorted, 0.99), "service_s_sum": sum(service),
+                         "path": "ft_b200_search per request, in arrival order"},
+               "speedup_vs_plain": plain_makespan / makespan,
+               "e2e": {"value": world * total_adds / makespan, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                       "d2h_bytes_per_step": d2h},
+               "clocks": clk, "completed": st["completed"], "gpu_launches": st["launches"],
+               "bit_identical_to_alone": sum(a == b for a, b in zip(results, alone))}
+        print(json.dumps(out), flush=True)
     if dist:
         dist.destroy_process_group()
 

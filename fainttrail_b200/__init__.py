@@ -42,7 +42,8 @@ class SearchParams(C.Structure):
         "weight_scatter", "min_coverage", "threshold_snr", "min_snr_floor", "target_false_per_run",
         "max_frame_fraction", "half_tolerance")] + [
         ("static_exclude", C.c_int), ("null_runs", C.c_int), ("max_candidates", C.c_int), ("edge_px", C.c_int),
-        ("threads", C.c_int), ("seed", C.c_ulonglong), ("null_tested", C.c_int), ("null_model_gauss", C.c_int)]
+        ("threads", C.c_int), ("seed", C.c_ulonglong), ("null_tested", C.c_int), ("null_model_gauss", C.c_int),
+        ("passes_per_launch", C.c_int)]
 
 
 class Injection(C.Structure):
@@ -95,6 +96,9 @@ def _declare(L):
     L.ft_b200_search_batch.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
                                        C.POINTER(SearchParams), C.c_int, C.c_void_p, C.c_void_p, PROGRESS_FN,
                                        C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p]
+    L.ft_b200_search_batch_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
+                                           C.POINTER(SearchParams), C.c_int, C.c_void_p, C.c_void_p,
+                                           C.POINTER(C.c_void_p), C.c_void_p]
     L.ft_b200_result_free.argtypes = [C.c_void_p]
     L.ft_b200_result_threshold.argtypes = [C.c_void_p, C.c_char_p, C.c_int] + [C.POINTER(C.c_double)] * 4
     L.ft_b200_result_threshold.restype = C.c_double
@@ -118,7 +122,7 @@ def _declare_server(L):
     L.ft_b200_server_pause.argtypes = [C.c_void_p, C.c_int]
     L.ft_b200_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double),
                                        C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_longlong),
-                                       C.POINTER(C.c_double)]
+                                       C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
 
 
 FT_B200_PENDING = 3
@@ -162,12 +166,12 @@ class Server:
         self.L.ft_b200_server_pause(self.h, 1 if paused else 0)
 
     def stats(self):
-        c, r = C.c_longlong(), C.c_longlong()
+        c, r, nl = C.c_longlong(), C.c_longlong(), C.c_longlong()
         p50, p99, sps, mb = C.c_double(), C.c_double(), C.c_double(), C.c_double()
         self.L.ft_b200_server_stats(self.h, C.byref(c), C.byref(p50), C.byref(p99), C.byref(sps), C.byref(r),
-                                    C.byref(mb))
+                                    C.byref(mb), C.byref(nl))
         return dict(completed=c.value, p50_s=p50.value, p99_s=p99.value, searches_per_s=sps.value, rounds=r.value,
-                    mean_batch=mb.value)
+                    mean_batch=mb.value, launches=nl.value)
 
     def close(self):
         if getattr(self, "h", None):
@@ -309,6 +313,22 @@ class Device:
         self.check(rc, "search_batch")
         res = self._result(base, w, h, maps)
         return res, [self._result(C.c_void_p(outs[k]), w, h, maps) for k in range(len(copies))]
+
+    def search_batch_dev(self, d_frames, width, height, pitch, nframes, mjd, exptime, copies, maps=True, **kw):
+        """ft_b200_search_batch_dev: search_batch over frames in device memory."""
+        p = self._search_params(self.L, kw)
+        counts = (C.c_int * max(1, len(copies)))(*[len(c) for c in copies])
+        flat = [o for c in copies for o in c]
+        objs = (Injection * max(1, len(flat)))(*[Injection(*o) for o in flat])
+        base = C.c_void_p()
+        outs = (C.c_void_p * max(1, len(copies)))()
+        rc = self.L.ft_b200_search_batch_dev(self.h, C.c_void_p(d_frames), width, height, pitch, nframes,
+                                             np.ascontiguousarray(mjd, dtype=np.float64),
+                                             np.ascontiguousarray(exptime, dtype=np.float64), C.byref(p),
+                                             len(copies), counts, objs, C.byref(base), outs)
+        self.check(rc, "search_batch_dev")
+        res = self._result(base, width, height, maps)
+        return res, [self._result(C.c_void_p(outs[k]), width, height, maps) for k in range(len(copies))]
 
     def _result(self, r, w, h, maps):
         L = self.L

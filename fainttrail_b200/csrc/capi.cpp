@@ -210,6 +210,7 @@ void ft_b200_search_params_default(ft_b200_search_params* p) {
     p->seed = d.seed;
     p->null_tested = d.null_tested;
     p->null_model_gauss = d.gauss_model ? 1 : 0;
+    p->passes_per_launch = d.passes_per_launch;
 }
 
 namespace {
@@ -237,6 +238,7 @@ ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
     p.max_candidates = q.max_candidates;
     p.edge_px = q.edge_px;
     p.gauss_model = q.null_model_gauss != 0;
+    p.passes_per_launch = std::max(0, q.passes_per_launch);
     p.seed = q.seed;
     return p;
 }
@@ -255,16 +257,19 @@ int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height,
     });
 }
 
-int ft_b200_search_batch(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes,
-                         const double* mjd, const double* exptime, const ft_b200_search_params* params, int copies,
-                         const int* objects_per_copy, const ft_b200_injection* objects, ft_b200_progress_fn progress,
-                         void* user, ft_b200_result** base, ft_b200_result** copy_results) {
+namespace {
+int search_batch_common(ft_b200_ctx* ctx, const float* frames, bool on_device, int pitch, int width, int height,
+                        int nframes, const double* mjd, const double* exptime, const ft_b200_search_params* params,
+                        int copies, const int* objects_per_copy, const ft_b200_injection* objects,
+                        ft_b200_progress_fn progress, void* user, ft_b200_result** base,
+                        ft_b200_result** copy_results) {
     if (base) *base = nullptr;
     for (int k = 0; copy_results && k < copies; ++k) copy_results[k] = nullptr;
     return guarded(ctx, [&](ftb::Context& c) {
         if (!frames || !mjd || !exptime || !base) throw std::runtime_error("search: missing frames, times or result");
         if (copies < 0 || (copies > 0 && (!objects_per_copy || !objects || !copy_results)))
             throw std::runtime_error("search: malformed injection copies");
+        if (on_device && pitch < width) throw std::runtime_error("search: row pitch below the width");
         std::vector<std::vector<ftb::Injection>> sets(static_cast<size_t>(copies));
         size_t at = 0;
         for (int k = 0; k < copies; ++k) {
@@ -276,7 +281,7 @@ int ft_b200_search_batch(ft_b200_ctx* ctx, const float* frames, int width, int h
         std::vector<ftb::SearchOut> outs;
         auto r = std::make_unique<ft_b200_result>();
         r->o = ftb::search_batch_host(c, frames, width, height, nframes, mjd, exptime, to_search_params(params), sets,
-                                      outs, wrap(progress, user));
+                                      outs, wrap(progress, user), on_device, on_device ? pitch : width);
         std::vector<std::unique_ptr<ft_b200_result>> rs;
         for (auto& o : outs) {
             rs.push_back(std::make_unique<ft_b200_result>());
@@ -285,6 +290,23 @@ int ft_b200_search_batch(ft_b200_ctx* ctx, const float* frames, int width, int h
         *base = r.release();
         for (int k = 0; k < copies; ++k) copy_results[k] = rs[static_cast<size_t>(k)].release();
     });
+}
+}  // namespace
+
+int ft_b200_search_batch(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes,
+                         const double* mjd, const double* exptime, const ft_b200_search_params* params, int copies,
+                         const int* objects_per_copy, const ft_b200_injection* objects, ft_b200_progress_fn progress,
+                         void* user, ft_b200_result** base, ft_b200_result** copy_results) {
+    return search_batch_common(ctx, frames, false, width, width, height, nframes, mjd, exptime, params, copies,
+                               objects_per_copy, objects, progress, user, base, copy_results);
+}
+
+int ft_b200_search_batch_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
+                             const double* mjd, const double* exptime, const ft_b200_search_params* params,
+                             int copies, const int* objects_per_copy, const ft_b200_injection* objects,
+                             ft_b200_result** base, ft_b200_result** copy_results) {
+    return search_batch_common(ctx, d_frames, true, pitch, width, height, nframes, mjd, exptime, params, copies,
+                               objects_per_copy, objects, nullptr, nullptr, base, copy_results);
 }
 
 int ft_b200_search_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
@@ -354,7 +376,7 @@ int ft_b200_server_pause(ft_b200_server* s, int paused) {
 }
 
 int ft_b200_server_stats(ft_b200_server* s, long long* completed, double* p50_s, double* p99_s,
-                         double* searches_per_s, long long* rounds, double* mean_batch) {
+                         double* searches_per_s, long long* rounds, double* mean_batch, long long* launches) {
     if (!s) return FT_B200_ERROR;
     const ftb::ServerStats st = s->s->stats();
     if (completed) *completed = st.completed;
@@ -363,6 +385,7 @@ int ft_b200_server_stats(ft_b200_server* s, long long* completed, double* p50_s,
     if (searches_per_s) *searches_per_s = st.searches_per_s;
     if (rounds) *rounds = st.rounds;
     if (mean_batch) *mean_batch = st.mean_batch;
+    if (launches) *launches = st.launches;
     return FT_B200_OK;
 }
 

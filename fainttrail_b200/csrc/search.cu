@@ -517,11 +517,16 @@ SearchOut search_batch_host(Context& c, const float* frames, int w, int h, int n
     const int items = r.runs() + static_cast<int>(copies.size());
     const size_t reserve = size_t{256} << 20;  // plans, peaks, descriptors
     const size_t avail = c.budget() > c.used() + reserve ? c.budget() - c.used() - reserve : 0;
-    const int per_batch =
+    int per_batch =
         static_cast<int>(std::max<size_t>(1, std::min<size_t>(std::max(items, 1), avail / r.item_bytes())));
+    // a launch cap: the real pass goes alone first, then at most k items per launch
+    const bool capped = p.passes_per_launch > 0 && items > 0;
+    if (capped) per_batch = std::min(per_batch, p.passes_per_launch);
+    std::vector<std::pair<int, int>> batches;
+    if (capped) batches.emplace_back(0, 0);
+    for (int k0 = 0; k0 < std::max(items, 1); k0 += per_batch) batches.emplace_back(k0, std::min(items, k0 + per_batch));
     const double share = 0.9 / (1 + items);
-    for (int k0 = 0; k0 < std::max(items, 1); k0 += per_batch) {
-        const int k1 = std::min(items, k0 + per_batch);
+    for (const auto& [k0, k1] : batches) {
         report(0.1 + 0.9 * share * (k0 + 1), "null");
         std::vector<PassJob> jobs;
         r.stage_items(k0, k1, copies, jobs);

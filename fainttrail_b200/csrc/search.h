@@ -24,6 +24,7 @@ struct SearchParams {
     double max_frame_fraction = 0.25;
     int static_exclude = -1, null_runs = 3, null_tested = 3000, max_candidates = 300, edge_px = 4;
     bool gauss_model = true;  // null_model "gauss" (else "linear")
+    int passes_per_launch = 0;  // 0: as many as fit; k: at most k per launch
     uint64_t seed = 12345;
 };
 

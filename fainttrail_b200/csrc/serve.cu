@@ -129,6 +129,7 @@ ServerStats Server::stats() {
         s.searches_per_s = last_done_ > first_submit_ ? s.completed / (last_done_ - first_submit_) : 0.0;
     }
     s.rounds = rounds_;
+    s.launches = launches_;
     s.mean_batch = rounds_ ? static_cast<double>(batched_) / rounds_ : 0.0;
     return s;
 }
@@ -165,6 +166,7 @@ void Server::loop() {
                 if (r->error.empty()) latencies_.push_back(r->t_done - r->t_submit);
             }
             last_done_ = t;
+            launches_ += ctx_->launches;
             ++rounds_;
             batched_ += static_cast<long long>(round.size());
         }

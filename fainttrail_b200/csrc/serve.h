@@ -16,7 +16,7 @@
 namespace ftb {
 
 struct ServerStats {
-    long long completed = 0, rounds = 0;
+    long long completed = 0, rounds = 0, launches = 0;
     double p50_s = 0, p99_s = 0, searches_per_s = 0, mean_batch = 0;
 };
 
@@ -43,7 +43,7 @@ private:
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;
     bool stop_ = false, paused_ = false;
-    long long next_id_ = 0, rounds_ = 0, batched_ = 0;
+    long long next_id_ = 0, rounds_ = 0, batched_ = 0, launches_ = 0;
     std::deque<std::shared_ptr<Req>> queue_;
     std::unordered_map<long long, std::shared_ptr<Req>> reqs_;
     std::vector<double> latencies_;

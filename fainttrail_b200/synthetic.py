@@ -116,3 +116,65 @@ def generate(wl, seed=7, device="cuda"):
                 t = t_h[i] - half + (k + 0.5) / steps * 2 * half
                 _add_gauss(f, m["x"] + m["vx"] * t, m["y"] + m["vy"] * t, m["flux"] / steps, sigma, torch)
     return frames, mjd, exptime, truth
+
+
+def injection_copies(wl, frames_shape, seed=11):
+    """The injection-recovery copies of a batched workload: `injection_copies`
+    sets of `injected_movers` objects (x_ref, y_ref, vx_pxh, vy_pxh, flux) at a
+    stack S/N drawn from wl.snr, rates from wl.rate_px_min, uniform PA, placed
+    24 px inside the frame, flux by the flux_for_snr rule."""
+    n, h, w = frames_shape
+    rng = np.random.default_rng(seed)
+    pix_sigma = math.sqrt(wl.sky_adu + wl.read_noise ** 2)
+    copies = []
+    for _ in range(int(wl.extra.get("injection_copies", 0))):
+        objs = []
+        for _ in range(int(wl.extra.get("injected_movers", 0))):
+            snr = rng.uniform(*wl.snr)
+            rate = rng.uniform(*wl.rate_px_min) * 60.0
+            pa = rng.uniform(0, 2 * math.pi)
+            objs.append((rng.uniform(24, w - 24), rng.uniform(24, h - 24), rate * math.cos(pa), rate * math.sin(pa),
+                         flux_for_snr(snr, pix_sigma, wl.fwhm_px, n)))
+        copies.append(objs)
+    return copies
+
+
+def motion_count(span_h, vmin_pxh, vmax_pxh, grid_tol_px):
+    """Trial motions of the square velocity lattice inside the annulus (the
+    velocity_grid rule, counted exactly)."""
+    dv = 4.0 * max(0.05, grid_tol_px) / span_h
+    k = int(math.ceil((vmax_pxh + 0.5 * dv) / dv))
+    lo, hi = (vmin_pxh - 0.5 * dv) ** 2, (vmax_pxh + 0.5 * dv) ** 2
+    i = np.arange(-k, k + 1) * dv
+    r2 = i[:, None] ** 2 + i[None, :] ** 2
+    return int(np.count_nonzero((r2 >= lo) & (r2 <= hi)))
+
+
+def serving_requests(count=40, rate_per_s=20.0, seed=2024, max_adds=2.0e12, max_frame_bytes=1 << 30):
+    """A seeded stream of search requests: Poisson arrivals at rate_per_s; frame
+    counts 8-120, sizes from 512 x 512 to 6000 x 4000, rate ranges inside
+    0.1-3 px/min, 8-32 null runs, 30 s cadence. Draws whose work (motions x
+    frames x pixels x passes) exceeds max_adds, or whose frames exceed
+    max_frame_bytes, are drawn again, which keeps the request mix servable on one
+    GPU (the unbounded mix reaches 1e17 adds for one request). Returns a list of
+    (arrival_s, Workload)."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while len(out) < count:
+        n = int(rng.integers(8, 121))
+        w = int(rng.integers(512, 6001)) // 16 * 16
+        h = int(rng.integers(512, 4001)) // 16 * 16
+        lo = float(rng.uniform(0.1, 2.5))
+        hi = float(rng.uniform(lo + 0.2, 3.0))
+        runs = int(rng.integers(8, 33))
+        if 4.0 * n * w * h > max_frame_bytes:
+            continue
+        span_h = (n - 1) * 30.0 / 3600.0
+        m = motion_count(span_h, lo * 60.0, hi * 60.0, 0.125)
+        if float(m) * n * w * h * (1 + runs) > max_adds:
+            continue
+        t += float(rng.exponential(1.0 / rate_per_s))
+        k = len(out)
+        out.append((t, Workload(f"serve-{k}", w, h, n, 30.0, 30.0, max(20, w * h // 20000), 3, (5.0, 10.0),
+                                (lo, hi), runs)))
+    return out

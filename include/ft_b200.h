@@ -131,6 +131,9 @@ typedef struct ft_b200_search_params {
     unsigned long long seed;
     int null_tested;      /* strongest null peaks per run screened for artefacts (3000) */
     int null_model_gauss; /* 1: "gauss" tail model (default), 0: "linear" */
+    int passes_per_launch; /* 0 (default): every pass that fits the HBM budget in one
+                              persistent launch; k > 0: at most k passes per launch,
+                              the real pass alone first (1 = one pass per launch) */
 } ft_b200_search_params;
 
 void ft_b200_search_params_default(ft_b200_search_params* p);
@@ -184,6 +187,12 @@ int ft_b200_search_batch(ft_b200_ctx* ctx, const float* frames, int width, int h
                          const double* mjd, const double* exptime, const ft_b200_search_params* params, int copies,
                          const int* objects_per_copy, const ft_b200_injection* objects, ft_b200_progress_fn progress,
                          void* user, ft_b200_result** base, ft_b200_result** copy_results);
+/* The same over frames already in device memory (nframes x height rows of
+ * `pitch` floats, read only), as ft_b200_search_dev. Synchronous. */
+int ft_b200_search_batch_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
+                             const double* mjd, const double* exptime, const ft_b200_search_params* params,
+                             int copies, const int* objects_per_copy, const ft_b200_injection* objects,
+                             ft_b200_result** base, ft_b200_result** copy_results);
 /* threshold_snr and the tail model (SearchResult, search.hpp:163-172); method
  * receives "fixed", "null-fit gauss", "null-fit linear", "null-quantile" or
  * "gaussian". Any pointer may be NULL. */
@@ -229,10 +238,10 @@ const char* ft_b200_server_error(const ft_b200_server* s);
 /* Hold (1) or resume (0) admission; held requests queue up and start together. */
 int ft_b200_server_pause(ft_b200_server* s, int paused);
 /* Completed requests, their p50 / p99 latency (submit to done, seconds),
- * throughput (completed / time from first submit to last completion), rounds
- * and mean requests per round. */
+ * throughput (completed / time from first submit to last completion), rounds,
+ * mean requests per round and kernels launched. */
 int ft_b200_server_stats(ft_b200_server* s, long long* completed, double* p50_s, double* p99_s,
-                         double* searches_per_s, long long* rounds, double* mean_batch);
+                         double* searches_per_s, long long* rounds, double* mean_batch, long long* launches);
 
 /* Kernels launched by the last call on the context (its stacking passes, stage,
  * peak and screening kernels). pixel_adds is reserved (left unchanged). */

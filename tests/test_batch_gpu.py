@@ -38,3 +38,28 @@ def test_copies_match_reference_inject_and_search(device, reference, oracle):
         assert same(got["max_snr"], want["max_snr"])
         px, py, ps, pv = oracle.find_peaks(got["max_snr"], got["best_v"], np.float32(ref["threshold"]), 2, 4, 100000)
         assert got["peaks"] == [(int(a), int(b), float(c), int(d)) for a, b, c, d in zip(px, py, ps, pv)]
+
+
+def test_launch_cap_and_device_frames(device):
+    """One pass per launch (passes_per_launch 1, the plain path) and the batch
+    over device-resident frames give the same results as the batched host call."""
+    import torch
+    from conftest import golden
+    g = golden("search_small.npz")
+    raw, mjd, exp = g["raw"], g["mjd"], g["exptime"]
+    n, h, w = raw.shape
+    copies = [[(30.0, 40.0, 20.0, -9.0, 900.0)], [(50.5, 20.25, -11.0, 15.0, 1200.0), (20.0, 20.0, 5.0, 5.0, 700.0)]]
+    kw = dict(fwhm_px=2.5, null_runs=3)
+    base, outs = device.search_batch(raw, mjd, exp, copies, **kw)
+    base1, outs1 = device.search_batch(raw, mjd, exp, copies, passes_per_launch=1, **kw)
+    base2, outs2 = device.search_batch(raw, mjd, exp, copies, passes_per_launch=2, **kw)
+    d = torch.from_numpy(np.ascontiguousarray(raw)).cuda()
+    base3, outs3 = device.search_batch_dev(d.data_ptr(), w, h, w, n, mjd, exp, copies, **kw)
+    for b, o in ((base1, outs1), (base2, outs2), (base3, outs3)):
+        assert b["threshold"] == base["threshold"] and same(b["null_peaks"], base["null_peaks"])
+        assert same(b["max_snr"], base["max_snr"]) and same(b["best_v"], base["best_v"])
+        assert b["peaks"] == base["peaks"]
+        for x, y in zip(o, outs):
+            assert same(x["max_snr"], y["max_snr"]) and x["peaks"] == y["peaks"]
+    one = device.search(raw, mjd, exp, passes_per_launch=1, **kw)
+    assert one["threshold"] == base["threshold"] and same(one["max_snr"], base["max_snr"])
