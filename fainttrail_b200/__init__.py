@@ -43,7 +43,7 @@ class SearchParams(C.Structure):
         "max_frame_fraction", "half_tolerance")] + [
         ("static_exclude", C.c_int), ("null_runs", C.c_int), ("max_candidates", C.c_int), ("edge_px", C.c_int),
         ("threads", C.c_int), ("seed", C.c_ulonglong), ("null_tested", C.c_int), ("null_model_gauss", C.c_int),
-        ("passes_per_launch", C.c_int)]
+        ("passes_per_launch", C.c_int), ("shard_index", C.c_int), ("shard_count", C.c_int)]
 
 
 class Injection(C.Structure):
@@ -183,6 +183,28 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def null_threshold(pooled, runs, psf_fwhm_px, width, height, motions, **kw):
+    """ft_b200_null_threshold: the null-tail threshold from pooled null-peak S/N
+    values (host only; no GPU), with the search's PSF width (a result's "fwhm")
+    and search parameters **kw. Returns a dict like a search result's threshold
+    fields."""
+    L = lib()
+    L.ft_b200_null_threshold.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(SearchParams), C.POINTER(C.c_double), C.c_char_p, C.c_int,
+                                         C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double)]
+    p = Device._search_params(L, kw)
+    v = np.ascontiguousarray(pooled, dtype=np.float64)
+    thr, a, b, k, s2 = (C.c_double() for _ in range(5))
+    meth = C.create_string_buffer(32)
+    rc = L.ft_b200_null_threshold(v.ctypes.data_as(C.c_void_p), v.size, runs, psf_fwhm_px, width, height, motions,
+                                  C.byref(p), C.byref(thr), meth, 32, C.byref(a), C.byref(b), C.byref(k), C.byref(s2))
+    if rc != FT_B200_OK:
+        raise RuntimeError("ft_b200_null_threshold: " + L.ft_b200_last_error(None).decode())
+    return dict(threshold=thr.value, method=meth.value.decode(), null_a=a.value, null_b=b.value, null_k=k.value,
+                null_inv_s2=s2.value)
 
 
 def exported_symbols():
@@ -351,7 +373,8 @@ class Device:
             if maps:
                 ms = np.empty((h, w), np.float32)
                 bv = np.empty((h, w), np.int32)
-                L.ft_b200_result_maps(r, ms.ctypes.data_as(C.c_void_p), bv.ctypes.data_as(C.c_void_p))
+                if L.ft_b200_result_maps(r, ms.ctypes.data_as(C.c_void_p), bv.ctypes.data_as(C.c_void_p)) != FT_B200_OK:
+                    ms = bv = None  # a null-run shard other than 0 has no maps
             grid = np.empty((nv.value, 2))
             vx, vy = C.c_double(), C.c_double()
             for j in range(nv.value):

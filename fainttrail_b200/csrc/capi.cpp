@@ -211,6 +211,8 @@ void ft_b200_search_params_default(ft_b200_search_params* p) {
     p->null_tested = d.null_tested;
     p->null_model_gauss = d.gauss_model ? 1 : 0;
     p->passes_per_launch = d.passes_per_launch;
+    p->shard_index = d.shard_index;
+    p->shard_count = d.shard_count;
 }
 
 namespace {
@@ -239,6 +241,10 @@ ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
     p.edge_px = q.edge_px;
     p.gauss_model = q.null_model_gauss != 0;
     p.passes_per_launch = std::max(0, q.passes_per_launch);
+    p.shard_count = std::max(1, q.shard_count);
+    p.shard_index = q.shard_index;
+    if (p.shard_index < 0 || p.shard_index >= p.shard_count)
+        throw std::runtime_error("search: shard_index must lie in [0, shard_count)");
     p.seed = q.seed;
     return p;
 }
@@ -431,6 +437,35 @@ int ft_b200_result_peaks(const ft_b200_result* r, int which, ft_b200_peak* out, 
     return static_cast<int>(v.size());
 }
 
+int ft_b200_null_threshold(const double* pooled, long long count, int runs, double fwhm_px, int width, int height,
+                           int motions, const ft_b200_search_params* params, double* threshold, char* method,
+                           int method_cap, double* a, double* b, double* k, double* inv_s2) {
+    try {
+        if (count < 0 || (count > 0 && !pooled)) throw std::runtime_error("null threshold: missing pooled peaks");
+        if (runs < 0 || width < 1 || height < 1 || motions < 0) throw std::runtime_error("null threshold: bad sizes");
+        ftb::SearchParams p = to_search_params(params);
+        p.shard_index = 0;
+        p.shard_count = 1;
+        // the engine pools the S/N values as float; doubles that came from a result convert back exactly
+        std::vector<float> v(static_cast<size_t>(count));
+        for (long long q = 0; q < count; ++q) v[static_cast<size_t>(q)] = static_cast<float>(pooled[q]);
+        const ftb::Threshold t = ftb::set_threshold(p, v, runs, fwhm_px, width, height, static_cast<size_t>(motions));
+        if (threshold) *threshold = t.snr;
+        if (method && method_cap > 0) {
+            std::strncpy(method, t.method.c_str(), static_cast<size_t>(method_cap) - 1);
+            method[method_cap - 1] = 0;
+        }
+        if (a) *a = t.a;
+        if (b) *b = t.b;
+        if (k) *k = t.k;
+        if (inv_s2) *inv_s2 = t.inv_s2;
+        return FT_B200_OK;
+    } catch (const std::exception& e) {
+        g_open_error = e.what();
+        return FT_B200_ERROR;
+    }
+}
+
 int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap) {
     if (!r) return 0;
     const auto& v = r->o.null_peaks;
@@ -439,7 +474,7 @@ int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap) {
 }
 
 int ft_b200_result_maps(const ft_b200_result* r, float* max_snr, int* best_v) {
-    if (!r) return FT_B200_ERROR;
+    if (!r || r->o.max_snr.empty()) return FT_B200_ERROR;  // a null-run shard other than 0 has no maps
     if (max_snr) std::memcpy(max_snr, r->o.max_snr.data(), sizeof(float) * r->o.max_snr.size());
     if (best_v) std::memcpy(best_v, r->o.best_v.data(), sizeof(int) * r->o.best_v.size());
     return FT_B200_OK;

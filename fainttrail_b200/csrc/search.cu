@@ -346,7 +346,21 @@ void SearchRequest::prepare(const float* frames, const double* mjd, const double
     edge_ = std::max(p_.edge_px, 1);
     min_count_ = pass_min_count(p_.min_coverage, n);
     floor_ = static_cast<float>(auto_thr_ ? p_.min_snr_floor : p_.threshold_snr);
-    orders_ = null_time_orders(o_.t_h, runs_, p_.seed);
+    runs_total_ = runs_;
+    orders_ = null_time_orders(o_.t_h, runs_total_, p_.seed);
+    sharded_ = p_.shard_count > 1;
+    if (sharded_) {
+        // this shard's block of the null runs: the same permutations (one seeded
+        // stream for all runs) and, pooled in shard order, the same null peaks
+        if (!auto_thr_) throw std::runtime_error("search: sharding splits the null runs; a fixed threshold has none");
+        if (keep_raw) throw std::runtime_error("search: injection copies need the whole null calibration on one GPU");
+        const long long k0 = static_cast<long long>(runs_total_) * p_.shard_index / p_.shard_count;
+        const long long k1 = static_cast<long long>(runs_total_) * (p_.shard_index + 1) / p_.shard_count;
+        orders_ = std::vector<std::vector<double>>(orders_.begin() + k0, orders_.begin() + k1);
+        runs_ = static_cast<int>(k1 - k0);
+        real_ = p_.shard_index == 0;
+        real_queued_ = real_done_ = !real_;
+    }
     raw_needed_ = keep_raw;
     if (!keep_raw) raw_.reset();
 }
@@ -442,15 +456,25 @@ void SearchRequest::finish_items(int k0, int k1) {
 SearchOut SearchRequest::finalize(std::vector<SearchOut>* copies_out) {
     Context& c = c_;
     const int w = o_.w, h = o_.h, n = o_.n;
-    o_.thr = set_threshold(p_, pooled_, runs_, o_.fwhm_px, w, h, m_);
-    if (runs_ > 0 && auto_thr_) o_.null_peaks.assign(pooled_.begin(), pooled_.end());
-    for (const Peak& pk : o_.peaks)
-        if (pk.snr >= o_.thr.snr && pk.vidx >= 0) o_.selected.push_back(pk);
-    if (static_cast<int>(o_.selected.size()) > p_.max_candidates) o_.selected.resize(static_cast<size_t>(p_.max_candidates));
-    o_.max_snr.resize(static_cast<size_t>(w) * h);
-    o_.best_v.resize(static_cast<size_t>(w) * h);
-    FTB_CHECK(cudaMemcpyAsync(o_.max_snr.data(), max_.as<float>(), map_bytes_, cudaMemcpyDeviceToHost, c.stream()));
-    FTB_CHECK(cudaMemcpyAsync(o_.best_v.data(), bv_.as<int>(), map_bytes_, cudaMemcpyDeviceToHost, c.stream()));
+    if (sharded_) {
+        // the threshold needs every shard's null peaks: the caller pools them
+        // (ft_b200_null_threshold) and selects from shard 0's peaks
+        o_.thr.method = "shard";
+        o_.null_peaks.assign(pooled_.begin(), pooled_.end());
+    } else {
+        o_.thr = set_threshold(p_, pooled_, runs_, o_.fwhm_px, w, h, m_);
+        if (runs_ > 0 && auto_thr_) o_.null_peaks.assign(pooled_.begin(), pooled_.end());
+        for (const Peak& pk : o_.peaks)
+            if (pk.snr >= o_.thr.snr && pk.vidx >= 0) o_.selected.push_back(pk);
+        if (static_cast<int>(o_.selected.size()) > p_.max_candidates)
+            o_.selected.resize(static_cast<size_t>(p_.max_candidates));
+    }
+    if (real_) {
+        o_.max_snr.resize(static_cast<size_t>(w) * h);
+        o_.best_v.resize(static_cast<size_t>(w) * h);
+        FTB_CHECK(cudaMemcpyAsync(o_.max_snr.data(), max_.as<float>(), map_bytes_, cudaMemcpyDeviceToHost, c.stream()));
+        FTB_CHECK(cudaMemcpyAsync(o_.best_v.data(), bv_.as<int>(), map_bytes_, cudaMemcpyDeviceToHost, c.stream()));
+    }
     if (copies_out) {
         // the copies: peaks above the calibrated threshold, which they were searched with
         copies_out->clear();

@@ -25,6 +25,9 @@ struct SearchParams {
     int static_exclude = -1, null_runs = 3, null_tested = 3000, max_candidates = 300, edge_px = 4;
     bool gauss_model = true;  // null_model "gauss" (else "linear")
     int passes_per_launch = 0;  // 0: as many as fit; k: at most k per launch
+    // null runs split over shard_count calls (one per GPU): this call runs block
+    // shard_index of the null runs and, on shard 0 only, the real pass
+    int shard_index = 0, shard_count = 1;
     uint64_t seed = 12345;
 };
 
@@ -137,7 +140,8 @@ private:
     int pitch_ = 0;
     size_t plane_ = 0, map_bytes_ = 0, m_ = 0;
     bool auto_thr_ = true, real_queued_ = false, real_done_ = false, raw_needed_ = false;
-    int runs_ = 0, nms_ = 2, edge_ = 1, min_count_ = 3;
+    int runs_ = 0, runs_total_ = 0, nms_ = 2, edge_ = 1, min_count_ = 3;
+    bool real_ = true, sharded_ = false;
     float floor_ = 0;
     std::vector<std::vector<double>> orders_;
     std::vector<double> exp_sorted_;

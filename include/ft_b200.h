@@ -134,6 +134,15 @@ typedef struct ft_b200_search_params {
     int passes_per_launch; /* 0 (default): every pass that fits the HBM budget in one
                               persistent launch; k > 0: at most k passes per launch,
                               the real pass alone first (1 = one pass per launch) */
+    int shard_index, shard_count; /* null runs split over shard_count calls, one per GPU
+                              (default 0, 1: no split). Call k runs null runs
+                              [runs*k/count, runs*(k+1)/count) with the permutations
+                              an unsplit search would give them, and only call 0
+                              runs the real pass. A shard's result holds its pooled
+                              null peaks (method "shard", no threshold, no selection;
+                              maps and peaks on shard 0 only): concatenate the
+                              shards' null peaks in shard order, then
+                              ft_b200_null_threshold gives the unsplit threshold. */
 } ft_b200_search_params;
 
 void ft_b200_search_params_default(ft_b200_search_params* p);
@@ -147,6 +156,16 @@ typedef struct ft_b200_peak {
 } ft_b200_peak;
 
 typedef struct ft_b200_result ft_b200_result;
+
+/* The null-tail threshold from pooled null-peak S/N values (set_threshold,
+ * search.cpp:573-612; fit_null_tail_gauss :471-510, gauss_tail_level :517-527):
+ * `pooled` is every run's surviving null peaks, run after run, `runs` the number
+ * of null runs, `motions` the trial motions of the grid. Host only (no device
+ * work, no context): the reduction step of a search whose null runs were split
+ * over GPUs. method receives "null-fit gauss", "null-fit linear", "floor", ... */
+int ft_b200_null_threshold(const double* pooled, long long count, int runs, double fwhm_px, int width, int height,
+                           int motions, const ft_b200_search_params* params, double* threshold, char* method,
+                           int method_cap, double* a, double* b, double* k, double* inv_s2);
 
 /* A whole search from raw registered frames, as ft_search does (c_api.cpp:172-204:
  * frames stable-sorted by mid-exposure time, prepare, then search): background

@@ -89,13 +89,47 @@ def search_case(R):
                 null_inv_s2=np.float64(res["null_inv_s2"]), grid=grid)
 
 
+def null_runs_case(R):
+    """The null calibration of a search split by run: 5 null runs on the search
+    case's sequence. The permutations come from one seeded stream, so the pooled
+    null peaks of k runs are the first part of those of k + 1 runs; the run
+    boundaries follow from searches with 1..5 runs. Pins the threshold that
+    pooled per-run lists must reproduce, whichever process computed each run."""
+    frames, mjd, exp = R.simulate(width=96, height=80, nframes=12, nstars=60, nmovers=2, seed=5)
+    runs = 5
+    prep = R.prepare(frames, mjd, exp, fwhm_px=2.5, null_runs=runs)
+    full = prep.search(fwhm_px=2.5, null_runs=runs, backend="cpu")
+    pooled = np.asarray(full["null_peaks"], np.float64)
+    counts, prev = [], 0
+    for k in range(1, runs + 1):
+        part = np.asarray(prep.search(fwhm_px=2.5, null_runs=k, backend="cpu")["null_peaks"], np.float64)
+        assert np.array_equal(part, pooled[:part.size]), "pooled null peaks are not run-prefix ordered"
+        counts.append(part.size - prev)
+        prev = part.size
+    assert prev == pooled.size
+    return dict(raw=frames, mjd=mjd, exptime=exp, runs=np.int32(runs), pooled=pooled,
+                run_counts=np.array(counts, np.int32), threshold=np.float64(full["threshold"]),
+                method=np.array(full["method"]), null_a=np.float64(full["null_a"]),
+                null_k=np.float64(full["null_k"]), null_inv_s2=np.float64(full["null_inv_s2"]),
+                fwhm=np.float64(prep.fwhm), width=np.int32(96), height=np.int32(80),
+                n_velocities=np.int32(full["n_velocities"]))
+
+
+CASES = {
+    "stack_contract": lambda R: contract_case(R, False, 4242),
+    "stack_constant": lambda R: contract_case(R, True, 4242),
+    "stack_nan_table": lambda R: nan_table_case(R, 99),
+    "stage_small": stage_case,
+    "search_small": search_case,
+    "null_runs_small": null_runs_case,
+}
+
+
 def main():
+    """python make_golden.py [case ...]: the named fixtures, or all of them."""
     R = Reference()
-    np.savez_compressed(os.path.join(HERE, "stack_contract.npz"), **contract_case(R, False, 4242))
-    np.savez_compressed(os.path.join(HERE, "stack_constant.npz"), **contract_case(R, True, 4242))
-    np.savez_compressed(os.path.join(HERE, "stack_nan_table.npz"), **nan_table_case(R, 99))
-    np.savez_compressed(os.path.join(HERE, "stage_small.npz"), **stage_case(R))
-    np.savez_compressed(os.path.join(HERE, "search_small.npz"), **search_case(R))
+    for name in (sys.argv[1:] or list(CASES)):
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **CASES[name](R))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
