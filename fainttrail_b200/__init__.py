@@ -112,7 +112,7 @@ def _declare(L):
 
 
 def _declare_server(L):
-    L.ft_b200_server_open.argtypes = [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_void_p)]
+    L.ft_b200_server_open.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
     L.ft_b200_server_close.argtypes = [C.c_void_p]
     L.ft_b200_server_submit.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
                                         C.POINTER(SearchParams), C.POINTER(C.c_longlong)]
@@ -132,11 +132,11 @@ class Server:
     """The serving loop (ft_b200_server_*): submit searches at any time, poll
     results; requests admitted together share their stacking launches."""
 
-    def __init__(self, device=-1, hbm_budget_bytes=0.0, max_batch=16):
+    def __init__(self, device=-1, hbm_budget_bytes=0.0, max_batch=16, workers=2):
         self.L = lib()
         _declare_server(self.L)
         h = C.c_void_p()
-        if self.L.ft_b200_server_open(device, hbm_budget_bytes, max_batch, C.byref(h)) != FT_B200_OK:
+        if self.L.ft_b200_server_open(device, hbm_budget_bytes, max_batch, workers, C.byref(h)) != FT_B200_OK:
             raise RuntimeError("ft_b200_server_open: " + self.L.ft_b200_last_error(None).decode())
         self.h = h
         self._dev = None
@@ -183,6 +183,33 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def set_tile_shape(shape):
+    """ft_b200_set_tile_shape: 0 automatic, 1 = 32 x 16, 2 = 64 x 8 paired
+    columns, 3 = 32 x 8, 4 = 32 x 4 (process-wide)."""
+    L = lib()
+    L.ft_b200_set_tile_shape.argtypes = [C.c_int]
+    if L.ft_b200_set_tile_shape(int(shape)) != FT_B200_OK:
+        raise ValueError("ft_b200_set_tile_shape: " + L.ft_b200_last_error(None).decode())
+
+
+def tile_shape():
+    return lib().ft_b200_tile_shape()
+
+
+def tuned_shapes():
+    """The autotuner's cache: {(frames, motions, width, height): shape}."""
+    L = lib()
+    cnt = L.ft_b200_tuned_shapes(None, None, 0)
+    keys = (C.c_int * max(1, 4 * cnt))()
+    shapes = (C.c_int * max(1, cnt))()
+    L.ft_b200_tuned_shapes(keys, shapes, cnt)
+    return {tuple(keys[4 * k:4 * k + 4]): shapes[k] for k in range(cnt)}
+
+
+def clear_tuned_shapes():
+    lib().ft_b200_clear_tuned_shapes()
 
 
 def null_threshold(pooled, runs, psf_fwhm_px, width, height, motions, **kw):

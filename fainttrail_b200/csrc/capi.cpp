@@ -329,12 +329,36 @@ int ft_b200_search_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int h
     });
 }
 
-int ft_b200_server_open(int device, double hbm_budget_bytes, int max_batch, ft_b200_server** out) {
+int ft_b200_set_tile_shape(int shape) {
+    try {
+        ftb::set_stack_shape(shape);
+        return FT_B200_OK;
+    } catch (const std::exception& e) {
+        g_open_error = e.what();
+        return FT_B200_ERROR;
+    }
+}
+
+int ft_b200_tile_shape(void) { return ftb::stack_shape(); }
+
+int ft_b200_tuned_shapes(int* keys, int* shapes, int cap) {
+    const auto v = ftb::tuned_shapes();
+    for (size_t k = 0; k < v.size() && static_cast<int>(k) < cap; ++k) {
+        if (keys)
+            for (int q = 0; q < 4; ++q) keys[4 * k + q] = v[k].first[static_cast<size_t>(q)];
+        if (shapes) shapes[k] = v[k].second;
+    }
+    return static_cast<int>(v.size());
+}
+
+void ft_b200_clear_tuned_shapes(void) { ftb::clear_tuned_shapes(); }
+
+int ft_b200_server_open(int device, double hbm_budget_bytes, int max_batch, int workers, ft_b200_server** out) {
     if (!out) return FT_B200_ERROR;
     *out = nullptr;
     try {
         auto h = std::make_unique<ft_b200_server>();
-        h->s = std::make_unique<ftb::Server>(device, hbm_budget_bytes, max_batch);
+        h->s = std::make_unique<ftb::Server>(device, hbm_budget_bytes, max_batch, workers > 0 ? workers : 2);
         *out = h.release();
         return FT_B200_OK;
     } catch (const std::exception& e) {

@@ -5,7 +5,10 @@
 
 #include <algorithm>
 #include <chrono>
+#include <map>
+#include <mutex>
 #include <thread>
+#include <tuple>
 #include <cmath>
 #include <cstdlib>
 
@@ -301,10 +304,114 @@ void stage_host(Context& c, const float* sub, int w, int h, int n, const double*
     if (cr) std::copy(crv.begin(), crv.end(), cr);
 }
 
+// ------------------------------------------------------------------ tile-shape autotuner
+
+namespace {
+
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tuned;  // (frames, motions, width, height) -> shape
+
+// Passes below this many adds keep the frame-count rule: a probe would cost
+// more than a better shape can save.
+constexpr double kTuneMinAdds = 5e11;
+
+// The tile shape for a pass: the cached choice for its (frames, motions, size),
+// else, for a large pass, every shape whose windows fit is planned and timed on a
+// band of tile rows in the middle of the image (about 8 tiles per SM, so each
+// probe is a few per cent of the pass), and the fastest per output pixel wins.
+// The probes write the pass's own output maps, which its real launch rewrites.
+// Returns 0 for "use the frame-count rule".
+int autotune_shape(Context& c, const PassJob& j) {
+    if (stack_shape() != 0) return 0;  // a fixed shape was asked for
+    if (static_cast<double>(j.m) * j.n * j.w * j.h < kTuneMinAdds) return 0;
+    const auto key = std::make_tuple(j.n, j.m, j.w, j.h);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) return it->second;
+    }
+    std::vector<int> cands;
+    for (int s = 1; s <= kStackShapes; ++s)
+        if (stack_shape_fits(stack_shape_config(s, c.smem_optin()), j.n)) cands.push_back(s);
+    int best = cands.empty() ? 0 : cands[0];
+    if (cands.size() > 1) {
+        const double t0 = wall_seconds();
+        double best_t = 1e300;
+        cudaEvent_t e0, e1;
+        FTB_CHECK(cudaEventCreate(&e0));
+        FTB_CHECK(cudaEventCreate(&e1));
+        try {
+            const std::vector<int> order = motion_order(j.dx.data(), j.dy.data(), j.m, j.n, 4.0, 4.0);
+            for (int s : cands) {
+                const StackConfig cfg = stack_shape_config(s, c.smem_optin());
+                StackPlan plan = make_stack_plan(j.w, j.h, j.n, j.dx.data(), j.dy.data(), j.m, j.min_count, order, cfg);
+                plan.pitch = j.pitch;
+                StackPlanDev dev;
+                dev.upload(plan, c.stream());
+                const int tiles_x = (j.w + cfg.tile_w - 1) / cfg.tile_w, tiles_y = (j.h + cfg.p - 1) / cfg.p;
+                const int band = std::min(tiles_y, std::max(1, (8 * c.sms() + tiles_x - 1) / tiles_x));
+                BatchPass bp;
+                bp.plan = &plan;
+                bp.dev = &dev;
+                bp.frames = j.d_frames;
+                bp.g0 = 0;
+                bp.g1 = static_cast<int>(plan.groups.size());
+                bp.max_snr = j.d_max;
+                bp.best_v = j.d_bv;
+                bp.tile_rows0 = (tiles_y - band) / 2;
+                bp.tile_rows = band;
+                DevBuf& desc = c.scratch(kDesc, batch_desc_bytes(1), "stack descriptors");
+                FTB_CHECK(cudaEventRecord(e0, c.stream()));
+                stack_launch_batch({bp}, desc.as<unsigned char>(), desc.bytes(), c.err_flag(), c.sms(), c.stream());
+                FTB_CHECK(cudaEventRecord(e1, c.stream()));
+                ++c.launches;
+                c.check_kernel_error("stack kernel (autotune probe)");
+                float ms = 0.0f;
+                FTB_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+                dev.release();
+                const double per_px = ms / (static_cast<double>(band) * cfg.p * j.w);
+                if (per_px < best_t) {
+                    best_t = per_px;
+                    best = s;
+                }
+            }
+        } catch (...) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        c.host_time("autotune", wall_seconds() - t0);
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = best;
+    return best;
+}
+
+}  // namespace
+
+std::vector<std::pair<std::array<int, 4>, int>> tuned_shapes() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::vector<std::pair<std::array<int, 4>, int>> out;
+    for (const auto& kv : g_tuned)
+        out.push_back({{std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first), std::get<3>(kv.first)},
+                       kv.second});
+    return out;
+}
+
+void clear_tuned_shapes() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned.clear();
+}
+
 // ------------------------------------------------------------------ batched passes
 
 void stack_passes_device(Context& c, std::vector<PassJob>& jobs) {
     if (jobs.empty()) return;
+    // tile shapes first (probes run on the stream, before this batch's launches)
+    std::vector<int> shapes_for(jobs.size(), 0);
+    for (size_t k = 0; k < jobs.size(); ++k) shapes_for[k] = autotune_shape(c, jobs[k]);
     const double t0 = wall_seconds();
     // plans on host threads (the GPU keeps running whatever was queued before)
     std::vector<StackPlan> plans(jobs.size());
@@ -317,7 +424,8 @@ void stack_passes_device(Context& c, std::vector<PassJob>& jobs) {
             try {
                 for (size_t k = wkr; k < jobs.size(); k += workers) {
                     const PassJob& j = jobs[k];
-                    const StackConfig cfg = choose_stack_config(j.w, j.h, j.n, c.smem_optin());
+                    const StackConfig cfg = shapes_for[k] > 0 ? stack_shape_config(shapes_for[k], c.smem_optin())
+                                                              : choose_stack_config(j.w, j.h, j.n, c.smem_optin());
                     plans[k] = make_stack_plan(j.w, j.h, j.n, j.dx.data(), j.dy.data(), j.m, j.min_count,
                                                motion_order(j.dx.data(), j.dy.data(), j.m, j.n, 4.0, 4.0), cfg);
                     plans[k].pitch = j.pitch;
@@ -334,15 +442,15 @@ void stack_passes_device(Context& c, std::vector<PassJob>& jobs) {
     try {
         for (size_t k = 0; k < jobs.size(); ++k) devs[k].upload(plans[k], c.stream());
         // one persistent launch per kernel shape
+        auto key = [](const StackConfig& q) { return std::make_pair(q.ty * 1000 + q.p, q.tile_w); };
         std::vector<std::pair<int, int>> shapes;
         for (const auto& p : plans)
-            if (std::find(shapes.begin(), shapes.end(), std::make_pair(p.cfg.ty, p.cfg.p)) == shapes.end())
-                shapes.emplace_back(p.cfg.ty, p.cfg.p);
+            if (std::find(shapes.begin(), shapes.end(), key(p.cfg)) == shapes.end()) shapes.push_back(key(p.cfg));
         const int span = c.span_begin("kernel");
         for (const auto& sh : shapes) {
             std::vector<BatchPass> batch;
             for (size_t k = 0; k < jobs.size(); ++k) {
-                if (plans[k].cfg.ty != sh.first || plans[k].cfg.p != sh.second) continue;
+                if (key(plans[k].cfg) != sh) continue;
                 BatchPass bp;
                 bp.plan = &plans[k];
                 bp.dev = &devs[k];

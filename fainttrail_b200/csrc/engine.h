@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <functional>
 #include <memory>
 #include <string>
@@ -134,6 +135,10 @@ struct PassJob {
 // Several passes, possibly of different shapes: plans built on host threads,
 // then one persistent launch per kernel shape; returns when all are complete.
 void stack_passes_device(Context& c, std::vector<PassJob>& jobs);
+
+// The tile-shape autotuner's cache: ((frames, motions, width, height), shape).
+std::vector<std::pair<std::array<int, 4>, int>> tuned_shapes();
+void clear_tuned_shapes();
 
 struct StageParams;
 

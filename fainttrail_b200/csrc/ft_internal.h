@@ -80,6 +80,16 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
 
 StackConfig choose_stack_config(int w, int h, int n, int device_smem_optin);
 
+// Compiled stack kernel shapes: 1 = 32 x 16 tiles (12 warps), 2 = 64 x 8 tiles with
+// paired columns (12 warps), 3 = 32 x 8 (16 warps), 4 = 32 x 4 (16 warps).
+constexpr int kStackShapes = 4;
+StackConfig stack_shape_config(int shape, int device_smem_optin);
+bool stack_shape_fits(const StackConfig& c, int n);
+// A process-wide choice for choose_stack_config: 0 = by frame count, else a shape
+// (used when its windows fit).
+void set_stack_shape(int shape);
+int stack_shape();
+
 // Device copy of a plan.
 struct StackPlanDev {
     StackGroup* groups = nullptr;
@@ -108,6 +118,7 @@ struct BatchPass {
     int* arg = nullptr;
     float* max_snr = nullptr;
     int* best_v = nullptr;
+    int tile_rows0 = 0, tile_rows = 0;  // a band of tile rows only (0 rows: the whole pass)
 };
 
 // Device bytes of the descriptors of a batch (a work-queue counter, one tensor

@@ -44,9 +44,17 @@ struct Server::Req {
     }
 };
 
-Server::Server(int device, double budget_bytes, int max_batch)
-    : ctx_(std::make_unique<Context>(device, budget_bytes)), max_batch_(std::max(1, max_batch)) {
-    worker_ = std::thread([this] { loop(); });
+Server::Server(int device, double budget_bytes, int max_batch, int workers) : max_batch_(std::max(1, max_batch)) {
+    workers = std::max(1, std::min(workers, 8));
+    // the first context resolves the device and the default budget (90 % of free)
+    ctx_.push_back(std::make_unique<Context>(device, budget_bytes));
+    const double share = static_cast<double>(ctx_[0]->budget()) / workers;
+    ctx_[0] = std::make_unique<Context>(ctx_[0]->device(), share);
+    for (int k = 1; k < workers; ++k) ctx_.push_back(std::make_unique<Context>(ctx_[0]->device(), share));
+    for (auto& c : ctx_) {
+        Context* cp = c.get();
+        workers_.emplace_back([this, cp] { loop(*cp); });
+    }
 }
 
 Server::~Server() {
@@ -55,7 +63,8 @@ Server::~Server() {
         stop_ = true;
     }
     cv_.notify_all();
-    if (worker_.joinable()) worker_.join();
+    for (auto& t : workers_)
+        if (t.joinable()) t.join();
 }
 
 long long Server::submit(const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
@@ -134,21 +143,29 @@ ServerStats Server::stats() {
     return s;
 }
 
-void Server::loop() {
+void Server::loop(Context& c) {
     try {
-        ctx_->bind();
+        c.bind();
     } catch (...) {
     }
     for (;;) {
         std::vector<std::shared_ptr<Req>> round;
         {
             std::unique_lock<std::mutex> lk(mu_);
+            ++idle_;
             cv_.wait(lk, [&] { return stop_ || (!paused_ && !queue_.empty()); });
-            if (stop_ && (queue_.empty() || paused_)) break;
-            // admission: the oldest requests whose device memory fits the budget
+            if (stop_ && (queue_.empty() || paused_)) {
+                --idle_;
+                break;
+            }
+            // admission: the oldest requests whose device memory fits this worker's
+            // budget, the queue shared out among the idle workers
+            const int share = static_cast<int>((queue_.size() + idle_ - 1) / std::max(1, idle_));
+            const int cap = std::max(1, std::min(max_batch_, share));
+            --idle_;
             size_t need = 0;
-            const size_t budget = ctx_->budget() > ctx_->used() ? ctx_->budget() - ctx_->used() : 0;
-            while (!queue_.empty() && static_cast<int>(round.size()) < max_batch_) {
+            const size_t budget = c.budget() > c.used() ? c.budget() - c.used() : 0;
+            while (!queue_.empty() && static_cast<int>(round.size()) < cap) {
                 const size_t b = queue_.front()->bytes();
                 if (!round.empty() && need + b > budget) break;
                 need += b;
@@ -156,7 +173,7 @@ void Server::loop() {
                 queue_.pop_front();
             }
         }
-        run_round(round);
+        run_round(c, round);
         {
             std::lock_guard<std::mutex> lk(mu_);
             const double t = now_s();
@@ -166,7 +183,7 @@ void Server::loop() {
                 if (r->error.empty()) latencies_.push_back(r->t_done - r->t_submit);
             }
             last_done_ = t;
-            launches_ += ctx_->launches;
+            launches_ += c.launches;
             ++rounds_;
             batched_ += static_cast<long long>(round.size());
         }
@@ -174,8 +191,7 @@ void Server::loop() {
     }
 }
 
-void Server::run_round(std::vector<std::shared_ptr<Req>>& round) {
-    Context& c = *ctx_;
+void Server::run_round(Context& c, std::vector<std::shared_ptr<Req>>& round) {
     c.timing_reset();
     std::vector<std::unique_ptr<SearchRequest>> rs(round.size());
     for (size_t k = 0; k < round.size(); ++k) {

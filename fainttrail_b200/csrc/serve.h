@@ -22,7 +22,10 @@ struct ServerStats {
 
 class Server {
 public:
-    Server(int device, double budget_bytes, int max_batch);
+    // workers: rounds in flight at once, each on its own stream with an equal
+    // share of the budget, so one round's host phases (plans, peak sorting, the
+    // threshold fit) overlap another's kernels
+    Server(int device, double budget_bytes, int max_batch, int workers = 2);
     ~Server();
     // copies the request; returns its id
     long long submit(const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
@@ -35,11 +38,11 @@ public:
 
 private:
     struct Req;
-    void loop();
-    void run_round(std::vector<std::shared_ptr<Req>>& round);
-    std::unique_ptr<Context> ctx_;
-    int max_batch_ = 16;
-    std::thread worker_;
+    void loop(Context& c);
+    void run_round(Context& c, std::vector<std::shared_ptr<Req>>& round);
+    std::vector<std::unique_ptr<Context>> ctx_;
+    int max_batch_ = 16, idle_ = 0;
+    std::vector<std::thread> workers_;
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;
     bool stop_ = false, paused_ = false;

@@ -31,6 +31,7 @@
 #include <math_constants.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -92,22 +93,54 @@ inline int floor4(int v) { return (v >> 2) * 4; }  // arithmetic shift: floor fo
 inline int roundup(int v, int q) { return (v + q - 1) / q * q; }
 }  // namespace
 
+namespace {
+std::atomic<int> g_shape{0};
+}
+
+void set_stack_shape(int shape) {
+    if (shape < 0 || shape > kStackShapes) throw std::runtime_error("stack: unknown tile shape");
+    g_shape = shape;
+}
+
+int stack_shape() { return g_shape; }
+
+StackConfig stack_shape_config(int shape, int smem_optin) {
+    StackConfig c;
+    c.mblock = 4;  // motions per register block
+    c.bh = 4;
+    c.smem_bytes = std::min(smem_optin - 1024, 224 * 1024);
+    switch (shape) {
+        case 1: c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 12; break;
+        case 2: c.tile_w = 64; c.wp = 72; c.p = 8; c.ty = 12; break;
+        case 3: c.tile_w = 32; c.wp = 40; c.p = 8; c.ty = 16; break;
+        case 4: c.tile_w = 32; c.wp = 40; c.p = 4; c.ty = 16; break;
+        default: throw std::runtime_error("stack: unknown tile shape");
+    }
+    return c;
+}
+
+bool stack_shape_fits(const StackConfig& c, int n) {
+    // the windows of all frames with 4 rows of vertical spread in at most 70 % of
+    // shared memory (the rest: more spread and the offset table)
+    const long long need = static_cast<long long>(n) * roundup(c.p + 4, c.bh) * c.wp * 4;
+    return need <= static_cast<long long>(c.smem_bytes) * 7 / 10;
+}
+
 StackConfig choose_stack_config(int w, int h, int n, int smem_optin) {
     (void)w;
     (void)h;
-    StackConfig c;
-    c.ty = 12;     // warps per CTA, sharing one tile
-    c.mblock = 4;  // motions per register block
-    c.smem_bytes = std::min(smem_optin - 1024, 224 * 1024);
-    // the tallest tile (16, 8 or 4 rows) whose windows, with 4 rows of vertical
-    // spread, use at most 70 % of shared memory (the rest: spread and offsets)
-    auto need = [&](int p) { return static_cast<long long>(n) * roundup(p + 4, c.bh) * c.wp * 4; };
-    const long long cap = static_cast<long long>(c.smem_bytes) * 7 / 10;
-    c.p = need(16) <= cap ? 16 : need(8) <= cap ? 8 : 4;
-    // 16-row tiles hold 64 accumulators per thread: 12 warps fit the register
-    // file; shorter tiles run 16 warps for latency hiding
-    if (c.p < 16) c.ty = 16;
-    return c;
+    const int forced = g_shape;
+    if (forced > 0) {
+        const StackConfig c = stack_shape_config(forced, smem_optin);
+        if (stack_shape_fits(c, n)) return c;
+    }
+    // the first shape whose windows fit: paired 64 x 8 tiles, then single-column
+    // tiles of 16, 8 and 4 rows (taller frame stacks need the shorter tiles)
+    for (int s : {2, 1, 3}) {
+        const StackConfig c = stack_shape_config(s, smem_optin);
+        if (stack_shape_fits(c, n)) return c;
+    }
+    return stack_shape_config(4, smem_optin);
 }
 
 StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int m, int min_count,
@@ -330,7 +363,8 @@ namespace {
 struct StackArgs {
     int w, h, n, min_count;
     int g0, g1, first, last;
-    int tiles_x, tiles_y;  // tile grid of this pass
+    int tiles_x, tiles_y;  // tile grid of this pass (tiles_y: rows of it in this launch)
+    int ty0;               // first tile row
     long long item0;       // its first work item in the batch
     const StackGroup* groups;
     const StackWin* wins;
@@ -598,10 +632,245 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
     return true;
 }
 
+// ---- paired columns: each thread owns two adjacent columns of P rows, so a
+// warp covers a 64-wide tile. Every add is a packed add.rn.f32x2 on the pair
+// (two independent round-to-nearest float adds, bit-identical to two scalar
+// adds), which halves the add instructions; a window offset that is even loads
+// both columns with one 64-bit shared load, an odd one with two 32-bit loads.
+
+__device__ __forceinline__ uint64_t pack2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+__device__ __forceinline__ void unpack2(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+template <int P, int WP>
+__device__ __forceinline__ void load_pairs(uint64_t (&v)[P], const float* __restrict__ src, uint32_t odd) {
+    if (!odd) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) v[p] = *reinterpret_cast<const uint64_t*>(src + p * WP);
+    } else {
+#pragma unroll
+        for (int p = 0; p < P; ++p) v[p] = pack2(src[p * WP], src[p * WP + 1]);
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void add_pairs(uint64_t (&acc)[P], const uint64_t (&v)[P]) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) acc[p] = add2(acc[p], v[p]);
+}
+
+// motion_quad for paired columns: x is the thread's first column
+template <int P, int WP, bool BORDER>
+__device__ __forceinline__ void motion_quad2(const StackArgs& a, const StackGroup& G, int s0,
+                                             const float* __restrict__ win, const uint16_t* __restrict__ offs, int tb,
+                                             int x, int x0, int y0, float inv_n, float (&best)[P][2],
+                                             int (&arg)[P][2]) {
+    constexpr int M = 4;
+    constexpr int PW = (P + 3) / 4;
+    uint64_t acc[M][P];
+#pragma unroll
+    for (int k = 0; k < M; ++k)
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[k][p] = 0ull;  // (+0.0f, +0.0f)
+    int cfull[M] = {0, 0, 0, 0};
+    uint32_t cpart[M][2][PW];
+#pragma unroll
+    for (int k = 0; k < M; ++k)
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int w = 0; w < PW; ++w) cpart[k][c][w] = 0;
+    const uint16_t* op = offs + s0;
+    uint2 qn = *reinterpret_cast<const uint2*>(op);
+    for (int i = 0; i < a.n; ++i) {
+        const uint2 q = qn;
+        if (i + 1 < a.n) qn = *reinterpret_cast<const uint2*>(op + (i + 1) * G.nslots);
+        const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
+        uint64_t v[P];
+        load_pairs<P, WP>(v, win + o0 + tb, o0 & 1u);
+        add_pairs<P>(acc[0], v);
+        if (o1 != o0) load_pairs<P, WP>(v, win + o1 + tb, o1 & 1u);
+        add_pairs<P>(acc[1], v);
+        if (o2 != o1) load_pairs<P, WP>(v, win + o2 + tb, o2 & 1u);
+        add_pairs<P>(acc[2], v);
+        if (o3 != o2) load_pairs<P, WP>(v, win + o3 + tb, o3 & 1u);
+        add_pairs<P>(acc[3], v);
+        if constexpr (BORDER) {
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * a.n + i];
+                const bool whole = x0 + sh.x >= 0 && x0 + 63 + sh.x < a.w && y0 + sh.y >= 0 && y0 + P - 1 + sh.y < a.h;
+                if (whole) {
+                    ++cfull[k];
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const bool inx = static_cast<unsigned>(x + c + sh.x) < static_cast<unsigned>(a.w);
+#pragma unroll
+                        for (int p = 0; p < P; ++p)
+                            if (inx && static_cast<unsigned>(y0 + p + sh.y) < static_cast<unsigned>(a.h))
+                                cpart[k][c][p / 4] += 1u << (8 * (p % 4));
+                    }
+                }
+            }
+        }
+    }
+    const uint64_t inv2 = pack2(inv_n, inv_n);
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        const int j = a.slot_motion[G.slot0 + s0 + k];
+        if (j < 0) continue;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            float s[2];
+            if constexpr (BORDER) {
+                bool ok[2];
+                float f[2];
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const int cc = cfull[k] + static_cast<int>((cpart[k][c][p / 4] >> (8 * (p % 4))) & 0xffu);
+                    ok[c] = cc >= a.min_count;
+                    f[c] = a.inv_sqrt[ok[c] ? cc : 0];
+                }
+                unpack2(mul2(acc[k][p], pack2(f[0], f[1])), s[0], s[1]);
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    if (ok[c] && (s[c] > best[p][c] || (s[c] == best[p][c] && j < arg[p][c]))) {
+                        best[p][c] = s[c];
+                        arg[p][c] = j;
+                    }
+            } else {
+                unpack2(mul2(acc[k][p], inv2), s[0], s[1]);
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    if (s[c] > best[p][c] || (s[c] == best[p][c] && j < arg[p][c])) {
+                        best[p][c] = s[c];
+                        arg[p][c] = j;
+                    }
+            }
+        }
+    }
+}
+
+// One 64 x P output tile of one pass with paired columns (as stack_tile).
+template <int NW, int P, int WP, int BH>
+__device__ bool stack_tile2(const StackArgs& a, const CUtensorMap* tmap, int x0, int y0, uint64_t* bar, float* win,
+                            int* err, uint32_t& phase) {
+    constexpr int M = 4;
+    constexpr int TW = 64;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int x = x0 + 2 * lane;
+    const int tb = 2 * lane;
+
+    float best[P][2];
+    int arg[P][2];
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            best[p][c] = -CUDART_INF_F;
+            arg[p][c] = -1;
+        }
+    const bool full = x0 + TW - 1 < a.w && y0 + P - 1 < a.h;
+    const float inv_n = a.inv_sqrt[a.n];
+    for (int g = a.g0; g < a.g1; ++g) {
+        const StackGroup G = a.groups[g];
+        uint16_t* offs = reinterpret_cast<uint16_t*>(win + G.rows_total * WP);
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            mbar_expect_tx(bar, static_cast<uint32_t>(G.rows_total * WP * 4));
+            for (int i = 0; i < a.n; ++i) {
+                const StackWin wv = a.wins[G.win0 + i];
+                for (int b = 0; b < wv.rows; b += BH)
+                    tma_load_3d(win + (wv.row0 + b) * WP, tmap, x0 + wv.dx0, y0 + wv.dy0 + b, i, bar);
+            }
+        }
+        {
+            const int nvec = (G.nslots * a.n + 7) / 8;
+            const uint4* src = reinterpret_cast<const uint4*>(a.slot_off + a.slot_off_base[g]);
+            uint4* dst = reinterpret_cast<uint4*>(offs);
+            for (int q = tid; q < nvec; q += blockDim.x) dst[q] = src[q];
+        }
+        __syncthreads();
+        const bool ok = mbar_wait_bounded(bar, phase, err);
+        if (__syncthreads_or(!ok)) return false;
+        phase ^= 1u;
+        const bool interior = full && x0 + G.gdxmin >= 0 && x0 + TW - 1 + G.gdxmax < a.w && y0 + G.gdymin >= 0 &&
+                              y0 + P - 1 + G.gdymax < a.h;
+        if (interior) {
+            for (int s0 = warp * M; s0 < G.nslots; s0 += NW * M)
+                motion_quad2<P, WP, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+        } else {
+            for (int s0 = warp * M; s0 < G.nslots; s0 += NW * M)
+                motion_quad2<P, WP, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+        }
+    }
+    __syncthreads();
+    float* mb = win;
+    int* ma = reinterpret_cast<int*>(win + NW * TW * P);
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            mb[(warp * P + p) * TW + tb + c] = best[p][c];
+            ma[(warp * P + p) * TW + tb + c] = arg[p][c];
+        }
+    __syncthreads();
+    for (int q = tid; q < TW * P; q += 32 * NW) {
+        const int p = q / TW, l = q % TW;
+        const int xx = x0 + l, yy = y0 + p;
+        if (xx >= a.w || yy >= a.h) continue;
+        const size_t o = static_cast<size_t>(yy) * a.w + xx;
+        float b = -CUDART_INF_F;
+        int ar = -1;
+        if (!a.first) {
+            b = a.best[o];
+            ar = a.arg[o];
+        }
+        for (int w = 0; w < NW; ++w) {
+            const float s = mb[(w * P + p) * TW + l];
+            const int j = ma[(w * P + p) * TW + l];
+            if (j >= 0 && (s > b || (s == b && (ar < 0 || j < ar)))) {
+                b = s;
+                ar = j;
+            }
+        }
+        if (a.last) {
+            a.max_snr[o] = isfinite(b) ? b : 0.0f;
+            a.best_v[o] = ar;
+        } else {
+            a.best[o] = b;
+            a.arg[o] = ar;
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
 // Persistent: one CTA per SM takes (pass, tile) work items from a queue until the
 // batch is done, so passes of different shapes and sizes share one launch and
-// the SMs stay busy to the end.
-template <int NW, int P, int WP, int BH>
+// the SMs stay busy to the end. TW: tile width, 32 (one column per thread) or
+// 64 (paired columns).
+template <int NW, int P, int WP, int BH, int TW>
 __global__ void __launch_bounds__(32 * NW, 1)
     stack_batch_kernel(const StackArgs* __restrict__ passes, const CUtensorMap* __restrict__ maps, int npasses,
                        long long items, int* queue, int* err) {
@@ -624,8 +893,12 @@ __global__ void __launch_bounds__(32 * NW, 1)
         while (p + 1 < npasses && passes[p + 1].item0 <= item) ++p;
         const StackArgs& a = passes[p];
         const long long t = item - a.item0;
-        const int tx = static_cast<int>(t % a.tiles_x), ty = static_cast<int>(t / a.tiles_x);
-        if (!stack_tile<NW, P, WP, BH>(a, maps + p, tx * 32, ty * P, bar, win, err, phase)) return;
+        const int tx = static_cast<int>(t % a.tiles_x), ty = a.ty0 + static_cast<int>(t / a.tiles_x);
+        if constexpr (TW == 64) {
+            if (!stack_tile2<NW, P, WP, BH>(a, maps + p, tx * 64, ty * P, bar, win, err, phase)) return;
+        } else {
+            if (!stack_tile<NW, P, WP, BH>(a, maps + p, tx * 32, ty * P, bar, win, err, phase)) return;
+        }
     }
 }
 
@@ -643,7 +916,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-template <int NW, int P, int WP, int BH>
+template <int NW, int P, int WP, int BH, int TW>
 void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, size_t desc_bytes, int* d_err,
                   int sms, cudaStream_t s) {
     const size_t np = batch.size();
@@ -652,11 +925,12 @@ void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, si
     CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(host.data() + 128);
     StackArgs* args = reinterpret_cast<StackArgs*>(host.data() + 128 + 128 * np);
     long long items = 0;
-    size_t smem = 256 + static_cast<size_t>(NW) * 32 * P * 8;
+    size_t smem = 256 + static_cast<size_t>(NW) * TW * P * 8;  // the warps' maxima at the end of a tile
     for (size_t k = 0; k < np; ++k) {
         const BatchPass& bp = batch[k];
         const StackPlan& plan = *bp.plan;
-        if (plan.cfg.ty != NW || plan.cfg.p != P) throw std::runtime_error("stack batch: passes of different kernel shapes");
+        if (plan.cfg.ty != NW || plan.cfg.p != P || plan.cfg.tile_w != TW || plan.cfg.wp != WP)
+            throw std::runtime_error("stack batch: passes of different kernel shapes");
         const cuuint64_t dims[3] = {static_cast<cuuint64_t>(plan.w), static_cast<cuuint64_t>(plan.h),
                                     static_cast<cuuint64_t>(plan.n)};
         const cuuint64_t strides[2] = {static_cast<cuuint64_t>(plan.pitch) * 4,
@@ -677,8 +951,13 @@ void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, si
         a.g1 = bp.g1;
         a.first = bp.first;
         a.last = bp.last;
-        a.tiles_x = (plan.w + 31) / 32;
+        a.tiles_x = (plan.w + TW - 1) / TW;
         a.tiles_y = (plan.h + P - 1) / P;
+        a.ty0 = 0;
+        if (bp.tile_rows > 0) {  // a band of tile rows (autotuning probes)
+            a.ty0 = std::min(std::max(0, bp.tile_rows0), a.tiles_y - 1);
+            a.tiles_y = std::min(bp.tile_rows, a.tiles_y - a.ty0);
+        }
         a.item0 = items;
         items += static_cast<long long>(a.tiles_x) * a.tiles_y;
         const StackPlanDev& dev = *bp.dev;
@@ -700,7 +979,7 @@ void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, si
     }
     if (items == 0) return;
     FTB_CHECK(cudaMemcpyAsync(d_desc, host.data(), host.size(), cudaMemcpyHostToDevice, s));
-    auto kern = stack_batch_kernel<NW, P, WP, BH>;
+    auto kern = stack_batch_kernel<NW, P, WP, BH, TW>;
     FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     const int ctas = static_cast<int>(std::min<long long>(items, sms));
     kern<<<ctas, 32 * NW, smem, s>>>(reinterpret_cast<const StackArgs*>(d_desc + 128 + 128 * np),
@@ -719,13 +998,15 @@ void stack_launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_de
                         int sms, cudaStream_t s) {
     if (batch.empty()) return;
     const StackConfig& c = batch[0].plan->cfg;
-    if (c.wp != 40 || c.bh != 4 || c.mblock != 4) throw std::runtime_error("stack: unsupported kernel configuration");
-    if (c.ty == 12 && c.p == 16)
-        launch_batch<12, 16, 40, 4>(batch, d_desc, desc_bytes, d_err, sms, s);
-    else if (c.ty == 16 && c.p == 8)
-        launch_batch<16, 8, 40, 4>(batch, d_desc, desc_bytes, d_err, sms, s);
-    else if (c.ty == 16 && c.p == 4)
-        launch_batch<16, 4, 40, 4>(batch, d_desc, desc_bytes, d_err, sms, s);
+    if (c.bh != 4 || c.mblock != 4) throw std::runtime_error("stack: unsupported kernel configuration");
+    if (c.tile_w == 64 && c.wp == 72 && c.ty == 12 && c.p == 8)
+        launch_batch<12, 8, 72, 4, 64>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 12 && c.p == 16)
+        launch_batch<12, 16, 40, 4, 32>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 8)
+        launch_batch<16, 8, 40, 4, 32>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 4)
+        launch_batch<16, 4, 40, 4, 32>(batch, d_desc, desc_bytes, d_err, sms, s);
     else
         throw std::runtime_error("stack: unsupported tile shape");
 }

@@ -45,90 +45,123 @@ struct SkyArgs {
     int w, h, pitch, n, exclude, need;
 };
 
-// One thread per pixel. The finite (value, rank) pairs of the pixel's column are
-// placed in sorted order by counting, for each, the pairs that sort before it
-// (the pairs are distinct because the ranks are); the leave-out median of frame
-// i is then the lo-th / hi-th sorted pair outside the exclusion window, found by
-// selecting zero bits of a bitmask of the excluded sorted positions.
+// One thread per pixel. The pixel's values are held in time-rank order, so the
+// reference's sort of (value, time rank) pairs orders equal values by index.
+// Each finite value's sorted position is counted against all others, eight
+// values per pass over the column (the non-finite ones are held as +inf and
+// never counted). The leave-out median of the frame of rank r is then the lo-th /
+// hi-th sorted value outside the exclusion window [r - exclude, r + exclude]; the
+// window's sorted positions are a bitmask of W words that slides one rank per
+// frame (one position leaves, one enters), and the kept positions are picked
+// with popc / fns.
+// flips sorted position p (255: a non-finite value, no position) in the window
+// mask; returns 1 if a position was flipped
+template <int W>
+__device__ __forceinline__ int sky_toggle(uint32_t (&ex)[W], int p) {
+    if (p == 255) return 0;
+#pragma unroll
+    for (int wd = 0; wd < W; ++wd) ex[wd] ^= (p >> 5) == wd ? 1u << (p & 31) : 0u;
+    return 1;
+}
+
+template <int W>
 __global__ void __launch_bounds__(64) sky_kernel(const SkyArgs a) {
     extern __shared__ unsigned char sm[];
     const int T = blockDim.x, t = threadIdx.x;
-    float* V = reinterpret_cast<float*>(sm);                  // [n][T] values by frame
-    float* S = V + a.n * T;                                             // [n][T] sorted values
-    unsigned char* PF = reinterpret_cast<unsigned char*>(S + a.n * T);  // [n][T] sorted position of each frame
+    const int n = a.n;
+    float* V = reinterpret_cast<float*>(sm);                            // [n][T] values by time rank, +inf if not finite
+    float* S = V + n * T;                                               // [n][T] finite values in sorted order
+    unsigned char* PF = reinterpret_cast<unsigned char*>(S + n * T);    // [n][T] sorted position by rank, 255: none
     const long long q = static_cast<long long>(blockIdx.x) * T + t;
     const int x = static_cast<int>(q % a.w), y = static_cast<int>(q / a.w);
     if (y >= a.h) return;
     const size_t plane = static_cast<size_t>(a.pitch) * a.h;
     const size_t pix = static_cast<size_t>(y) * a.pitch + x;
     int m_all = 0;
-    for (int i = 0; i < a.n; ++i) {
-        const float v = a.sub[i * plane + pix];
-        V[i * T + t] = v;
-        m_all += finitef(v);
+    for (int r = 0; r < n; ++r) {
+        const float v = a.sub[a.frame_of[r] * plane + pix];
+        const bool fin = finitef(v);
+        V[r * T + t] = fin ? v : CUDART_INF_F;
+        m_all += fin;
     }
     if (m_all < a.need) {
         a.sky[pix] = CUDART_NAN_F;
-        for (int i = 0; i < a.n; ++i) a.residual[i * plane + pix] = CUDART_NAN_F;
+        for (int i = 0; i < n; ++i) a.residual[i * plane + pix] = CUDART_NAN_F;
         return;
     }
-    for (int e = 0; e < a.n; ++e) {
-        const float ve = V[e * T + t];
-        if (!finitef(ve)) {
-            PF[e * T + t] = 255;
-            continue;
+    constexpr int B = 8;
+    for (int e0 = 0; e0 < n; e0 += B) {
+        float ve[B];
+        int pos[B];
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            ve[b] = e0 + b < n ? V[(e0 + b) * T + t] : CUDART_INF_F;
+            pos[b] = 0;
         }
-        const int re = a.rank[e];
-        int pos = 0;
-        for (int f = 0; f < a.n; ++f) {
+        for (int f = 0; f < e0; ++f) {  // lower ranks: equal values sort first
             const float vf = V[f * T + t];
-            pos += finitef(vf) && (vf < ve || (vf == ve && a.rank[f] < re));
+#pragma unroll
+            for (int b = 0; b < B; ++b) pos[b] += vf <= ve[b];
         }
-        S[pos * T + t] = ve;
-        PF[e * T + t] = static_cast<unsigned char>(pos);
+        const int e1 = min(e0 + B, n);
+        for (int f = e0; f < e1; ++f) {
+            const float vf = V[f * T + t];
+#pragma unroll
+            for (int b = 0; b < B; ++b) pos[b] += vf < ve[b] || (vf == ve[b] && f < e0 + b);
+        }
+        for (int f = e1; f < n; ++f) {  // higher ranks: only smaller values
+            const float vf = V[f * T + t];
+#pragma unroll
+            for (int b = 0; b < B; ++b) pos[b] += vf < ve[b];
+        }
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            if (e0 + b >= n) break;
+            const bool fin = ve[b] != CUDART_INF_F;
+            if (fin) S[pos[b] * T + t] = ve[b];
+            PF[(e0 + b) * T + t] = fin ? static_cast<unsigned char>(pos[b]) : 255;
+        }
     }
     // global median: the two middle floats are added in float (preprocess.cpp:171)
     const float mid_sum = __fadd_rn(S[((m_all - 1) / 2) * T + t], S[(m_all / 2) * T + t]);
     const double global = 0.5 * static_cast<double>(mid_sum);
     a.sky[pix] = __double2float_rn(global);
-    const int words = (m_all + 31) / 32;
-    for (int i = 0; i < a.n; ++i) {
-        const float v = V[i * T + t];
-        if (!finitef(v)) {
-            a.residual[i * plane + pix] = CUDART_NAN_F;
+    uint32_t ex[W];
+#pragma unroll
+    for (int wd = 0; wd < W; ++wd) ex[wd] = 0;
+    int excluded = 0;
+    if (a.exclude > 0)
+        for (int r = 0; r <= min(a.exclude, n - 1); ++r) excluded += sky_toggle<W>(ex, PF[r * T + t]);  // rank 0's window
+    for (int r = 0; r < n; ++r) {
+        if (a.exclude > 0 && r > 0) {
+            if (r - 1 - a.exclude >= 0) excluded -= sky_toggle<W>(ex, PF[(r - 1 - a.exclude) * T + t]);
+            if (r + a.exclude < n) excluded += sky_toggle<W>(ex, PF[(r + a.exclude) * T + t]);
+        }
+        const float v = V[r * T + t];
+        float* out = a.residual + a.frame_of[r] * plane + pix;
+        if (v == CUDART_INF_F) {
+            *out = CUDART_NAN_F;
             continue;
         }
         double st = global;
-        if (a.exclude > 0) {
-            uint32_t ex[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            const int ri = a.rank[i];
-            int excluded = 0;
-            const int r0 = max(0, ri - a.exclude), r1 = min(a.n - 1, ri + a.exclude);
-            for (int r = r0; r <= r1; ++r) {
-                const int p = PF[a.frame_of[r] * T + t];
-                if (p == 255) continue;
-                ex[p >> 5] |= 1u << (p & 31);
-                ++excluded;
+        const int m = m_all - excluded;
+        if (a.exclude > 0 && m >= 5) {
+            const int lo = (m - 1) / 2, hi = m / 2;
+            int plo = -1, phi = -1, seen = 0;
+#pragma unroll
+            for (int wd = 0; wd < W; ++wd) {
+                const int nb = min(32, max(0, m_all - wd * 32));
+                const uint32_t valid = nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u);
+                const uint32_t keep = ~ex[wd] & valid;
+                const int c = __popc(keep);
+                if (plo < 0 && lo < seen + c) plo = wd * 32 + static_cast<int>(__fns(keep, 0, lo - seen + 1));
+                if (phi < 0 && hi < seen + c) phi = wd * 32 + static_cast<int>(__fns(keep, 0, hi - seen + 1));
+                seen += c;
             }
-            const int m = m_all - excluded;
-            if (m >= 5) {
-                const int lo = (m - 1) / 2, hi = m / 2;
-                // positions of the lo-th and hi-th kept (zero) bits below m_all
-                int plo = -1, phi = -1, seen = 0;
-                for (int wd = 0; wd < words && phi < 0; ++wd) {
-                    const int nb = min(32, m_all - wd * 32);
-                    const uint32_t valid = nb == 32 ? 0xffffffffu : ((1u << nb) - 1u);
-                    const uint32_t keep = ~ex[wd] & valid;
-                    const int c = __popc(keep);
-                    if (plo < 0 && lo < seen + c) plo = wd * 32 + static_cast<int>(__fns(keep, 0, lo - seen + 1));
-                    if (hi < seen + c) phi = wd * 32 + static_cast<int>(__fns(keep, 0, hi - seen + 1));
-                    seen += c;
-                }
-                // double add of the two middle values (preprocess.cpp:198)
-                st = 0.5 * (static_cast<double>(S[plo * T + t]) + static_cast<double>(S[phi * T + t]));
-            }
+            // double add of the two middle values (preprocess.cpp:198)
+            st = 0.5 * (static_cast<double>(S[plo * T + t]) + static_cast<double>(S[phi * T + t]));
         }
-        a.residual[i * plane + pix] = __double2float_rn(static_cast<double>(v) - st);
+        *out = __double2float_rn(static_cast<double>(v) - st);
     }
 }
 
@@ -552,8 +585,9 @@ void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h,
                   std::max(5, static_cast<int>(0.6 * n))};
         const int T = 64;
         const size_t smem = static_cast<size_t>(T) * n * 9;
-        FTB_CHECK(cudaFuncSetAttribute(sky_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        sky_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
+        auto kern = n <= 32 ? sky_kernel<1> : n <= 64 ? sky_kernel<2> : n <= 128 ? sky_kernel<4> : sky_kernel<8>;
+        FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        kern<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
         FTB_CHECK(cudaGetLastError());
         ++c.launches;
         c.span_end(span);

@@ -231,6 +231,24 @@ int ft_b200_result_maps(const ft_b200_result* r, float* max_snr, int* best_v);
 /* The trial motion vidx of the grid (velocity_grid, search.cpp:39-58), px/hour. */
 int ft_b200_result_velocity(const ft_b200_result* r, int vidx, double* vx_pxh, double* vy_pxh);
 
+/* Stack kernel tile shape for every later pass in this process: 0 = automatic
+ * (the default: the autotuned choice where one is cached for the pass's frame
+ * count, else the first shape whose windows fit), 1 = 32 x 16 output tiles,
+ * 2 = 64 x 8 tiles with paired columns, 3 = 32 x 8, 4 = 32 x 4. A fixed shape
+ * whose frame windows do not fit shared memory falls back to automatic. Results
+ * do not depend on the shape. No counterpart in the reference (its CUDA kernel
+ * has one shape, backend_cuda.cu:55-72). */
+int ft_b200_set_tile_shape(int shape);
+int ft_b200_tile_shape(void);
+/* The autotuner's choices so far: for a pass of at least 5e11 adds whose
+ * (frames, motions, width, height) it has not seen, automatic mode plans every
+ * shape that fits, times each on a band of tile rows in the middle of the image
+ * and keeps the fastest per output pixel. Fills keys[4 * k .. 4 * k + 3] (frames,
+ * motions, width, height) and shapes[k] for up to cap entries; returns the count.
+ * ft_b200_clear_tuned_shapes forgets them. */
+int ft_b200_tuned_shapes(int* keys, int* shapes, int cap);
+void ft_b200_clear_tuned_shapes(void);
+
 /* The serving loop. A server owns a device context and a worker thread; requests
  * (frames of any count and size, any motion range) are copied on submission,
  * admitted in arrival order as the HBM budget allows, and run in rounds: every
@@ -242,7 +260,9 @@ int ft_b200_result_velocity(const ft_b200_result* r, int vidx, double* vx_pxh, d
  * per round. */
 typedef struct ft_b200_server ft_b200_server;
 
-int ft_b200_server_open(int device, double hbm_budget_bytes, int max_batch, ft_b200_server** out);
+/* workers: rounds in flight at once (each on its own stream with an equal share
+ * of the budget; <= 0: 2), so one round's host work overlaps another's kernels. */
+int ft_b200_server_open(int device, double hbm_budget_bytes, int max_batch, int workers, ft_b200_server** out);
 /* Finishes the queued requests, then stops the worker. */
 void ft_b200_server_close(ft_b200_server* s);
 int ft_b200_server_submit(ft_b200_server* s, const float* frames, int width, int height, int nframes,

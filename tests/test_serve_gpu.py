@@ -41,7 +41,7 @@ def test_server_batch_matches_standalone(device):
     import fainttrail_b200 as ftb
     reqs = _requests()
     alone = [device.search(f, m, e, **kw) for f, m, e, kw in reqs]
-    srv = ftb.Server(0, 0.0, max_batch=16)
+    srv = ftb.Server(0, 0.0, max_batch=16, workers=1)
     try:
         srv.pause(True)
         tickets = [None] * len(reqs)
@@ -64,6 +64,26 @@ def test_server_batch_matches_standalone(device):
         _same(a, b)
     assert st["completed"] == len(reqs) and st["rounds"] == 1 and st["mean_batch"] == len(reqs)
     assert 0 < st["p50_s"] <= st["p99_s"]
+
+
+def test_server_two_workers_share_the_queue(device):
+    """Two rounds in flight on two streams: the held queue is shared out, and
+    every result still equals the search run alone."""
+    import fainttrail_b200 as ftb
+    reqs = _requests()
+    alone = [device.search(f, m, e, **kw) for f, m, e, kw in reqs]
+    srv = ftb.Server(0, 0.0, max_batch=16, workers=2)
+    try:
+        srv.pause(True)
+        tickets = [srv.submit(f, m, e, **kw) for f, m, e, kw in reqs]
+        srv.pause(False)
+        got = [srv.poll(t) for t in tickets]
+        st = srv.stats()
+    finally:
+        srv.close()
+    for a, b in zip(got, alone):
+        _same(a, b)
+    assert st["completed"] == len(reqs) and st["rounds"] >= 2
 
 
 def test_server_streaming_and_errors(device):

@@ -19,8 +19,16 @@ def run(backend, frames, **kw):
     return r.max_snr, r.best_v
 
 
+@pytest.fixture(params=[0, 1, 2, 3, 4], ids=["auto", "32x16", "64x8pair", "32x8", "32x4"])
+def shape(request):
+    """Every compiled tile shape (a shape whose windows do not fit falls back)."""
+    ftb.set_tile_shape(request.param)
+    yield request.param
+    ftb.set_tile_shape(0)
+
+
 @pytest.mark.parametrize("name", ["stack_contract.npz", "stack_constant.npz", "stack_nan_table.npz"])
-def test_golden_passes(backend, name):
+def test_golden_passes(backend, shape, name):
     g = golden(name)
     ms, bv = run(backend, g["frames"], t_h=g["t_h"], velocities=g["vel"], min_count=int(g["min_count"]))
     assert same(ms, g["max_snr"]) and same(bv, g["best_v"])
@@ -37,7 +45,7 @@ def test_tie_known_answer(backend):
 
 @pytest.mark.parametrize("w,h,n,seed", [(1, 1, 1, 0), (33, 17, 5, 1), (64, 64, 20, 2), (130, 70, 40, 3),
                                         (200, 37, 64, 4), (96, 40, 120, 5)])
-def test_random_lattice_passes(backend, oracle, w, h, n, seed):
+def test_random_lattice_passes(backend, oracle, shape, w, h, n, seed):
     rng = np.random.default_rng(seed)
     frames = rng.standard_normal((n, h, w)).astype(np.float32)
     if w * h > 4:
@@ -52,7 +60,7 @@ def test_random_lattice_passes(backend, oracle, w, h, n, seed):
     assert same(ms, ms2) and same(bv, bv2)
 
 
-def test_arbitrary_tables_and_integer_ties(backend, oracle):
+def test_arbitrary_tables_and_integer_ties(backend, oracle, shape):
     rng = np.random.default_rng(7)
     n, h, w, m = 11, 45, 70, 300
     # small integers: many exact ties between motions

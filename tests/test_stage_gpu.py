@@ -33,7 +33,7 @@ def test_null_time_orders(device, oracle):
 
 
 @pytest.mark.parametrize("n,w,h,seed,fwhm", [(5, 40, 30, 1, 2.5), (20, 97, 61, 2, 2.5), (40, 128, 96, 3, 3.3),
-                                             (64, 70, 50, 4, 2.0), (120, 48, 40, 5, 4.0)])
+                                             (64, 70, 50, 4, 2.0), (120, 48, 40, 5, 4.0), (200, 40, 24, 6, 2.5)])
 def test_random_sequences(device, oracle, n, w, h, seed, fwhm):
     rng = np.random.default_rng(seed)
     sub = rng.normal(0, 10, (n, h, w)).astype(np.float32)
@@ -47,6 +47,7 @@ def test_random_sequences(device, oracle, n, w, h, seed, fwhm):
     sub[:, :, :3] = np.nan
     sub[rng.integers(0, n), 5:9, 10:14] = np.nan
     sub[: n // 3, -2:, :] = np.nan
+    sub[: n // 2, 2:4, 20:24] = np.nan  # fewer finite values than the static sky needs
     sub[:, 7, :] = np.round(sub[:, 7, :])
     t = np.sort(rng.uniform(-0.3, 0.3, n))
     rng.shuffle(t)
