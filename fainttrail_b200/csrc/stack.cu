@@ -429,6 +429,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return true;
 }
 
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ uint32_t half16(const uint4& q, int k) {
     const uint32_t w = k < 2 ? q.x : k < 4 ? q.y : k < 6 ? q.z : q.w;
     return (k & 1) ? (w >> 16) : (w & 0xffffu);
@@ -536,12 +543,53 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
     }
 }
 
+// Stages group g for the tile at (x0, y0): every frame's window by TMA (the
+// lanes of warp 0 share the copies) and the group's 16-bit offset table by one
+// bulk copy, all completing on the one mbarrier; resets the block counter the
+// warps take 4-motion blocks from. Returns false if the staging wait timed out
+// (every thread then returns; the host reports the error).
+template <int NW, int WP, int BH>
+__device__ __forceinline__ bool stage_group(const StackArgs& a, const StackGroup& G, int g, const CUtensorMap* tmap,
+                                            int x0, int y0, uint64_t* bar, float* win, uint16_t* offs, int* block_next,
+                                            int* err, uint32_t& phase) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    // the previous group's windows and offsets are no longer read, and this
+    // thread's generic-proxy stores are ordered before the async writes below
+    fence_proxy_async();
+    __syncthreads();
+    if (tid < 32) {
+        const uint32_t tab_bytes = static_cast<uint32_t>((G.nslots * a.n + 7) / 8) * 16u;
+        if (lane == 0) {
+            *block_next = NW;  // blocks 0 .. NW-1 go to the warps in order
+            mbar_expect_tx(bar, static_cast<uint32_t>(G.rows_total * WP * 4) + tab_bytes);
+        }
+        __syncwarp();
+        if (lane == 0) bulk_load(offs, a.slot_off + a.slot_off_base[g], tab_bytes, bar);
+        for (int i = lane; i < a.n; i += 32) {
+            const StackWin wv = a.wins[G.win0 + i];
+            for (int b = 0; b < wv.rows; b += BH)
+                tma_load_3d(win + (wv.row0 + b) * WP, tmap, x0 + wv.dx0, y0 + wv.dy0 + b, i, bar);
+        }
+    }
+    const bool ok = mbar_wait_bounded(bar, phase, err);
+    if (__syncthreads_or(!ok)) return false;
+    phase ^= 1u;
+    return true;
+}
+
+// The next 4-motion block for this warp from the group's counter.
+__device__ __forceinline__ int next_block(int* block_next) {
+    int q = 0;
+    if ((threadIdx.x & 31) == 0) q = atomicAdd(block_next, 1);
+    return __shfl_sync(0xffffffffu, q, 0);
+}
+
 // One 32 x P output tile of one pass: the CTA's NW warps share the tile and
 // split each group's 4-motion blocks; per-warp maxima merge through shared memory
 // at the end. Returns false if a staging wait timed out.
 template <int NW, int P, int WP, int BH>
 __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, int y0, uint64_t* bar, float* win,
-                           int* err, uint32_t& phase) {
+                           int* block_next, int* err, uint32_t& phase) {
     constexpr int M = 4;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int x = x0 + lane;
@@ -559,35 +607,15 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
     for (int g = a.g0; g < a.g1; ++g) {
         const StackGroup G = a.groups[g];
         uint16_t* offs = reinterpret_cast<uint16_t*>(win + G.rows_total * WP);
-        // the previous group's windows and offsets are no longer read, and this
-        // thread's generic-proxy stores are ordered before the TMA writes below
-        fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) {
-            mbar_expect_tx(bar, static_cast<uint32_t>(G.rows_total * WP * 4));
-            for (int i = 0; i < a.n; ++i) {
-                const StackWin wv = a.wins[G.win0 + i];
-                for (int b = 0; b < wv.rows; b += BH)
-                    tma_load_3d(win + (wv.row0 + b) * WP, tmap, x0 + wv.dx0, y0 + wv.dy0 + b, i, bar);
-            }
-        }
-        {
-            const int nvec = (G.nslots * a.n + 7) / 8;  // 16-byte chunks of the offset table
-            const uint4* src = reinterpret_cast<const uint4*>(a.slot_off + a.slot_off_base[g]);
-            uint4* dst = reinterpret_cast<uint4*>(offs);
-            for (int q = tid; q < nvec; q += blockDim.x) dst[q] = src[q];
-        }
-        __syncthreads();
-        const bool ok = mbar_wait_bounded(bar, phase, err);
-        if (__syncthreads_or(!ok)) return false;  // staging did not complete: the host reports the error
-        phase ^= 1u;
+        if (!stage_group<NW, WP, BH>(a, G, g, tmap, x0, y0, bar, win, offs, block_next, err, phase)) return false;
         const bool interior = full && x0 + G.gdxmin >= 0 && x0 + 31 + G.gdxmax < a.w && y0 + G.gdymin >= 0 &&
                               y0 + P - 1 + G.gdymax < a.h;
+        // blocks by a shared counter: a warp whose blocks reuse more loads takes more of them
         if (interior) {
-            for (int s0 = warp * M; s0 < G.nslots; s0 += NW * M)
+            for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
                 motion_quad<P, WP, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
         } else {
-            for (int s0 = warp * M; s0 < G.nslots; s0 += NW * M)
+            for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
                 motion_quad<P, WP, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
         }
     }
@@ -773,7 +801,7 @@ __device__ __forceinline__ void motion_quad2(const StackArgs& a, const StackGrou
 // One 64 x P output tile of one pass with paired columns (as stack_tile).
 template <int NW, int P, int WP, int BH>
 __device__ bool stack_tile2(const StackArgs& a, const CUtensorMap* tmap, int x0, int y0, uint64_t* bar, float* win,
-                            int* err, uint32_t& phase) {
+                            int* block_next, int* err, uint32_t& phase) {
     constexpr int M = 4;
     constexpr int TW = 64;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -794,33 +822,14 @@ __device__ bool stack_tile2(const StackArgs& a, const CUtensorMap* tmap, int x0,
     for (int g = a.g0; g < a.g1; ++g) {
         const StackGroup G = a.groups[g];
         uint16_t* offs = reinterpret_cast<uint16_t*>(win + G.rows_total * WP);
-        fence_proxy_async();
-        __syncthreads();
-        if (tid == 0) {
-            mbar_expect_tx(bar, static_cast<uint32_t>(G.rows_total * WP * 4));
-            for (int i = 0; i < a.n; ++i) {
-                const StackWin wv = a.wins[G.win0 + i];
-                for (int b = 0; b < wv.rows; b += BH)
-                    tma_load_3d(win + (wv.row0 + b) * WP, tmap, x0 + wv.dx0, y0 + wv.dy0 + b, i, bar);
-            }
-        }
-        {
-            const int nvec = (G.nslots * a.n + 7) / 8;
-            const uint4* src = reinterpret_cast<const uint4*>(a.slot_off + a.slot_off_base[g]);
-            uint4* dst = reinterpret_cast<uint4*>(offs);
-            for (int q = tid; q < nvec; q += blockDim.x) dst[q] = src[q];
-        }
-        __syncthreads();
-        const bool ok = mbar_wait_bounded(bar, phase, err);
-        if (__syncthreads_or(!ok)) return false;
-        phase ^= 1u;
+        if (!stage_group<NW, WP, BH>(a, G, g, tmap, x0, y0, bar, win, offs, block_next, err, phase)) return false;
         const bool interior = full && x0 + G.gdxmin >= 0 && x0 + TW - 1 + G.gdxmax < a.w && y0 + G.gdymin >= 0 &&
                               y0 + P - 1 + G.gdymax < a.h;
         if (interior) {
-            for (int s0 = warp * M; s0 < G.nslots; s0 += NW * M)
+            for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
                 motion_quad2<P, WP, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
         } else {
-            for (int s0 = warp * M; s0 < G.nslots; s0 += NW * M)
+            for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
                 motion_quad2<P, WP, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
         }
     }
@@ -879,6 +888,7 @@ __global__ void __launch_bounds__(32 * NW, 1)
     unsigned char* base = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     uint64_t* bar = reinterpret_cast<uint64_t*>(base);
     long long* next = reinterpret_cast<long long*>(base + 8);
+    int* block_next = reinterpret_cast<int*>(base + 16);  // the current group's next 4-motion block
     float* win = reinterpret_cast<float*>(base + 128);
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();
@@ -895,9 +905,9 @@ __global__ void __launch_bounds__(32 * NW, 1)
         const long long t = item - a.item0;
         const int tx = static_cast<int>(t % a.tiles_x), ty = a.ty0 + static_cast<int>(t / a.tiles_x);
         if constexpr (TW == 64) {
-            if (!stack_tile2<NW, P, WP, BH>(a, maps + p, tx * 64, ty * P, bar, win, err, phase)) return;
+            if (!stack_tile2<NW, P, WP, BH>(a, maps + p, tx * 64, ty * P, bar, win, block_next, err, phase)) return;
         } else {
-            if (!stack_tile<NW, P, WP, BH>(a, maps + p, tx * 32, ty * P, bar, win, err, phase)) return;
+            if (!stack_tile<NW, P, WP, BH>(a, maps + p, tx * 32, ty * P, bar, win, block_next, err, phase)) return;
         }
     }
 }

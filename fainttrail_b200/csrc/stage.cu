@@ -328,7 +328,6 @@ __global__ void mask_kernel(const float* scatter, float* mask, int w, int h, int
 
 // ------------------------------------------------------------------ matched filter
 
-constexpr int kFTW = 32, kFTH = 16;  // output tile of the filter kernel
 
 struct FilterArgs {
     const float* residual;
@@ -349,16 +348,29 @@ struct FilterArgs {
 // columns and the vertical pass. Pixels outside the image hold 0: a product with
 // 0 adds +0.0f to a sum that starts at +0.0f, which equals the reference's
 // truncated sums at the borders (preprocess.cpp:133-135, 140-145).
+// RT > 0: the filter radius fixed at compile time (the tile loops' index
+// arithmetic by constants, the taps in registers); RT = 0: any radius (a.R).
+// TWc x THc: the output tile.
+template <int RT, int TWc, int THc>
 __global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
     extern __shared__ float fs[];
-    const int R = a.R, H = R + 2;
-    const int ZW = kFTW + 2 * H, ZH = kFTH + 2 * H;
+    const int R = RT > 0 ? RT : a.R, H = R + 2;
+    const int ZW = TWc + 2 * H, ZH = THc + 2 * H;
     float* Z = fs;                                    // ZH x ZW  z, then cleaned z
     unsigned char* F = reinterpret_cast<unsigned char*>(Z + ZW * ZH);  // ZH x ZW cosmic-ray centre flags
-    float* Tt = reinterpret_cast<float*>(F + ((ZW * ZH + 15) / 16) * 16);  // (kFTH + 2R) x kFTW horizontal pass
+    float* Tt = reinterpret_cast<float*>(F + ((ZW * ZH + 15) / 16) * 16);  // (THc + 2R) x TWc horizontal pass
     __shared__ int cr_tile;
+    constexpr int KN = RT > 0 ? 2 * RT + 1 : 1;
+    float kr[KN], kn[KN];  // taps and taps x norm (the reference's float product) when RT > 0
+    if constexpr (RT > 0) {
+#pragma unroll
+        for (int j = 0; j < KN; ++j) {
+            kr[j] = a.k[j];
+            kn[j] = __fmul_rn(kr[j], a.norm);
+        }
+    }
     const int f = blockIdx.z;
-    const int x0 = blockIdx.x * kFTW, y0 = blockIdx.y * kFTH;
+    const int x0 = blockIdx.x * TWc, y0 = blockIdx.y * THc;
     const size_t plane = static_cast<size_t>(a.pitch) * a.h;
     const float inv = __double2float_rn(__ddiv_rn(1.0, a.sigma[f]));
     if (threadIdx.x == 0) cr_tile = 0;
@@ -370,8 +382,9 @@ __global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
             const float v = a.residual[f * plane + pix];
             if (a.mask[pix] != 0.0f && finitef(v)) {
                 const float s = a.scatter[pix];
-                const float ew = s > a.wscat ? s : 1.0f;
-                z = __fdiv_rn(__fmul_rn(v, inv), ew);
+                const float vm = __fmul_rn(v, inv);
+                // (v / sigma) / e with e = scatter above weight_scatter, else 1 (an exact division)
+                z = s > a.wscat ? __fdiv_rn(vm, s) : vm;
             }
         }
         Z[e] = z;
@@ -389,7 +402,7 @@ __global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
                 const float n4 = __fmul_rn(0.25f, s4);
                 if (!(n4 >= __fmul_rn(a.ratio, v))) {
                     flag = 1;
-                    if (gx >= x0 && gx < x0 + kFTW && gy >= y0 && gy < y0 + kFTH) atomicAdd(&cr_tile, 1);
+                    if (gx >= x0 && gx < x0 + TWc && gy >= y0 && gy < y0 + THc) atomicAdd(&cr_tile, 1);
                 }
             }
         }
@@ -414,27 +427,63 @@ __global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
         Zc[e] = zc < -a.clip ? -a.clip : (a.clip < zc ? a.clip : zc);
     }
     __syncthreads();
-    // horizontal pass over rows y0-R .. y0+kFTH+R-1, the tile's columns
-    const int TR = kFTH + 2 * R;
-    for (int e = threadIdx.x; e < TR * kFTW; e += blockDim.x) {
-        const int c = e % kFTW, r = e / kFTW;
+    // horizontal pass over rows y0-R .. y0+THc+R-1, the tile's columns
+    const int TR = THc + 2 * R;
+    for (int e = threadIdx.x; e < TR * TWc; e += blockDim.x) {
+        const int c = e % TWc, r = e / TWc;
         const float* row = Zc + (r + 2) * ZW + (c + 2);  // centre column at H + c, row at 2 + r (= H - R + r)
         float acc = 0.0f;
-        for (int j = 0; j <= 2 * R; ++j) acc = __fadd_rn(acc, __fmul_rn(row[j], a.k[j]));
+        if constexpr (RT > 0) {
+#pragma unroll
+            for (int j = 0; j < KN; ++j) acc = __fadd_rn(acc, __fmul_rn(row[j], kr[j]));
+        } else {
+            for (int j = 0; j <= 2 * R; ++j) acc = __fadd_rn(acc, __fmul_rn(row[j], a.k[j]));
+        }
         const int gy = y0 - R + r;
         Tt[e] = (gy >= 0 && gy < a.h) ? acc : 0.0f;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < kFTW * kFTH; e += blockDim.x) {
-        const int c = e % kFTW, r = e / kFTW;
+    for (int e = threadIdx.x; e < TWc * THc; e += blockDim.x) {
+        const int c = e % TWc, r = e / TWc;
         const int gx = x0 + c, gy = y0 + r;
         if (gx >= a.w || gy >= a.h) continue;
         float acc = 0.0f;
-        for (int j = 0; j <= 2 * R; ++j) acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(a.k[j], a.norm), Tt[(r + j) * kFTW + c]));
+        if constexpr (RT > 0) {
+#pragma unroll
+            for (int j = 0; j < KN; ++j) acc = __fadd_rn(acc, __fmul_rn(kn[j], Tt[(r + j) * TWc + c]));
+        } else {
+            for (int j = 0; j <= 2 * R; ++j)
+                acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(a.k[j], a.norm), Tt[(r + j) * TWc + c]));
+        }
         a.out[f * plane + static_cast<size_t>(gy) * a.pitch + gx] = acc;
     }
     __syncthreads();
     if (threadIdx.x == 0 && cr_tile) atomicAdd(&a.cr[f], cr_tile);
+}
+
+// one launch of the filter kernel for radius R (compile-time radius up to 8)
+template <int RT, int TWc, int THc>
+void launch_filter(const FilterArgs& a, int n, cudaStream_t s) {
+    const int R = RT > 0 ? RT : a.R, H = R + 2, ZW = TWc + 2 * H, ZH = THc + 2 * H;
+    const size_t smem = sizeof(float) * ZW * ZH + ((ZW * ZH + 15) / 16) * 16 + sizeof(float) * (THc + 2 * R) * TWc;
+    auto kern = filter_kernel<RT, TWc, THc>;
+    FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    kern<<<dim3((a.w + TWc - 1) / TWc, (a.h + THc - 1) / THc, n), 256, smem, s>>>(a);
+    FTB_CHECK(cudaGetLastError());
+}
+
+void launch_filter_any(const FilterArgs& a, int n, cudaStream_t s) {
+    switch (a.R) {
+        case 1: launch_filter<1, 64, 32>(a, n, s); break;
+        case 2: launch_filter<2, 64, 32>(a, n, s); break;
+        case 3: launch_filter<3, 64, 32>(a, n, s); break;
+        case 4: launch_filter<4, 64, 32>(a, n, s); break;
+        case 5: launch_filter<5, 64, 32>(a, n, s); break;
+        case 6: launch_filter<6, 64, 32>(a, n, s); break;
+        case 7: launch_filter<7, 64, 32>(a, n, s); break;
+        case 8: launch_filter<8, 64, 32>(a, n, s); break;
+        default: launch_filter<0, 32, 16>(a, n, s); break;
+    }
 }
 
 __global__ void rescale_kernel(float* g, size_t plane, int w, int h, int pitch, const double* sg) {
@@ -674,11 +723,7 @@ void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const Stage
         a.h = h;
         a.pitch = pitch;
         a.R = R;
-        const int H = R + 2, ZW = kFTW + 2 * H, ZH = kFTH + 2 * H;
-        const size_t smem = sizeof(float) * ZW * ZH + ((ZW * ZH + 15) / 16) * 16 + sizeof(float) * (kFTH + 2 * R) * kFTW;
-        FTB_CHECK(cudaFuncSetAttribute(filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        filter_kernel<<<dim3((w + kFTW - 1) / kFTW, (h + kFTH - 1) / kFTH, n), 256, smem, s>>>(a);
-        FTB_CHECK(cudaGetLastError());
+        launch_filter_any(a, n, s);
         ++c.launches;
         c.span_end(span);
     }

@@ -33,7 +33,8 @@ def test_null_time_orders(device, oracle):
 
 
 @pytest.mark.parametrize("n,w,h,seed,fwhm", [(5, 40, 30, 1, 2.5), (20, 97, 61, 2, 2.5), (40, 128, 96, 3, 3.3),
-                                             (64, 70, 50, 4, 2.0), (120, 48, 40, 5, 4.0), (200, 40, 24, 6, 2.5)])
+                                             (64, 70, 50, 4, 2.0), (120, 48, 40, 5, 4.0), (200, 40, 24, 6, 2.5),
+                                             (12, 90, 70, 7, 7.0), (16, 150, 100, 8, 1.2)])
 def test_random_sequences(device, oracle, n, w, h, seed, fwhm):
     rng = np.random.default_rng(seed)
     sub = rng.normal(0, 10, (n, h, w)).astype(np.float32)
