@@ -8,7 +8,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <numeric>
+#include <thread>
 
 #include "search.h"
 
@@ -202,7 +204,10 @@ std::vector<Peak> device_peaks(Context& c, const float* d_max, const int* d_best
             continue;
         }
         std::vector<PeakRec> rec(static_cast<size_t>(count));
-        if (count) FTB_CHECK(cudaMemcpy(rec.data(), d_out, sizeof(PeakRec) * count, cudaMemcpyDeviceToHost));
+        if (count) {
+            FTB_CHECK(cudaMemcpyAsync(rec.data(), d_out, sizeof(PeakRec) * count, cudaMemcpyDeviceToHost, s));
+            FTB_CHECK(cudaStreamSynchronize(s));
+        }
         // the reference visits pixels in raster order; restore it
         std::sort(rec.begin(), rec.end(), [](const PeakRec& a, const PeakRec& b) {
             return a.y != b.y ? a.y < b.y : a.x < b.x;
@@ -211,6 +216,119 @@ std::vector<Peak> device_peaks(Context& c, const float* d_max, const int* d_best
         for (size_t k = 0; k < rec.size(); ++k) out[k] = {rec[k].x, rec[k].y, rec[k].snr, rec[k].vidx};
         return out;
     }
+}
+
+std::vector<std::vector<Peak>> device_peaks_many(Context& c, const std::vector<PeakMap>& maps, int w, int h,
+                                                 float floor, int radius, int edge, size_t keep) {
+    const size_t k_maps = maps.size();
+    std::vector<std::vector<Peak>> out(k_maps);
+    if (k_maps == 0) return out;
+    cudaStream_t s = c.stream();
+    const int cap = std::max(1 << 16, static_cast<int>(std::min<long long>(1LL << 22, static_cast<long long>(w) * h / 16)));
+    const size_t head = ((sizeof(int) * k_maps + 255) / 256) * 256;
+    DevBuf& buf = c.scratch(22, head + sizeof(PeakRec) * static_cast<size_t>(cap) * k_maps, "peaks (batch)");
+    int* d_count = reinterpret_cast<int*>(buf.as<unsigned char>());
+    PeakRec* d_rec = reinterpret_cast<PeakRec*>(buf.as<unsigned char>() + head);
+    FTB_CHECK(cudaMemsetAsync(d_count, 0, sizeof(int) * k_maps, s));
+    const long long npix = static_cast<long long>(w) * h;
+    for (size_t k = 0; k < k_maps; ++k) {
+        peak_kernel<<<static_cast<unsigned>((npix + 255) / 256), 256, 0, s>>>(
+            maps[k].d_max, maps[k].d_best_v, w, h, floor, radius, edge, d_count + k, d_rec + k * cap, cap);
+        FTB_CHECK(cudaGetLastError());
+        ++c.launches;
+    }
+    std::vector<int> count(k_maps);
+    FTB_CHECK(cudaMemcpyAsync(count.data(), d_count, sizeof(int) * k_maps, cudaMemcpyDeviceToHost, s));
+    FTB_CHECK(cudaStreamSynchronize(s));
+    std::vector<std::vector<PeakRec>> rec(k_maps);
+    for (size_t k = 0; k < k_maps; ++k) {
+        if (count[k] > cap) continue;  // overflow: found again alone below
+        rec[k].resize(static_cast<size_t>(count[k]));
+        if (count[k])
+            FTB_CHECK(cudaMemcpyAsync(rec[k].data(), d_rec + k * cap, sizeof(PeakRec) * count[k],
+                                      cudaMemcpyDeviceToHost, s));
+    }
+    FTB_CHECK(cudaStreamSynchronize(s));
+    for (size_t k = 0; k < k_maps; ++k)
+        if (count[k] > cap) out[k] = device_peaks(c, maps[k].d_max, maps[k].d_best_v, w, h, floor, radius, edge);
+    // host ordering, one map per thread: raster order (the reference's visit
+    // order), then order_peaks' std::sort by S/N and the truncation
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t workers = std::min<size_t>(hw, k_maps);
+    std::vector<std::thread> pool;
+    for (size_t wk = 0; wk < workers; ++wk)
+        pool.emplace_back([&, wk] {
+            for (size_t k = wk; k < k_maps; k += workers) {
+                if (count[k] > cap) {
+                    order_peaks(out[k], keep);
+                    continue;
+                }
+                std::vector<PeakRec>& r = rec[k];
+                std::sort(r.begin(), r.end(),
+                          [](const PeakRec& a, const PeakRec& b) { return a.y != b.y ? a.y < b.y : a.x < b.x; });
+                out[k].resize(r.size());
+                for (size_t q = 0; q < r.size(); ++q) out[k][q] = {r[q].x, r[q].y, r[q].snr, r[q].vidx};
+                order_peaks(out[k], keep);
+            }
+        });
+    for (auto& t : pool) t.join();
+    return out;
+}
+
+std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vector<ArtefactJob>& jobs,
+                                                     const std::vector<std::pair<double, double>>& grid,
+                                                     const float* d_sub, int w, int h, int n, double fwhm_px,
+                                                     double max_frame_fraction) {
+    std::vector<std::vector<char>> out(jobs.size());
+    size_t total = 0;
+    for (size_t k = 0; k < jobs.size(); ++k) {
+        out[k].assign(jobs[k].count, 0);
+        total += jobs[k].count;
+    }
+    if (total == 0) return out;
+    cudaStream_t s = c.stream();
+    // per job: its peaks and times, then one flag per peak; the grid once
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    std::vector<size_t> off(jobs.size());
+    size_t bytes = al(sizeof(double) * 2 * grid.size());
+    for (size_t k = 0; k < jobs.size(); ++k) {
+        off[k] = bytes;
+        bytes += al(sizeof(PeakRec) * jobs[k].count) + al(sizeof(double) * n) + al(jobs[k].count);
+    }
+    DevBuf& buf = c.scratch(23, bytes, "artefact screen (batch)");
+    unsigned char* base = buf.as<unsigned char>();
+    std::vector<unsigned char> host(bytes);
+    std::memcpy(host.data(), grid.data(), sizeof(double) * 2 * grid.size());
+    for (size_t k = 0; k < jobs.size(); ++k) {
+        PeakRec* r = reinterpret_cast<PeakRec*>(host.data() + off[k]);
+        for (size_t q = 0; q < jobs[k].count; ++q) {
+            const Peak& p = (*jobs[k].peaks)[q];
+            r[q] = {p.x, p.y, p.snr, p.vidx};
+        }
+        std::memcpy(host.data() + off[k] + al(sizeof(PeakRec) * jobs[k].count), jobs[k].t_h->data(), sizeof(double) * n);
+    }
+    FTB_CHECK(cudaMemcpyAsync(base, host.data(), bytes, cudaMemcpyHostToDevice, s));
+    const int r = static_cast<int>(std::ceil(2.0 * fwhm_px)) + 1;
+    for (size_t k = 0; k < jobs.size(); ++k) {
+        if (jobs[k].count == 0) continue;
+        unsigned char* b = base + off[k];
+        const double* d_t = reinterpret_cast<const double*>(b + al(sizeof(PeakRec) * jobs[k].count));
+        char* d_out = reinterpret_cast<char*>(b + al(sizeof(PeakRec) * jobs[k].count) + al(sizeof(double) * n));
+        ArtArgs a{reinterpret_cast<const PeakRec*>(b), static_cast<int>(jobs[k].count),
+                  reinterpret_cast<const double*>(base), jobs[k].d_filtered, d_sub, jobs[k].d_sky, d_t, w, h,
+                  frame_pitch(w), n, r, max_frame_fraction, d_out};
+        artefact_kernel<<<static_cast<unsigned>((jobs[k].count + 127) / 128), 128, 0, s>>>(a);
+        FTB_CHECK(cudaGetLastError());
+        ++c.launches;
+    }
+    FTB_CHECK(cudaMemcpyAsync(host.data(), base, bytes, cudaMemcpyDeviceToHost, s));
+    FTB_CHECK(cudaStreamSynchronize(s));
+    for (size_t k = 0; k < jobs.size(); ++k)
+        if (jobs[k].count)
+            std::memcpy(out[k].data(),
+                        host.data() + off[k] + al(sizeof(PeakRec) * jobs[k].count) + al(sizeof(double) * n),
+                        jobs[k].count);
+    return out;
 }
 
 std::vector<char> device_artefacts(Context& c, const std::vector<Peak>& peaks, size_t count,
@@ -434,18 +552,33 @@ void SearchRequest::finish_items(int k0, int k1) {
         order_peaks(o_.peaks, 100000);
         real_done_ = true;
     }
-    for (int k = k0; k < std::min(k1, runs_); ++k) {
-        Item& it = items_.at(k);
-        std::vector<Peak> npk = device_peaks(c, it.max.as<float>(), it.bv.as<int>(), w, h, 3.0f, nms_, edge_);
-        order_peaks(npk, 20000);
-        const size_t tested =
-            (p_.gauss_model && p_.null_tested > 0) ? std::min(npk.size(), static_cast<size_t>(p_.null_tested)) : 0;
-        const std::vector<char> art = device_artefacts(c, npk, tested, o_.grid, it.filt.as<float>(), sub_.as<float>(),
-                                                       it.sky.as<float>(), orders_[static_cast<size_t>(k)], w, h, n,
-                                                       o_.fwhm_px, p_.max_frame_fraction);
-        for (size_t q = 0; q < npk.size(); ++q)
-            if (q >= art.size() || !art[q]) pooled_.push_back(npk[q].snr);
-        items_.erase(k);  // the null run's buffers are released in stream order
+    // the null runs of this batch together: peaks of every map, then the
+    // artefact screen of every run's strongest peaks, then pooling in run order
+    const int kn1 = std::min(k1, runs_);
+    if (k0 < kn1) {
+        std::vector<PeakMap> maps;
+        for (int k = k0; k < kn1; ++k) {
+            Item& it = items_.at(k);
+            maps.push_back({it.max.as<float>(), it.bv.as<int>()});
+        }
+        const std::vector<std::vector<Peak>> npk = device_peaks_many(c, maps, w, h, 3.0f, nms_, edge_, 20000);
+        std::vector<ArtefactJob> jobs;
+        for (int k = k0; k < kn1; ++k) {
+            Item& it = items_.at(k);
+            const std::vector<Peak>& pk = npk[static_cast<size_t>(k - k0)];
+            const size_t tested =
+                (p_.gauss_model && p_.null_tested > 0) ? std::min(pk.size(), static_cast<size_t>(p_.null_tested)) : 0;
+            jobs.push_back({&pk, tested, it.filt.as<float>(), it.sky.as<float>(), &orders_[static_cast<size_t>(k)]});
+        }
+        const std::vector<std::vector<char>> art = device_artefacts_many(c, jobs, o_.grid, sub_.as<float>(), w, h, n,
+                                                                         o_.fwhm_px, p_.max_frame_fraction);
+        for (int k = k0; k < kn1; ++k) {
+            const std::vector<Peak>& pk = npk[static_cast<size_t>(k - k0)];
+            const std::vector<char>& a = art[static_cast<size_t>(k - k0)];
+            for (size_t q = 0; q < pk.size(); ++q)
+                if (q >= a.size() || !a[q]) pooled_.push_back(pk[q].snr);
+            items_.erase(k);  // the null run's buffers are released in stream order
+        }
     }
     for (int k = std::max(k0, runs_); k < k1; ++k) {  // copies keep only their maps
         Item& it = items_.at(k);

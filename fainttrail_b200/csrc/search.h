@@ -75,6 +75,28 @@ std::vector<char> device_artefacts(Context& c, const std::vector<Peak>& peaks, s
                                    const float* d_sub, const float* d_sky, const std::vector<double>& t_h, int w,
                                    int h, int n, double fwhm_px, double max_frame_fraction);
 
+// The same for many maps at once (the null runs of a batch): every peak kernel
+// is queued, one sync brings all candidate lists back, and the host orders them
+// (raster order, then order_peaks with `keep`) on a thread per map.
+struct PeakMap {
+    const float* d_max;
+    const int* d_best_v;
+};
+std::vector<std::vector<Peak>> device_peaks_many(Context& c, const std::vector<PeakMap>& maps, int w, int h,
+                                                 float floor, int radius, int edge, size_t keep);
+// artefact flags of the first count[k] peaks of every null run k, one sync
+struct ArtefactJob {
+    const std::vector<Peak>* peaks;
+    size_t count;
+    const float* d_filtered;
+    const float* d_sky;
+    const std::vector<double>* t_h;
+};
+std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vector<ArtefactJob>& jobs,
+                                                     const std::vector<std::pair<double, double>>& grid,
+                                                     const float* d_sub, int w, int h, int n, double fwhm_px,
+                                                     double max_frame_fraction);
+
 // An object injected into every frame of a copy (Injection, validate.hpp:18-23).
 struct Injection {
     double x_ref = 0, y_ref = 0, vx_pxh = 0, vy_pxh = 0, flux = 0;
