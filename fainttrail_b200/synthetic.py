@@ -53,6 +53,8 @@ WORKLOADS = {
     "fullframe-4k": Workload("fullframe-4k", 4096, 4096, 40, 30.0, 30.0, 200, 20, (4.0, 10.0), (0.1, 2.0), 3),
     # the full-frame search on a quarter of the area (profiling case; frames still exceed L2)
     "fullframe-2k": Workload("fullframe-2k", 2048, 2048, 40, 30.0, 30.0, 200, 20, (4.0, 10.0), (0.1, 2.0), 3),
+    # the full-frame search on 1/16 of the area (ncu captures of the whole-search kernels)
+    "fullframe-1k": Workload("fullframe-1k", 1024, 1024, 40, 30.0, 30.0, 50, 5, (4.0, 10.0), (0.1, 2.0), 3),
     # batched null calibration + completeness: 30 x 2048^2, 64 nulls + 16 injection copies
     "batched-2k": Workload("batched-2k", 2048, 2048, 30, 60.0, 45.0, 200, 0, (2.0, 8.0), (0.2, 1.1), 64,
                            extra=dict(injection_copies=16, injected_movers=50)),
