@@ -47,6 +47,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "pixel·frame·motion/s"
+SHAPES = {0: "by frame count", 1: "32x16, 12 warps", 2: "64x8 paired columns, 12 warps", 3: "32x8, 16 warps",
+          4: "32x4, 16 warps", 5: "32x16 shared maximum, 16 warps", 6: "32x16 shared maximum, 14 warps"}
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -59,6 +61,7 @@ def parse():
     ap.add_argument("--workload", default="fullframe-4k")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tile-shape", type=int, default=0, help="stack kernel tile shape (0: autotuned)")
     return ap.parse_args()
 
 
@@ -215,6 +218,7 @@ def b200_arm(args):
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local_rank)
+    ftb.set_tile_shape(args.tile_shape)
     if args.workload == "serving":
         return serving_arm(args, rank, local_rank, world, dist)
     wl = synthetic.WORKLOADS[args.workload]
@@ -263,6 +267,7 @@ def b200_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total = float(t.item())
     value = world * args.steps * adds_step / total
+    shape_used = args.tile_shape or ftb.tuned_shapes().get((n, m, w, h), 0)
     peaks, peak_kind = measured_peaks()
     sms = dev.info()[1]
     fp32_peak = sms * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12  # non-FMA adds, TFLOP/s
@@ -341,7 +346,8 @@ def b200_arm(args):
                           "l2": f"inputs ({4 * n * h * w / 1e9:.1f} GB of frames) exceed the {L2_BYTES >> 20} MB L2"},
                "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                             "frac": achieved / fp32_peak, "traffic": traffic,
-                            "kernel": "stack_batch_kernel (one persistent launch for all passes of a search)",
+                            "kernel": "stack_batch_kernel (one persistent launch for all passes of a search), "
+                                      "tile shape " + SHAPES.get(shape_used, str(shape_used)),
                             "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x sm_max_mhz "
                                            f"{peaks.get('sm_max_mhz', 1965.0):g} MHz ({peak_kind} peaks file has no "
                                            f"FP32 figure); adds are non-FMA, one per lane per clock"},

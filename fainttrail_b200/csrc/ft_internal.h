@@ -51,6 +51,7 @@ struct StackConfig {         // one compiled kernel variant
     int wp = 40;             // window pitch in floats
     int bh = 4;              // TMA box height (rows)
     int mblock = 4;          // motions accumulated together in registers
+    int merge = 0;           // 0: best/argmax per thread; 1: one shared maximum per tile (atomicMax)
     int smem_bytes = 200 * 1024;
 };
 
@@ -81,8 +82,9 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
 StackConfig choose_stack_config(int w, int h, int n, int device_smem_optin);
 
 // Compiled stack kernel shapes: 1 = 32 x 16 tiles (12 warps), 2 = 64 x 8 tiles with
-// paired columns (12 warps), 3 = 32 x 8 (16 warps), 4 = 32 x 4 (16 warps).
-constexpr int kStackShapes = 4;
+// paired columns (12 warps), 3 = 32 x 8 (16 warps), 4 = 32 x 4 (16 warps),
+// 5 = 32 x 16 with one shared maximum per tile (16 warps), 6 = the same with 14 warps.
+constexpr int kStackShapes = 6;
 StackConfig stack_shape_config(int shape, int device_smem_optin);
 bool stack_shape_fits(const StackConfig& c, int n);
 // A process-wide choice for choose_stack_config: 0 = by frame count, else a shape

@@ -114,6 +114,14 @@ StackConfig stack_shape_config(int shape, int smem_optin) {
         case 2: c.tile_w = 64; c.wp = 72; c.p = 8; c.ty = 12; break;
         case 3: c.tile_w = 32; c.wp = 40; c.p = 8; c.ty = 16; break;
         case 4: c.tile_w = 32; c.wp = 40; c.p = 4; c.ty = 16; break;
+        case 5:  // 32 x 16 with the shared maximum: 16 warps
+            c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 16; c.merge = 1;
+            c.smem_bytes -= 32 * 16 * 8;  // the keys sit ahead of the windows
+            break;
+        case 6:  // the same with 14 warps (146 registers a thread)
+            c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 14; c.merge = 1;
+            c.smem_bytes -= 32 * 16 * 8;
+            break;
         default: throw std::runtime_error("stack: unknown tile shape");
     }
     return c;
@@ -134,9 +142,9 @@ StackConfig choose_stack_config(int w, int h, int n, int smem_optin) {
         const StackConfig c = stack_shape_config(forced, smem_optin);
         if (stack_shape_fits(c, n)) return c;
     }
-    // the first shape whose windows fit: paired 64 x 8 tiles, then single-column
-    // tiles of 16, 8 and 4 rows (taller frame stacks need the shorter tiles)
-    for (int s : {2, 1, 3}) {
+    // the first shape whose windows fit: single-column tiles of 16, 8 and 4 rows
+    // (taller frame stacks need the shorter tiles)
+    for (int s : {1, 3}) {
         const StackConfig c = stack_shape_config(s, smem_optin);
         if (stack_shape_fits(c, n)) return c;
     }
@@ -660,6 +668,156 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
     return true;
 }
 
+// ---- one shared maximum per tile: instead of a best/argmax pair per pixel in
+// every thread, the CTA's warps merge into one array of 64-bit keys in shared
+// memory with atomicMax. key = (order-preserving bits of S/N) << 32 | ~index,
+// so a larger S/N wins and equal S/N goes to the lower motion index -- the
+// reference's rule. S/N is never -0.0 (sums start at +0.0f and round to
+// nearest) and -inf / NaN never enter, as in the register rule. Frees 2P
+// registers per thread, so 16-row tiles run 16 warps.
+
+__device__ __forceinline__ unsigned long long snr_key(float s, int j) {
+    const uint32_t b = __float_as_uint(s);
+    const uint32_t o = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    return (static_cast<unsigned long long>(o) << 32) | static_cast<uint32_t>(~j);
+}
+
+__device__ __forceinline__ void snr_unkey(unsigned long long k, float& s, int& j) {
+    const uint32_t o = static_cast<uint32_t>(k >> 32);
+    s = __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+    j = static_cast<int>(~static_cast<uint32_t>(k));
+}
+
+template <int P, int WP, bool BORDER>
+__device__ __forceinline__ void motion_quad_atom(const StackArgs& a, const StackGroup& G, int s0,
+                                                 const float* __restrict__ win, const uint16_t* __restrict__ offs,
+                                                 int tb, int x, int x0, int y0, float inv_n, unsigned long long* keys) {
+    constexpr int M = 4;
+    constexpr int PW = (P + 3) / 4;
+    float acc[M][P];
+#pragma unroll
+    for (int k = 0; k < M; ++k)
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[k][p] = 0.0f;
+    int cfull[M] = {0, 0, 0, 0};
+    uint32_t cpart[M][PW];
+#pragma unroll
+    for (int k = 0; k < M; ++k)
+#pragma unroll
+        for (int w = 0; w < PW; ++w) cpart[k][w] = 0;
+    const uint16_t* op = offs + s0;
+    uint2 qn = *reinterpret_cast<const uint2*>(op);
+    for (int i = 0; i < a.n; ++i) {
+        const uint2 q = qn;
+        if (i + 1 < a.n) qn = *reinterpret_cast<const uint2*>(op + (i + 1) * G.nslots);
+        const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
+        float v[P];
+        load_column<P, WP>(v, win + o0 + tb);
+        add_column<P>(acc[0], v);
+        if (o1 != o0) load_column<P, WP>(v, win + o1 + tb);
+        add_column<P>(acc[1], v);
+        if (o2 != o1) load_column<P, WP>(v, win + o2 + tb);
+        add_column<P>(acc[2], v);
+        if (o3 != o2) load_column<P, WP>(v, win + o3 + tb);
+        add_column<P>(acc[3], v);
+        if constexpr (BORDER) {
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * a.n + i];
+                const bool whole = x0 + sh.x >= 0 && x0 + 31 + sh.x < a.w && y0 + sh.y >= 0 && y0 + P - 1 + sh.y < a.h;
+                if (whole) {
+                    ++cfull[k];
+                } else {
+                    const bool inx = static_cast<unsigned>(x + sh.x) < static_cast<unsigned>(a.w);
+#pragma unroll
+                    for (int p = 0; p < P; ++p)
+                        if (inx && static_cast<unsigned>(y0 + p + sh.y) < static_cast<unsigned>(a.h))
+                            cpart[k][p / 4] += 1u << (8 * (p % 4));
+                }
+            }
+        }
+    }
+    int js[M];
+#pragma unroll
+    for (int k = 0; k < M; ++k) js[k] = a.slot_motion[G.slot0 + s0 + k];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        // the block's best for this pixel, then one atomic
+        float bs = -CUDART_INF_F;
+        int bj = -1;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            if (js[k] < 0) continue;
+            float f = inv_n;
+            if constexpr (BORDER) {
+                const int c = cfull[k] + static_cast<int>((cpart[k][p / 4] >> (8 * (p % 4))) & 0xffu);
+                if (c < a.min_count) continue;
+                f = a.inv_sqrt[c];
+            }
+            const float sv = __fmul_rn(acc[k][p], f);
+            if (sv > bs || (sv == bs && bj >= 0 && js[k] < bj)) {
+                bs = sv;
+                bj = js[k];
+            }
+        }
+        if (bj >= 0 && bs > -CUDART_INF_F) atomicMax(keys + p * 32 + (tb & 31), snr_key(bs, bj));
+    }
+}
+
+// One 32 x P output tile with the shared maximum (as stack_tile otherwise).
+template <int NW, int P, int WP, int BH>
+__device__ bool stack_tile_atom(const StackArgs& a, const CUtensorMap* tmap, int x0, int y0, uint64_t* bar,
+                                unsigned long long* keys, float* win, int* block_next, int* err, uint32_t& phase) {
+    constexpr int M = 4;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int x = x0 + lane;
+    const int tb = lane;
+    // the tile's running maximum: empty, or the stored one of a continued pass
+    for (int q = tid; q < 32 * P; q += 32 * NW) {
+        unsigned long long k = 0ull;
+        const int xx = x0 + (q & 31), yy = y0 + (q >> 5);
+        if (!a.first && xx < a.w && yy < a.h) {
+            const size_t o = static_cast<size_t>(yy) * a.w + xx;
+            if (a.arg[o] >= 0) k = snr_key(a.best[o], a.arg[o]);
+        }
+        keys[q] = k;
+    }
+    const bool full = x0 + 31 < a.w && y0 + P - 1 < a.h;
+    const float inv_n = a.inv_sqrt[a.n];
+    for (int g = a.g0; g < a.g1; ++g) {
+        const StackGroup G = a.groups[g];
+        uint16_t* offs = reinterpret_cast<uint16_t*>(win + G.rows_total * WP);
+        if (!stage_group<NW, WP, BH>(a, G, g, tmap, x0, y0, bar, win, offs, block_next, err, phase)) return false;
+        const bool interior = full && x0 + G.gdxmin >= 0 && x0 + 31 + G.gdxmax < a.w && y0 + G.gdymin >= 0 &&
+                              y0 + P - 1 + G.gdymax < a.h;
+        if (interior) {
+            for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
+                motion_quad_atom<P, WP, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
+        } else {
+            for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
+                motion_quad_atom<P, WP, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
+        }
+    }
+    __syncthreads();
+    for (int q = tid; q < 32 * P; q += 32 * NW) {
+        const int xx = x0 + (q & 31), yy = y0 + (q >> 5);
+        if (xx >= a.w || yy >= a.h) continue;
+        const size_t o = static_cast<size_t>(yy) * a.w + xx;
+        float b = -CUDART_INF_F;
+        int ar = -1;
+        if (keys[q] != 0ull) snr_unkey(keys[q], b, ar);
+        if (a.last) {
+            a.max_snr[o] = isfinite(b) ? b : 0.0f;
+            a.best_v[o] = ar;
+        } else {
+            a.best[o] = b;
+            a.arg[o] = ar;
+        }
+    }
+    __syncthreads();  // the keys are reset by the next tile
+    return true;
+}
+
 // ---- paired columns: each thread owns two adjacent columns of P rows, so a
 // warp covers a 64-wide tile. Every add is a packed add.rn.f32x2 on the pair
 // (two independent round-to-nearest float adds, bit-identical to two scalar
@@ -879,7 +1037,7 @@ __device__ bool stack_tile2(const StackArgs& a, const CUtensorMap* tmap, int x0,
 // batch is done, so passes of different shapes and sizes share one launch and
 // the SMs stay busy to the end. TW: tile width, 32 (one column per thread) or
 // 64 (paired columns).
-template <int NW, int P, int WP, int BH, int TW>
+template <int NW, int P, int WP, int BH, int TW, int MERGE>
 __global__ void __launch_bounds__(32 * NW, 1)
     stack_batch_kernel(const StackArgs* __restrict__ passes, const CUtensorMap* __restrict__ maps, int npasses,
                        long long items, int* queue, int* err) {
@@ -889,7 +1047,9 @@ __global__ void __launch_bounds__(32 * NW, 1)
     uint64_t* bar = reinterpret_cast<uint64_t*>(base);
     long long* next = reinterpret_cast<long long*>(base + 8);
     int* block_next = reinterpret_cast<int*>(base + 16);  // the current group's next 4-motion block
-    float* win = reinterpret_cast<float*>(base + 128);
+    // MERGE: the tile's shared maximum (32 x P keys) ahead of the windows
+    unsigned long long* keys = reinterpret_cast<unsigned long long*>(base + 128);
+    float* win = reinterpret_cast<float*>(base + 128 + (MERGE ? 32 * P * 8 : 0));
     if (threadIdx.x == 0) mbar_init(bar, 1);
     __syncthreads();
     uint32_t phase = 0;
@@ -906,6 +1066,9 @@ __global__ void __launch_bounds__(32 * NW, 1)
         const int tx = static_cast<int>(t % a.tiles_x), ty = a.ty0 + static_cast<int>(t / a.tiles_x);
         if constexpr (TW == 64) {
             if (!stack_tile2<NW, P, WP, BH>(a, maps + p, tx * 64, ty * P, bar, win, block_next, err, phase)) return;
+        } else if constexpr (MERGE == 1) {
+            if (!stack_tile_atom<NW, P, WP, BH>(a, maps + p, tx * 32, ty * P, bar, keys, win, block_next, err, phase))
+                return;
         } else {
             if (!stack_tile<NW, P, WP, BH>(a, maps + p, tx * 32, ty * P, bar, win, block_next, err, phase)) return;
         }
@@ -926,7 +1089,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-template <int NW, int P, int WP, int BH, int TW>
+template <int NW, int P, int WP, int BH, int TW, int MERGE>
 void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, size_t desc_bytes, int* d_err,
                   int sms, cudaStream_t s) {
     const size_t np = batch.size();
@@ -935,11 +1098,13 @@ void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, si
     CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(host.data() + 128);
     StackArgs* args = reinterpret_cast<StackArgs*>(host.data() + 128 + 128 * np);
     long long items = 0;
-    size_t smem = 256 + static_cast<size_t>(NW) * TW * P * 8;  // the warps' maxima at the end of a tile
+    // the warps' maxima at the end of a tile, or (MERGE) the shared keys ahead of the windows
+    const size_t keys_bytes = MERGE ? static_cast<size_t>(32) * P * 8 : 0;
+    size_t smem = MERGE ? 256 + keys_bytes : 256 + static_cast<size_t>(NW) * TW * P * 8;
     for (size_t k = 0; k < np; ++k) {
         const BatchPass& bp = batch[k];
         const StackPlan& plan = *bp.plan;
-        if (plan.cfg.ty != NW || plan.cfg.p != P || plan.cfg.tile_w != TW || plan.cfg.wp != WP)
+        if (plan.cfg.ty != NW || plan.cfg.p != P || plan.cfg.tile_w != TW || plan.cfg.wp != WP || plan.cfg.merge != MERGE)
             throw std::runtime_error("stack batch: passes of different kernel shapes");
         const cuuint64_t dims[3] = {static_cast<cuuint64_t>(plan.w), static_cast<cuuint64_t>(plan.h),
                                     static_cast<cuuint64_t>(plan.n)};
@@ -983,13 +1148,13 @@ void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, si
         a.max_snr = bp.max_snr;
         a.best_v = bp.best_v;
         a.err = d_err;
-        smem = std::max(smem, 256 + static_cast<size_t>(plan.max_group_bytes));
-        if (smem > static_cast<size_t>(plan.cfg.smem_bytes) + 256)
+        smem = std::max(smem, 256 + keys_bytes + static_cast<size_t>(plan.max_group_bytes));
+        if (smem > static_cast<size_t>(plan.cfg.smem_bytes) + 256 + keys_bytes)
             throw std::runtime_error("stack plan exceeds shared memory");
     }
     if (items == 0) return;
     FTB_CHECK(cudaMemcpyAsync(d_desc, host.data(), host.size(), cudaMemcpyHostToDevice, s));
-    auto kern = stack_batch_kernel<NW, P, WP, BH, TW>;
+    auto kern = stack_batch_kernel<NW, P, WP, BH, TW, MERGE>;
     FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     const int ctas = static_cast<int>(std::min<long long>(items, sms));
     kern<<<ctas, 32 * NW, smem, s>>>(reinterpret_cast<const StackArgs*>(d_desc + 128 + 128 * np),
@@ -1009,14 +1174,18 @@ void stack_launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_de
     if (batch.empty()) return;
     const StackConfig& c = batch[0].plan->cfg;
     if (c.bh != 4 || c.mblock != 4) throw std::runtime_error("stack: unsupported kernel configuration");
-    if (c.tile_w == 64 && c.wp == 72 && c.ty == 12 && c.p == 8)
-        launch_batch<12, 8, 72, 4, 64>(batch, d_desc, desc_bytes, d_err, sms, s);
-    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 12 && c.p == 16)
-        launch_batch<12, 16, 40, 4, 32>(batch, d_desc, desc_bytes, d_err, sms, s);
-    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 8)
-        launch_batch<16, 8, 40, 4, 32>(batch, d_desc, desc_bytes, d_err, sms, s);
-    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 4)
-        launch_batch<16, 4, 40, 4, 32>(batch, d_desc, desc_bytes, d_err, sms, s);
+    if (c.tile_w == 64 && c.wp == 72 && c.ty == 12 && c.p == 8 && c.merge == 0)
+        launch_batch<12, 8, 72, 4, 64, 0>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 12 && c.p == 16 && c.merge == 0)
+        launch_batch<12, 16, 40, 4, 32, 0>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 8 && c.merge == 0)
+        launch_batch<16, 8, 40, 4, 32, 0>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 4 && c.merge == 0)
+        launch_batch<16, 4, 40, 4, 32, 0>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 16 && c.merge == 1)
+        launch_batch<16, 16, 40, 4, 32, 1>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 14 && c.p == 16 && c.merge == 1)
+        launch_batch<14, 16, 40, 4, 32, 1>(batch, d_desc, desc_bytes, d_err, sms, s);
     else
         throw std::runtime_error("stack: unsupported tile shape");
 }
