@@ -408,9 +408,16 @@ class Device:
             for j in range(nv.value):
                 L.ft_b200_result_velocity(r, j, C.byref(vx), C.byref(vy))
                 grid[j] = (vx.value, vy.value)
+            L.ft_b200_result_candidates.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]
+            nc = L.ft_b200_result_candidates(r, None, None, 0)
+            rows = np.empty((max(nc, 1), 17))
+            fl = C.create_string_buffer(64 * max(nc, 1))
+            L.ft_b200_result_candidates(r, rows.ctypes.data_as(C.c_void_p), fl, nc)
+            cands = [(rows[q].copy(), fl.raw[64 * q:64 * q + 64].split(b"\0", 1)[0].decode()) for q in range(nc)]
             return dict(threshold=thr, method=meth.value.decode(), null_a=a.value, null_b=b.value, null_k=k.value,
                         null_inv_s2=s2.value, fwhm=fw.value, dv=dv.value, t_ref=tref.value, n_velocities=nv.value,
-                        peaks=peaks(0), selected=peaks(1), null_peaks=nulls, max_snr=ms, best_v=bv, grid=grid)
+                        peaks=peaks(0), selected=peaks(1), null_peaks=nulls, max_snr=ms, best_v=bv, grid=grid,
+                        candidates=cands)
         finally:
             L.ft_b200_result_free(r)
 

@@ -201,7 +201,7 @@ void ft_b200_search_params_default(ft_b200_search_params* p) {
     p->min_snr_floor = d.min_snr_floor;
     p->target_false_per_run = d.target_false_per_run;
     p->max_frame_fraction = d.max_frame_fraction;
-    p->half_tolerance = 3.0;
+    p->half_tolerance = d.half_tolerance;
     p->static_exclude = d.static_exclude;
     p->null_runs = d.null_runs;
     p->max_candidates = d.max_candidates;
@@ -241,6 +241,7 @@ ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
     p.edge_px = q.edge_px;
     p.gauss_model = q.null_model_gauss != 0;
     p.passes_per_launch = std::max(0, q.passes_per_launch);
+    p.half_tolerance = q.half_tolerance;
     p.shard_count = std::max(1, q.shard_count);
     p.shard_index = q.shard_index;
     if (p.shard_index < 0 || p.shard_index >= p.shard_count)
@@ -494,6 +495,25 @@ int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap) {
     if (!r) return 0;
     const auto& v = r->o.null_peaks;
     for (size_t k = 0; out && k < v.size() && static_cast<int>(k) < cap; ++k) out[k] = v[k];
+    return static_cast<int>(v.size());
+}
+
+int ft_b200_result_candidates(const ft_b200_result* r, double* rows, char* flags, int cap) {
+    if (!r) return 0;
+    const auto& v = r->o.candidates;
+    for (size_t k = 0; k < v.size() && static_cast<int>(k) < cap; ++k) {
+        const ftb::Candidate& c = v[k];
+        if (rows) {
+            const double row[17] = {c.x, c.y, c.vx_pxh, c.vy_pxh, c.pos_err_px, c.vel_err_pxh, c.snr, c.snr_coarse,
+                                    c.snr_half1, c.snr_half2, c.max_frame_fraction, c.false_alarms_per_run, c.flux,
+                                    c.mag_inst, c.ok ? 1.0 : 0.0, static_cast<double>(c.id), c.inv_dist_au};
+            std::memcpy(rows + 17 * k, row, sizeof row);
+        }
+        if (flags) {
+            std::strncpy(flags + 64 * k, c.flags.c_str(), 63);
+            flags[64 * k + 63] = 0;
+        }
+    }
     return static_cast<int>(v.size());
 }
 

@@ -13,6 +13,7 @@
 #include <thread>
 
 #include "search.h"
+#include "track.cuh"
 
 namespace ftb {
 
@@ -47,23 +48,8 @@ __global__ void peak_kernel(const float* M, const int* best_v, int w, int h, flo
     if (k < cap) out[k] = {x, y, v, best_v[static_cast<size_t>(y) * w + x]};
 }
 
-// bilinear sample with the reference's border rule, double arithmetic, no
-// contraction (common.hpp:125-138)
-__device__ float bilinear(const float* img, int w, int h, int pitch, double x, double y) {
-    const int x0 = static_cast<int>(floor(x)), y0 = static_cast<int>(floor(y));
-    if (x0 < 0 || y0 < 0 || x0 + 1 >= w || y0 + 1 >= h) {
-        const int xr = static_cast<int>(lround(x)), yr = static_cast<int>(lround(y));
-        if (xr >= 0 && yr >= 0 && xr < w && yr < h && fabs(x - xr) < 1e-9 && fabs(y - yr) < 1e-9)
-            return img[static_cast<size_t>(yr) * pitch + xr];
-        return CUDART_NAN_F;
-    }
-    const double fx = __dsub_rn(x, static_cast<double>(x0)), fy = __dsub_rn(y, static_cast<double>(y0));
-    const float* r0 = img + static_cast<size_t>(y0) * pitch + x0;
-    const float* r1 = r0 + pitch;
-    const double gx = __dsub_rn(1.0, fx), gy = __dsub_rn(1.0, fy);
-    const double top = __dadd_rn(__dmul_rn(gx, r0[0]), __dmul_rn(fx, r0[1]));
-    const double bot = __dadd_rn(__dmul_rn(gx, r1[0]), __dmul_rn(fx, r1[1]));
-    return __double2float_rn(__dadd_rn(__dmul_rn(gy, top), __dmul_rn(fy, bot)));
+__device__ __forceinline__ float bilinear(const float* img, int w, int h, int pitch, double x, double y) {
+    return track_bilinear(img, w, h, pitch, x, y);
 }
 
 struct ArtArgs {
@@ -376,8 +362,8 @@ SearchRequest::SearchRequest(Context& c, const SearchParams& p, int w, int h, in
 
 size_t SearchRequest::base_bytes(int w, int h, int n) {
     const size_t plane = static_cast<size_t>(frame_pitch(w)) * h;
-    // raw, sub, filtered, residuals (stage scratch) + sky, mask, scatter + maps + samples
-    return sizeof(float) * (4 * plane * n + 3 * plane) + 2 * sizeof(float) * static_cast<size_t>(w) * h +
+    // raw, sub, filtered, residuals (stage scratch), the real residuals + sky, mask, scatter + maps + samples
+    return sizeof(float) * (5 * plane * n + 3 * plane) + 2 * sizeof(float) * static_cast<size_t>(w) * h +
            (size_t{64} << 20);
 }
 
@@ -454,6 +440,12 @@ void SearchRequest::prepare(const float* frames, const double* mjd, const double
     sp_.fwhm_px = o_.fwhm_px;
     if (!sc_->fits(w, h, n, sp_.fwhm_px)) throw std::runtime_error("PSF too wide for the sample buffers");
     stage_filter(c, *sc_, w, h, n, sp_, filt_.as<float>(), mask_.as<float>(), nullptr, nullptr);
+    // the real residuals stay for the candidates' photometry (null runs reuse the stage scratch)
+    if (p_.shard_count <= 1 || p_.shard_index == 0) {
+        res_ = DevBuf(&c, sizeof(float) * plane_ * n, "real residuals");
+        FTB_CHECK(cudaMemcpyAsync(res_.as<float>(), sc_->residual.as<float>(), sizeof(float) * plane_ * n,
+                                  cudaMemcpyDeviceToDevice, c.stream()));
+    }
     if (report) report(0.1, "prepared");
     // search setup (search.cpp:716-746)
     o_.grid = velocity_grid(o_.span_h, p_, &o_.dv);
@@ -601,7 +593,15 @@ SearchOut SearchRequest::finalize(std::vector<SearchOut>* copies_out) {
             if (pk.snr >= o_.thr.snr && pk.vidx >= 0) o_.selected.push_back(pk);
         if (static_cast<int>(o_.selected.size()) > p_.max_candidates)
             o_.selected.resize(static_cast<size_t>(p_.max_candidates));
+        if (!o_.selected.empty()) {
+            const int rf = c.span_begin("refine");
+            o_.candidates = refine_candidates(c, o_, p_,
+                                              {filt_.as<float>(), res_.as<float>(), sub_.as<float>(), sky_.as<float>(),
+                                               mask_.as<float>(), w, h, pitch_, n});
+            c.span_end(rf);
+        }
     }
+    res_.reset();
     if (real_) {
         o_.max_snr.resize(static_cast<size_t>(w) * h);
         o_.best_v.resize(static_cast<size_t>(w) * h);

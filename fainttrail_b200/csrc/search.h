@@ -25,6 +25,7 @@ struct SearchParams {
     int static_exclude = -1, null_runs = 3, null_tested = 3000, max_candidates = 300, edge_px = 4;
     bool gauss_model = true;  // null_model "gauss" (else "linear")
     int passes_per_launch = 0;  // 0: as many as fit; k: at most k per launch
+    double half_tolerance = 3.0;  // allowed shortfall of each half's S/N (search.hpp:66)
     // null runs split over shard_count calls (one per GPU): this call runs block
     // shard_index of the null runs and, on shard 0 only, the real pass
     int shard_index = 0, shard_count = 1;
@@ -117,6 +118,16 @@ void apply_patches(Context& c, const InjectionPatches& ip, float* d_frames, int 
 
 // One whole search from raw frames (ft_search's prepare + search, without the
 // candidate refinement).
+// A refined candidate (Candidate, search.hpp:131-154) without sky coordinates.
+struct Candidate {
+    int id = 0;
+    double x = 0, y = 0, vx_pxh = 0, vy_pxh = 0, pos_err_px = 0, vel_err_pxh = 0;
+    double snr = 0, snr_coarse = 0, snr_half1 = 0, snr_half2 = 0, max_frame_fraction = 0;
+    double false_alarms_per_run = 0, flux = 0, mag_inst = 0, inv_dist_au = 0;
+    bool ok = false;
+    std::string flags;
+};
+
 struct SearchOut {
     int w = 0, h = 0, n = 0;
     double fwhm_px = 0, span_h = 0, t_ref_mjd = 0, dv = 0;
@@ -128,8 +139,26 @@ struct SearchOut {
     std::vector<Peak> selected;          // select_peaks (search.cpp:614-620)
     std::vector<float> max_snr;          // real detection map
     std::vector<int> best_v;
+    std::vector<Candidate> candidates;   // refined selected peaks (search.cpp:786-804)
     double adds = 0;                     // pixel x frame x motion additions of all passes
 };
+
+// expected_null_peaks (search.cpp:697-702): null peaks per run above `snr`
+double expected_null_peaks(const Threshold& t, double snr);
+
+// The device frames a refinement reads: filtered, the real residuals, sub,
+// static sky and mask, all with the frame pitch.
+struct RefineInputs {
+    const float* d_filt;
+    const float* d_res;
+    const float* d_sub;
+    const float* d_sky;
+    const float* d_mask;
+    int w, h, pitch, n;
+};
+// refine() of every selected peak and finish_candidates() (search.cpp:245-400,
+// 620-676): the candidate list, ordered and numbered as the reference's
+std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const SearchParams& p, const RefineInputs& in);
 
 // One search request in phases, so that the passes of several searches (or of
 // one search's null runs and copies) can be stacked in shared launches:
@@ -169,6 +198,7 @@ private:
     std::vector<double> exp_sorted_;
     std::vector<float> pooled_;
     DevBuf raw_, raw0_, sub_, filt_, sky_, mask_, max_, bv_, sub2_, copy_sky_, copy_mask_;
+    DevBuf res_;  // the real residuals, for the candidates' photometry
     std::unique_ptr<StageScratch> sc_;
     std::map<int, Item> items_;
 };

@@ -196,6 +196,12 @@ bool fit_linear(std::vector<float> pooled, double runs, double& a, double& b) {
 
 }  // namespace
 
+double expected_null_peaks(const Threshold& t, double snr) {
+    if (t.inv_s2 > 0.0 && snr > 0.0) return std::exp(log_rate(t.a, t.k, t.inv_s2, snr));
+    if (t.b > 0.0) return std::exp(t.a - t.b * snr);
+    return 0.0;
+}
+
 Threshold set_threshold(const SearchParams& p, const std::vector<float>& pooled, int runs, double fwhm_px, int w,
                         int h, size_t n_motions) {
     Threshold t;

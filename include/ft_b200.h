@@ -185,6 +185,13 @@ int ft_b200_search_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int h
                        const double* mjd, const double* exptime, const ft_b200_search_params* params,
                        ft_b200_result** out);
 void ft_b200_result_free(ft_b200_result* r);
+/* The refined candidates (refine() and finish_candidates(), search.cpp:245-400,
+ * 620-676): 17 doubles per candidate into rows[17 * k ..] -- x, y, vx, vy,
+ * pos_err, vel_err, snr, snr_coarse, snr_half1, snr_half2, max_frame_fraction,
+ * false_alarms_per_run, flux, mag_inst, ok (0/1), id, inv_dist -- and the
+ * comma-separated flags into flags[64 * k ..]; up to cap candidates; returns
+ * the count. Sky coordinates are not computed (no WCS). */
+int ft_b200_result_candidates(const ft_b200_result* r, double* rows, char* flags, int cap);
 
 /* An object to inject into every frame of a copy: Injection (validate.hpp:18-23),
  * position at the reference epoch (0-based px), motion (px/hour), flux per frame. */

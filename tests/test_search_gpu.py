@@ -27,6 +27,9 @@ def test_golden_search(device, oracle):
     px, py, ps, pv = oracle.find_peaks(r["max_snr"], r["best_v"], 5.0, 2, 4, 100000)
     assert [(a, b, c, d) for a, b, c, d in zip(px, py, ps, pv)] == [(x, y, np.float32(s), v) for x, y, s, v in
                                                                  r["peaks"]]
+    # refined candidates: all 17 fields of the reference's list, bit for bit
+    got = np.array([row for row, _ in r["candidates"]]).reshape(-1, 17)
+    assert got.shape == g["candidates"].shape and np.array_equal(got, g["candidates"])
 
 
 @pytest.mark.parametrize("seed,w,h,n,runs,fwhm", [(21, 160, 128, 24, 3, 2.5), (8, 128, 100, 16, 2, 0.0)])
@@ -42,6 +45,27 @@ def test_live_reference_search(device, reference, seed, w, h, n, runs, fwhm):
     assert got["threshold"] == ref["threshold"] and got["method"] == ref["method"]
     assert same(got["null_peaks"], ref["null_peaks"])
     assert same(got["max_snr"], ref["max_snr"])
+    assert len(got["candidates"]) == len(ref["candidates"])
+    for (row, flags), (want, wflags) in zip(got["candidates"], ref["candidates"]):
+        assert np.array_equal(row, want) and flags == wflags
+
+
+@pytest.mark.parametrize("seed,nmovers,threshold", [(31, 6, 0.0), (44, 4, 4.0)])
+def test_candidates_match_reference(device, reference, seed, nmovers, threshold):
+    """Refined candidates on sequences with movers (and, with a low fixed
+    threshold, many noise candidates: duplicates, ghosts and flags)."""
+    R = reference
+    frames, mjd, exp = R.simulate(width=200, height=150, nframes=20, nstars=60, nmovers=nmovers, seed=seed,
+                                  rate_min_arcsec_min=0.3, rate_max_arcsec_min=1.5)
+    frames[:, :, :5] = np.nan
+    kw = dict(fwhm_px=2.5, null_runs=2, threshold_snr=threshold, vmin_pxh=5.0, vmax_pxh=60.0)
+    prep = R.prepare(frames, mjd, exp, fwhm_px=2.5, null_runs=2)
+    ref = prep.search(backend="cpu", **kw)
+    got = device.search(frames, mjd, exp, **kw)
+    assert got["threshold"] == ref["threshold"]
+    assert len(ref["candidates"]) > 0 and len(got["candidates"]) == len(ref["candidates"])
+    for (row, flags), (want, wflags) in zip(got["candidates"], ref["candidates"]):
+        assert np.array_equal(row, want) and flags == wflags
 
 
 def test_fixed_threshold_and_cancel(device):
