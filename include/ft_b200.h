@@ -171,9 +171,10 @@ int ft_b200_null_threshold(const double* pooled, long long count, int runs, doub
  * frames stable-sorted by mid-exposure time, prepare, then search): background
  * and blank-border growth, preprocessing, the real stacking pass and its peaks,
  * params->null_runs time-shuffled null runs (preprocessing rebuilt, stacked,
- * peaks screened for artefacts), the null-tail fit and threshold, and the peaks
- * selected for refinement (search.cpp:716-788). Candidate refinement is left to
- * the caller. frames: host, nframes x height x width; mjd/exptime per frame.
+ * peaks screened for artefacts), the null-tail fit and threshold, the peaks
+ * selected for refinement and their refined candidates (search.cpp:716-804;
+ * ft_b200_result_candidates). Sky coordinates and photometric calibration are
+ * left to the caller. frames: host, nframes x height x width; mjd/exptime per frame.
  * On success *out receives a result to release with ft_b200_result_free. */
 int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
                    const double* exptime, const ft_b200_search_params* params, ft_b200_progress_fn progress,
