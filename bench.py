@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-shape", type=int, default=0, help="stack kernel tile shape (0: autotuned)")
+    ap.add_argument("--workers", type=int, default=2, help="serving: rounds in flight at once")
     return ap.parse_args()
 
 
@@ -412,34 +413,42 @@ def serving_arm(args, rank, local_rank, world, dist):
         finish = max(finish, t_arr) + sv
         lat.append(finish - t_arr)
     plain_makespan = finish  # from the stream's start, as the served run
-    srv = ftb.Server(local_rank, 0.0, max_batch=16, workers=2)
+    srv = ftb.Server(local_rank, 0.0, max_batch=16, workers=args.workers)
     tk = [srv.submit(f, mjd, exptime, **wl.search_params()) for _, wl, f, mjd, exptime in inputs[:3]]
     for t in tk:  # warm-up round on the server's own context
         srv.poll(t)
     srv.close()
-    srv = ftb.Server(local_rank, 0.0, max_batch=16, workers=2)
-    if dist:
-        dist.barrier()
+    def served_run():
+        srv = ftb.Server(local_rank, 0.0, max_batch=16, workers=args.workers)
+        if dist:
+            dist.barrier()
+        tickets = [None] * len(inputs)
+        t_start = time.perf_counter()
+
+        def submitter():
+            for k, (t_arr, wl, f, mjd, exptime) in enumerate(inputs):
+                d = t_arr - (time.perf_counter() - t_start)
+                if d > 0:
+                    time.sleep(d)
+                tickets[k] = srv.submit(f, mjd, exptime, **wl.search_params())
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        results = [result_digest(srv.poll(t, maps=True)) for t in tickets]
+        t_end = time.perf_counter()
+        st = srv.stats()
+        srv.close()
+        return t_end - t_start, st, results
+
+    # the served stream three times (the median makespan is reported; the GPUs
+    # are shared and single runs vary by about 10 %)
     clocks = ClockSampler(local_rank)
     clocks.start()
-    tickets = [None] * len(inputs)
-    t_start = time.perf_counter()
-
-    def submitter():
-        for k, (t_arr, wl, f, mjd, exptime) in enumerate(inputs):
-            d = t_arr - (time.perf_counter() - t_start)
-            if d > 0:
-                time.sleep(d)
-            tickets[k] = srv.submit(f, mjd, exptime, **wl.search_params())
-    th = threading.Thread(target=submitter)
-    th.start()
-    th.join()
-    results = [result_digest(srv.poll(t, maps=True)) for t in tickets]
-    t_end = time.perf_counter()
-    st = srv.stats()
-    srv.close()
+    runs = [served_run() for _ in range(3)]
     clk = clocks.stop()
-    makespan = t_end - t_start
+    runs.sort(key=lambda r: r[0])
+    makespan, st, results = runs[1]
+    spread = [r[0] for r in runs]
     if dist:
         t = torch.tensor([makespan], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -463,7 +472,7 @@ def serving_arm(args, rank, local_rank, world, dist):
                                        f"{max(i[1].height for i in inputs)}, rates 0.1-3 px/min, 8-32 null runs, "
                                        f"each request at most 2e12 pixel-frame-motion adds"),
                           "parallelism": f"independent request streams x{world}", "max_batch": 16,
-                          "workers": 2},
+                          "workers": args.workers},
                "searches_per_s": world * len(inputs) / makespan,
                "p50_s": st["p50_s"], "p99_s": st["p99_s"], "rounds": st["rounds"], "mean_batch": st["mean_batch"],
                "plain": {"value": total_adds / plain_makespan, "unit": METRIC,
@@ -475,7 +484,8 @@ def serving_arm(args, rank, local_rank, world, dist):
                "e2e": {"value": world * total_adds / makespan, "unit": METRIC, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h},
                "clocks": clk, "completed": st["completed"], "gpu_launches": st["launches"],
-               "bit_identical_to_alone": sum(a == b for a, b in zip(results, alone))}
+               "bit_identical_to_alone": min(sum(a == b for a, b in zip(r[2], alone)) for r in runs),
+               "served_makespans_s": spread}
         print(json.dumps(out), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -81,6 +81,12 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
 
 StackConfig choose_stack_config(int w, int h, int n, int device_smem_optin);
 
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`, never lowering it: the attribute is process-wide, so setting it
+// per launch from several threads (the server's workers) could lower it under
+// another thread's launch.
+void allow_dynamic_smem(const void* func, size_t bytes);
+
 // Compiled stack kernel shapes: 1 = 32 x 16 tiles (12 warps), 2 = 64 x 8 tiles with
 // paired columns (12 warps), 3 = 32 x 8 (16 warps), 4 = 32 x 4 (16 warps),
 // 5 = 32 x 16 with one shared maximum per tile (16 warps), 6 = the same with 14 warps.

@@ -36,6 +36,7 @@
 #include <cstring>
 #include <functional>
 #include <limits>
+#include <map>
 #include <mutex>
 #include <numeric>
 
@@ -45,6 +46,18 @@ namespace ftb {
 
 void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaError(std::string("CUDA: ") + what + ": " + cudaGetErrorString(e));
+}
+
+void allow_dynamic_smem(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limit;
+    int dev = 0;
+    FTB_CHECK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = limit[{dev, func}];
+    if (bytes <= cur) return;
+    FTB_CHECK(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+    cur = bytes;
 }
 
 // ------------------------------------------------------------------ host plan
@@ -1155,7 +1168,7 @@ void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, si
     if (items == 0) return;
     FTB_CHECK(cudaMemcpyAsync(d_desc, host.data(), host.size(), cudaMemcpyHostToDevice, s));
     auto kern = stack_batch_kernel<NW, P, WP, BH, TW, MERGE>;
-    FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     const int ctas = static_cast<int>(std::min<long long>(items, sms));
     kern<<<ctas, 32 * NW, smem, s>>>(reinterpret_cast<const StackArgs*>(d_desc + 128 + 128 * np),
                                      reinterpret_cast<const CUtensorMap*>(d_desc + 128), static_cast<int>(np), items,

@@ -467,7 +467,7 @@ void launch_filter(const FilterArgs& a, int n, cudaStream_t s) {
     const int R = RT > 0 ? RT : a.R, H = R + 2, ZW = TWc + 2 * H, ZH = THc + 2 * H;
     const size_t smem = sizeof(float) * ZW * ZH + ((ZW * ZH + 15) / 16) * 16 + sizeof(float) * (THc + 2 * R) * TWc;
     auto kern = filter_kernel<RT, TWc, THc>;
-    FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     kern<<<dim3((a.w + TWc - 1) / TWc, (a.h + THc - 1) / THc, n), 256, smem, s>>>(a);
     FTB_CHECK(cudaGetLastError());
 }
@@ -635,7 +635,7 @@ void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h,
         const int T = 64;
         const size_t smem = static_cast<size_t>(T) * n * 9;
         auto kern = n <= 32 ? sky_kernel<1> : n <= 64 ? sky_kernel<2> : n <= 128 ? sky_kernel<4> : sky_kernel<8>;
-        FTB_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
         kern<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
         FTB_CHECK(cudaGetLastError());
         ++c.launches;
@@ -692,7 +692,7 @@ void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const Stage
         ScatterArgs a{sc.residual.as<float>(), d_sigma, sc.scatter.as<float>(), w, h, pitch, n};
         const int T = 128;
         const size_t smem = static_cast<size_t>(T) * n * 4;
-        FTB_CHECK(cudaFuncSetAttribute(scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        allow_dynamic_smem(reinterpret_cast<const void*>(scatter_kernel), smem);
         scatter_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
         FTB_CHECK(cudaGetLastError());
         ++c.launches;
