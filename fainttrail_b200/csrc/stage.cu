@@ -15,6 +15,7 @@
 // Arithmetic follows the reference operation by operation: float adds and
 // multiplies with round-to-nearest and no contraction, double where the
 // reference promotes to double, the same summation orders, NaN rules and casts.
+#include <cooperative_groups.h>
 #include <math_constants.h>
 
 #include <algorithm>
@@ -195,69 +196,96 @@ __device__ __forceinline__ float key_value(uint32_t k) {
 // k-th smallest key (0-based) of the CTA's values, by four 8-bit radix passes.
 // MODE 0: keys of x; MODE 1: keys of float(|x - med|) (the MAD deviations,
 // common.hpp:80). Needs >= 256 threads.
+// ---- exact order statistics of a frame's samples by a cluster of CTAs: four
+// 8-bit radix passes over order-preserving keys; each CTA counts its share of
+// the samples into its own histogram, CTA 0 merges the cluster's histograms
+// through distributed shared memory and picks the digit, and a cluster barrier
+// separates the passes (eight SMs per frame).
+
+namespace cg = cooperative_groups;
+constexpr int kSelCluster = 8;
+
 template <int MODE>
-__device__ uint32_t cta_select(const float* x, int cnt, int k, double med, uint32_t* hist, uint32_t* shared_out) {
+__device__ uint32_t cluster_select(const float* x, int cnt, int k, double med, uint32_t* hist, uint32_t* merged,
+                                   uint32_t* res) {
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    const int stride = static_cast<int>(blockDim.x) * kSelCluster;
     uint32_t prefix = 0, pmask = 0;
     for (int shift = 24; shift >= 0; shift -= 8) {
         for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
-        __syncthreads();
-        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+        cl.sync();  // no CTA still reads a histogram of the previous pass
+        for (int e = static_cast<int>(rank * blockDim.x + threadIdx.x); e < cnt; e += stride) {
             float v = x[e];
             if (MODE == 1) v = __double2float_rn(fabs(static_cast<double>(v) - med));
             const uint32_t key = order_key(v);
             if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t acc = 0;
-            int d = 0;
-            for (; d < 255; ++d) {
-                if (acc + hist[d] > static_cast<uint32_t>(k)) break;
-                acc += hist[d];
+        cl.sync();
+        if (rank == 0) {
+            for (int b = threadIdx.x; b < 256; b += blockDim.x) {
+                uint32_t sum = 0;
+                for (int r = 0; r < kSelCluster; ++r) sum += cl.map_shared_rank(hist, r)[b];
+                merged[b] = sum;
             }
-            shared_out[0] = static_cast<uint32_t>(d);
-            shared_out[1] = acc;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t acc = 0;
+                int d = 0;
+                for (; d < 255; ++d) {
+                    if (acc + merged[d] > static_cast<uint32_t>(k)) break;
+                    acc += merged[d];
+                }
+                res[0] = static_cast<uint32_t>(d);
+                res[1] = acc;
+            }
         }
-        __syncthreads();
-        const uint32_t d = shared_out[0];
-        k -= static_cast<int>(shared_out[1]);
+        cl.sync();
+        const uint32_t* r0 = cl.map_shared_rank(res, 0);
+        const uint32_t d = r0[0];
+        k -= static_cast<int>(r0[1]);
         prefix |= d << shift;
         pmask |= 255u << shift;
-        __syncthreads();
     }
+    cl.sync();  // CTA 0's result is read before it is overwritten
     return prefix;
 }
 
-// median_inplace (common.hpp:64-74) of the CTA's values: the mid-th smallest,
-// averaged (in double) with the (mid-1)-th for an even count; 0 when empty.
 template <int MODE>
-__device__ double cta_median(const float* x, int cnt, double med, uint32_t* hist, uint32_t* sh) {
+__device__ double cluster_median(const float* x, int cnt, double med, uint32_t* hist, uint32_t* merged, uint32_t* res) {
     if (cnt == 0) return 0.0;
     const int mid = cnt / 2;
-    double m = key_value(cta_select<MODE>(x, cnt, mid, med, hist, sh));
+    double m = key_value(cluster_select<MODE>(x, cnt, mid, med, hist, merged, res));
     if (cnt % 2 == 0) {
-        const float lower = key_value(cta_select<MODE>(x, cnt, mid - 1, med, hist, sh));
+        const float lower = key_value(cluster_select<MODE>(x, cnt, mid - 1, med, hist, merged, res));
         m = 0.5 * (m + lower);
     }
     return m;
 }
 
-// robust_sigma (common.hpp:77-82) per frame, one CTA per frame.
-// out_sigma: sigma_from_samples (1 if not positive, preprocess.cpp:265-268) when
-// `unit_if_zero`, else the raw value.
-__global__ void __launch_bounds__(1024) robust_sigma_kernel(const float* samples, int cap, const int* counts,
-                                                            double* out, int unit_if_zero) {
-    __shared__ uint32_t hist[256];
-    __shared__ uint32_t sh[2];
-    const int f = blockIdx.x;
+// robust_sigma_kernel with a cluster of kSelCluster CTAs per frame
+__global__ void __cluster_dims__(kSelCluster, 1, 1) __launch_bounds__(256)
+    robust_sigma_cluster_kernel(const float* samples, int cap, const int* counts, double* out, int unit_if_zero) {
+    __shared__ uint32_t hist[256], merged[256], res[2];
+    const int f = blockIdx.x / kSelCluster;
     const int cnt = min(counts[f], cap);
     const float* x = samples + static_cast<size_t>(f) * cap;
     double sg = 0.0;
     if (cnt >= 3) {
-        const double med = cta_median<0>(x, cnt, 0.0, hist, sh);
-        sg = 1.4826 * cta_median<1>(x, cnt, med, hist, sh);
+        const double med = cluster_median<0>(x, cnt, 0.0, hist, merged, res);
+        sg = 1.4826 * cluster_median<1>(x, cnt, med, hist, merged, res);
     }
-    if (threadIdx.x == 0) out[f] = (unit_if_zero && !(sg > 0.0)) ? 1.0 : sg;
+    if (cg::this_cluster().block_rank() == 0 && threadIdx.x == 0) out[f] = (unit_if_zero && !(sg > 0.0)) ? 1.0 : sg;
+}
+
+// median_kernel with a cluster per frame
+__global__ void __cluster_dims__(kSelCluster, 1, 1) __launch_bounds__(256)
+    median_cluster_kernel(const float* samples, int cap, const int* counts, double* out) {
+    __shared__ uint32_t hist[256], merged[256], res[2];
+    const int f = blockIdx.x / kSelCluster;
+    const int cnt = min(counts[f], cap);
+    const double m = cluster_median<0>(samples + static_cast<size_t>(f) * cap, cnt, 0.0, hist, merged, res);
+    if (cg::this_cluster().block_rank() == 0 && threadIdx.x == 0) out[f] = m;
 }
 
 // ------------------------------------------------------------------ scatter + mask
@@ -498,16 +526,6 @@ __global__ void rescale_kernel(float* g, size_t plane, int w, int h, int pitch, 
     *p = __fmul_rn(*p, ig);
 }
 
-// median_inplace of each frame's samples (the background, preprocess.cpp:574-575)
-__global__ void __launch_bounds__(1024) median_kernel(const float* samples, int cap, const int* counts, double* out) {
-    __shared__ uint32_t hist[256];
-    __shared__ uint32_t sh[2];
-    const int f = blockIdx.x;
-    const int cnt = min(counts[f], cap);
-    const double m = cta_median<0>(samples + static_cast<size_t>(f) * cap, cnt, 0.0, hist, sh);
-    if (threadIdx.x == 0) out[f] = m;
-}
-
 // v -> float(v - bg), NaN stays NaN (preprocess.cpp:235), in place
 __global__ void subtract_kernel(float* img, size_t plane, int w, int h, int pitch, const double* bg) {
     const int f = blockIdx.y;
@@ -654,7 +672,8 @@ void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h,
             FTB_CHECK(cudaGetLastError());
         ++c.launches;
         }
-        robust_sigma_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, tb.counts, tb.sigma, 1);
+        robust_sigma_cluster_kernel<<<n * kSelCluster, 256, 0, s>>>(sc.samples.as<float>(), sc.cap, tb.counts,
+                                                                     tb.sigma, 1);
         FTB_CHECK(cudaGetLastError());
         ++c.launches;
         c.span_end(span);
@@ -742,7 +761,8 @@ void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const Stage
             FTB_CHECK(cudaGetLastError());
         ++c.launches;
         }
-        robust_sigma_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, d_counts, d_sg, 0);
+        robust_sigma_cluster_kernel<<<n * kSelCluster, 256, 0, s>>>(sc.samples.as<float>(), sc.cap, d_counts, d_sg,
+                                                                     0);
         FTB_CHECK(cudaGetLastError());
         ++c.launches;
         rescale_kernel<<<dim3(static_cast<unsigned>((npix + 255) / 256), n), 256, 0, s>>>(d_filtered, plane, w, h, pitch,
@@ -783,7 +803,7 @@ void prepare_sub(Context& c, StageScratch& sc, float* d_raw, float* d_sub, int w
         FTB_CHECK(cudaGetLastError());
         ++c.launches;
     }
-    median_kernel<<<n, 1024, 0, s>>>(sc.samples.as<float>(), sc.cap, tb.counts, tb.sg);
+    median_cluster_kernel<<<n * kSelCluster, 256, 0, s>>>(sc.samples.as<float>(), sc.cap, tb.counts, tb.sg);
     FTB_CHECK(cudaGetLastError());
         ++c.launches;
     const dim3 grid(static_cast<unsigned>((npix + 255) / 256), n);
