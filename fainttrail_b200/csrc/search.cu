@@ -27,13 +27,11 @@ struct PeakRec {
 
 // local maxima above `floor` inside the edge margin, strict for later pixels and
 // non-strict for earlier ones, so a plateau yields one peak (search.cpp:110-129)
-__global__ void peak_kernel(const float* M, const int* best_v, int w, int h, float floor, int radius, int edge,
-                            int* count, PeakRec* out, int cap) {
-    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int x = static_cast<int>(q % w), y = static_cast<int>(q / w);
-    if (y >= h || x < edge || y < edge || x >= w - edge || y >= h - edge) return;
-    const float v = M[static_cast<size_t>(y) * w + x];
-    if (v < floor) return;
+__device__ __forceinline__ bool is_peak(const float* M, int w, int h, float floor, int radius, int edge, int x, int y,
+                                        float& v) {
+    if (y >= h || x < edge || y < edge || x >= w - edge || y >= h - edge) return false;
+    v = M[static_cast<size_t>(y) * w + x];
+    if (v < floor) return false;
     for (int dy = -radius; dy <= radius; ++dy) {
         const int yy = y + dy;
         if (yy < 0 || yy >= h) continue;
@@ -41,11 +39,90 @@ __global__ void peak_kernel(const float* M, const int* best_v, int w, int h, flo
             const int xx = x + dx;
             if ((!dx && !dy) || xx < 0 || xx >= w) continue;
             const float u = M[static_cast<size_t>(yy) * w + xx];
-            if (u > v || (u == v && (dy < 0 || (dy == 0 && dx < 0)))) return;
+            if (u > v || (u == v && (dy < 0 || (dy == 0 && dx < 0)))) return false;
         }
     }
-    const int k = atomicAdd(count, 1);
-    if (k < cap) out[k] = {x, y, v, best_v[static_cast<size_t>(y) * w + x]};
+    return true;
+}
+
+// The peaks in raster order (the reference's visit order) without a sort: the
+// peaks of each block of kPeakBlock consecutive pixels are counted, the counts
+// scanned, and each block writes its peaks at its offset in pixel order.
+constexpr int kPeakBlock = 256;
+
+__global__ void __launch_bounds__(kPeakBlock) peak_count_kernel(const float* M, int w, int h, float floor, int radius,
+                                                                int edge, int* block_count) {
+    const long long q = static_cast<long long>(blockIdx.x) * kPeakBlock + threadIdx.x;
+    float v;
+    const bool pk = is_peak(M, w, h, floor, radius, edge, static_cast<int>(q % w), static_cast<int>(q / w), v);
+    const int c = __syncthreads_count(pk);
+    if (threadIdx.x == 0) block_count[blockIdx.x] = c;
+}
+
+// exclusive scan of the block counts in place (one CTA of 1024 threads, a
+// contiguous chunk per thread); the sum into *total
+__global__ void __launch_bounds__(1024) peak_scan_kernel(int* cnt, int nblocks, int* total) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x;
+    const int chunk = (nblocks + 1023) / 1024;
+    const int b0 = min(nblocks, t * chunk), b1 = min(nblocks, b0 + chunk);
+    int s = 0;
+    for (int b = b0; b < b1; ++b) s += cnt[b];
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {  // inclusive scan of the chunk sums
+        const int add = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += add;
+        __syncthreads();
+    }
+    int run = part[t] - s;
+    for (int b = b0; b < b1; ++b) {
+        const int c = cnt[b];
+        cnt[b] = run;
+        run += c;
+    }
+    if (t == 1023) *total = part[1023];
+}
+
+__global__ void __launch_bounds__(kPeakBlock) peak_write_kernel(const float* M, const int* best_v, int w, int h,
+                                                                float floor, int radius, int edge,
+                                                                const int* block_offset, PeakRec* out, int cap) {
+    __shared__ int warp_base[kPeakBlock / 32];
+    const long long q = static_cast<long long>(blockIdx.x) * kPeakBlock + threadIdx.x;
+    const int x = static_cast<int>(q % w), y = static_cast<int>(q / w);
+    float v = 0.0f;
+    const bool pk = is_peak(M, w, h, floor, radius, edge, x, y, v);
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned bal = __ballot_sync(0xffffffffu, pk);
+    if (lane == 0) warp_base[warp] = __popc(bal);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int k = 0; k < kPeakBlock / 32; ++k) {
+            const int c = warp_base[k];
+            warp_base[k] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+    if (pk) {
+        const int pos = block_offset[blockIdx.x] + warp_base[warp] + __popc(bal & ((1u << lane) - 1u));
+        if (pos < cap) out[pos] = {x, y, v, best_v[static_cast<size_t>(y) * w + x]};
+    }
+}
+
+// the three launches for one map; the count of its peaks lands in *d_total
+void launch_peaks(Context& c, const float* d_max, const int* d_bv, int w, int h, float floor, int radius, int edge,
+                  int* d_blocks, int* d_total, PeakRec* d_out, int cap) {
+    cudaStream_t s = c.stream();
+    const long long npix = static_cast<long long>(w) * h;
+    const int nb = static_cast<int>((npix + kPeakBlock - 1) / kPeakBlock);
+    peak_count_kernel<<<nb, kPeakBlock, 0, s>>>(d_max, w, h, floor, radius, edge, d_blocks);
+    peak_scan_kernel<<<1, 1024, 0, s>>>(d_blocks, nb, d_total);
+    peak_write_kernel<<<nb, kPeakBlock, 0, s>>>(d_max, d_bv, w, h, floor, radius, edge, d_blocks, d_out, cap);
+    FTB_CHECK(cudaGetLastError());
+    c.launches += 3;
 }
 
 __device__ __forceinline__ float bilinear(const float* img, int w, int h, int pitch, double x, double y) {
@@ -170,38 +247,7 @@ void apply_patches(Context& c, const InjectionPatches& ip, float* d_frames, int 
 
 std::vector<Peak> device_peaks(Context& c, const float* d_max, const int* d_best_v, int w, int h, float floor,
                                int radius, int edge) {
-    cudaStream_t s = c.stream();
-    int cap = std::max(1 << 16, static_cast<int>(std::min<long long>(1LL << 22, static_cast<long long>(w) * h / 16)));
-    for (;;) {
-        DevBuf& buf = c.scratch(20, sizeof(PeakRec) * static_cast<size_t>(cap) + 256, "peaks");
-        int* d_count = reinterpret_cast<int*>(buf.as<unsigned char>());
-        PeakRec* d_out = reinterpret_cast<PeakRec*>(buf.as<unsigned char>() + 256);
-        FTB_CHECK(cudaMemsetAsync(d_count, 0, sizeof(int), s));
-        const long long npix = static_cast<long long>(w) * h;
-        peak_kernel<<<static_cast<unsigned>((npix + 255) / 256), 256, 0, s>>>(d_max, d_best_v, w, h, floor, radius,
-                                                                             edge, d_count, d_out, cap);
-        FTB_CHECK(cudaGetLastError());
-        ++c.launches;
-        int count = 0;
-        FTB_CHECK(cudaMemcpyAsync(&count, d_count, sizeof(int), cudaMemcpyDeviceToHost, s));
-        FTB_CHECK(cudaStreamSynchronize(s));
-        if (count > cap) {
-            cap = count;
-            continue;
-        }
-        std::vector<PeakRec> rec(static_cast<size_t>(count));
-        if (count) {
-            FTB_CHECK(cudaMemcpyAsync(rec.data(), d_out, sizeof(PeakRec) * count, cudaMemcpyDeviceToHost, s));
-            FTB_CHECK(cudaStreamSynchronize(s));
-        }
-        // the reference visits pixels in raster order; restore it
-        std::sort(rec.begin(), rec.end(), [](const PeakRec& a, const PeakRec& b) {
-            return a.y != b.y ? a.y < b.y : a.x < b.x;
-        });
-        std::vector<Peak> out(rec.size());
-        for (size_t k = 0; k < rec.size(); ++k) out[k] = {rec[k].x, rec[k].y, rec[k].snr, rec[k].vidx};
-        return out;
-    }
+    return device_peaks_many(c, {{d_max, d_best_v}}, w, h, floor, radius, edge, 0)[0];
 }
 
 std::vector<std::vector<Peak>> device_peaks_many(Context& c, const std::vector<PeakMap>& maps, int w, int h,
@@ -210,55 +256,59 @@ std::vector<std::vector<Peak>> device_peaks_many(Context& c, const std::vector<P
     std::vector<std::vector<Peak>> out(k_maps);
     if (k_maps == 0) return out;
     cudaStream_t s = c.stream();
-    const int cap = std::max(1 << 16, static_cast<int>(std::min<long long>(1LL << 22, static_cast<long long>(w) * h / 16)));
-    const size_t head = ((sizeof(int) * k_maps + 255) / 256) * 256;
-    DevBuf& buf = c.scratch(22, head + sizeof(PeakRec) * static_cast<size_t>(cap) * k_maps, "peaks (batch)");
-    int* d_count = reinterpret_cast<int*>(buf.as<unsigned char>());
-    PeakRec* d_rec = reinterpret_cast<PeakRec*>(buf.as<unsigned char>() + head);
-    FTB_CHECK(cudaMemsetAsync(d_count, 0, sizeof(int) * k_maps, s));
     const long long npix = static_cast<long long>(w) * h;
-    for (size_t k = 0; k < k_maps; ++k) {
-        peak_kernel<<<static_cast<unsigned>((npix + 255) / 256), 256, 0, s>>>(
-            maps[k].d_max, maps[k].d_best_v, w, h, floor, radius, edge, d_count + k, d_rec + k * cap, cap);
-        FTB_CHECK(cudaGetLastError());
-        ++c.launches;
-    }
+    const size_t nb = static_cast<size_t>((npix + kPeakBlock - 1) / kPeakBlock);
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    int cap = std::max(1 << 16, static_cast<int>(std::min<long long>(1LL << 22, npix / 16)));
     std::vector<int> count(k_maps);
-    FTB_CHECK(cudaMemcpyAsync(count.data(), d_count, sizeof(int) * k_maps, cudaMemcpyDeviceToHost, s));
-    FTB_CHECK(cudaStreamSynchronize(s));
-    std::vector<std::vector<PeakRec>> rec(k_maps);
-    for (size_t k = 0; k < k_maps; ++k) {
-        if (count[k] > cap) continue;  // overflow: found again alone below
-        rec[k].resize(static_cast<size_t>(count[k]));
-        if (count[k])
-            FTB_CHECK(cudaMemcpyAsync(rec[k].data(), d_rec + k * cap, sizeof(PeakRec) * count[k],
-                                      cudaMemcpyDeviceToHost, s));
-    }
-    FTB_CHECK(cudaStreamSynchronize(s));
-    for (size_t k = 0; k < k_maps; ++k)
-        if (count[k] > cap) out[k] = device_peaks(c, maps[k].d_max, maps[k].d_best_v, w, h, floor, radius, edge);
-    // host ordering, one map per thread: raster order (the reference's visit
-    // order), then order_peaks' std::sort by S/N and the truncation
-    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    const size_t workers = std::min<size_t>(hw, k_maps);
-    std::vector<std::thread> pool;
-    for (size_t wk = 0; wk < workers; ++wk)
-        pool.emplace_back([&, wk] {
+    for (;;) {
+        // per map: block counts (scanned in place), then its peaks; the totals first
+        const size_t per = al(sizeof(int) * nb) + al(sizeof(PeakRec) * static_cast<size_t>(cap));
+        DevBuf& buf = c.scratch(22, al(sizeof(int) * k_maps) + per * k_maps, "peaks (batch)");
+        unsigned char* base = buf.as<unsigned char>();
+        int* d_total = reinterpret_cast<int*>(base);
+        auto blocks = [&](size_t k) { return reinterpret_cast<int*>(base + al(sizeof(int) * k_maps) + per * k); };
+        auto recs = [&](size_t k) {
+            return reinterpret_cast<PeakRec*>(base + al(sizeof(int) * k_maps) + per * k + al(sizeof(int) * nb));
+        };
+        for (size_t k = 0; k < k_maps; ++k)
+            launch_peaks(c, maps[k].d_max, maps[k].d_best_v, w, h, floor, radius, edge, blocks(k), d_total + k, recs(k),
+                         cap);
+        FTB_CHECK(cudaMemcpyAsync(count.data(), d_total, sizeof(int) * k_maps, cudaMemcpyDeviceToHost, s));
+        FTB_CHECK(cudaStreamSynchronize(s));
+        const int most = *std::max_element(count.begin(), count.end());
+        if (most > cap) {  // more peaks than room: again with room for all
+            cap = most;
+            continue;
+        }
+        std::vector<std::vector<PeakRec>> rec(k_maps);
+        for (size_t k = 0; k < k_maps; ++k) {
+            rec[k].resize(static_cast<size_t>(count[k]));
+            if (count[k])
+                FTB_CHECK(cudaMemcpyAsync(rec[k].data(), recs(k), sizeof(PeakRec) * count[k], cudaMemcpyDeviceToHost, s));
+        }
+        FTB_CHECK(cudaStreamSynchronize(s));
+        // already in raster order; order_peaks' std::sort by S/N (ties as the
+        // reference's) and the truncation, one map per host thread
+        const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        const size_t workers = std::min<size_t>(hw, k_maps);
+        auto work = [&](size_t wk) {
             for (size_t k = wk; k < k_maps; k += workers) {
-                if (count[k] > cap) {
-                    order_peaks(out[k], keep);
-                    continue;
-                }
-                std::vector<PeakRec>& r = rec[k];
-                std::sort(r.begin(), r.end(),
-                          [](const PeakRec& a, const PeakRec& b) { return a.y != b.y ? a.y < b.y : a.x < b.x; });
+                const std::vector<PeakRec>& r = rec[k];
                 out[k].resize(r.size());
                 for (size_t q = 0; q < r.size(); ++q) out[k][q] = {r[q].x, r[q].y, r[q].snr, r[q].vidx};
-                order_peaks(out[k], keep);
+                if (keep) order_peaks(out[k], keep);
             }
-        });
-    for (auto& t : pool) t.join();
-    return out;
+        };
+        if (workers == 1) {
+            work(0);
+        } else {
+            std::vector<std::thread> pool;
+            for (size_t wk = 0; wk < workers; ++wk) pool.emplace_back(work, wk);
+            for (auto& t : pool) t.join();
+        }
+        return out;
+    }
 }
 
 std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vector<ArtefactJob>& jobs,
