@@ -132,7 +132,7 @@ def profiled_traffic(workload):
     """DRAM bytes (read + write) per stack_batch_kernel launch for a workload, from
     the committed ncu summary (a line `traffic_bytes_per_launch[<workload>] = N`)."""
     import re
-    path = os.path.join(ROOT, "profiles", "stack_batch_kernel_fullframe-2k.md")
+    path = os.path.join(ROOT, "profiles", "stack_batch_kernel_fullframe-1k.md")
     try:
         with open(path) as f:
             for line in f:
