@@ -39,6 +39,20 @@ void DevBuf::reset() {
 }
 
 Context::Context(int device, double budget_bytes) {
+    init(device);
+    size_t free_b = 0, total_b = 0;
+    FTB_CHECK(cudaMemGetInfo(&free_b, &total_b));
+    acct_ = std::make_shared<BudgetAccount>();
+    acct_->budget = budget_bytes > 0 ? static_cast<size_t>(budget_bytes) : static_cast<size_t>(0.9 * free_b);
+}
+
+Context::Context(int device, std::shared_ptr<BudgetAccount> account) {
+    if (!account) throw std::runtime_error("context: no budget account");
+    init(device);
+    acct_ = std::move(account);
+}
+
+void Context::init(int device) {
     if (device < 0) {
         const char* e = std::getenv("FAINTTRAIL_CUDA_DEVICE");
         device = e ? std::atoi(e) : 0;
@@ -57,9 +71,6 @@ Context::Context(int device, double budget_bytes) {
     sms_ = prop.multiProcessorCount;
     smem_optin_ = static_cast<int>(prop.sharedMemPerBlockOptin);
     total_ = static_cast<double>(prop.totalGlobalMem);
-    size_t free_b = 0, total_b = 0;
-    FTB_CHECK(cudaMemGetInfo(&free_b, &total_b));
-    budget_ = budget_bytes > 0 ? static_cast<size_t>(budget_bytes) : static_cast<size_t>(0.9 * free_b);
     FTB_CHECK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     FTB_CHECK(cudaMalloc(&d_err_, sizeof(int)));
     FTB_CHECK(cudaMemset(d_err_, 0, sizeof(int)));
@@ -144,11 +155,13 @@ Context::~Context() {
 void Context::bind() const { FTB_CHECK(cudaSetDevice(device_)); }
 
 void Context::charge(size_t bytes, const char* what) {
-    if (used_ + bytes > budget_)
-        throw std::runtime_error(std::string("HBM budget exceeded allocating ") + what + ": " +
-                                 std::to_string((used_ + bytes) / 1048576) + " MiB needed, budget " +
-                                 std::to_string(budget_ / 1048576) + " MiB");
-    used_ += bytes;
+    size_t cur = acct_->used.load();
+    do {
+        if (cur + bytes > acct_->budget)
+            throw std::runtime_error(std::string("HBM budget exceeded allocating ") + what + ": " +
+                                     std::to_string((cur + bytes) / 1048576) + " MiB needed, budget " +
+                                     std::to_string(acct_->budget / 1048576) + " MiB");
+    } while (!acct_->used.compare_exchange_weak(cur, cur + bytes));
 }
 
 void Context::check_kernel_error(const char* what) {

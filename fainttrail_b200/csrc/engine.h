@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <atomic>
 #include <functional>
 #include <memory>
 #include <string>
@@ -54,9 +55,18 @@ private:
     size_t bytes_ = 0;
 };
 
+// An HBM budget and what is charged against it; contexts on one device can
+// share one (the server's workers), so each sees the others' allocations.
+struct BudgetAccount {
+    size_t budget = 0;
+    std::atomic<size_t> used{0};
+};
+
 class Context {
 public:
     Context(int device, double budget_bytes);
+    // a context charging a shared account (its budget is the account's)
+    Context(int device, std::shared_ptr<BudgetAccount> account);
     ~Context();
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
@@ -64,10 +74,11 @@ public:
     int smem_optin() const { return smem_optin_; }
     const std::string& name() const { return name_; }
     double total_bytes() const { return total_; }
-    size_t budget() const { return budget_; }
-    size_t used() const { return used_; }
+    size_t budget() const { return acct_->budget; }
+    size_t used() const { return acct_->used.load(); }
+    const std::shared_ptr<BudgetAccount>& account() const { return acct_; }
     void charge(size_t bytes, const char* what);
-    void release(size_t bytes) { used_ -= bytes; }
+    void release(size_t bytes) { acct_->used -= bytes; }
     int* err_flag() const { return d_err_; }
     void check_kernel_error(const char* what);  // syncs the stream, reads the error flag
     void bind() const;                          // make the device current on this thread
@@ -92,7 +103,8 @@ private:
     int sms_ = 0, smem_optin_ = 0;
     std::string name_;
     double total_ = 0;
-    size_t budget_ = 0, used_ = 0;
+    std::shared_ptr<BudgetAccount> acct_;
+    void init(int device);
     int* d_err_ = nullptr;
     std::vector<DevBuf> scratch_;
     struct Span {

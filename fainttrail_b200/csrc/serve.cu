@@ -46,11 +46,11 @@ struct Server::Req {
 
 Server::Server(int device, double budget_bytes, int max_batch, int workers) : max_batch_(std::max(1, max_batch)) {
     workers = std::max(1, std::min(workers, 8));
-    // the first context resolves the device and the default budget (90 % of free)
+    // the first context resolves the device and the budget (default 90 % of free);
+    // the others charge the same account, so every worker sees all allocations
     ctx_.push_back(std::make_unique<Context>(device, budget_bytes));
-    const double share = static_cast<double>(ctx_[0]->budget()) / workers;
-    ctx_[0] = std::make_unique<Context>(ctx_[0]->device(), share);
-    for (int k = 1; k < workers; ++k) ctx_.push_back(std::make_unique<Context>(ctx_[0]->device(), share));
+    for (int k = 1; k < workers; ++k)
+        ctx_.push_back(std::make_unique<Context>(ctx_[0]->device(), ctx_[0]->account()));
     for (auto& c : ctx_) {
         Context* cp = c.get();
         workers_.emplace_back([this, cp] { loop(*cp); });
@@ -150,6 +150,7 @@ void Server::loop(Context& c) {
     }
     for (;;) {
         std::vector<std::shared_ptr<Req>> round;
+        size_t round_bytes = 0;
         {
             std::unique_lock<std::mutex> lk(mu_);
             ++idle_;
@@ -158,20 +159,28 @@ void Server::loop(Context& c) {
                 --idle_;
                 break;
             }
-            // admission: the oldest requests whose device memory fits this worker's
-            // budget, the queue shared out among the idle workers
+            // admission: the oldest requests whose device memory fits what the
+            // rounds in flight leave of the budget, the queue shared out among the
+            // idle workers; a request is admitted alone when nothing else runs
             const int share = static_cast<int>((queue_.size() + idle_ - 1) / std::max(1, idle_));
             const int cap = std::max(1, std::min(max_batch_, share));
-            --idle_;
+            const size_t budget = c.budget() > reserved_ ? c.budget() - reserved_ : 0;
             size_t need = 0;
-            const size_t budget = c.budget() > c.used() ? c.budget() - c.used() : 0;
             while (!queue_.empty() && static_cast<int>(round.size()) < cap) {
                 const size_t b = queue_.front()->bytes();
-                if (!round.empty() && need + b > budget) break;
+                if (need + b > budget && !(round.empty() && reserved_ == 0)) break;
                 need += b;
                 round.push_back(queue_.front());
                 queue_.pop_front();
             }
+            if (round.empty()) {  // waits for a round in flight to end
+                cv_.wait(lk);
+                --idle_;
+                continue;
+            }
+            --idle_;
+            reserved_ += need;
+            round_bytes = need;
         }
         run_round(c, round);
         {
@@ -184,10 +193,12 @@ void Server::loop(Context& c) {
             }
             last_done_ = t;
             launches_ += c.launches;
+            reserved_ -= round_bytes;
             ++rounds_;
             batched_ += static_cast<long long>(round.size());
         }
         done_cv_.notify_all();
+        cv_.notify_all();  // memory freed: a waiting worker may admit now
     }
 }
 

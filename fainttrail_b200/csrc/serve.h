@@ -42,6 +42,7 @@ private:
     void run_round(Context& c, std::vector<std::shared_ptr<Req>>& round);
     std::vector<std::unique_ptr<Context>> ctx_;
     int max_batch_ = 16, idle_ = 0;
+    size_t reserved_ = 0;  // estimated device bytes of the rounds in flight
     std::vector<std::thread> workers_;
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;

@@ -269,8 +269,10 @@ void ft_b200_clear_tuned_shapes(void);
  * per round. */
 typedef struct ft_b200_server ft_b200_server;
 
-/* workers: rounds in flight at once (each on its own stream with an equal share
- * of the budget; <= 0: 2), so one round's host work overlaps another's kernels. */
+/* workers: rounds in flight at once (each on its own stream; <= 0: 2), so one
+ * round's host work overlaps another's kernels. The workers share the HBM budget:
+ * requests are admitted while their estimated memory fits what the rounds in
+ * flight leave, and one that needs the whole budget runs alone. */
 int ft_b200_server_open(int device, double hbm_budget_bytes, int max_batch, int workers, ft_b200_server** out);
 /* Finishes the queued requests, then stops the worker. */
 void ft_b200_server_close(ft_b200_server* s);

@@ -106,3 +106,22 @@ def test_server_streaming_and_errors(device):
     for a, b in zip(got, alone):
         _same(a, b)
     assert st["completed"] == 3 and st["rounds"] >= 2
+
+
+def test_server_shared_budget_admits_as_memory_frees(device):
+    """A budget that holds one request at a time (each needs about 64 MB here):
+    the two workers share it, the others wait for memory, and every result still
+    equals the search run alone."""
+    import fainttrail_b200 as ftb
+    reqs = _requests()[:4]
+    alone = [device.search(f, m, e, **kw) for f, m, e, kw in reqs]
+    srv = ftb.Server(0, 100e6, max_batch=16, workers=2)
+    try:
+        tickets = [srv.submit(f, m, e, **kw) for f, m, e, kw in reqs]
+        got = [srv.poll(t) for t in tickets]
+        st = srv.stats()
+    finally:
+        srv.close()
+    for a, b in zip(got, alone):
+        _same(a, b)
+    assert st["completed"] == len(reqs) and st["rounds"] == len(reqs)
