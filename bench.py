@@ -153,7 +153,8 @@ def workload_desc(wl, m):
 # --------------------------------------------------------------------------- reference CPU timing
 def reference_search_rate(wl, frames_np, mjd, exptime, target_s=15.0, steps=1):
     """The reference CPU search (prepare + search, all host threads) on a crop of
-    the workload sized to about target_s seconds. Returns adds/s and a note."""
+    the workload sized to about target_s seconds. Returns adds/s, the crop side,
+    the seconds of a step and the motion count."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from ftoracle import Reference
     R = Reference()
@@ -176,7 +177,7 @@ def reference_search_rate(wl, frames_np, mjd, exptime, target_s=15.0, steps=1):
         side *= 2
         rate, dt = run(side)
     rates = [rate] + [run(side)[0] for _ in range(steps - 1)]
-    return statistics.median(rates), side, dt
+    return statistics.median(rates), side, dt, m
 
 
 # --------------------------------------------------------------------------- arms
@@ -193,14 +194,15 @@ def reference_arm(args):
     frames_np = frames[:, :side_max, :side_max].cpu().numpy()
     del frames
     t0 = time.perf_counter()
-    rate, side, dt = reference_search_rate(wl, frames_np, mjd, exptime, steps=max(1, args.steps))
+    rate, side, dt, m = reference_search_rate(wl, frames_np, mjd, exptime, steps=max(1, args.steps))
     cores = os.cpu_count()
     sample = (f"reference search() (prepare + real pass + {wl.null_runs} null runs, backend cpu) on a "
               f"{side} x {side} crop of all {wl.nframes} frames, full motion grid; {dt:.1f} s per step")
     out = {"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": 0, "ms_per_step": dt * 1000.0, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-           "config": {"workload": args.workload, "crop": f"{side}x{side}"},
+           "config": {"workload": workload_desc(wl, m), "crop": f"{side}x{side} of every frame",
+                      "parallelism": f"{cores} host threads"},
            "cpu_baseline": {"value": rate, "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample},
            "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "wall_s": time.perf_counter() - t0}
@@ -331,7 +333,7 @@ def b200_arm(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             frames_np = frames[:, :1024, :1024].cpu().numpy()
-            rate, side, dt = reference_search_rate(wl, frames_np, mjd, exptime)
+            rate, side, dt, _ = reference_search_rate(wl, frames_np, mjd, exptime)
             cpu = {"value": rate, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"reference search() with backend cpu on a {side} x {side} crop of all {n} frames, "
                              f"full motion grid, {wl.null_runs} null runs ({dt:.1f} s)"}
