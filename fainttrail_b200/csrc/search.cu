@@ -418,7 +418,9 @@ size_t SearchRequest::base_bytes(int w, int h, int n) {
 }
 
 size_t SearchRequest::item_bytes() const {
-    return sizeof(float) * (plane_ * o_.n + 2 * plane_) + 2 * map_bytes_;
+    // a null run: filtered frames, sky, mask, maps; an injection copy also keeps
+    // its sub frames and residuals until it is refined
+    return sizeof(float) * ((copies_ ? 3 : 1) * plane_ * o_.n + 2 * plane_) + 2 * map_bytes_;
 }
 
 void SearchRequest::prepare(const float* frames, const double* mjd, const double* exptime, bool on_device,
@@ -564,21 +566,22 @@ void SearchRequest::stage_items(int k0, int k1, const std::vector<std::vector<In
         } else {
             // an injection copy: raw frames + objects, prepared again with the same PSF width
             const int j = k - runs_;
-            if (!sub2_) {
-                sub2_ = DevBuf(&c, sizeof(float) * plane_ * n, "copy sub frames");
-                copy_sky_ = DevBuf(&c, sizeof(float) * plane_, "copy static sky");
-                copy_mask_ = DevBuf(&c, sizeof(float) * plane_, "copy mask");
-                if (!raw_) raw_ = DevBuf(&c, sizeof(float) * plane_ * n, "raw frames");
-            }
+            if (!raw_) raw_ = DevBuf(&c, sizeof(float) * plane_ * n, "raw frames");
+            it.sub = DevBuf(&c, sizeof(float) * plane_ * n, "copy sub frames");
+            it.res = DevBuf(&c, sizeof(float) * plane_ * n, "copy residuals");
+            it.sky = DevBuf(&c, sizeof(float) * plane_, "copy static sky");
+            it.mask = DevBuf(&c, sizeof(float) * plane_, "copy mask");
             FTB_CHECK(cudaMemcpyAsync(raw_.as<float>(), raw0_.as<float>(), sizeof(float) * plane_ * n,
                                       cudaMemcpyDeviceToDevice, c.stream()));
             apply_patches(c, injection_patches(copies[static_cast<size_t>(j)], o_.t_h, exp_sorted_, o_.fwhm_px, w, h),
                           raw_.as<float>(), w, h, n);
             it.background.resize(static_cast<size_t>(n));
             it.sigma.resize(static_cast<size_t>(n));
-            prepare_sub(c, *sc_, raw_.as<float>(), sub2_.as<float>(), w, h, n, it.background.data());
-            stage_run(c, *sc_, sub2_.as<float>(), w, h, n, o_.t_h.data(), sp_, it.filt.as<float>(),
-                      copy_sky_.as<float>(), copy_mask_.as<float>(), it.sigma.data(), nullptr);
+            prepare_sub(c, *sc_, raw_.as<float>(), it.sub.as<float>(), w, h, n, it.background.data());
+            stage_run(c, *sc_, it.sub.as<float>(), w, h, n, o_.t_h.data(), sp_, it.filt.as<float>(),
+                      it.sky.as<float>(), it.mask.as<float>(), it.sigma.data(), nullptr);
+            FTB_CHECK(cudaMemcpyAsync(it.res.as<float>(), sc_->residual.as<float>(), sizeof(float) * plane_ * n,
+                                      cudaMemcpyDeviceToDevice, c.stream()));
             jobs.push_back(job(it.filt.as<float>(), o_.t_h, it.max.as<float>(), it.bv.as<int>()));
         }
         items_.emplace(k, std::move(it));
@@ -622,10 +625,7 @@ void SearchRequest::finish_items(int k0, int k1) {
             items_.erase(k);  // the null run's buffers are released in stream order
         }
     }
-    for (int k = std::max(k0, runs_); k < k1; ++k) {  // copies keep only their maps
-        Item& it = items_.at(k);
-        it.filt.reset();
-    }
+    // the copies keep their frames: they are refined with the calibrated threshold
 }
 
 SearchOut SearchRequest::finalize(std::vector<SearchOut>* copies_out) {
@@ -686,6 +686,11 @@ SearchOut SearchRequest::finalize(std::vector<SearchOut>* copies_out) {
                 if (pk.snr >= co.thr.snr && pk.vidx >= 0) co.selected.push_back(pk);
             if (static_cast<int>(co.selected.size()) > p_.max_candidates)
                 co.selected.resize(static_cast<size_t>(p_.max_candidates));
+            // the copy's candidates, as completeness() reads them (validate.cpp:126-130)
+            if (!co.selected.empty())
+                co.candidates = refine_candidates(c, co, p_,
+                                                  {it.filt.as<float>(), it.res.as<float>(), it.sub.as<float>(),
+                                                   it.sky.as<float>(), it.mask.as<float>(), w, h, pitch_, n});
             co.max_snr.resize(static_cast<size_t>(w) * h);
             co.best_v.resize(static_cast<size_t>(w) * h);
             FTB_CHECK(cudaMemcpyAsync(co.max_snr.data(), it.max.as<float>(), map_bytes_, cudaMemcpyDeviceToHost,
@@ -718,6 +723,7 @@ SearchOut search_batch_host(Context& c, const float* frames, int w, int h, int n
     c.timing_reset();
     const int total = c.span_begin("total");
     SearchRequest r(c, p, w, h, n);
+    r.expect_copies(!copies.empty());
     r.prepare(frames, mjd, exptime, frames_on_device, in_pitch, !copies.empty(), report);
     // the real pass, the null runs and the copies as batches, each batch stacked
     // in persistent launches; a batch holds as many items as the HBM budget allows

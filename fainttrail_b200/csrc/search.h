@@ -173,6 +173,7 @@ public:
                  bool keep_raw, const std::function<void(double, const char*)>& report);
     int runs() const { return runs_; }
     size_t item_bytes() const;                        // device bytes one null run or copy holds in flight
+    void expect_copies(bool on) { copies_ = on; }     // copies hold their own frames until their refinement
     static size_t base_bytes(int w, int h, int n);    // device bytes of a prepared request
     void stage_items(int k0, int k1, const std::vector<std::vector<Injection>>& copies, std::vector<PassJob>& jobs);
     void finish_items(int k0, int k1);
@@ -181,6 +182,7 @@ public:
 private:
     struct Item {
         DevBuf filt, sky, mask, max, bv;
+        DevBuf sub, res;  // a copy's own background-subtracted frames and residuals
         std::vector<double> background, sigma;
     };
     PassJob job(const float* frames, const std::vector<double>& t, float* d_max, int* d_bv) const;
@@ -197,7 +199,8 @@ private:
     std::vector<std::vector<double>> orders_;
     std::vector<double> exp_sorted_;
     std::vector<float> pooled_;
-    DevBuf raw_, raw0_, sub_, filt_, sky_, mask_, max_, bv_, sub2_, copy_sky_, copy_mask_;
+    DevBuf raw_, raw0_, sub_, filt_, sky_, mask_, max_, bv_;
+    bool copies_ = false;
     DevBuf res_;  // the real residuals, for the candidates' photometry
     std::unique_ptr<StageScratch> sc_;
     std::map<int, Item> items_;

@@ -36,6 +36,9 @@ def test_copies_match_reference_inject_and_search(device, reference, oracle):
                          threshold_snr=ref["threshold"])
         assert got["method"] == "fixed" and got["threshold"] == ref["threshold"]
         assert same(got["max_snr"], want["max_snr"])
+        assert len(got["candidates"]) == len(want["candidates"])
+        for (row, flags), (wrow, wflags) in zip(got["candidates"], want["candidates"]):
+            assert np.array_equal(row, wrow) and flags == wflags
         px, py, ps, pv = oracle.find_peaks(got["max_snr"], got["best_v"], np.float32(ref["threshold"]), 2, 4, 100000)
         assert got["peaks"] == [(int(a), int(b), float(c), int(d)) for a, b, c, d in zip(px, py, ps, pv)]
 
