@@ -185,6 +185,38 @@ class Server:
             pass
 
 
+class CompletenessRow(C.Structure):
+    _fields_ = [("target_snr", C.c_double), ("injected", C.c_int), ("recovered", C.c_int), ("detected", C.c_int),
+                ("mean_snr", C.c_double), ("mean_dpos", C.c_double), ("mean_dv", C.c_double)]
+
+
+def completeness(device, frames, mjd, exptime, snr_levels=(4.0, 5.0, 6.0, 7.0, 8.0, 10.0, 12.0, 15.0), per_level=10,
+                 min_separation=40.0, seed=99, **kw):
+    """ft_b200_completeness (completeness(), validate.cpp:62-165) on `device` (a
+    Device): returns dict(rows=[dict per level], threshold, method, baseline_ok,
+    snr50)."""
+    L = device.L
+    L.ft_b200_completeness.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
+                                       C.POINTER(SearchParams), _f64p, C.c_int, C.c_int, C.c_double, C.c_ulonglong,
+                                       C.POINTER(CompletenessRow), C.POINTER(C.c_double), C.c_char_p, C.c_int,
+                                       C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    frames = np.ascontiguousarray(frames, dtype=np.float32)
+    n, h, w = frames.shape
+    p = Device._search_params(L, kw)
+    lv = np.ascontiguousarray(snr_levels, dtype=np.float64)
+    rows = (CompletenessRow * max(1, lv.size))()
+    thr, snr50 = C.c_double(), C.c_double()
+    ok = C.c_int()
+    meth = C.create_string_buffer(32)
+    rc = L.ft_b200_completeness(device.h, frames, w, h, n, np.ascontiguousarray(mjd, dtype=np.float64),
+                                np.ascontiguousarray(exptime, dtype=np.float64), C.byref(p), lv, lv.size, per_level,
+                                min_separation, seed, rows, C.byref(thr), meth, 32, C.byref(ok), C.byref(snr50))
+    device.check(rc, "completeness")
+    out = [dict(target_snr=r.target_snr, injected=r.injected, recovered=r.recovered, detected=r.detected,
+                mean_snr=r.mean_snr, mean_dpos=r.mean_dpos, mean_dv=r.mean_dv) for r in rows[:lv.size]]
+    return dict(rows=out, threshold=thr.value, method=meth.value.decode(), baseline_ok=ok.value, snr50=snr50.value)
+
+
 def set_tile_shape(shape):
     """ft_b200_set_tile_shape: 0 automatic, 1 = 32 x 16, 2 = 64 x 8 paired
     columns, 3 = 32 x 8, 4 = 32 x 4, 5 / 6 = 32 x 16 with one shared maximum per

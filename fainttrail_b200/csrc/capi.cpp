@@ -462,6 +462,32 @@ int ft_b200_result_peaks(const ft_b200_result* r, int which, ft_b200_peak* out, 
     return static_cast<int>(v.size());
 }
 
+int ft_b200_completeness(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
+                         const double* exptime, const ft_b200_search_params* params, const double* snr_levels,
+                         int nlevels, int per_level, double min_separation, unsigned long long seed,
+                         ft_b200_completeness_row* rows, double* threshold_snr, char* method, int method_cap,
+                         int* baseline_ok, double* snr50) {
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (!frames || !mjd || !exptime || !rows || nlevels < 0 || (nlevels > 0 && !snr_levels) || per_level < 0)
+            throw std::runtime_error("completeness: missing or malformed arguments");
+        const std::vector<double> levels(snr_levels, snr_levels + nlevels);
+        const ftb::CompletenessOut r = ftb::completeness_host(c, frames, width, height, nframes, mjd, exptime,
+                                                               to_search_params(params), levels, per_level,
+                                                               min_separation, seed);
+        for (int k = 0; k < nlevels; ++k) {
+            const ftb::CompletenessRow& q = r.rows[static_cast<size_t>(k)];
+            rows[k] = {q.target_snr, q.injected, q.recovered, q.detected, q.mean_snr, q.mean_dpos, q.mean_dv};
+        }
+        if (threshold_snr) *threshold_snr = r.threshold_snr;
+        if (method && method_cap > 0) {
+            std::strncpy(method, r.threshold_method.c_str(), static_cast<size_t>(method_cap) - 1);
+            method[method_cap - 1] = 0;
+        }
+        if (baseline_ok) *baseline_ok = r.baseline_ok;
+        if (snr50) *snr50 = r.snr50;
+    });
+}
+
 int ft_b200_null_threshold(const double* pooled, long long count, int runs, double fwhm_px, int width, int height,
                            int motions, const ft_b200_search_params* params, double* threshold, char* method,
                            int method_cap, double* a, double* b, double* k, double* inv_s2) {

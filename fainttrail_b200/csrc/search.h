@@ -38,6 +38,38 @@ struct Peak {
     int vidx = -1;
 };
 
+// xoshiro256** seeded by splitmix64, the reference's Rng (random.hpp:14-38):
+// the null-run permutations and the completeness placements draw from it.
+class Xoshiro {
+public:
+    explicit Xoshiro(uint64_t seed) {
+        uint64_t z = seed;
+        for (auto& v : s_) {
+            uint64_t r = (z += 0x9e3779b97f4a7c15ULL);
+            r = (r ^ (r >> 30)) * 0xbf58476d1ce4e5b9ULL;
+            r = (r ^ (r >> 27)) * 0x94d049bb133111ebULL;
+            v = r ^ (r >> 31);
+        }
+    }
+    double uniform() { return static_cast<double>(next() >> 11) * (1.0 / 9007199254740992.0); }
+    double uniform(double a, double b) { return a + (b - a) * uniform(); }
+
+private:
+    static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+    uint64_t next() {
+        const uint64_t out = rotl(s_[1] * 5, 7) * 9;
+        const uint64_t t = s_[1] << 17;
+        s_[2] ^= s_[0];
+        s_[3] ^= s_[1];
+        s_[1] ^= s_[2];
+        s_[0] ^= s_[3];
+        s_[2] ^= t;
+        s_[3] = rotl(s_[3], 45);
+        return out;
+    }
+    uint64_t s_[4];
+};
+
 // ---- host steps (bit-identical restatements of the reference's host code)
 std::vector<std::pair<double, double>> velocity_grid(double span_h, const SearchParams& p, double* dv_out);
 std::vector<std::vector<double>> null_time_orders(const std::vector<double>& t_h, int runs, uint64_t seed);
@@ -218,6 +250,27 @@ SearchOut search_host(Context& c, const float* frames, int w, int h, int n, cons
 // (fixed, no null runs) and the same PSF width. The real pass, the null runs and
 // the copies are stacked together in persistent launches. copies_out receives
 // one result per copy (peaks above the threshold, selected peaks, maps).
+// The injection-recovery test (completeness, validate.cpp:62-165): the
+// threshold calibrated once on the data, then per S/N level `per_level` objects
+// placed by the seeded generator away from each other and from the objects the
+// data already holds, injected, searched with that threshold held fixed (all
+// levels' copies in one batch), and matched to the candidates.
+struct CompletenessRow {
+    double target_snr = 0;
+    int injected = 0, recovered = 0, detected = 0;
+    double mean_snr = 0, mean_dpos = 0, mean_dv = 0;
+};
+struct CompletenessOut {
+    std::vector<CompletenessRow> rows;
+    double threshold_snr = 0;
+    std::string threshold_method;
+    int baseline_ok = 0;
+    double snr50 = 0;
+};
+CompletenessOut completeness_host(Context& c, const float* frames, int w, int h, int n, const double* mjd,
+                                  const double* exptime, const SearchParams& p, const std::vector<double>& levels,
+                                  int per_level, double min_separation, uint64_t seed);
+
 SearchOut search_batch_host(Context& c, const float* frames, int w, int h, int n, const double* mjd,
                             const double* exptime, const SearchParams& p,
                             const std::vector<std::vector<Injection>>& copies, std::vector<SearchOut>& copies_out,

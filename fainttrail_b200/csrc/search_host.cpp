@@ -36,38 +36,6 @@ std::vector<std::pair<double, double>> velocity_grid(double span_h, const Search
     return g;
 }
 
-namespace {
-// xoshiro256** seeded through splitmix64 (random.hpp:14-42, 75-82)
-class Xoshiro {
-public:
-    explicit Xoshiro(uint64_t seed) {
-        uint64_t z = seed;
-        for (auto& v : s_) {
-            uint64_t r = (z += 0x9e3779b97f4a7c15ULL);
-            r = (r ^ (r >> 30)) * 0xbf58476d1ce4e5b9ULL;
-            r = (r ^ (r >> 27)) * 0x94d049bb133111ebULL;
-            v = r ^ (r >> 31);
-        }
-    }
-    double uniform() { return static_cast<double>(next() >> 11) * (1.0 / 9007199254740992.0); }
-
-private:
-    static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
-    uint64_t next() {
-        const uint64_t out = rotl(s_[1] * 5, 7) * 9;
-        const uint64_t t = s_[1] << 17;
-        s_[2] ^= s_[0];
-        s_[3] ^= s_[1];
-        s_[1] ^= s_[2];
-        s_[0] ^= s_[3];
-        s_[2] ^= t;
-        s_[3] = rotl(s_[3], 45);
-        return out;
-    }
-    uint64_t s_[4];
-};
-}  // namespace
-
 // search.cpp:559-571: K Fisher-Yates shuffles of the frame times
 std::vector<std::vector<double>> null_time_orders(const std::vector<double>& t_h, int runs, uint64_t seed) {
     Xoshiro rng(seed);

@@ -157,6 +157,25 @@ typedef struct ft_b200_peak {
 
 typedef struct ft_b200_result ft_b200_result;
 
+/* The injection-recovery test, as completeness() (validate.cpp:62-165): the
+ * threshold calibrated on the data (a full search), then per S/N level
+ * per_level objects placed by the seeded xoshiro256** generator (at least
+ * min_separation apart and from the objects the data holds), injected as
+ * trailed Gaussians, searched with the threshold fixed and no null runs (all
+ * levels' copies in one batch) and matched to the candidates within 2 px and
+ * max(3, 2 dv) px/h. rows: nlevels entries. */
+typedef struct ft_b200_completeness_row {
+    double target_snr;
+    int injected, recovered, detected; /* recovered: matched candidates that passed every test */
+    double mean_snr, mean_dpos, mean_dv;
+} ft_b200_completeness_row;
+
+int ft_b200_completeness(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
+                         const double* exptime, const ft_b200_search_params* params, const double* snr_levels,
+                         int nlevels, int per_level, double min_separation, unsigned long long seed,
+                         ft_b200_completeness_row* rows, double* threshold_snr, char* method, int method_cap,
+                         int* baseline_ok, double* snr50);
+
 /* The null-tail threshold from pooled null-peak S/N values (set_threshold,
  * search.cpp:573-612; fit_null_tail_gauss :471-510, gauss_tail_level :517-527):
  * `pooled` is every run's surviving null peaks, run after run, `runs` the number

@@ -401,6 +401,45 @@ void ftref_result_candidate(void* rp, int k, double* out, char* flags_out) {
     flags_out[63] = 0;
 }
 
+// completeness() on raw frames: rows of 7 doubles per level (target_snr,
+// injected, recovered, detected, mean_snr, mean_dpos, mean_dv).
+int ftref_completeness(int n, int w, int h, const float* frames, const double* mjd, const double* exptime,
+                       const ft_params* params, const double* levels, int nlevels, int per_level, double min_sep,
+                       unsigned long long seed, double* rows, double* thr, char* method_out, int* baseline_ok,
+                       double* snr50) {
+    try {
+        std::vector<Frame> fr(static_cast<std::size_t>(n));
+        const std::size_t plane = static_cast<std::size_t>(w) * h;
+        for (int i = 0; i < n; ++i) {
+            fr[static_cast<std::size_t>(i)].image = Image(w, h);
+            std::memcpy(fr[static_cast<std::size_t>(i)].image.data.data(), frames + i * plane, plane * sizeof(float));
+            fr[static_cast<std::size_t>(i)].mjd_mid = mjd[i];
+            fr[static_cast<std::size_t>(i)].exptime_s = exptime[i];
+        }
+        CompletenessParams cp;
+        cp.snr_levels.assign(levels, levels + nlevels);
+        cp.per_level = per_level;
+        cp.min_separation = min_sep;
+        cp.seed = seed;
+        const CompletenessReport r = completeness(fr, to_search_params(params), cp);
+        for (std::size_t k = 0; k < r.rows.size(); ++k) {
+            const CompletenessRow& q = r.rows[k];
+            const double v[7] = {q.target_snr, static_cast<double>(q.injected), static_cast<double>(q.recovered),
+                                 static_cast<double>(q.detected), q.mean_snr, q.mean_dpos, q.mean_dv};
+            std::memcpy(rows + 7 * k, v, sizeof v);
+        }
+        *thr = r.threshold_snr;
+        std::strncpy(method_out, r.threshold_method.c_str(), 31);
+        method_out[31] = 0;
+        *baseline_ok = r.baseline_ok;
+        *snr50 = r.snr50;
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 // Injection of trailed movers (validate.cpp inject) into raw frames, in place.
 void ftref_inject(float* frames, int n, int w, int h, const double* mjd, const double* exptime, const double* obj,
                   int nobj, double t_ref_mjd, double fwhm_px) {

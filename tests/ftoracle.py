@@ -221,6 +221,11 @@ class Reference:
         L.ftref_result_candidate.argtypes = [C.c_void_p, C.c_int, _f64p, C.c_char_p]
         L.ftref_inject.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, _f64p, C.c_int, C.c_double,
                                    C.c_double]
+        if hasattr(L, "ftref_completeness"):
+            L.ftref_completeness.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f64p, _f64p, C.c_void_p, _f64p,
+                                             C.c_int, C.c_int, C.c_double, C.c_ulonglong, C.c_void_p,
+                                             C.POINTER(C.c_double), C.c_char_p, C.POINTER(C.c_int),
+                                             C.POINTER(C.c_double)]
 
     def err(self):
         return self.L.ftref_last_error().decode()
@@ -330,6 +335,27 @@ class Reference:
         if not hp:
             raise RuntimeError(self.err())
         return Prepared(self, hp)
+
+    def completeness(self, frames, mjd, exptime, snr_levels, per_level, min_separation, seed, **kw):
+        """The reference's completeness() (validate.cpp:62-165) on raw frames."""
+        frames = _f32(frames)
+        n, h, w = frames.shape
+        lv = _f64(snr_levels)
+        rows = np.empty((lv.size, 7))
+        thr, s50 = C.c_double(), C.c_double()
+        ok = C.c_int()
+        meth = C.create_string_buffer(32)
+        p = self.params(**kw)
+        if self.L.ftref_completeness(n, w, h, frames, _f64(mjd), _f64(exptime), C.byref(p), lv, lv.size, per_level,
+                                     C.c_double(min_separation), C.c_ulonglong(seed), rows.ctypes.data_as(C.c_void_p),
+                                     C.byref(thr), meth, C.byref(ok), C.byref(s50)):
+            raise RuntimeError(self.err())
+        keys = ("target_snr", "injected", "recovered", "detected", "mean_snr", "mean_dpos", "mean_dv")
+        out = [dict(zip(keys, r)) for r in rows]
+        for r in out:
+            for k in ("injected", "recovered", "detected"):
+                r[k] = int(r[k])
+        return dict(rows=out, threshold=thr.value, method=meth.value.decode(), baseline_ok=ok.value, snr50=s50.value)
 
     def inject(self, frames, mjd, exptime, objects, t_ref_mjd, fwhm_px):
         frames = _f32(frames).copy()

@@ -66,3 +66,23 @@ def test_launch_cap_and_device_frames(device):
             assert same(x["max_snr"], y["max_snr"]) and x["peaks"] == y["peaks"]
     one = device.search(raw, mjd, exp, passes_per_launch=1, **kw)
     assert one["threshold"] == base["threshold"] and same(one["max_snr"], base["max_snr"])
+
+
+def test_completeness_matches_reference(device, reference):
+    """completeness() end to end: the calibrated threshold, the seeded placements,
+    every level's copy search and the matching -- each row, the baseline count and
+    the interpolated S/N at 50 % equal the reference's."""
+    import fainttrail_b200 as ftb
+    R = reference
+    frames, mjd, exp = R.simulate(width=200, height=150, nframes=16, nstars=60, nmovers=2, seed=12,
+                                  rate_min_arcsec_min=0.3, rate_max_arcsec_min=1.2)
+    kw = dict(fwhm_px=2.5, null_runs=2, vmin_pxh=5.0, vmax_pxh=50.0)
+    args = ([4.0, 7.0, 9.0, 12.0], 5, 30.0, 7)
+    want = R.completeness(frames, mjd, exp, *args, **kw)
+    got = ftb.completeness(device, frames, mjd, exp, snr_levels=args[0], per_level=args[1], min_separation=args[2],
+                           seed=args[3], **kw)
+    assert got["threshold"] == want["threshold"] and got["method"] == want["method"]
+    assert got["baseline_ok"] == want["baseline_ok"] and got["snr50"] == want["snr50"]
+    assert sum(r["injected"] for r in want["rows"]) > 0 and sum(r["recovered"] for r in want["rows"]) > 0
+    for g, r in zip(got["rows"], want["rows"]):
+        assert g == {k: (type(g[k])(v)) for k, v in r.items()}
