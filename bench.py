@@ -48,7 +48,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "pixel·frame·motion/s"
 SHAPES = {0: "by frame count", 1: "32x16, 12 warps", 2: "64x8 paired columns, 12 warps", 3: "32x8, 16 warps",
-          4: "32x4, 16 warps", 5: "32x16 shared maximum, 16 warps", 6: "32x16 shared maximum, 14 warps"}
+          4: "32x4, 16 warps", 5: "32x16 shared maximum, 16 warps", 6: "32x16 shared maximum, 14 warps",
+          7: "32x12, 16 warps"}
 L2_BYTES = 126 * 1024 * 1024
 
 

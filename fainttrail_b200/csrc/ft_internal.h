@@ -89,8 +89,9 @@ void allow_dynamic_smem(const void* func, size_t bytes);
 
 // Compiled stack kernel shapes: 1 = 32 x 16 tiles (12 warps), 2 = 64 x 8 tiles with
 // paired columns (12 warps), 3 = 32 x 8 (16 warps), 4 = 32 x 4 (16 warps),
-// 5 = 32 x 16 with one shared maximum per tile (16 warps), 6 = the same with 14 warps.
-constexpr int kStackShapes = 6;
+// 5 = 32 x 16 with one shared maximum per tile (16 warps), 6 = the same with 14 warps,
+// 7 = 32 x 12 (16 warps).
+constexpr int kStackShapes = 7;
 StackConfig stack_shape_config(int shape, int device_smem_optin);
 bool stack_shape_fits(const StackConfig& c, int n);
 // A process-wide choice for choose_stack_config: 0 = by frame count, else a shape

@@ -135,6 +135,7 @@ StackConfig stack_shape_config(int shape, int smem_optin) {
             c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 14; c.merge = 1;
             c.smem_bytes -= 32 * 16 * 8;
             break;
+        case 7: c.tile_w = 32; c.wp = 40; c.p = 12; c.ty = 16; break;
         default: throw std::runtime_error("stack: unknown tile shape");
     }
     return c;
@@ -1199,6 +1200,9 @@ void stack_launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_de
         launch_batch<16, 16, 40, 4, 32, 1>(batch, d_desc, desc_bytes, d_err, sms, s);
     else if (c.tile_w == 32 && c.wp == 40 && c.ty == 14 && c.p == 16 && c.merge == 1)
         launch_batch<14, 16, 40, 4, 32, 1>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 12 && c.merge == 0)
+        launch_batch<16, 12, 40, 4, 32, 0>(batch, d_desc, desc_bytes, d_err, sms, s);
+
     else
         throw std::runtime_error("stack: unsupported tile shape");
 }

@@ -262,7 +262,7 @@ int ft_b200_result_velocity(const ft_b200_result* r, int vidx, double* vx_pxh, d
  * (the default: the autotuned choice where one is cached for the pass's frame
  * count, else the first shape whose windows fit), 1 = 32 x 16 output tiles,
  * 2 = 64 x 8 tiles with paired columns, 3 = 32 x 8, 4 = 32 x 4, 5 and 6 = 32 x 16
- * with one shared maximum per tile (16 and 14 warps). A fixed shape
+ * with one shared maximum per tile (16 and 14 warps), 7 = 32 x 12. A fixed shape
  * whose frame windows do not fit shared memory falls back to automatic. Results
  * do not depend on the shape. No counterpart in the reference (its CUDA kernel
  * has one shape, backend_cuda.cu:55-72). */
