@@ -43,7 +43,8 @@ class SearchParams(C.Structure):
         "max_frame_fraction", "half_tolerance")] + [
         ("static_exclude", C.c_int), ("null_runs", C.c_int), ("max_candidates", C.c_int), ("edge_px", C.c_int),
         ("threads", C.c_int), ("seed", C.c_ulonglong), ("null_tested", C.c_int), ("null_model_gauss", C.c_int),
-        ("passes_per_launch", C.c_int), ("shard_index", C.c_int), ("shard_count", C.c_int)]
+        ("passes_per_launch", C.c_int), ("shard_index", C.c_int), ("shard_count", C.c_int),
+        ("calibrated_threshold", C.c_double), ("calibrated_tail", C.c_double * 4)]
 
 
 class Injection(C.Structure):
@@ -352,6 +353,8 @@ class Device:
         p = SearchParams()
         L.ft_b200_search_params_default(C.byref(p))
         for k, v in kw.items():
+            if k == "calibrated_tail":
+                v = (C.c_double * 4)(*v)
             setattr(p, k, v)
         return p
 

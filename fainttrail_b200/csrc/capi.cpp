@@ -242,6 +242,11 @@ ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
     p.gauss_model = q.null_model_gauss != 0;
     p.passes_per_launch = std::max(0, q.passes_per_launch);
     p.half_tolerance = q.half_tolerance;
+    p.calibrated_threshold = q.calibrated_threshold;
+    p.cal_a = q.calibrated_tail[0];
+    p.cal_b = q.calibrated_tail[1];
+    p.cal_k = q.calibrated_tail[2];
+    p.cal_inv_s2 = q.calibrated_tail[3];
     p.shard_count = std::max(1, q.shard_count);
     p.shard_index = q.shard_index;
     if (p.shard_index < 0 || p.shard_index >= p.shard_count)

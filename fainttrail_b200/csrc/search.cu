@@ -493,7 +493,7 @@ void SearchRequest::prepare(const float* frames, const double* mjd, const double
     if (!sc_->fits(w, h, n, sp_.fwhm_px)) throw std::runtime_error("PSF too wide for the sample buffers");
     stage_filter(c, *sc_, w, h, n, sp_, filt_.as<float>(), mask_.as<float>(), nullptr, nullptr);
     // the real residuals stay for the candidates' photometry (null runs reuse the stage scratch)
-    if (p_.shard_count <= 1 || p_.shard_index == 0) {
+    if (p_.shard_count <= 1) {
         res_ = DevBuf(&c, sizeof(float) * plane_ * n, "real residuals");
         FTB_CHECK(cudaMemcpyAsync(res_.as<float>(), sc_->residual.as<float>(), sizeof(float) * plane_ * n,
                                   cudaMemcpyDeviceToDevice, c.stream()));
@@ -503,7 +503,8 @@ void SearchRequest::prepare(const float* frames, const double* mjd, const double
     o_.grid = velocity_grid(o_.span_h, p_, &o_.dv);
     m_ = o_.grid.size();
     auto_thr_ = p_.threshold_snr <= 0.0;
-    runs_ = auto_thr_ ? std::max(0, p_.null_runs) : 0;
+    calibrated_ = auto_thr_ && p_.calibrated_threshold > 0.0;  // the null runs ran elsewhere
+    runs_ = auto_thr_ && !calibrated_ ? std::max(0, p_.null_runs) : 0;
     nms_ = std::max(2, static_cast<int>(std::lround(o_.fwhm_px)));
     edge_ = std::max(p_.edge_px, 1);
     min_count_ = pass_min_count(p_.min_coverage, n);
@@ -514,14 +515,15 @@ void SearchRequest::prepare(const float* frames, const double* mjd, const double
     if (sharded_) {
         // this shard's block of the null runs: the same permutations (one seeded
         // stream for all runs) and, pooled in shard order, the same null peaks
-        if (!auto_thr_) throw std::runtime_error("search: sharding splits the null runs; a fixed threshold has none");
+        if (!auto_thr_ || calibrated_)
+            throw std::runtime_error("search: sharding splits the null runs; a fixed threshold has none");
         if (keep_raw) throw std::runtime_error("search: injection copies need the whole null calibration on one GPU");
         const long long k0 = static_cast<long long>(runs_total_) * p_.shard_index / p_.shard_count;
         const long long k1 = static_cast<long long>(runs_total_) * (p_.shard_index + 1) / p_.shard_count;
         orders_ = std::vector<std::vector<double>>(orders_.begin() + k0, orders_.begin() + k1);
         runs_ = static_cast<int>(k1 - k0);
-        real_ = p_.shard_index == 0;
-        real_queued_ = real_done_ = !real_;
+        real_ = false;  // the real pass runs once the pooled threshold is known
+        real_queued_ = real_done_ = true;
     }
     raw_needed_ = keep_raw;
     if (!keep_raw) raw_.reset();
@@ -637,7 +639,16 @@ SearchOut SearchRequest::finalize(std::vector<SearchOut>* copies_out) {
         o_.thr.method = "shard";
         o_.null_peaks.assign(pooled_.begin(), pooled_.end());
     } else {
-        o_.thr = set_threshold(p_, pooled_, runs_, o_.fwhm_px, w, h, m_);
+        if (calibrated_) {
+            o_.thr.snr = p_.calibrated_threshold;
+            o_.thr.method = "calibrated";
+            o_.thr.a = p_.cal_a;
+            o_.thr.b = p_.cal_b;
+            o_.thr.k = p_.cal_k;
+            o_.thr.inv_s2 = p_.cal_inv_s2;
+        } else {
+            o_.thr = set_threshold(p_, pooled_, runs_, o_.fwhm_px, w, h, m_);
+        }
         if (runs_ > 0 && auto_thr_) o_.null_peaks.assign(pooled_.begin(), pooled_.end());
         for (const Peak& pk : o_.peaks)
             if (pk.snr >= o_.thr.snr && pk.vidx >= 0) o_.selected.push_back(pk);

@@ -29,6 +29,8 @@ struct SearchParams {
     // null runs split over shard_count calls (one per GPU): this call runs block
     // shard_index of the null runs and, on shard 0 only, the real pass
     int shard_index = 0, shard_count = 1;
+    // > 0: the null-run threshold (and its tail fit) is given: no null runs
+    double calibrated_threshold = 0.0, cal_a = 0.0, cal_b = 0.0, cal_k = 0.0, cal_inv_s2 = 0.0;
     uint64_t seed = 12345;
 };
 
@@ -226,7 +228,7 @@ private:
     size_t plane_ = 0, map_bytes_ = 0, m_ = 0;
     bool auto_thr_ = true, real_queued_ = false, real_done_ = false, raw_needed_ = false;
     int runs_ = 0, runs_total_ = 0, nms_ = 2, edge_ = 1, min_count_ = 3;
-    bool real_ = true, sharded_ = false;
+    bool real_ = true, sharded_ = false, calibrated_ = false;
     float floor_ = 0;
     std::vector<std::vector<double>> orders_;
     std::vector<double> exp_sorted_;

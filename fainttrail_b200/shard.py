@@ -4,12 +4,13 @@ The null runs of a search (FaintTrail search.cpp:757-785) are independent: each
 permutes the frame times, rebuilds the preprocessing, stacks and screens its
 peaks. Rank k of N runs the block [runs*k/N, runs*(k+1)/N) with the permutations
 an unsplit search gives those runs (one seeded stream, search.cpp:559-571), and
-rank 0 also runs the real pass. The one exchange is the pooled null-peak S/N
-lists (at most 20,000 values per run, pool_null_peaks, search.cpp:690-693):
-every rank all-gathers them in rank order, which is run order, and computes the
-same threshold from the concatenation (set_threshold, search.cpp:573-612), so no
-broadcast is needed. Rank 0 then keeps the peaks above it (select_peaks,
-search.cpp:614-620). The result equals the unsplit search bit for bit.
+the one exchange is the pooled null-peak S/N lists (at most 20,000 values per
+run, pool_null_peaks, search.cpp:690-693): every rank all-gathers them in rank
+order, which is run order, and computes the same threshold from the
+concatenation (set_threshold, search.cpp:573-612), so no broadcast is needed.
+Rank 0 then runs the real pass with that threshold given (calibrated_threshold):
+its peaks, the selection (select_peaks, search.cpp:614-620) and the refined
+candidates. The result equals the unsplit search bit for bit.
 
 The exchange runs over whatever process group the caller passes: NCCL between
 GPUs (tensors on the current device) or gloo on the host.
@@ -55,8 +56,9 @@ def select_peaks(peaks, threshold, max_candidates):
 def sharded_search(dev, frames, mjd, exptime, group=None, **kw):
     """One search with its null runs split over the ranks of `group`; every rank
     calls it with the same frames and parameters. Returns the search result on
-    rank 0 (maps, peaks, threshold, pooled null peaks, selected peaks) and, on
-    the other ranks, their shard's result with the common threshold."""
+    rank 0 (maps, peaks, threshold and tail fit, pooled null peaks, selected
+    peaks, candidates) and, on the other ranks, their shard's result with the
+    common threshold."""
     import torch.distributed as dist
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     runs = kw.get("null_runs", 3)
@@ -64,10 +66,18 @@ def sharded_search(dev, frames, mjd, exptime, group=None, **kw):
     pooled = gather_pooled(r["null_peaks"], group)
     n, h, w = np.shape(frames)
     thr = null_threshold_for(r, pooled, runs, w, h, **kw)
+    if rank == 0:
+        r = finish_on_rank0(dev, frames, mjd, exptime, thr, **kw)
     r.update(thr)
     r["null_peaks"] = pooled
-    r["selected"] = select_peaks(r["peaks"], thr["threshold"], kw.get("max_candidates", 300)) if rank == 0 else []
     return r
+
+
+def finish_on_rank0(dev, frames, mjd, exptime, thr, **kw):
+    """The real pass, its peaks, selection and candidates with the pooled
+    threshold and tail fit given."""
+    return dev.search(frames, mjd, exptime, calibrated_threshold=thr["threshold"],
+                      calibrated_tail=(thr["null_a"], thr["null_b"], thr["null_k"], thr["null_inv_s2"]), **kw)
 
 
 def null_threshold_for(result, pooled, runs, width, height, **kw):

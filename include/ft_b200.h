@@ -137,12 +137,18 @@ typedef struct ft_b200_search_params {
     int shard_index, shard_count; /* null runs split over shard_count calls, one per GPU
                               (default 0, 1: no split). Call k runs null runs
                               [runs*k/count, runs*(k+1)/count) with the permutations
-                              an unsplit search would give them, and only call 0
-                              runs the real pass. A shard's result holds its pooled
-                              null peaks (method "shard", no threshold, no selection;
-                              maps and peaks on shard 0 only): concatenate the
-                              shards' null peaks in shard order, then
-                              ft_b200_null_threshold gives the unsplit threshold. */
+                              an unsplit search would give them. A shard's result
+                              holds its pooled null peaks (method "shard",
+                              no real pass): concatenate the shards' null peaks in
+                              shard order, then ft_b200_null_threshold gives the
+                              unsplit threshold; one call with it as
+                              calibrated_threshold finishes the search. */
+    double calibrated_threshold; /* > 0: the null-run threshold is given (no null runs
+                              are run): the real pass, its peaks above min_snr_floor,
+                              the selection at this threshold and the refined
+                              candidates, as the unsplit search gives them */
+    double calibrated_tail[4];   /* a, b, k, inv_s2 of that threshold's null-tail fit
+                              (the candidates' false-alarm rates) */
 } ft_b200_search_params;
 
 void ft_b200_search_params_default(ft_b200_search_params* p);
