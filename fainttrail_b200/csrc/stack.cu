@@ -458,11 +458,6 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
         : "memory");
 }
 
-__device__ __forceinline__ uint32_t half16(const uint4& q, int k) {
-    const uint32_t w = k < 2 ? q.x : k < 4 ? q.y : k < 6 ? q.z : q.w;
-    return (k & 1) ? (w >> 16) : (w & 0xffffu);
-}
-
 template <int P, int WP>
 __device__ __forceinline__ void load_column(float (&v)[P], const float* __restrict__ src) {
 #pragma unroll
@@ -500,23 +495,13 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
     for (int k = 0; k < M; ++k)
 #pragma unroll
         for (int w = 0; w < PW; ++w) cpart[k][w] = 0;
-#ifndef FTB_STACK_PIPE
-#define FTB_STACK_PIPE 1
-#endif
     // the next frame's four offsets are loaded one frame ahead, so the reuse
     // tests below do not wait on a shared-memory load
     const uint16_t* op = offs + s0;
     uint2 qn = *reinterpret_cast<const uint2*>(op);
-#if FTB_STACK_PIPE == 2
-#pragma unroll 2
-#endif
     for (int i = 0; i < a.n; ++i) {
-#if FTB_STACK_PIPE >= 1
         const uint2 q = qn;
         if (i + 1 < a.n) qn = *reinterpret_cast<const uint2*>(op + (i + 1) * G.nslots);
-#else
-        const uint2 q = *reinterpret_cast<const uint2*>(offs + i * G.nslots + s0);
-#endif
         const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
         float v[P];
         load_column<P, WP>(v, win + o0 + tb);
