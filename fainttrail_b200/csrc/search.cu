@@ -367,35 +367,6 @@ std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vect
     return out;
 }
 
-std::vector<char> device_artefacts(Context& c, const std::vector<Peak>& peaks, size_t count,
-                                   const std::vector<std::pair<double, double>>& grid, const float* d_filtered,
-                                   const float* d_sub, const float* d_sky, const std::vector<double>& t_h, int w,
-                                   int h, int n, double fwhm_px, double max_frame_fraction) {
-    std::vector<char> art(count, 0);
-    if (count == 0) return art;
-    cudaStream_t s = c.stream();
-    std::vector<PeakRec> rec(count);
-    for (size_t k = 0; k < count; ++k) rec[k] = {peaks[k].x, peaks[k].y, peaks[k].snr, peaks[k].vidx};
-    const size_t bytes = sizeof(PeakRec) * count + sizeof(double) * (2 * grid.size() + t_h.size()) + count + 1024;
-    DevBuf& buf = c.scratch(21, bytes, "artefact screen");
-    unsigned char* base = buf.as<unsigned char>();
-    PeakRec* d_peaks = reinterpret_cast<PeakRec*>(base);
-    double* d_vel = reinterpret_cast<double*>(base + ((sizeof(PeakRec) * count + 255) / 256) * 256);
-    double* d_t = d_vel + 2 * grid.size();
-    char* d_out = reinterpret_cast<char*>(d_t + t_h.size());
-    FTB_CHECK(cudaMemcpyAsync(d_peaks, rec.data(), sizeof(PeakRec) * count, cudaMemcpyHostToDevice, s));
-    FTB_CHECK(cudaMemcpyAsync(d_vel, grid.data(), sizeof(double) * 2 * grid.size(), cudaMemcpyHostToDevice, s));
-    FTB_CHECK(cudaMemcpyAsync(d_t, t_h.data(), sizeof(double) * t_h.size(), cudaMemcpyHostToDevice, s));
-    ArtArgs a{d_peaks, static_cast<int>(count), d_vel, d_filtered, d_sub, d_sky, d_t, w, h, frame_pitch(w), n,
-              static_cast<int>(std::ceil(2.0 * fwhm_px)) + 1, max_frame_fraction, d_out};
-    artefact_kernel<<<static_cast<unsigned>((count + 127) / 128), 128, 0, s>>>(a);
-    FTB_CHECK(cudaGetLastError());
-    ++c.launches;
-    FTB_CHECK(cudaMemcpyAsync(art.data(), d_out, count, cudaMemcpyDeviceToHost, s));
-    FTB_CHECK(cudaStreamSynchronize(s));
-    return art;
-}
-
 // ------------------------------------------------------------------ a search request in phases
 
 SearchRequest::SearchRequest(Context& c, const SearchParams& p, int w, int h, int n) : c_(c), p_(p) {

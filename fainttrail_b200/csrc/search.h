@@ -103,13 +103,6 @@ void prepare_sub(Context& c, StageScratch& sc, float* d_raw, float* d_sub, int w
 // raster order
 std::vector<Peak> device_peaks(Context& c, const float* d_max, const int* d_best_v, int w, int h, float floor,
                                int radius, int edge);
-// artefact flags (single-frame share, field edge) of peaks at their grid motion
-// (is_artefact_peak, search.cpp:229-243, 142-190), on the device
-std::vector<char> device_artefacts(Context& c, const std::vector<Peak>& peaks, size_t count,
-                                   const std::vector<std::pair<double, double>>& grid, const float* d_filtered,
-                                   const float* d_sub, const float* d_sky, const std::vector<double>& t_h, int w,
-                                   int h, int n, double fwhm_px, double max_frame_fraction);
-
 // The same for many maps at once (the null runs of a batch): every peak kernel
 // is queued, one sync brings all candidate lists back, and the host orders them
 // (raster order, then order_peaks with `keep`) on a thread per map.
@@ -119,7 +112,9 @@ struct PeakMap {
 };
 std::vector<std::vector<Peak>> device_peaks_many(Context& c, const std::vector<PeakMap>& maps, int w, int h,
                                                  float floor, int radius, int edge, size_t keep);
-// artefact flags of the first count[k] peaks of every null run k, one sync
+// artefact flags (single-frame share, field edge) of the first count[k] peaks of
+// every null run k at their grid motions (is_artefact_peak, search.cpp:229-243,
+// 142-190), on the device, one sync
 struct ArtefactJob {
     const std::vector<Peak>* peaks;
     size_t count;
