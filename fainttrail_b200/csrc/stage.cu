@@ -406,10 +406,12 @@ __global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
         const int gx = x0 - H + e % ZW, gy = y0 - H + e / ZW;
         float z = 0.0f;
         if (gx >= 0 && gy >= 0 && gx < a.w && gy < a.h) {
+            // the three loads are independent, so they are in flight together
             const size_t pix = static_cast<size_t>(gy) * a.pitch + gx;
-            const float v = a.residual[f * plane + pix];
-            if (a.mask[pix] != 0.0f && finitef(v)) {
-                const float s = a.scatter[pix];
+            const float v = __ldg(a.residual + f * plane + pix);
+            const float mk = __ldg(a.mask + pix);
+            const float s = __ldg(a.scatter + pix);
+            if (mk != 0.0f && finitef(v)) {
                 const float vm = __fmul_rn(v, inv);
                 // (v / sigma) / e with e = scatter above weight_scatter, else 1 (an exact division)
                 z = s > a.wscat ? __fdiv_rn(vm, s) : vm;
