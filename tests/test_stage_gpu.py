@@ -72,3 +72,23 @@ def test_stage_then_stack_matches_reference_pass(device, backend, oracle):
     dx, dy = oracle.shift_table(g["t_h"], grid)
     ms, bv = oracle.stack(g["filtered"], dx, dy, mc)
     assert same(r.max_snr, ms) and same(r.best_v, bv)
+
+
+def test_noise_normalisation(device, reference):
+    """The reference's test_noise_normalisation (tests/test_main.cpp:146-167) on
+    the device stage: on a star field without movers (192 x 192 x 40, hot pixels,
+    cosmic rays), every seventh filtered frame has mean |m| < 0.1 and standard
+    deviation in (0.9, 1.15) over the unmasked pixels 10 px inside the edge."""
+    R = reference
+    frames, mjd, exp = R.simulate(width=192, height=192, nframes=40, exptime_s=45.0, cadence_s=60.0, nstars=200,
+                                  hot_pixels=15, cosmic_rays_per_frame=2.0, nmovers=0, seed=11)
+    prep = R.prepare(frames, mjd, exp, vmin_pxh=8.0, vmax_pxh=30.0, null_runs=2)
+    got = device.stage(prep.images()["sub"], prep.vectors()["t_h"], prep.fwhm)
+    flt, mask = got["filtered"], got["mask"]
+    inner = np.zeros(mask.shape, bool)
+    inner[10:-10, 10:-10] = True
+    keep = inner & (mask != 0.0)
+    for i in range(0, flt.shape[0], 7):
+        v = flt[i][keep].astype(np.float64)
+        mean, sd = v.mean(), v.std()
+        assert abs(mean) < 0.1 and 0.9 < sd < 1.15
