@@ -101,6 +101,7 @@ def _declare(L):
                                            C.POINTER(SearchParams), C.c_int, C.c_void_p, C.c_void_p,
                                            C.POINTER(C.c_void_p), C.c_void_p]
     L.ft_b200_result_free.argtypes = [C.c_void_p]
+    L.ft_b200_result_candidates.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]
     L.ft_b200_result_threshold.argtypes = [C.c_void_p, C.c_char_p, C.c_int] + [C.POINTER(C.c_double)] * 4
     L.ft_b200_result_threshold.restype = C.c_double
     L.ft_b200_result_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 3 + [C.POINTER(C.c_int)]
@@ -161,7 +162,7 @@ class Server:
             return None
         if rc != FT_B200_OK:
             raise RuntimeError("poll: " + self.L.ft_b200_server_error(self.h).decode())
-        return Device._result(self, r, w, h, maps)
+        return _read_result(self.L, r, w, h, maps)
 
     def pause(self, paused=True):
         self.L.ft_b200_server_pause(self.h, 1 if paused else 0)
@@ -416,51 +417,54 @@ class Device:
         return res, [self._result(C.c_void_p(outs[k]), width, height, maps) for k in range(len(copies))]
 
     def _result(self, r, w, h, maps):
-        L = self.L
-        try:
-            meth = C.create_string_buffer(32)
-            a, b, k, s2 = C.c_double(), C.c_double(), C.c_double(), C.c_double()
-            thr = L.ft_b200_result_threshold(r, meth, 32, C.byref(a), C.byref(b), C.byref(k), C.byref(s2))
-            fw, dv, tref, nv = C.c_double(), C.c_double(), C.c_double(), C.c_int()
-            L.ft_b200_result_info(r, C.byref(fw), C.byref(dv), C.byref(tref), C.byref(nv))
-
-            def peaks(which):
-                cnt = L.ft_b200_result_peaks(r, which, None, 0)
-                arr = (Peak * max(cnt, 1))()
-                L.ft_b200_result_peaks(r, which, arr, cnt)
-                return [(q.x, q.y, q.snr, q.vidx) for q in arr[:cnt]]
-            cnt = L.ft_b200_result_null_peaks(r, None, 0)
-            nulls = np.empty(cnt)
-            L.ft_b200_result_null_peaks(r, nulls.ctypes.data_as(C.c_void_p), cnt)
-            ms = bv = None
-            if maps:
-                ms = np.empty((h, w), np.float32)
-                bv = np.empty((h, w), np.int32)
-                if L.ft_b200_result_maps(r, ms.ctypes.data_as(C.c_void_p), bv.ctypes.data_as(C.c_void_p)) != FT_B200_OK:
-                    ms = bv = None  # a null-run shard other than 0 has no maps
-            grid = np.empty((nv.value, 2))
-            vx, vy = C.c_double(), C.c_double()
-            for j in range(nv.value):
-                L.ft_b200_result_velocity(r, j, C.byref(vx), C.byref(vy))
-                grid[j] = (vx.value, vy.value)
-            L.ft_b200_result_candidates.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]
-            nc = L.ft_b200_result_candidates(r, None, None, 0)
-            rows = np.empty((max(nc, 1), 17))
-            fl = C.create_string_buffer(64 * max(nc, 1))
-            L.ft_b200_result_candidates(r, rows.ctypes.data_as(C.c_void_p), fl, nc)
-            cands = [(rows[q].copy(), fl.raw[64 * q:64 * q + 64].split(b"\0", 1)[0].decode()) for q in range(nc)]
-            return dict(threshold=thr, method=meth.value.decode(), null_a=a.value, null_b=b.value, null_k=k.value,
-                        null_inv_s2=s2.value, fwhm=fw.value, dv=dv.value, t_ref=tref.value, n_velocities=nv.value,
-                        peaks=peaks(0), selected=peaks(1), null_peaks=nulls, max_snr=ms, best_v=bv, grid=grid,
-                        candidates=cands)
-        finally:
-            L.ft_b200_result_free(r)
+        return _read_result(self.L, r, w, h, maps)
 
     def info(self):
         name = C.create_string_buffer(256)
         sms, mem = C.c_int(), C.c_double()
         self.check(self.L.ft_b200_device_info(self.h, name, 256, C.byref(sms), C.byref(mem)), "device_info")
         return name.value.decode(), sms.value, mem.value
+
+
+def _read_result(L, r, w, h, maps):
+    """The getters of an ft_b200_result (freed here) as a dict."""
+    try:
+        meth = C.create_string_buffer(32)
+        a, b, k, s2 = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        thr = L.ft_b200_result_threshold(r, meth, 32, C.byref(a), C.byref(b), C.byref(k), C.byref(s2))
+        fw, dv, tref, nv = C.c_double(), C.c_double(), C.c_double(), C.c_int()
+        L.ft_b200_result_info(r, C.byref(fw), C.byref(dv), C.byref(tref), C.byref(nv))
+
+        def peaks(which):
+            cnt = L.ft_b200_result_peaks(r, which, None, 0)
+            arr = (Peak * max(cnt, 1))()
+            L.ft_b200_result_peaks(r, which, arr, cnt)
+            return [(q.x, q.y, q.snr, q.vidx) for q in arr[:cnt]]
+        cnt = L.ft_b200_result_null_peaks(r, None, 0)
+        nulls = np.empty(cnt)
+        L.ft_b200_result_null_peaks(r, nulls.ctypes.data_as(C.c_void_p), cnt)
+        ms = bv = None
+        if maps:
+            ms = np.empty((h, w), np.float32)
+            bv = np.empty((h, w), np.int32)
+            if L.ft_b200_result_maps(r, ms.ctypes.data_as(C.c_void_p), bv.ctypes.data_as(C.c_void_p)) != FT_B200_OK:
+                ms = bv = None  # a null-run shard other than 0 has no maps
+        grid = np.empty((nv.value, 2))
+        vx, vy = C.c_double(), C.c_double()
+        for j in range(nv.value):
+            L.ft_b200_result_velocity(r, j, C.byref(vx), C.byref(vy))
+            grid[j] = (vx.value, vy.value)
+        nc = L.ft_b200_result_candidates(r, None, None, 0)
+        rows = np.empty((max(nc, 1), 17))
+        fl = C.create_string_buffer(64 * max(nc, 1))
+        L.ft_b200_result_candidates(r, rows.ctypes.data_as(C.c_void_p), fl, nc)
+        cands = [(rows[q].copy(), fl.raw[64 * q:64 * q + 64].split(b"\0", 1)[0].decode()) for q in range(nc)]
+        return dict(threshold=thr, method=meth.value.decode(), null_a=a.value, null_b=b.value, null_k=k.value,
+                    null_inv_s2=s2.value, fwhm=fw.value, dv=dv.value, t_ref=tref.value, n_velocities=nv.value,
+                    peaks=peaks(0), selected=peaks(1), null_peaks=nulls, max_snr=ms, best_v=bv, grid=grid,
+                    candidates=cands)
+    finally:
+        L.ft_b200_result_free(r)
 
 
 def _progress(fn):
