@@ -45,7 +45,7 @@ def test_tie_known_answer(backend):
 
 
 @pytest.mark.parametrize("w,h,n,seed", [(1, 1, 1, 0), (33, 17, 5, 1), (64, 64, 20, 2), (130, 70, 40, 3),
-                                        (200, 37, 64, 4), (96, 40, 120, 5)])
+                                        (200, 37, 64, 4), (96, 40, 120, 5), (48, 20, 255, 6)])
 def test_random_lattice_passes(backend, oracle, shape, w, h, n, seed):
     rng = np.random.default_rng(seed)
     frames = rng.standard_normal((n, h, w)).astype(np.float32)
