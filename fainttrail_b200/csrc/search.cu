@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <numeric>
 #include <thread>
 
@@ -145,48 +146,59 @@ struct ArtArgs {
 // is_artefact_peak without registration offsets (search.cpp:229-243): the
 // single-frame share of the track's positive signal, then the field-edge test
 // (blank sub-frame or static-sky pixels within r of the track in more than
-// max(1, n/10) frames). One thread per peak.
-__global__ void artefact_kernel(const ArtArgs a) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= a.count) return;
+// max(1, n/10) frames). One warp per peak: the lanes sample the frames and scan
+// the edge boxes; lane 0 adds the positive signal in frame order, as the
+// reference does.
+constexpr int kArtWarps = 4;
+
+__global__ void __launch_bounds__(32 * kArtWarps) artefact_kernel(const ArtArgs a) {
+    __shared__ double vals[kArtWarps][256];  // a warp's track values, n <= 255 frames
+    const int warp = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
+    const int k = blockIdx.x * kArtWarps + warp;
+    if (k >= a.count) return;  // the whole warp
     const PeakRec pk = a.peaks[k];
     const double vx = a.vel[2 * pk.vidx], vy = a.vel[2 * pk.vidx + 1];
     const size_t plane = static_cast<size_t>(a.pitch) * a.h;
-    double pos_sum = 0.0, maxc = 0.0;
-    for (int i = 0; i < a.n; ++i) {
+    for (int i = lane; i < a.n; i += 32) {
         const double t = a.t_h[i];
         const double px = __dadd_rn(static_cast<double>(pk.x), __dmul_rn(vx, t));
         const double py = __dadd_rn(static_cast<double>(pk.y), __dmul_rn(vy, t));
         const float v = bilinear(a.filtered + i * plane, a.w, a.h, a.pitch, px, py);
-        if (!isfinite(v)) continue;
-        const double d = v;
-        pos_sum = __dadd_rn(pos_sum, d > 0.0 ? d : 0.0);
-        maxc = maxc < d ? d : maxc;
+        vals[warp][i] = isfinite(v) ? static_cast<double>(v) : CUDART_NAN;
     }
-    const double frac = pos_sum > 0.0 ? maxc / pos_sum : 1.0;
-    if (a.n >= 8 && frac > a.max_frame_fraction) {
-        a.out[k] = 1;
+    __syncwarp();
+    int single = 0;
+    if (lane == 0) {
+        double pos_sum = 0.0, maxc = 0.0;
+        for (int i = 0; i < a.n; ++i) {
+            const double d = vals[warp][i];
+            if (!isfinite(d)) continue;
+            pos_sum = __dadd_rn(pos_sum, d > 0.0 ? d : 0.0);
+            maxc = maxc < d ? d : maxc;
+        }
+        const double frac = pos_sum > 0.0 ? maxc / pos_sum : 1.0;
+        single = a.n >= 8 && frac > a.max_frame_fraction;
+    }
+    if (__shfl_sync(0xffffffffu, single, 0)) {
+        if (lane == 0) a.out[k] = 1;
         return;
     }
+    const int side = 2 * a.r + 1, box = side * side;
     int near_blank = 0;
     for (int i = 0; i < a.n; ++i) {
         const double t = a.t_h[i];
         const int xi = static_cast<int>(lround(__dadd_rn(static_cast<double>(pk.x), __dmul_rn(vx, t))));
         const int yi = static_cast<int>(lround(__dadd_rn(static_cast<double>(pk.y), __dmul_rn(vy, t))));
         bool blank = false;
-        for (int dy = -a.r; dy <= a.r && !blank; ++dy)
-            for (int dx = -a.r; dx <= a.r; ++dx) {
-                const int xx = xi + dx, yy = yi + dy;
-                if (xx < 0 || yy < 0 || xx >= a.w || yy >= a.h ||
+        for (int e = lane; e < box && !blank; e += 32) {
+            const int xx = xi + e % side - a.r, yy = yi + e / side - a.r;
+            blank = xx < 0 || yy < 0 || xx >= a.w || yy >= a.h ||
                     !isfinite(a.sub[i * plane + static_cast<size_t>(yy) * a.pitch + xx]) ||
-                    !isfinite(a.sky[static_cast<size_t>(yy) * a.pitch + xx])) {
-                    blank = true;
-                    break;
-                }
-            }
-        near_blank += blank;
+                    !isfinite(a.sky[static_cast<size_t>(yy) * a.pitch + xx]);
+        }
+        near_blank += __any_sync(0xffffffffu, blank) ? 1 : 0;
     }
-    a.out[k] = (near_blank > max(1, a.n / 10)) ? 1 : 0;
+    if (lane == 0) a.out[k] = (near_blank > max(1, a.n / 10)) ? 1 : 0;
 }
 
 // Injection increments added in order: one CTA per frame walks its patches in
@@ -245,6 +257,25 @@ void apply_patches(Context& c, const InjectionPatches& ip, float* d_frames, int 
     ++c.launches;
 }  // buf is released in stream order after the kernel
 
+namespace {
+// f(k) for k < count on up to 16 host threads
+template <class F>
+void for_each_map(size_t count, const F& f) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t workers = std::min<size_t>(hw, count);
+    if (workers <= 1) {
+        for (size_t k = 0; k < count; ++k) f(k);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t wk = 0; wk < workers; ++wk)
+        pool.emplace_back([&, wk] {
+            for (size_t k = wk; k < count; k += workers) f(k);
+        });
+    for (auto& t : pool) t.join();
+}
+}  // namespace
+
 std::vector<Peak> device_peaks(Context& c, const float* d_max, const int* d_best_v, int w, int h, float floor,
                                int radius, int edge) {
     return device_peaks_many(c, {{d_max, d_best_v}}, w, h, floor, radius, edge, 0)[0];
@@ -290,25 +321,51 @@ std::vector<std::vector<Peak>> device_peaks_many(Context& c, const std::vector<P
         FTB_CHECK(cudaStreamSynchronize(s));
         // already in raster order; order_peaks' std::sort by S/N (ties as the
         // reference's) and the truncation, one map per host thread
-        const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-        const size_t workers = std::min<size_t>(hw, k_maps);
-        auto work = [&](size_t wk) {
-            for (size_t k = wk; k < k_maps; k += workers) {
-                const std::vector<PeakRec>& r = rec[k];
-                out[k].resize(r.size());
-                for (size_t q = 0; q < r.size(); ++q) out[k][q] = {r[q].x, r[q].y, r[q].snr, r[q].vidx};
-                if (keep) order_peaks(out[k], keep);
-            }
-        };
-        if (workers == 1) {
-            work(0);
-        } else {
-            std::vector<std::thread> pool;
-            for (size_t wk = 0; wk < workers; ++wk) pool.emplace_back(work, wk);
-            for (auto& t : pool) t.join();
+        for (size_t k = 0; k < k_maps; ++k) {
+            const std::vector<PeakRec>& r = rec[k];
+            out[k].resize(r.size());
+            for (size_t q = 0; q < r.size(); ++q) out[k][q] = {r[q].x, r[q].y, r[q].snr, r[q].vidx};
         }
+        if (keep) for_each_map(k_maps, [&](size_t k) { order_peaks(out[k], keep); });
         return out;
     }
+}
+
+NullPeaks split_null_peaks(std::vector<Peak> raster, size_t keep, size_t tested) {
+    NullPeaks out;
+    const size_t N = raster.size(), nk = std::min(N, keep), t = std::min(nk, tested);
+    if (N == 0) return out;
+    std::vector<float> v(N);
+    for (size_t q = 0; q < N; ++q) v[q] = raster[q].snr;
+    if (t > 0 && t < N) {
+        // the t-th and (t+1)-th largest S/N: the screened set is unique unless they tie
+        std::nth_element(v.begin(), v.begin() + static_cast<std::ptrdiff_t>(t), v.end(), std::greater<float>());
+        const float after = v[t];
+        const float last = *std::min_element(v.begin(), v.begin() + static_cast<std::ptrdiff_t>(t));
+        if (!(last > after)) {  // a tie at the boundary: the reference's sort decides
+            order_peaks(raster, keep);
+            out.tested.assign(raster.begin(), raster.begin() + static_cast<std::ptrdiff_t>(t));
+            for (size_t q = t; q < raster.size(); ++q) out.rest.push_back(raster[q].snr);
+            return out;
+        }
+        for (const Peak& p : raster)
+            if (p.snr >= last) out.tested.push_back(p);
+        out.rest.assign(v.begin() + static_cast<std::ptrdiff_t>(t), v.end());
+    } else if (t == 0) {
+        out.rest = v;
+    } else {  // t == N: every peak is screened
+        out.tested = std::move(raster);
+        return out;
+    }
+    // the untested values down to the truncation, descending (equal values are
+    // interchangeable in the pooled list)
+    if (out.rest.size() > nk - t) {
+        std::nth_element(out.rest.begin(), out.rest.begin() + static_cast<std::ptrdiff_t>(nk - t), out.rest.end(),
+                         std::greater<float>());
+        out.rest.resize(nk - t);
+    }
+    std::sort(out.rest.begin(), out.rest.end(), std::greater<float>());
+    return out;
 }
 
 std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vector<ArtefactJob>& jobs,
@@ -353,7 +410,7 @@ std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vect
         ArtArgs a{reinterpret_cast<const PeakRec*>(b), static_cast<int>(jobs[k].count),
                   reinterpret_cast<const double*>(base), jobs[k].d_filtered, d_sub, jobs[k].d_sky, d_t, w, h,
                   frame_pitch(w), n, r, max_frame_fraction, d_out};
-        artefact_kernel<<<static_cast<unsigned>((jobs[k].count + 127) / 128), 128, 0, s>>>(a);
+        artefact_kernel<<<static_cast<unsigned>((jobs[k].count + kArtWarps - 1) / kArtWarps), 32 * kArtWarps, 0, s>>>(a);
         FTB_CHECK(cudaGetLastError());
         ++c.launches;
     }
@@ -579,22 +636,32 @@ void SearchRequest::finish_items(int k0, int k1) {
             Item& it = items_.at(k);
             maps.push_back({it.max.as<float>(), it.bv.as<int>()});
         }
-        const std::vector<std::vector<Peak>> npk = device_peaks_many(c, maps, w, h, 3.0f, nms_, edge_, 20000);
+        // raster-ordered peaks of every map, then per map the screened set and
+        // the rest of the pooled values (no full sort unless a tie needs one)
+        std::vector<std::vector<Peak>> raster = device_peaks_many(c, maps, w, h, 3.0f, nms_, edge_, 0);
+        const size_t tested = (p_.gauss_model && p_.null_tested > 0) ? static_cast<size_t>(p_.null_tested) : 0;
+        std::vector<NullPeaks> np(raster.size());
+        for_each_map(raster.size(), [&](size_t k) { np[k] = split_null_peaks(std::move(raster[k]), 20000, tested); });
         std::vector<ArtefactJob> jobs;
         for (int k = k0; k < kn1; ++k) {
             Item& it = items_.at(k);
-            const std::vector<Peak>& pk = npk[static_cast<size_t>(k - k0)];
-            const size_t tested =
-                (p_.gauss_model && p_.null_tested > 0) ? std::min(pk.size(), static_cast<size_t>(p_.null_tested)) : 0;
-            jobs.push_back({&pk, tested, it.filt.as<float>(), it.sky.as<float>(), &orders_[static_cast<size_t>(k)]});
+            const NullPeaks& q = np[static_cast<size_t>(k - k0)];
+            jobs.push_back({&q.tested, q.tested.size(), it.filt.as<float>(), it.sky.as<float>(),
+                            &orders_[static_cast<size_t>(k)]});
         }
         const std::vector<std::vector<char>> art = device_artefacts_many(c, jobs, o_.grid, sub_.as<float>(), w, h, n,
                                                                          o_.fwhm_px, p_.max_frame_fraction);
+        // pool_null_peaks (search.cpp:690-693): the screened peaks that are not
+        // artefacts, then the rest, in descending S/N as the reference's list
         for (int k = k0; k < kn1; ++k) {
-            const std::vector<Peak>& pk = npk[static_cast<size_t>(k - k0)];
+            const NullPeaks& q = np[static_cast<size_t>(k - k0)];
             const std::vector<char>& a = art[static_cast<size_t>(k - k0)];
-            for (size_t q = 0; q < pk.size(); ++q)
-                if (q >= a.size() || !a[q]) pooled_.push_back(pk[q].snr);
+            std::vector<float> kept;
+            for (size_t e = 0; e < q.tested.size(); ++e)
+                if (!a[e]) kept.push_back(q.tested[e].snr);
+            std::sort(kept.begin(), kept.end(), std::greater<float>());
+            pooled_.insert(pooled_.end(), kept.begin(), kept.end());
+            pooled_.insert(pooled_.end(), q.rest.begin(), q.rest.end());
             items_.erase(k);  // the null run's buffers are released in stream order
         }
     }

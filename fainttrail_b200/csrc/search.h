@@ -112,6 +112,18 @@ struct PeakMap {
 };
 std::vector<std::vector<Peak>> device_peaks_many(Context& c, const std::vector<PeakMap>& maps, int w, int h,
                                                  float floor, int radius, int edge, size_t keep);
+// A null run's peaks as its pooled list needs them (order_peaks with `keep`, then
+// the first `tested` screened for artefacts, search.cpp:766-781): the screened
+// peaks (in any order) and the S/N values of the ranks after them, down to the
+// truncation, in descending order. Equal values are interchangeable in the
+// pooled list, so a full sort is needed only when a tie straddles the screening
+// boundary (then the reference's std::sort decides which peaks are screened).
+struct NullPeaks {
+    std::vector<Peak> tested;
+    std::vector<float> rest;
+};
+NullPeaks split_null_peaks(std::vector<Peak> raster_ordered, size_t keep, size_t tested);
+
 // artefact flags (single-frame share, field edge) of the first count[k] peaks of
 // every null run k at their grid motions (is_artefact_peak, search.cpp:229-243,
 // 142-190), on the device, one sync
