@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <functional>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -491,6 +493,40 @@ int ft_b200_completeness(ft_b200_ctx* ctx, const float* frames, int width, int h
         if (baseline_ok) *baseline_ok = r.baseline_ok;
         if (snr50) *snr50 = r.snr50;
     });
+}
+
+int ft_b200_pool_null_peaks(const ft_b200_peak* raster, int count, const unsigned char* artefact, int keep,
+                            int tested, int mode, float* pooled, int cap) {
+    try {
+        if (count < 0 || (count > 0 && (!raster || !artefact)) || keep < 0 || tested < 0)
+            throw std::runtime_error("pool null peaks: bad arguments");
+        // the flags travel with the peaks (x, y identify a raster peak)
+        std::vector<ftb::Peak> pk(static_cast<size_t>(count));
+        std::map<std::pair<int, int>, unsigned char> flag;
+        for (int q = 0; q < count; ++q) {
+            pk[static_cast<size_t>(q)] = {raster[q].x, raster[q].y, raster[q].snr, raster[q].vidx};
+            flag[{raster[q].x, raster[q].y}] = artefact[q];
+        }
+        std::vector<float> out;
+        if (mode == 0) {
+            ftb::order_peaks(pk, static_cast<size_t>(keep));
+            for (size_t q = 0; q < pk.size(); ++q)
+                if (q >= static_cast<size_t>(tested) || !flag[{pk[q].x, pk[q].y}]) out.push_back(pk[q].snr);
+        } else {
+            const ftb::NullPeaks np = ftb::split_null_peaks(pk, static_cast<size_t>(keep), static_cast<size_t>(tested));
+            std::vector<float> kept;
+            for (const ftb::Peak& p : np.tested)
+                if (!flag[{p.x, p.y}]) kept.push_back(p.snr);
+            std::sort(kept.begin(), kept.end(), std::greater<float>());
+            out = kept;
+            out.insert(out.end(), np.rest.begin(), np.rest.end());
+        }
+        for (size_t q = 0; q < out.size() && static_cast<int>(q) < cap; ++q) pooled[q] = out[q];
+        return static_cast<int>(out.size());
+    } catch (const std::exception& e) {
+        g_open_error = e.what();
+        return -1;
+    }
 }
 
 int ft_b200_null_threshold(const double* pooled, long long count, int runs, double fwhm_px, int width, int height,

@@ -182,6 +182,16 @@ int ft_b200_completeness(ft_b200_ctx* ctx, const float* frames, int width, int h
                          ft_b200_completeness_row* rows, double* threshold_snr, char* method, int method_cap,
                          int* baseline_ok, double* snr50);
 
+/* One null run's pooled S/N list from its raster-ordered peaks (host only):
+ * order_peaks (std::sort by S/N, truncation at `keep`), the first `tested`
+ * screened with the given artefact flags (artefact[q] for raster peak q), then
+ * pool_null_peaks (search.cpp:766-781, 690-693). mode 0: the reference's full
+ * sort; mode 1: the search's path (the screened set by nth_element, the full
+ * sort only for a tie at the screening boundary). Writes up to cap values into
+ * pooled and returns their count. */
+int ft_b200_pool_null_peaks(const ft_b200_peak* raster, int count, const unsigned char* artefact, int keep,
+                            int tested, int mode, float* pooled, int cap);
+
 /* The null-tail threshold from pooled null-peak S/N values (set_threshold,
  * search.cpp:573-612; fit_null_tail_gauss :471-510, gauss_tail_level :517-527):
  * `pooled` is every run's surviving null peaks, run after run, `runs` the number
