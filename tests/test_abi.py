@@ -46,3 +46,29 @@ def test_validate_pass_mirrors_reference():
     ftb.validate_pass(ftb.StackPass(f, t_h=[0, 1, 2], velocities=[(1.0, 0.0)]))
     with pytest.raises(RuntimeError, match="unknown or unavailable"):
         ftb.make_backend("cuda")
+
+
+def test_host_only_entries_without_a_gpu():
+    """Entries that do no device work answer on a machine without a GPU: tile
+    shape selection and its checks, the tuner's (empty) cache, and the argument
+    checks of the null-threshold and pooling entries."""
+    import ctypes as C
+
+    import fainttrail_b200 as ftb
+    L = ftb.lib()
+    assert ftb.tile_shape() == 0
+    for shape in range(0, 8):
+        ftb.set_tile_shape(shape)
+        assert ftb.tile_shape() == shape
+    ftb.set_tile_shape(0)
+    for bad in (-1, 8, 99):
+        with pytest.raises(ValueError, match="tile shape"):
+            ftb.set_tile_shape(bad)
+    assert ftb.tile_shape() == 0
+    ftb.clear_tuned_shapes()
+    assert ftb.tuned_shapes() == {}
+    with pytest.raises(RuntimeError, match="bad sizes"):
+        ftb.null_threshold([5.0, 4.0], 1, 2.5, 0, 10, 100)
+    L.ft_b200_pool_null_peaks.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                          C.c_int]
+    assert L.ft_b200_pool_null_peaks(None, 3, None, 20000, 3000, 0, None, 0) == -1
