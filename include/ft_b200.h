@@ -38,8 +38,9 @@ const char* ft_b200_version(void);
 int ft_b200_open(int device, double hbm_budget_bytes, ft_b200_ctx** out);
 void ft_b200_close(ft_b200_ctx* ctx);
 /* Last error message of the context (ft_last_error, fainttrail.h:106); with a
- * NULL context, the last error of ft_b200_open or ft_b200_stack_dev_noalloc on
- * this thread. */
+ * NULL context, the last error on this thread of the entries that take no
+ * context: ft_b200_open, ft_b200_server_open, ft_b200_stack_dev_noalloc,
+ * ft_b200_set_tile_shape, ft_b200_null_threshold and ft_b200_pool_null_peaks. */
 const char* ft_b200_last_error(const ft_b200_ctx* ctx);
 /* Device name, SM count and memory; replaces SearchBackend::description()
  * (backend.hpp:113). name_len bytes are written to name, NUL-terminated. */
