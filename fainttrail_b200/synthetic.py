@@ -145,11 +145,11 @@ def motion_count(span_h, vmin_pxh, vmax_pxh, grid_tol_px):
     """Trial motions of the square velocity lattice inside the annulus (the
     velocity_grid rule, counted exactly)."""
     dv = 4.0 * max(0.05, grid_tol_px) / span_h
-    k = int(math.ceil((vmax_pxh + 0.5 * dv) / dv))
-    lo, hi = (vmin_pxh - 0.5 * dv) ** 2, (vmax_pxh + 0.5 * dv) ** 2
+    k = int(math.ceil(vmax_pxh / dv))
+    lo, hi = max(0.0, vmin_pxh - 0.5 * dv), vmax_pxh + 0.5 * dv
     i = np.arange(-k, k + 1) * dv
-    r2 = i[:, None] ** 2 + i[None, :] ** 2
-    return int(np.count_nonzero((r2 >= lo) & (r2 <= hi)))
+    v = np.hypot(i[None, :], i[:, None])
+    return int(np.count_nonzero((v >= lo) & (v <= hi)))
 
 
 def serving_requests(count=40, rate_per_s=20.0, seed=2024, max_adds=2.0e12, max_frame_bytes=1 << 30):
