@@ -44,7 +44,22 @@ class SearchParams(C.Structure):
         ("static_exclude", C.c_int), ("null_runs", C.c_int), ("max_candidates", C.c_int), ("edge_px", C.c_int),
         ("threads", C.c_int), ("seed", C.c_ulonglong), ("null_tested", C.c_int), ("null_model_gauss", C.c_int),
         ("passes_per_launch", C.c_int), ("shard_index", C.c_int), ("shard_count", C.c_int),
-        ("calibrated_threshold", C.c_double), ("calibrated_tail", C.c_double * 4)]
+        ("calibrated_threshold", C.c_double), ("calibrated_tail", C.c_double * 4), ("align", C.c_int)]
+
+
+ALIGN_MODES = {"off": 0, "check": 1, "auto": 2}
+
+
+class DriftCheck(C.Structure):
+    """ft_b200_drift_check (DriftCheck, registration.hpp:22-30)."""
+    _fields_ = [("measured", C.c_int), ("registered", C.c_int), ("stars", C.c_int), ("matched", C.c_int)] + [
+        (n, C.c_double) for n in ("dx", "dy", "mid_dx", "mid_dy", "rate_pxh")] + [("message", C.c_char * 1024)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k in ("measured", "registered", "dx", "dy", "mid_dx", "mid_dy", "rate_pxh",
+                                           "stars", "matched")}
+        d["message"] = self.message.decode()
+        return d
 
 
 class Injection(C.Structure):
@@ -101,6 +116,11 @@ def _declare(L):
                                            C.POINTER(SearchParams), C.c_int, C.c_void_p, C.c_void_p,
                                            C.POINTER(C.c_void_p), C.c_void_p]
     L.ft_b200_result_free.argtypes = [C.c_void_p]
+    L.ft_b200_check_registration.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p,
+                                             C.POINTER(DriftCheck)]
+    L.ft_b200_check_registration_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p,
+                                                 C.POINTER(DriftCheck)]
+    L.ft_b200_result_registration.argtypes = [C.c_void_p, C.POINTER(DriftCheck)]
     L.ft_b200_result_candidates.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]
     L.ft_b200_result_threshold.argtypes = [C.c_void_p, C.c_char_p, C.c_int] + [C.POINTER(C.c_double)] * 4
     L.ft_b200_result_threshold.restype = C.c_double
@@ -356,8 +376,32 @@ class Device:
         for k, v in kw.items():
             if k == "calibrated_tail":
                 v = (C.c_double * 4)(*v)
+            elif k == "align" and isinstance(v, str):
+                if v not in ALIGN_MODES:
+                    raise ValueError(f"align must be one of {sorted(ALIGN_MODES)} (this backend does not resample "
+                                     f"frames, so 'always' has no counterpart), not {v!r}")
+                v = ALIGN_MODES[v]
             setattr(p, k, v)
         return p
+
+    def check_registration(self, frames, t_h):
+        """The registration check (ft_b200_check_registration) of frames
+        (n, h, w) observed at t_h hours; returns the DriftCheck as a dict."""
+        frames = np.ascontiguousarray(frames, dtype=np.float32)
+        n, h, w = frames.shape
+        out = DriftCheck()
+        rc = self.L.ft_b200_check_registration(self.h, frames, w, h, n, np.ascontiguousarray(t_h, dtype=np.float64),
+                                               C.byref(out))
+        self.check(rc, "check_registration")
+        return out.as_dict()
+
+    def check_registration_dev(self, d_frames, width, height, pitch, nframes, t_h):
+        """ft_b200_check_registration_dev on a device pointer."""
+        out = DriftCheck()
+        rc = self.L.ft_b200_check_registration_dev(self.h, C.c_void_p(d_frames), width, height, pitch, nframes,
+                                                   np.ascontiguousarray(t_h, dtype=np.float64), C.byref(out))
+        self.check(rc, "check_registration_dev")
+        return out.as_dict()
 
     def search_dev(self, d_frames, width, height, pitch, nframes, mjd, exptime, maps=True, **kw):
         """ft_b200_search_dev on a device pointer; returns the result dict."""
@@ -459,10 +503,12 @@ def _read_result(L, r, w, h, maps):
         fl = C.create_string_buffer(64 * max(nc, 1))
         L.ft_b200_result_candidates(r, rows.ctypes.data_as(C.c_void_p), fl, nc)
         cands = [(rows[q].copy(), fl.raw[64 * q:64 * q + 64].split(b"\0", 1)[0].decode()) for q in range(nc)]
+        reg = DriftCheck()
+        L.ft_b200_result_registration(r, C.byref(reg))
         return dict(threshold=thr, method=meth.value.decode(), null_a=a.value, null_b=b.value, null_k=k.value,
                     null_inv_s2=s2.value, fwhm=fw.value, dv=dv.value, t_ref=tref.value, n_velocities=nv.value,
                     peaks=peaks(0), selected=peaks(1), null_peaks=nulls, max_snr=ms, best_v=bv, grid=grid,
-                    candidates=cands)
+                    candidates=cands, registration=reg.as_dict())
     finally:
         L.ft_b200_result_free(r)
 

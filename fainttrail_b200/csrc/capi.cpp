@@ -12,6 +12,8 @@
 #include <vector>
 
 #include "engine.h"
+#include "ft_internal.h"
+#include "registration.h"
 #include "search.h"
 #include "serve.h"
 #include "stage.h"
@@ -157,6 +159,71 @@ int ft_b200_stack_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int he
     });
 }
 
+namespace {
+void put_drift(const ftb::DriftCheck& d, ft_b200_drift_check* out) {
+    std::memset(out, 0, sizeof *out);
+    out->measured = d.measured ? 1 : 0;
+    out->registered = d.registered ? 1 : 0;
+    out->stars = d.stars;
+    out->matched = d.matched;
+    out->dx = d.dx;
+    out->dy = d.dy;
+    out->mid_dx = d.mid_dx;
+    out->mid_dy = d.mid_dy;
+    out->rate_pxh = d.rate_pxh;
+    std::strncpy(out->message, d.message.c_str(), sizeof out->message - 1);
+}
+}  // namespace
+
+int ft_b200_check_registration(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes,
+                               const double* t_h, ft_b200_drift_check* out) {
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (!frames || !t_h || !out) throw std::runtime_error("registration check: missing frames, times or output");
+        if (nframes < 0 || width < 1 || height < 1) throw std::runtime_error("registration check: empty frames");
+        c.timing_reset();
+        ftb::DriftCheck d;
+        if (nframes >= 3) {  // only the first, middle and last frame by time are read
+            int fi[3];
+            ftb::registration_frames(t_h, nframes, &fi[0], &fi[1], &fi[2]);
+            const int pitch = ftb::frame_pitch(width);
+            const size_t plane = static_cast<size_t>(pitch) * height;
+            ftb::DevBuf buf(&c, sizeof(float) * plane * 3, "registration frames");
+            const float* three[3];
+            for (int k = 0; k < 3; ++k) {
+                float* dst = buf.as<float>() + static_cast<size_t>(k) * plane;
+                FTB_CHECK(cudaMemcpy2DAsync(dst, sizeof(float) * pitch,
+                                            frames + static_cast<size_t>(fi[k]) * width * height, sizeof(float) * width,
+                                            sizeof(float) * width, static_cast<size_t>(height), cudaMemcpyHostToDevice,
+                                            c.stream()));
+                three[k] = dst;
+            }
+            d = ftb::check_registration_three(c, three, pitch, width, height, t_h[fi[2]] - t_h[fi[0]]);
+        }
+        c.timing_resolve();
+        put_drift(d, out);
+    });
+}
+
+int ft_b200_check_registration_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch,
+                                   int nframes, const double* t_h, ft_b200_drift_check* out) {
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (!d_frames || !t_h || !out) throw std::runtime_error("registration check: missing frames, times or output");
+        if (nframes < 0 || width < 1 || height < 1) throw std::runtime_error("registration check: empty frames");
+        if (pitch < width) throw std::runtime_error("registration check: pitch must be >= width");
+        c.timing_reset();
+        const ftb::DriftCheck d = ftb::check_registration_device(c, d_frames, static_cast<size_t>(pitch) * height,
+                                                                 pitch, width, height, nframes, t_h);
+        c.timing_resolve();
+        put_drift(d, out);
+    });
+}
+
+int ft_b200_result_registration(const ft_b200_result* r, ft_b200_drift_check* out) {
+    if (!r || !out) return FT_B200_ERROR;
+    put_drift(r->o.registration, out);
+    return FT_B200_OK;
+}
+
 void ft_b200_stage_params_default(ft_b200_stage_params* p) {
     if (!p) return;
     const ftb::StageParams d;
@@ -215,6 +282,7 @@ void ft_b200_search_params_default(ft_b200_search_params* p) {
     p->passes_per_launch = d.passes_per_launch;
     p->shard_index = d.shard_index;
     p->shard_count = d.shard_count;
+    p->align = d.align;
 }
 
 namespace {
@@ -254,6 +322,8 @@ ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
     if (p.shard_index < 0 || p.shard_index >= p.shard_count)
         throw std::runtime_error("search: shard_index must lie in [0, shard_count)");
     p.seed = q.seed;
+    p.align = q.align;
+    if (p.align < 0 || p.align > 2) throw std::runtime_error("search: align must be 0 (off), 1 (check) or 2 (auto)");
     return p;
 }
 }  // namespace

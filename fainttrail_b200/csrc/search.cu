@@ -490,6 +490,18 @@ void SearchRequest::prepare(const float* frames, const double* mjd, const double
                                     static_cast<size_t>(h), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                     c.stream()));
     c.span_end(up);
+    if (p_.align != 0) {
+        // the registration check of the raw frames (preprocess.cpp:605-630), with
+        // the times from the first frame that prepare_frames gives it
+        std::vector<double> t0(static_cast<size_t>(n));
+        for (int i = 0; i < n; ++i)
+            t0[static_cast<size_t>(i)] = (mjd[order[static_cast<size_t>(i)]] - mjd[order[0]]) * 24.0;
+        o_.registration = check_registration_device(c, raw_.as<float>(), plane_, pitch_, w, h, n, t0.data());
+        if (!o_.registration.registered)
+            throw std::runtime_error(p_.align == 1 ? o_.registration.message
+                                                   : o_.registration.message +
+                                                         " This backend does not align frames: register them first.");
+    }
     if (report) report(0.0, "background");
     if (keep_raw) {
         raw0_ = DevBuf(&c, sizeof(float) * plane_ * n, "raw frames (copies)");

@@ -13,6 +13,7 @@
 
 #include "engine.h"
 #include "stage.h"
+#include "registration.h"
 
 namespace ftb {
 
@@ -32,6 +33,10 @@ struct SearchParams {
     // > 0: the null-run threshold (and its tail fit) is given: no null runs
     double calibrated_threshold = 0.0, cal_a = 0.0, cal_b = 0.0, cal_k = 0.0, cal_inv_s2 = 0.0;
     uint64_t seed = 12345;
+    // registration check before the preprocessing (search.hpp:76-81): 0 off,
+    // 1 check, 2 auto (check; frames that are not registered are an error, as no
+    // alignment is done here)
+    int align = 0;
 };
 
 struct Peak {
@@ -181,6 +186,7 @@ struct SearchOut {
     std::vector<float> max_snr;          // real detection map
     std::vector<int> best_v;
     std::vector<Candidate> candidates;   // refined selected peaks (search.cpp:786-804)
+    DriftCheck registration;             // the registration check, if one ran (search.hpp:122)
     double adds = 0;                     // pixel x frame x motion additions of all passes
 };
 

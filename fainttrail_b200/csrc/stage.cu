@@ -819,4 +819,29 @@ void prepare_sub(Context& c, StageScratch& sc, float* d_raw, float* d_sub, int w
     if (h_bg) FTB_CHECK(cudaMemcpyAsync(h_bg, tb.sg, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
 }
 
+void frame_sample_stats(Context& c, const float* const* d_frames, int k, int w, int h, int pitch, float* d_samples,
+                        int cap, int* d_counts, double* d_stats) {
+    cudaStream_t s = c.stream();
+    FTB_CHECK(cudaMemsetAsync(d_counts, 0, sizeof(int) * k, s));
+    const int st = grid_step(w, h, 0, 200000);
+    if (st > 0) {
+        const int gw = grid_count(0, w, st), gh = grid_count(0, h, st);
+        const long long g = static_cast<long long>(gw) * gh;
+        if (g > cap) throw std::runtime_error("frame_sample_stats: sample buffer too small");
+        for (int i = 0; i < k; ++i) {
+            sample_kernel<<<dim3(static_cast<unsigned>((g + 255) / 256), 1), 256, 0, s>>>(
+                d_frames[i], 0, w, h, pitch, 1, 0, st, gw, gh, nullptr, d_samples + static_cast<size_t>(i) * cap, cap,
+                d_counts + i);
+            FTB_CHECK(cudaGetLastError());
+            ++c.launches;
+        }
+    }
+    median_cluster_kernel<<<k * kSelCluster, 256, 0, s>>>(d_samples, cap, d_counts, d_stats);
+    FTB_CHECK(cudaGetLastError());
+    ++c.launches;
+    robust_sigma_cluster_kernel<<<k * kSelCluster, 256, 0, s>>>(d_samples, cap, d_counts, d_stats + k, 0);
+    FTB_CHECK(cudaGetLastError());
+    ++c.launches;
+}
+
 }  // namespace ftb

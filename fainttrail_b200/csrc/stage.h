@@ -46,4 +46,12 @@ void stage_sigma_to_host(Context& c, StageScratch& sc, int n, double* h_sigma);
 void stage_run(Context& c, StageScratch& sc, const float* d_sub, int w, int h, int n, const double* t_h,
                const StageParams& sp, float* d_filtered, float* d_sky, float* d_mask, double* h_sigma, int* h_cr);
 
+// Median and robust sigma (common.hpp:64-82) of the regular sample of each of k
+// device frames (sample_pixels(frame, 200000), common.hpp:85-100; w x h, rows
+// `pitch` floats apart): d_stats[i] the median, d_stats[k + i] the robust sigma
+// (0 for fewer than 3 samples), d_counts[i] the number of samples. d_samples
+// holds k * cap floats, cap >= sample_grid_points(w, h, 0).
+void frame_sample_stats(Context& c, const float* const* d_frames, int k, int w, int h, int pitch, float* d_samples,
+                        int cap, int* d_counts, double* d_stats);
+
 }  // namespace ftb

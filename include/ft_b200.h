@@ -150,6 +150,15 @@ typedef struct ft_b200_search_params {
                               candidates, as the unsplit search gives them */
     double calibrated_tail[4];   /* a, b, k, inv_s2 of that threshold's null-tail fit
                               (the candidates' false-alarm rates) */
+    int align;            /* SearchParams::align (search.hpp:76-81, prepare_frames
+                              preprocess.cpp:589-630): 0 "off" (default here): the
+                              frames are taken as registered; 1 "check": the
+                              registration check runs first (ft_b200_check_registration)
+                              and frames that are not registered are an error with the
+                              reference's message; 2 "auto": the same check, and frames
+                              that are not registered are an error (the reference would
+                              align them; this backend does not resample frames).
+                              The check's outcome: ft_b200_result_registration. */
 } ft_b200_search_params;
 
 void ft_b200_search_params_default(ft_b200_search_params* p);
@@ -274,6 +283,37 @@ int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap);
 int ft_b200_result_maps(const ft_b200_result* r, float* max_snr, int* best_v);
 /* The trial motion vidx of the grid (velocity_grid, search.cpp:39-58), px/hour. */
 int ft_b200_result_velocity(const ft_b200_result* r, int vidx, double* vx_pxh, double* vy_pxh);
+
+/* The registration check of a frame sequence (DriftCheck, registration.hpp:22-30;
+ * check_registration, registration.cpp:260-312): stars (bright, extended local
+ * maxima) are found in the first, middle and last frame by time, the last and the
+ * middle frame's are matched to the first's by an offset vote and a similarity
+ * fit, and the sequence is registered when neither moves any point of the frame
+ * by more than 1.5 px. Fewer than 3 frames, or too few stars to match: not
+ * measured, and registered. */
+typedef struct ft_b200_drift_check {
+    int measured;          /* enough stars matched to tell */
+    int registered;        /* 1 when not measured */
+    int stars;             /* stars used in the first frame (at most 60) */
+    int matched;           /* stars matched between the first and the last frame */
+    double dx, dy;         /* displacement of the field centre, first -> last frame, px */
+    double mid_dx, mid_dy; /* the same, first -> middle frame */
+    double rate_pxh;       /* |(dx, dy)| / time between the first and the last frame */
+    char message[1024];    /* why the frames are not registered ("" when they are) */
+} ft_b200_drift_check;
+
+/* The check on host frames (nframes x height x width floats, NaN = blank)
+ * observed at t_h[nframes] hours (any order; the reference passes
+ * (mjd_mid - mjd_mid of the first frame) * 24). Only the three frames the check
+ * uses are copied to the device. */
+int ft_b200_check_registration(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes,
+                               const double* t_h, ft_b200_drift_check* out);
+/* The same on device frames (frame i at d_frames + i * pitch * height, pitch >= width). */
+int ft_b200_check_registration_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch,
+                                   int nframes, const double* t_h, ft_b200_drift_check* out);
+/* The registration check a search ran (align 1 or 2); not measured and
+ * registered when it ran none. */
+int ft_b200_result_registration(const ft_b200_result* r, ft_b200_drift_check* out);
 
 /* Stack kernel tile shape for every later pass in this process: 0 = automatic
  * (the default: the autotuned choice where one is cached for the pass's frame

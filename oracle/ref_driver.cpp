@@ -463,4 +463,28 @@ void ftref_inject(float* frames, int n, int w, int h, const double* mjd, const d
     for (int i = 0; i < n; ++i) std::memcpy(frames + i * plane, fr[static_cast<std::size_t>(i)].image.data.data(), plane * sizeof(float));
 }
 
+// check_registration (registration.cpp:260-312) of n frames (n x h x w) observed
+// at t_h hours: out[0..8] = measured, registered, dx, dy, mid_dx, mid_dy,
+// rate_pxh, stars, matched; the message into msg (NUL-terminated).
+int ftref_check_registration(const float* frames, int n, int w, int h, const double* t_h, double* out, char* msg,
+                             int msg_len) {
+    try {
+        const std::vector<Image> ims = images_from(frames, n, w, h);
+        std::vector<const Image*> ptrs;
+        for (const auto& im : ims) ptrs.push_back(&im);
+        const DriftCheck r = check_registration(ptrs, std::vector<double>(t_h, t_h + n));
+        const double v[9] = {r.measured ? 1.0 : 0.0, r.registered ? 1.0 : 0.0, r.dx, r.dy, r.mid_dx, r.mid_dy,
+                             r.rate_pxh, static_cast<double>(r.stars), static_cast<double>(r.matched)};
+        std::memcpy(out, v, sizeof v);
+        if (msg && msg_len > 0) {
+            std::strncpy(msg, r.message.c_str(), static_cast<std::size_t>(msg_len) - 1);
+            msg[msg_len - 1] = 0;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 }  // extern "C"

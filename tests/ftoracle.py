@@ -213,6 +213,7 @@ class Reference:
         L.ftref_with_times.restype = C.c_void_p
         L.ftref_search.argtypes = [C.c_void_p, C.POINTER(FtParams)]
         L.ftref_search.restype = C.c_void_p
+        L.ftref_check_registration.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_char_p, C.c_int]
         L.ftref_result_free.argtypes = [C.c_void_p]
         L.ftref_result_scalars.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double)] + \
             [C.POINTER(C.c_int)] * 3 + [C.POINTER(C.c_double)] * 3
@@ -364,6 +365,28 @@ class Reference:
         self.L.ftref_inject(frames, n, w, h, _f64(mjd), _f64(exptime), _f64(obj.ravel()), obj.shape[0], t_ref_mjd,
                             fwhm_px)
         return frames
+
+    def check_registration(self, frames, t_h):
+        """check_registration of frames (n, h, w) at t_h hours, as a dict."""
+        frames = _f32(frames)
+        n, h, w = frames.shape
+        out = np.zeros(9)
+        msg = C.create_string_buffer(1024)
+        if self.L.ftref_check_registration(frames, n, w, h, _f64(t_h), out, msg, 1024) != 0:
+            raise RuntimeError(self.L.ftref_last_error().decode())
+        return drift_dict(out, msg.value.decode())
+
+
+DRIFT_KEYS = ("measured", "registered", "dx", "dy", "mid_dx", "mid_dy", "rate_pxh", "stars", "matched")
+
+
+def drift_dict(values, message):
+    """A DriftCheck as a dict: flags and counts as ints, offsets as floats."""
+    d = {k: float(v) for k, v in zip(DRIFT_KEYS, values)}
+    for k in ("measured", "registered", "stars", "matched"):
+        d[k] = int(d[k])
+    d["message"] = message
+    return d
 
 
 class Prepared:

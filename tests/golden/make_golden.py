@@ -115,6 +115,59 @@ def null_runs_case(R):
                 n_velocities=np.int32(full["n_velocities"]))
 
 
+def _shifted(frames, sx, sy):
+    """frames[i] moved by (sx[i], sy[i]) whole pixels; uncovered pixels NaN."""
+    out = np.full_like(frames, np.nan)
+    n, h, w = frames.shape
+    for i in range(n):
+        dx, dy = int(sx[i]), int(sy[i])
+        ys, yd = (slice(0, h - dy), slice(dy, h)) if dy >= 0 else (slice(-dy, h), slice(0, h + dy))
+        xs, xd = (slice(0, w - dx), slice(dx, w)) if dx >= 0 else (slice(-dx, w), slice(0, w + dx))
+        out[i, yd, xd] = frames[i, ys, xs]
+    return out
+
+
+def registration_case(R):
+    """check_registration on simulated sequences (128 x 96, 12 frames, whole ADU):
+    registered; drifting by whole pixels; flipped by 180 degrees after the
+    meridian from frame 6 on; drifting with blank columns and a blank patch on
+    the brightest star; too few stars to tell. Only the first, middle and last
+    frame by time take part in the check, so those three (as uint16, NaN where
+    the mask says) and their times are stored with the reference's verdict on
+    the whole sequence; the verdict on the three alone is asserted equal."""
+    out = {}
+    names = ["registered", "drift", "flip", "blank", "few"]
+    for k, name in enumerate(names):
+        frames, mjd, _ = R.simulate(width=128, height=96, nframes=12, nstars=3 if name == "few" else 400,
+                                    nmovers=1, hot_pixels=8, cosmic_rays_per_frame=2.0, seed=31 + k)
+        frames = np.round(frames).astype(np.float32)
+        n = frames.shape[0]
+        if name in ("drift", "blank"):
+            frames = _shifted(frames, np.round(np.arange(n) * 0.45), np.round(np.arange(n) * -0.3))
+        if name == "flip":
+            frames[6:] = frames[6:, ::-1, ::-1]
+        if name == "blank":
+            frames[:, :, :5] = np.nan
+            y, x = np.unravel_index(np.nanargmax(frames[0]), frames[0].shape)
+            frames[0, max(0, y - 1):y + 2, max(0, x - 1):x + 2] = np.nan
+        t = (mjd - mjd[0]) * 24.0
+        full = R.check_registration(frames, t)
+        pick = [0, n // 2, n - 1]  # times ascend and are distinct
+        three = np.ascontiguousarray(frames[pick])
+        alone = R.check_registration(three, t[pick])
+        assert alone == full, name
+        nan = np.isnan(three)
+        assert np.all(three[~nan] >= 0) and np.all(three[~nan] <= 65535), "whole ADU must fit uint16"
+        out[name + "_frames"] = np.where(nan, 0, three).astype(np.uint16)
+        out[name + "_nan"] = np.packbits(nan)
+        out[name + "_t"] = t[pick]
+        out[name + "_values"] = np.array([full[k] for k in ("measured", "registered", "dx", "dy", "mid_dx",
+                                                             "mid_dy", "rate_pxh", "stars", "matched")], np.float64)
+        out[name + "_message"] = np.array(full["message"])
+    out["names"] = np.array(names)
+    return out
+
+
 CASES = {
     "stack_contract": lambda R: contract_case(R, False, 4242),
     "stack_constant": lambda R: contract_case(R, True, 4242),
@@ -122,6 +175,7 @@ CASES = {
     "stage_small": stage_case,
     "search_small": search_case,
     "null_runs_small": null_runs_case,
+    "registration_small": registration_case,
 }
 
 
