@@ -72,3 +72,19 @@ def test_host_only_entries_without_a_gpu():
     L.ft_b200_pool_null_peaks.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                           C.c_int]
     assert L.ft_b200_pool_null_peaks(None, 3, None, 20000, 3000, 0, None, 0) == -1
+
+
+def test_registration_entries_check_their_arguments():
+    """The registration entries refuse a missing context or result, and the
+    drift-check struct has the C layout (4 ints, 5 doubles, a 1024-byte message)."""
+    import ctypes as C
+
+    import fainttrail_b200 as ftb
+    L = ftb.lib()
+    out = ftb.DriftCheck()
+    assert C.sizeof(ftb.DriftCheck) == 4 * 4 + 5 * 8 + 1024
+    f = np.zeros((3, 16, 16), np.float32)
+    t = np.arange(3, dtype=np.float64)
+    assert L.ft_b200_check_registration(None, f, 16, 16, 3, t, C.byref(out)) == ftb.FT_B200_ERROR
+    assert L.ft_b200_check_registration_dev(None, None, 16, 16, 16, 3, t, C.byref(out)) == ftb.FT_B200_ERROR
+    assert L.ft_b200_result_registration(None, C.byref(out)) == ftb.FT_B200_ERROR
