@@ -121,6 +121,9 @@ def _declare(L):
     L.ft_b200_check_registration_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p,
                                                  C.POINTER(DriftCheck)]
     L.ft_b200_result_registration.argtypes = [C.c_void_p, C.POINTER(DriftCheck)]
+    L.ft_b200_result_candidates_csv.argtypes = [C.c_void_p, C.c_char_p, C.c_longlong]
+    L.ft_b200_result_candidates_csv.restype = C.c_longlong
+    L.ft_b200_write_candidates_csv.argtypes = [C.c_void_p, C.c_char_p]
     L.ft_b200_result_candidates.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]
     L.ft_b200_result_threshold.argtypes = [C.c_void_p, C.c_char_p, C.c_int] + [C.POINTER(C.c_double)] * 4
     L.ft_b200_result_threshold.restype = C.c_double
@@ -413,8 +416,10 @@ class Device:
         self.check(rc, "search_dev")
         return self._result(r, width, height, maps)
 
-    def search(self, frames, mjd, exptime, progress=None, maps=True, **kw):
-        """A whole search (ft_b200_search) from raw frames; returns a dict."""
+    def search(self, frames, mjd, exptime, progress=None, maps=True, csv_path=None, **kw):
+        """A whole search (ft_b200_search) from raw frames; returns a dict. With
+        csv_path, the candidate file is also written there
+        (ft_b200_write_candidates_csv)."""
         frames = np.ascontiguousarray(frames, dtype=np.float32)
         n, h, w = frames.shape
         p = self._search_params(self.L, kw)
@@ -423,7 +428,7 @@ class Device:
                                    np.ascontiguousarray(exptime, dtype=np.float64), C.byref(p), _progress(progress),
                                    None, C.byref(r))
         self.check(rc, "search")
-        return self._result(r, w, h, maps)
+        return self._result(r, w, h, maps, csv_path)
 
     def search_batch(self, frames, mjd, exptime, copies, progress=None, maps=True, **kw):
         """ft_b200_search_batch: the search plus injection copies. `copies` is a
@@ -460,8 +465,8 @@ class Device:
         res = self._result(base, width, height, maps)
         return res, [self._result(C.c_void_p(outs[k]), width, height, maps) for k in range(len(copies))]
 
-    def _result(self, r, w, h, maps):
-        return _read_result(self.L, r, w, h, maps)
+    def _result(self, r, w, h, maps, csv_path=None):
+        return _read_result(self.L, r, w, h, maps, csv_path)
 
     def info(self):
         name = C.create_string_buffer(256)
@@ -470,9 +475,12 @@ class Device:
         return name.value.decode(), sms.value, mem.value
 
 
-def _read_result(L, r, w, h, maps):
-    """The getters of an ft_b200_result (freed here) as a dict."""
+def _read_result(L, r, w, h, maps, csv_path=None):
+    """The getters of an ft_b200_result (freed here) as a dict; with csv_path,
+    the candidate file is written there first."""
     try:
+        if csv_path is not None and L.ft_b200_write_candidates_csv(r, os.fsencode(csv_path)) != FT_B200_OK:
+            raise RuntimeError(L.ft_b200_last_error(None).decode())
         meth = C.create_string_buffer(32)
         a, b, k, s2 = C.c_double(), C.c_double(), C.c_double(), C.c_double()
         thr = L.ft_b200_result_threshold(r, meth, 32, C.byref(a), C.byref(b), C.byref(k), C.byref(s2))
@@ -505,10 +513,13 @@ def _read_result(L, r, w, h, maps):
         cands = [(rows[q].copy(), fl.raw[64 * q:64 * q + 64].split(b"\0", 1)[0].decode()) for q in range(nc)]
         reg = DriftCheck()
         L.ft_b200_result_registration(r, C.byref(reg))
+        size = L.ft_b200_result_candidates_csv(r, None, 0)
+        text = C.create_string_buffer(size + 1)
+        L.ft_b200_result_candidates_csv(r, text, size + 1)
         return dict(threshold=thr, method=meth.value.decode(), null_a=a.value, null_b=b.value, null_k=k.value,
                     null_inv_s2=s2.value, fwhm=fw.value, dv=dv.value, t_ref=tref.value, n_velocities=nv.value,
                     peaks=peaks(0), selected=peaks(1), null_peaks=nulls, max_snr=ms, best_v=bv, grid=grid,
-                    candidates=cands, registration=reg.as_dict())
+                    candidates=cands, registration=reg.as_dict(), candidates_csv=text.value.decode())
     finally:
         L.ft_b200_result_free(r)
 

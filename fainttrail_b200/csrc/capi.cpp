@@ -3,6 +3,7 @@
 #include "ft_b200.h"
 
 #include <cmath>
+#include <cstdio>
 #include <cstdint>
 #include <cstring>
 #include <functional>
@@ -11,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "candidate.h"
 #include "engine.h"
 #include "ft_internal.h"
 #include "registration.h"
@@ -160,7 +162,7 @@ int ft_b200_stack_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int he
 }
 
 namespace {
-void put_drift(const ftb::DriftCheck& d, ft_b200_drift_check* out) {
+static void put_drift(const ftb::DriftCheck& d, ft_b200_drift_check* out) {
     std::memset(out, 0, sizeof *out);
     out->measured = d.measured ? 1 : 0;
     out->registered = d.registered ? 1 : 0;
@@ -286,7 +288,7 @@ void ft_b200_search_params_default(ft_b200_search_params* p) {
 }
 
 namespace {
-ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
+static ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
     ft_b200_search_params d;
     ft_b200_search_params_default(&d);
     const ft_b200_search_params& q = params ? *params : d;
@@ -342,11 +344,11 @@ int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height,
 }
 
 namespace {
-int search_batch_common(ft_b200_ctx* ctx, const float* frames, bool on_device, int pitch, int width, int height,
-                        int nframes, const double* mjd, const double* exptime, const ft_b200_search_params* params,
-                        int copies, const int* objects_per_copy, const ft_b200_injection* objects,
-                        ft_b200_progress_fn progress, void* user, ft_b200_result** base,
-                        ft_b200_result** copy_results) {
+static int search_batch_common(ft_b200_ctx* ctx, const float* frames, bool on_device, int pitch, int width, int height,
+                               int nframes, const double* mjd, const double* exptime, const ft_b200_search_params* params,
+                               int copies, const int* objects_per_copy, const ft_b200_injection* objects,
+                               ft_b200_progress_fn progress, void* user, ft_b200_result** base,
+                               ft_b200_result** copy_results) {
     if (base) *base = nullptr;
     for (int k = 0; copy_results && k < copies; ++k) copy_results[k] = nullptr;
     return guarded(ctx, [&](ftb::Context& c) {
@@ -652,6 +654,49 @@ int ft_b200_result_candidates(const ft_b200_result* r, double* rows, char* flags
         }
     }
     return static_cast<int>(v.size());
+}
+
+namespace {
+static std::string result_csv(const ft_b200_result* r) {
+    ftb::CandidateListInfo info;
+    info.t_ref_mjd = r->o.t_ref_mjd;
+    info.threshold_snr = r->o.thr.snr;
+    info.method = r->o.thr.method;
+    info.dv_pxh = r->o.dv;
+    info.fwhm_px = r->o.fwhm_px;
+    info.n_velocities = static_cast<long long>(r->o.grid.size());
+    return ftb::candidates_csv(info, r->o.candidates);
+}
+}  // namespace
+
+long long ft_b200_result_candidates_csv(const ft_b200_result* r, char* buf, long long cap) {
+    if (!r) return -1;
+    const std::string text = result_csv(r);
+    if (buf && cap > 0) {
+        const size_t k = std::min(text.size(), static_cast<size_t>(cap - 1));
+        std::memcpy(buf, text.data(), k);
+        buf[k] = 0;
+    }
+    return static_cast<long long>(text.size());
+}
+
+int ft_b200_write_candidates_csv(const ft_b200_result* r, const char* path) {
+    if (!r || !path) {
+        g_open_error = "write_candidates_csv: missing result or path";
+        return FT_B200_ERROR;
+    }
+    const std::string text = result_csv(r);
+    std::FILE* f = std::fopen(path, "wb");
+    if (!f) {
+        g_open_error = std::string("cannot write ") + path;
+        return FT_B200_ERROR;
+    }
+    const bool written = std::fwrite(text.data(), 1, text.size(), f) == text.size();
+    if (std::fclose(f) != 0 || !written) {
+        g_open_error = std::string("cannot write ") + path;
+        return FT_B200_ERROR;
+    }
+    return FT_B200_OK;
 }
 
 int ft_b200_result_maps(const ft_b200_result* r, float* max_snr, int* best_v) {

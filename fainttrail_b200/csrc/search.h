@@ -13,6 +13,7 @@
 
 #include "engine.h"
 #include "stage.h"
+#include "candidate.h"
 #include "registration.h"
 
 namespace ftb {
@@ -161,18 +162,6 @@ InjectionPatches injection_patches(const std::vector<Injection>& objects, const 
                                    const std::vector<double>& exptime_s, double fwhm_px, int w, int h);
 // Adds the patches to device frames (n x h x pitch) in order.
 void apply_patches(Context& c, const InjectionPatches& ip, float* d_frames, int w, int h, int n);
-
-// One whole search from raw frames (ft_search's prepare + search, without the
-// candidate refinement).
-// A refined candidate (Candidate, search.hpp:131-154) without sky coordinates.
-struct Candidate {
-    int id = 0;
-    double x = 0, y = 0, vx_pxh = 0, vy_pxh = 0, pos_err_px = 0, vel_err_pxh = 0;
-    double snr = 0, snr_coarse = 0, snr_half1 = 0, snr_half2 = 0, max_frame_fraction = 0;
-    double false_alarms_per_run = 0, flux = 0, mag_inst = 0, inv_dist_au = 0;
-    bool ok = false;
-    std::string flags;
-};
 
 struct SearchOut {
     int w = 0, h = 0, n = 0;

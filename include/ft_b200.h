@@ -40,7 +40,8 @@ void ft_b200_close(ft_b200_ctx* ctx);
 /* Last error message of the context (ft_last_error, fainttrail.h:106); with a
  * NULL context, the last error on this thread of the entries that take no
  * context: ft_b200_open, ft_b200_server_open, ft_b200_stack_dev_noalloc,
- * ft_b200_set_tile_shape, ft_b200_null_threshold and ft_b200_pool_null_peaks. */
+ * ft_b200_set_tile_shape, ft_b200_null_threshold, ft_b200_pool_null_peaks and
+ * ft_b200_write_candidates_csv. */
 const char* ft_b200_last_error(const ft_b200_ctx* ctx);
 /* Device name, SM count and memory; replaces SearchBackend::description()
  * (backend.hpp:113). name_len bytes are written to name, NUL-terminated. */
@@ -279,6 +280,16 @@ int ft_b200_result_info(const ft_b200_result* r, double* fwhm_px, double* dv_pxh
 int ft_b200_result_peaks(const ft_b200_result* r, int which, ft_b200_peak* out, int cap);
 /* The pooled null-peak S/N values (SearchResult::null_peaks). Returns the count. */
 int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap);
+/* The candidate file of the search (write_candidates_csv, io.cpp:82-115), byte
+ * for byte as the reference writes it for frames without a WCS, photometric
+ * calibration or near-Earth distances: two comment lines (reference epoch,
+ * threshold, motion grid, PSF width), the column names, and one line per
+ * candidate with ra_deg, dec_deg, rate_arcsec_min and pa_deg 0 and empty mag,
+ * mag_err and mag_band. ft_b200_write_candidates_csv writes it to path (error
+ * text in ft_b200_last_error(NULL)); ft_b200_result_candidates_csv copies it to
+ * buf (at most cap - 1 bytes and a NUL) and returns its length, or -1. */
+int ft_b200_write_candidates_csv(const ft_b200_result* r, const char* path);
+long long ft_b200_result_candidates_csv(const ft_b200_result* r, char* buf, long long cap);
 /* The real run's detection map: max_snr and best_v, height x width each. */
 int ft_b200_result_maps(const ft_b200_result* r, float* max_snr, int* best_v);
 /* The trial motion vidx of the grid (velocity_grid, search.cpp:39-58), px/hour. */

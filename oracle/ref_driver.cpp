@@ -13,6 +13,8 @@
 
 #include "fainttrail/backend.hpp"
 #include "fainttrail/fainttrail.h"
+#include "fainttrail/fits.hpp"
+#include "fainttrail/io.hpp"
 #include "fainttrail/search.hpp"
 #include "fainttrail/simulate.hpp"
 #include "fainttrail/validate.hpp"
@@ -399,6 +401,29 @@ void ftref_result_candidate(void* rp, int k, double* out, char* flags_out) {
     std::memcpy(out, v, sizeof v);
     std::strncpy(flags_out, c.flags.c_str(), 63);
     flags_out[63] = 0;
+}
+
+// The reference epoch and PSF width of a result, and its candidate file
+// (write_candidates_csv, io.cpp:82-115) written to path (NULL: not written).
+int ftref_result_csv(void* rp, const char* path, double* t_ref_mjd, double* fwhm_px) {
+    const SearchResult& r = static_cast<Result*>(rp)->r;
+    *t_ref_mjd = r.t_ref_mjd;
+    *fwhm_px = r.fwhm_px;
+    if (!path) return 0;
+    try {
+        write_candidates_csv(path, r);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+// iso_from_mjd (fits.cpp:474-504) into out (cap bytes, NUL-terminated).
+void ftref_iso_from_mjd(double mjd, int decimals, char* out, int cap) {
+    const std::string s = iso_from_mjd(mjd, decimals);
+    std::strncpy(out, s.c_str(), static_cast<std::size_t>(cap) - 1);
+    out[cap - 1] = 0;
 }
 
 // completeness() on raw frames: rows of 7 doubles per level (target_snr,

@@ -214,6 +214,8 @@ class Reference:
         L.ftref_search.argtypes = [C.c_void_p, C.POINTER(FtParams)]
         L.ftref_search.restype = C.c_void_p
         L.ftref_check_registration.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_char_p, C.c_int]
+        L.ftref_result_csv.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ftref_iso_from_mjd.argtypes = [C.c_double, C.c_int, C.c_char_p, C.c_int]
         L.ftref_result_free.argtypes = [C.c_void_p]
         L.ftref_result_scalars.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double)] + \
             [C.POINTER(C.c_int)] * 3 + [C.POINTER(C.c_double)] * 3
@@ -366,6 +368,11 @@ class Reference:
                             fwhm_px)
         return frames
 
+    def iso_from_mjd(self, mjd, decimals):
+        buf = C.create_string_buffer(96)
+        self.L.ftref_iso_from_mjd(mjd, decimals, buf, 96)
+        return buf.value.decode()
+
     def check_registration(self, frames, t_h):
         """check_registration of frames (n, h, w) at t_h hours, as a dict."""
         frames = _f32(frames)
@@ -432,12 +439,19 @@ class Prepared:
             raise RuntimeError(self.ref.err())
         return Prepared(self.ref, hp)
 
-    def search(self, **kw):
+    def search(self, csv_path=None, **kw):
+        """search() of the prepared sequence; with csv_path, the reference's
+        candidate file is written there and returned as candidates_csv."""
         p = self.ref.params(**kw)
         rp = self.ref.L.ftref_search(self.hp, C.byref(p))
         if not rp:
             raise RuntimeError(self.ref.err())
         L = self.ref.L
+        t_ref, fwhm = C.c_double(), C.c_double()
+        if L.ftref_result_csv(rp, csv_path.encode() if csv_path else None, C.byref(t_ref), C.byref(fwhm)) != 0:
+            L.ftref_result_free(rp)
+            raise RuntimeError(self.ref.err())
+        csv_text = open(csv_path).read() if csv_path else None
         meth = C.create_string_buffer(32)
         dv, a, k, s2 = C.c_double(), C.c_double(), C.c_double(), C.c_double()
         nv, nc, npk = C.c_int(), C.c_int(), C.c_int()
@@ -455,4 +469,4 @@ class Prepared:
         L.ftref_result_free(rp)
         return dict(threshold=thr, method=meth.value.decode(), dv=dv.value, n_velocities=nv.value,
                     null_peaks=nulls, max_snr=ms, candidates=cands, null_a=a.value, null_k=k.value,
-                    null_inv_s2=s2.value)
+                    null_inv_s2=s2.value, t_ref_mjd=t_ref.value, fwhm=fwhm.value, candidates_csv=csv_text)

@@ -8,6 +8,7 @@ that read them run anywhere.
 
     make -C oracle ref && python tests/golden/make_golden.py
 """
+import json
 import os
 import sys
 
@@ -168,6 +169,40 @@ def registration_case(R):
     return out
 
 
+CSV_CASES = {
+    # name: (simulate arguments, search parameters)
+    "null": (dict(width=96, height=80, nframes=12, nstars=60, nmovers=6, seed=21), dict(fwhm_px=2.5, null_runs=2)),
+    "fixed": (dict(width=96, height=80, nframes=12, nstars=60, nmovers=4, seed=9),
+              dict(fwhm_px=2.5, threshold_snr=3.5)),
+}
+
+
+def candidates_csv_case(R):
+    """The reference's candidate file (write_candidates_csv, io.cpp:82-115) of two
+    searches: a sequence with six movers and two null runs (candidates with
+    false-alarm rates from the null-tail fit), and a sequence with four movers at
+    a fixed threshold of S/N 3.5 (more candidates, rejected ones among them). Stored per case: the file's text and the result fields it is
+    written from (epoch, threshold, grid, PSF width, the candidates' 17 values and
+    flags), and the simulate() and search arguments (JSON), with which the
+    reference's simulate() makes the frames again."""
+    import tempfile
+    out = {"names": np.array(list(CSV_CASES))}
+    for name, (sim, kw) in CSV_CASES.items():
+        frames, mjd, exp = R.simulate(**sim)
+        prep = R.prepare(frames, mjd, exp, **kw)
+        with tempfile.TemporaryDirectory() as tmp:
+            res = prep.search(csv_path=os.path.join(tmp, "candidates.csv"), backend="cpu", **kw)
+        rows = np.array([c[0] for c in res["candidates"]]).reshape(-1, 17)
+        out[name + "_csv"] = np.array(res["candidates_csv"])
+        out[name + "_rows"] = rows
+        out[name + "_flags"] = np.array([c[1] for c in res["candidates"]] or [""])[:len(res["candidates"])]
+        out[name + "_info"] = np.array([res["t_ref_mjd"], res["threshold"], res["dv"], res["fwhm"],
+                                        res["n_velocities"]], np.float64)
+        out[name + "_method"] = np.array(res["method"])
+        out[name + "_setup"] = np.array(json.dumps({"simulate": sim, "search": kw}))
+    return out
+
+
 CASES = {
     "stack_contract": lambda R: contract_case(R, False, 4242),
     "stack_constant": lambda R: contract_case(R, True, 4242),
@@ -176,6 +211,7 @@ CASES = {
     "search_small": search_case,
     "null_runs_small": null_runs_case,
     "registration_small": registration_case,
+    "candidates_csv_small": candidates_csv_case,
 }
 
 

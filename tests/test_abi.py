@@ -88,3 +88,18 @@ def test_registration_entries_check_their_arguments():
     assert L.ft_b200_check_registration(None, f, 16, 16, 3, t, C.byref(out)) == ftb.FT_B200_ERROR
     assert L.ft_b200_check_registration_dev(None, None, 16, 16, 16, 3, t, C.byref(out)) == ftb.FT_B200_ERROR
     assert L.ft_b200_result_registration(None, C.byref(out)) == ftb.FT_B200_ERROR
+
+
+def test_only_the_declared_entries_have_c_names():
+    """Internal helpers of the C ABI layer keep internal linkage: every exported
+    unmangled symbol is one of the ft_b200_ entries the header declares."""
+    import shutil
+    import subprocess
+
+    nm = shutil.which("nm")
+    if not nm:
+        pytest.skip("no nm")
+    out = subprocess.run([nm, "-D", "--defined-only", ftb.LIB_PATH], capture_output=True, text=True, check=True)
+    names = [line.split()[-1] for line in out.stdout.splitlines() if line.split()[1] in ("T", "D", "B")]
+    c_names = {n for n in names if not n.startswith("_Z")}
+    assert c_names <= set(ftb.exported_symbols()), sorted(c_names - set(ftb.exported_symbols()))
