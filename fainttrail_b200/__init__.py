@@ -134,6 +134,8 @@ def _declare(L):
     L.ft_b200_result_velocity.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.ft_b200_stage.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, C.POINTER(StageParams),
                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.ft_b200_stage_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p,
+                                    C.POINTER(StageParams)] + [C.c_void_p] * 5
 
 
 def _declare_server(L):
@@ -365,6 +367,25 @@ class Device:
                                   ptr(filt), ptr(sky), ptr(mask), ptr(sigma), ptr(cr))
         self.check(rc, "stage")
         return dict(filtered=filt, static_sky=sky, mask=mask, sigma=sigma, cr=cr)
+
+    def stage_dev(self, d_sub, width, height, pitch, nframes, t_h, fwhm_px, d_filtered=None, d_static_sky=None,
+                  d_mask=None, **kw):
+        """build_stage on device frames (ft_b200_stage_dev): d_sub and the
+        outputs are device pointers with rows `pitch` floats apart (outputs may be
+        None). Returns dict(sigma, cr)."""
+        p = StageParams()
+        self.L.ft_b200_stage_params_default(C.byref(p))
+        p.fwhm_px = fwhm_px
+        for k, v in kw.items():
+            setattr(p, k, v)
+        sigma = np.empty(nframes, np.float64)
+        cr = np.empty(nframes, np.int32)
+        rc = self.L.ft_b200_stage_dev(self.h, C.c_void_p(d_sub), width, height, pitch, nframes,
+                                      np.ascontiguousarray(t_h, dtype=np.float64), C.byref(p),
+                                      C.c_void_p(d_filtered), C.c_void_p(d_static_sky), C.c_void_p(d_mask),
+                                      sigma.ctypes.data_as(C.c_void_p), cr.ctypes.data_as(C.c_void_p))
+        self.check(rc, "stage_dev")
+        return dict(sigma=sigma, cr=cr)
 
     def launches(self):
         """Kernels launched by the last call (ft_b200_stats)."""

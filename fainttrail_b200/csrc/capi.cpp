@@ -226,6 +226,26 @@ int ft_b200_result_registration(const ft_b200_result* r, ft_b200_drift_check* ou
     return FT_B200_OK;
 }
 
+int ft_b200_stage_dev(ft_b200_ctx* ctx, const float* d_sub, int width, int height, int pitch, int nframes,
+                      const double* t_h, const ft_b200_stage_params* params, float* d_filtered,
+                      float* d_static_sky, float* d_mask, double* sigma, int* cr_pixels) {
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (!d_sub || !t_h || !params) throw std::runtime_error("stage: missing frames, times or parameters");
+        if (nframes < 1 || width < 1 || height < 1) throw std::runtime_error("stage: empty frames");
+        if (pitch < width) throw std::runtime_error("stage: pitch must be >= width");
+        if (!(params->fwhm_px > 0.0)) throw std::runtime_error("stage: the PSF FWHM must be positive");
+        ftb::StageParams sp;
+        sp.fwhm_px = params->fwhm_px;
+        sp.static_exclude = params->static_exclude;
+        sp.clip_sigma = params->clip_sigma;
+        sp.cr_sigma = params->cr_sigma;
+        sp.mask_scatter = params->mask_scatter;
+        sp.weight_scatter = params->weight_scatter;
+        ftb::stage_device(c, d_sub, pitch, width, height, nframes, t_h, sp, d_filtered, d_static_sky, d_mask, sigma,
+                          cr_pixels);
+    });
+}
+
 void ft_b200_stage_params_default(ft_b200_stage_params* p) {
     if (!p) return;
     const ftb::StageParams d;

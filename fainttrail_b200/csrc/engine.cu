@@ -282,11 +282,19 @@ void stack_pass_host(Context& c, const float* frames, int w, int h, int n, const
 
 // ------------------------------------------------------------------ stage
 
-void stage_host(Context& c, const float* sub, int w, int h, int n, const double* t_h, const StageParams& sp,
-                float* filtered, float* static_sky, float* mask, double* sigma, int* cr) {
+namespace {
+
+// build_stage with the caller's frames and outputs in host memory (io_pitch =
+// w) or device memory (rows io_pitch floats apart), copied to and from the
+// stage's own layout around the device stage.
+void stage_io(Context& c, const float* sub, bool on_device, int io_pitch, int w, int h, int n, const double* t_h,
+              const StageParams& sp, float* filtered, float* static_sky, float* mask, double* sigma, int* cr) {
     c.bind();
     const int pitch = frame_pitch(w);
     const size_t plane = static_cast<size_t>(pitch) * h;
+    const cudaMemcpyKind in_kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out_kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const size_t io_row = sizeof(float) * static_cast<size_t>(io_pitch);
     c.timing_reset();
     float* d_sub = c.scratch(kFrames, sizeof(float) * plane * n, "frames").as<float>();
     float* d_filt = c.scratch(kStageOut, sizeof(float) * plane * n, "filtered frames").as<float>();
@@ -294,27 +302,40 @@ void stage_host(Context& c, const float* sub, int w, int h, int n, const double*
     float* d_mask = c.scratch(kMask, sizeof(float) * plane, "mask").as<float>();
     StageScratch sc(c, w, h, n, sp.fwhm_px);
     const int up = c.span_begin("upload");
-    FTB_CHECK(cudaMemcpy2DAsync(d_sub, sizeof(float) * pitch, sub, sizeof(float) * w, sizeof(float) * w,
-                                static_cast<size_t>(h) * n, cudaMemcpyHostToDevice, c.stream()));
+    FTB_CHECK(cudaMemcpy2DAsync(d_sub, sizeof(float) * pitch, sub, io_row, sizeof(float) * w,
+                                static_cast<size_t>(h) * n, in_kind, c.stream()));
     c.span_end(up);
     std::vector<double> sg(static_cast<size_t>(n));
     std::vector<int> crv(static_cast<size_t>(n));
     stage_run(c, sc, d_sub, w, h, n, t_h, sp, d_filt, d_sky, d_mask, sg.data(), crv.data());
     const int down = c.span_begin("download");
     if (filtered)
-        FTB_CHECK(cudaMemcpy2DAsync(filtered, sizeof(float) * w, d_filt, sizeof(float) * pitch, sizeof(float) * w,
-                                    static_cast<size_t>(h) * n, cudaMemcpyDeviceToHost, c.stream()));
+        FTB_CHECK(cudaMemcpy2DAsync(filtered, io_row, d_filt, sizeof(float) * pitch, sizeof(float) * w,
+                                    static_cast<size_t>(h) * n, out_kind, c.stream()));
     if (static_sky)
-        FTB_CHECK(cudaMemcpy2DAsync(static_sky, sizeof(float) * w, d_sky, sizeof(float) * pitch, sizeof(float) * w,
-                                    static_cast<size_t>(h), cudaMemcpyDeviceToHost, c.stream()));
+        FTB_CHECK(cudaMemcpy2DAsync(static_sky, io_row, d_sky, sizeof(float) * pitch, sizeof(float) * w,
+                                    static_cast<size_t>(h), out_kind, c.stream()));
     if (mask)
-        FTB_CHECK(cudaMemcpy2DAsync(mask, sizeof(float) * w, d_mask, sizeof(float) * pitch, sizeof(float) * w,
-                                    static_cast<size_t>(h), cudaMemcpyDeviceToHost, c.stream()));
+        FTB_CHECK(cudaMemcpy2DAsync(mask, io_row, d_mask, sizeof(float) * pitch, sizeof(float) * w,
+                                    static_cast<size_t>(h), out_kind, c.stream()));
     c.span_end(down);
     FTB_CHECK(cudaStreamSynchronize(c.stream()));
     c.timing_resolve();
     if (sigma) std::copy(sg.begin(), sg.end(), sigma);
     if (cr) std::copy(crv.begin(), crv.end(), cr);
+}
+
+}  // namespace
+
+void stage_host(Context& c, const float* sub, int w, int h, int n, const double* t_h, const StageParams& sp,
+                float* filtered, float* static_sky, float* mask, double* sigma, int* cr) {
+    stage_io(c, sub, false, w, w, h, n, t_h, sp, filtered, static_sky, mask, sigma, cr);
+}
+
+void stage_device(Context& c, const float* d_sub, int pitch, int w, int h, int n, const double* t_h,
+                  const StageParams& sp, float* d_filtered, float* d_static_sky, float* d_mask, double* sigma,
+                  int* cr) {
+    stage_io(c, d_sub, true, pitch, w, h, n, t_h, sp, d_filtered, d_static_sky, d_mask, sigma, cr);
 }
 
 // ------------------------------------------------------------------ tile-shape autotuner

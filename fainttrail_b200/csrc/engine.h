@@ -157,5 +157,10 @@ struct StageParams;
 // build_stage over host buffers (the C ABI's ft_b200_stage).
 void stage_host(Context& c, const float* sub, int w, int h, int n, const double* t_h, const StageParams& sp,
                 float* filtered, float* static_sky, float* mask, double* sigma, int* cr);
+// The same over device buffers whose rows are `pitch` floats apart
+// (ft_b200_stage_dev); sigma and cr are host arrays.
+void stage_device(Context& c, const float* d_sub, int pitch, int w, int h, int n, const double* t_h,
+                  const StageParams& sp, float* d_filtered, float* d_static_sky, float* d_mask, double* sigma,
+                  int* cr);
 
 }  // namespace ftb

@@ -120,6 +120,14 @@ void ft_b200_stage_params_default(ft_b200_stage_params* p);
 int ft_b200_stage(ft_b200_ctx* ctx, const float* sub, int width, int height, int nframes, const double* t_h,
                   const ft_b200_stage_params* params, float* filtered, float* static_sky, float* mask, double* sigma,
                   int* cr_pixels);
+/* The same for frames kept in HBM: d_sub is nframes x height rows of `pitch`
+ * floats (pitch >= width) on the device, read only; d_filtered (the same
+ * layout), d_static_sky and d_mask (height rows of `pitch` floats) are device
+ * outputs, sigma and cr_pixels host arrays; any output may be NULL. Returns when
+ * the outputs are complete. */
+int ft_b200_stage_dev(ft_b200_ctx* ctx, const float* d_sub, int width, int height, int pitch, int nframes,
+                      const double* t_h, const ft_b200_stage_params* params, float* d_filtered,
+                      float* d_static_sky, float* d_mask, double* sigma, int* cr_pixels);
 
 /* Parameters of a search: ft_params (fainttrail.h:32-54) plus the null-model
  * fields of SearchParams (search.hpp:58-68). Defaults: ft_b200_search_params_default,

@@ -92,3 +92,27 @@ def test_noise_normalisation(device, reference):
         v = flt[i][keep].astype(np.float64)
         mean, sd = v.mean(), v.std()
         assert abs(mean) < 0.1 and 0.9 < sd < 1.15
+
+
+def test_device_frames_with_row_pitch(device):
+    """ft_b200_stage_dev on frames in HBM with an odd row pitch: the golden
+    outputs, written into the caller's layout; NULL outputs are skipped."""
+    import torch
+    g = golden("stage_small.npz")
+    sub = np.ascontiguousarray(g["sub"], np.float32)
+    n, h, w = sub.shape
+    pitch = w + 5
+    d_sub = torch.full((n, h, pitch), 7.0, dtype=torch.float32, device="cuda")
+    d_sub[:, :, :w] = torch.from_numpy(sub).cuda()
+    d_filt = torch.full((n, h, pitch), -3.0, dtype=torch.float32, device="cuda")
+    d_sky = torch.full((h, pitch), -3.0, dtype=torch.float32, device="cuda")
+    d_mask = torch.full((h, pitch), -3.0, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    got = device.stage_dev(d_sub.data_ptr(), w, h, pitch, n, g["t_h"], float(g["fwhm"]), d_filt.data_ptr(),
+                           d_sky.data_ptr(), d_mask.data_ptr())
+    got.update(filtered=d_filt[:, :, :w].cpu().numpy(), static_sky=d_sky[:, :w].cpu().numpy(),
+               mask=d_mask[:, :w].cpu().numpy())
+    check(got, g)
+    assert torch.all(d_filt[:, :, w:] == -3.0) and torch.all(d_sky[:, w:] == -3.0)  # padding untouched
+    only = device.stage_dev(d_sub.data_ptr(), w, h, pitch, n, g["t_h"], float(g["fwhm"]))
+    assert same(only["sigma"], g["sigma"]) and same(only["cr"], g["cr"])
