@@ -50,6 +50,14 @@ class SearchParams(C.Structure):
 ALIGN_MODES = {"off": 0, "check": 1, "auto": 2}
 
 
+class CandidateRecord(C.Structure):
+    """ft_b200_candidate (ft_candidate, fainttrail.h:55-68)."""
+    _fields_ = [("id", C.c_int), ("ok", C.c_int)] + [(n, C.c_double) for n in (
+        "x", "y", "vx_pxh", "vy_pxh", "pos_err_px", "vel_err_pxh", "snr", "snr_coarse", "snr_half1", "snr_half2",
+        "max_frame_fraction", "false_alarms_per_run", "flux", "mag_inst", "ra_deg", "dec_deg", "rate_arcsec_min",
+        "pa_deg")] + [("flags", C.c_char * 64)]
+
+
 class DriftCheck(C.Structure):
     """ft_b200_drift_check (DriftCheck, registration.hpp:22-30)."""
     _fields_ = [("measured", C.c_int), ("registered", C.c_int), ("stars", C.c_int), ("matched", C.c_int)] + [
@@ -124,6 +132,8 @@ def _declare(L):
     L.ft_b200_result_candidates_csv.argtypes = [C.c_void_p, C.c_char_p, C.c_longlong]
     L.ft_b200_result_candidates_csv.restype = C.c_longlong
     L.ft_b200_write_candidates_csv.argtypes = [C.c_void_p, C.c_char_p]
+    L.ft_b200_result_candidate.argtypes = [C.c_void_p, C.c_int, C.POINTER(CandidateRecord)]
+    L.ft_b200_result_track_point.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.POINTER(C.c_double)] * 5
     L.ft_b200_result_candidates.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]
     L.ft_b200_result_threshold.argtypes = [C.c_void_p, C.c_char_p, C.c_int] + [C.POINTER(C.c_double)] * 4
     L.ft_b200_result_threshold.restype = C.c_double
@@ -534,13 +544,23 @@ def _read_result(L, r, w, h, maps, csv_path=None):
         cands = [(rows[q].copy(), fl.raw[64 * q:64 * q + 64].split(b"\0", 1)[0].decode()) for q in range(nc)]
         reg = DriftCheck()
         L.ft_b200_result_registration(r, C.byref(reg))
+        pt = [C.c_double() for _ in range(5)]
+        tracks = []
+        for q in range(nc):  # every frame of every candidate (ft_get_track_point)
+            f, rows_q = 0, []
+            while L.ft_b200_result_track_point(r, q, f, *[C.byref(v) for v in pt]) == FT_B200_OK:
+                rows_q.append([v.value for v in pt])
+                f += 1
+            tracks.append(rows_q)
+        track_points = np.array(tracks, np.float64).reshape(nc, -1, 5) if nc else np.zeros((0, 0, 5))
         size = L.ft_b200_result_candidates_csv(r, None, 0)
         text = C.create_string_buffer(size + 1)
         L.ft_b200_result_candidates_csv(r, text, size + 1)
         return dict(threshold=thr, method=meth.value.decode(), null_a=a.value, null_b=b.value, null_k=k.value,
                     null_inv_s2=s2.value, fwhm=fw.value, dv=dv.value, t_ref=tref.value, n_velocities=nv.value,
                     peaks=peaks(0), selected=peaks(1), null_peaks=nulls, max_snr=ms, best_v=bv, grid=grid,
-                    candidates=cands, registration=reg.as_dict(), candidates_csv=text.value.decode())
+                    candidates=cands, registration=reg.as_dict(), candidates_csv=text.value.decode(),
+                    track_points=track_points)
     finally:
         L.ft_b200_result_free(r)
 

@@ -18,6 +18,23 @@ struct Candidate {
     std::string flags;
 };
 
+// Where a candidate is predicted in a frame observed t_h hours after the
+// reference epoch, as ft_get_track_point reports it (c_api.cpp:248-261,
+// track_points search.cpp:893-905, track_pos internal.hpp:107-116): the
+// frame's MJD and the FITS 1-based position of the straight track.
+struct TrackPoint {
+    double mjd, x, y;
+};
+
+inline TrackPoint track_point(double t_ref_mjd, double t_h, const Candidate& c) {
+    TrackPoint p;
+    p.mjd = t_ref_mjd + t_h / 24.0;
+    const double x = c.x + c.vx_pxh * t_h, y = c.y + c.vy_pxh * t_h;
+    p.x = x + 1.0;
+    p.y = y + 1.0;
+    return p;
+}
+
 // The search-level values the candidate file's header line carries.
 struct CandidateListInfo {
     double t_ref_mjd = 0.0, threshold_snr = 0.0, dv_pxh = 0.0, fwhm_px = 0.0;

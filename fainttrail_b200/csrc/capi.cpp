@@ -689,6 +689,45 @@ static std::string result_csv(const ft_b200_result* r) {
 }
 }  // namespace
 
+int ft_b200_result_candidate(const ft_b200_result* r, int index, ft_b200_candidate* out) {
+    if (!r || !out || index < 0 || index >= static_cast<int>(r->o.candidates.size())) return FT_B200_ERROR;
+    const ftb::Candidate& c = r->o.candidates[static_cast<size_t>(index)];
+    std::memset(out, 0, sizeof *out);
+    out->id = c.id;
+    out->ok = c.ok ? 1 : 0;
+    out->x = c.x + 1.0;
+    out->y = c.y + 1.0;
+    out->vx_pxh = c.vx_pxh;
+    out->vy_pxh = c.vy_pxh;
+    out->pos_err_px = c.pos_err_px;
+    out->vel_err_pxh = c.vel_err_pxh;
+    out->snr = c.snr;
+    out->snr_coarse = c.snr_coarse;
+    out->snr_half1 = c.snr_half1;
+    out->snr_half2 = c.snr_half2;
+    out->max_frame_fraction = c.max_frame_fraction;
+    out->false_alarms_per_run = c.false_alarms_per_run;
+    out->flux = c.flux;
+    out->mag_inst = c.mag_inst;
+    std::strncpy(out->flags, c.flags.c_str(), sizeof out->flags - 1);
+    return FT_B200_OK;
+}
+
+int ft_b200_result_track_point(const ft_b200_result* r, int index, int frame, double* mjd, double* x, double* y,
+                               double* ra_deg, double* dec_deg) {
+    if (!r || index < 0 || index >= static_cast<int>(r->o.candidates.size()) || frame < 0 ||
+        frame >= static_cast<int>(r->o.t_h.size()))
+        return FT_B200_ERROR;
+    const ftb::TrackPoint p = ftb::track_point(r->o.t_ref_mjd, r->o.t_h[static_cast<size_t>(frame)],
+                                               r->o.candidates[static_cast<size_t>(index)]);
+    if (mjd) *mjd = p.mjd;
+    if (x) *x = p.x;
+    if (y) *y = p.y;
+    if (ra_deg) *ra_deg = 0.0;
+    if (dec_deg) *dec_deg = 0.0;
+    return FT_B200_OK;
+}
+
 long long ft_b200_result_candidates_csv(const ft_b200_result* r, char* buf, long long cap) {
     if (!r) return -1;
     const std::string text = result_csv(r);

@@ -288,6 +288,30 @@ int ft_b200_result_info(const ft_b200_result* r, double* fwhm_px, double* dv_pxh
 int ft_b200_result_peaks(const ft_b200_result* r, int which, ft_b200_peak* out, int cap);
 /* The pooled null-peak S/N values (SearchResult::null_peaks). Returns the count. */
 int ft_b200_result_null_peaks(const ft_b200_result* r, double* out, int cap);
+/* One candidate as ft_get_candidate reports it (ft_candidate, fainttrail.h:55-68;
+ * c_api.cpp:218-246), field for field: FITS 1-based x and y, ra_deg, dec_deg,
+ * rate_arcsec_min and pa_deg 0 (no WCS). */
+typedef struct ft_b200_candidate {
+    int id;
+    int ok;
+    double x, y;
+    double vx_pxh, vy_pxh;
+    double pos_err_px, vel_err_pxh;
+    double snr, snr_coarse, snr_half1, snr_half2;
+    double max_frame_fraction;
+    double false_alarms_per_run;
+    double flux, mag_inst;
+    double ra_deg, dec_deg;
+    double rate_arcsec_min, pa_deg;
+    char flags[64];
+} ft_b200_candidate;
+int ft_b200_result_candidate(const ft_b200_result* r, int index, ft_b200_candidate* out);
+/* Predicted position of candidate `index` in frame `frame` (0-based, in time
+ * order), as ft_get_track_point (fainttrail.h:102-104, c_api.cpp:248-261): the
+ * frame's mid-exposure MJD and the FITS 1-based position on the straight track;
+ * ra_deg and dec_deg 0 (no WCS). Any output may be NULL. */
+int ft_b200_result_track_point(const ft_b200_result* r, int index, int frame, double* mjd, double* x, double* y,
+                               double* ra_deg, double* dec_deg);
 /* The candidate file of the search (write_candidates_csv, io.cpp:82-115), byte
  * for byte as the reference writes it for frames without a WCS, photometric
  * calibration or near-Earth distances: two comment lines (reference epoch,

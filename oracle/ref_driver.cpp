@@ -419,6 +419,19 @@ int ftref_result_csv(void* rp, const char* path, double* t_ref_mjd, double* fwhm
     }
 }
 
+// ft_get_track_point (c_api.cpp:248-261) of candidate k in frame i of a result
+// of the prepared sequence hp: out = mjd, x, y (FITS 1-based), ra, dec.
+int ftref_track_point(void* hp, void* rp, int k, int frame, double* out) {
+    const Prepared& p = *static_cast<Prepared*>(hp);
+    const SearchResult& r = static_cast<Result*>(rp)->r;
+    if (k < 0 || k >= static_cast<int>(r.candidates.size()) || frame < 0 || frame >= p.nframes) return 1;
+    const auto pts = track_points(p, r.candidates[static_cast<std::size_t>(k)]);
+    const TrackPoint& q = pts[static_cast<std::size_t>(frame)];
+    const double v[5] = {q.mjd, q.x + 1.0, q.y + 1.0, q.ra_deg, q.dec_deg};
+    std::memcpy(out, v, sizeof v);
+    return 0;
+}
+
 // iso_from_mjd (fits.cpp:474-504) into out (cap bytes, NUL-terminated).
 void ftref_iso_from_mjd(double mjd, int decimals, char* out, int cap) {
     const std::string s = iso_from_mjd(mjd, decimals);

@@ -53,6 +53,28 @@ extern "C" long long ftb_host_candidates_csv(const double* info, const char* met
     return static_cast<long long>(text.size());
 }
 
+// track_point of every candidate (rows as above) in every frame (t_h[n]):
+// out[(k * n + i) * 5 ..] = mjd, x, y (FITS 1-based), ra 0, dec 0.
+extern "C" void ftb_host_track_points(double t_ref_mjd, const double* t_h, int n, const double* rows, int nc,
+                                      double* out) {
+    for (int k = 0; k < nc; ++k) {
+        ftb::Candidate c;
+        c.x = rows[17 * k];
+        c.y = rows[17 * k + 1];
+        c.vx_pxh = rows[17 * k + 2];
+        c.vy_pxh = rows[17 * k + 3];
+        for (int i = 0; i < n; ++i) {
+            const ftb::TrackPoint p = ftb::track_point(t_ref_mjd, t_h[i], c);
+            double* o = out + (static_cast<size_t>(k) * n + i) * 5;
+            o[0] = p.mjd;
+            o[1] = p.x;
+            o[2] = p.y;
+            o[3] = 0.0;
+            o[4] = 0.0;
+        }
+    }
+}
+
 // iso_utc_from_mjd for the date checks.
 extern "C" void ftb_host_iso_utc(double mjd, int decimals, char* out, int cap) {
     const std::string s = ftb::iso_utc_from_mjd(mjd, decimals);

@@ -216,6 +216,7 @@ class Reference:
         L.ftref_check_registration.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_char_p, C.c_int]
         L.ftref_result_csv.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.ftref_iso_from_mjd.argtypes = [C.c_double, C.c_int, C.c_char_p, C.c_int]
+        L.ftref_track_point.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, _f64p]
         L.ftref_result_free.argtypes = [C.c_void_p]
         L.ftref_result_scalars.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double)] + \
             [C.POINTER(C.c_int)] * 3 + [C.POINTER(C.c_double)] * 3
@@ -466,7 +467,12 @@ class Prepared:
             fl = C.create_string_buffer(64)
             L.ftref_result_candidate(rp, i, v, fl)
             cands.append((v, fl.value.decode()))
+        tracks = np.zeros((nc.value, self.n, 5))
+        for i in range(nc.value):
+            for f in range(self.n):
+                L.ftref_track_point(self.hp, rp, i, f, tracks[i, f])
         L.ftref_result_free(rp)
         return dict(threshold=thr, method=meth.value.decode(), dv=dv.value, n_velocities=nv.value,
                     null_peaks=nulls, max_snr=ms, candidates=cands, null_a=a.value, null_k=k.value,
-                    null_inv_s2=s2.value, t_ref_mjd=t_ref.value, fwhm=fwhm.value, candidates_csv=csv_text)
+                    null_inv_s2=s2.value, t_ref_mjd=t_ref.value, fwhm=fwhm.value, candidates_csv=csv_text,
+                    track_points=tracks)

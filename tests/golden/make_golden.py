@@ -183,8 +183,9 @@ def candidates_csv_case(R):
     false-alarm rates from the null-tail fit), and a sequence with four movers at
     a fixed threshold of S/N 3.5 (more candidates, rejected ones among them). Stored per case: the file's text and the result fields it is
     written from (epoch, threshold, grid, PSF width, the candidates' 17 values and
-    flags), and the simulate() and search arguments (JSON), with which the
-    reference's simulate() makes the frames again."""
+    flags), the frame times and every candidate's track points in every frame
+    (ft_get_track_point), and the simulate() and search arguments (JSON), with
+    which the reference's simulate() makes the frames again."""
     import tempfile
     out = {"names": np.array(list(CSV_CASES))}
     for name, (sim, kw) in CSV_CASES.items():
@@ -200,6 +201,8 @@ def candidates_csv_case(R):
                                         res["n_velocities"]], np.float64)
         out[name + "_method"] = np.array(res["method"])
         out[name + "_setup"] = np.array(json.dumps({"simulate": sim, "search": kw}))
+        out[name + "_t_h"] = prep.vectors()["t_h"]
+        out[name + "_tracks"] = res["track_points"]
     return out
 
 

@@ -103,3 +103,17 @@ def test_only_the_declared_entries_have_c_names():
     names = [line.split()[-1] for line in out.stdout.splitlines() if line.split()[1] in ("T", "D", "B")]
     c_names = {n for n in names if not n.startswith("_Z")}
     assert c_names <= set(ftb.exported_symbols()), sorted(c_names - set(ftb.exported_symbols()))
+
+
+def test_candidate_record_layout_and_checks():
+    """ft_b200_candidate has ft_candidate's layout (2 ints, 18 doubles, 64 flag
+    bytes); the candidate and track-point getters refuse a missing result."""
+    import ctypes as C
+
+    import fainttrail_b200 as ftb
+    assert C.sizeof(ftb.CandidateRecord) == 2 * 4 + 18 * 8 + 64
+    L = ftb.lib()
+    rec = ftb.CandidateRecord()
+    assert L.ft_b200_result_candidate(None, 0, C.byref(rec)) == ftb.FT_B200_ERROR
+    d = C.c_double()
+    assert L.ft_b200_result_track_point(None, 0, 0, *[C.byref(d)] * 5) == ftb.FT_B200_ERROR

@@ -2,7 +2,8 @@
 writer, built for the host from the product source
 (tests/candidates_csv_check.cpp), turns the reference's result fields into the
 reference's text byte for byte; its dates equal iso_from_mjd (fits.cpp:474-504)
-across day carries, leap years and eras. The device search's file is compared
+across day carries, leap years and eras; the track points equal the reference's
+ft_get_track_point values. The device search's file is compared
 in test_candidates_csv_gpu.py."""
 import ctypes as C
 import os
@@ -39,6 +40,7 @@ def writer(tmp_path_factory):
     L.ftb_host_candidates_csv.argtypes = [f64, C.c_char_p, f64, C.c_char_p, C.c_int, C.c_char_p, C.c_longlong]
     L.ftb_host_candidates_csv.restype = C.c_longlong
     L.ftb_host_iso_utc.argtypes = [C.c_double, C.c_int, C.c_char_p, C.c_int]
+    L.ftb_host_track_points.argtypes = [C.c_double, f64, C.c_int, f64, C.c_int, f64]
     return L
 
 
@@ -86,3 +88,15 @@ def test_dates_match_reference(writer):
         for dec in (0, 1, 2, 3):
             writer.ftb_host_iso_utc(mjd, dec, buf, 96)
             assert buf.value.decode() == R.iso_from_mjd(mjd, dec), (mjd, dec)
+
+
+@pytest.mark.parametrize("case", range(2))
+def test_track_points_match_reference(writer, case):
+    g = golden("candidates_csv_small.npz")
+    name = csv_cases()[case][0]
+    info, rows, t_h, want = g[name + "_info"], g[name + "_rows"], g[name + "_t_h"], g[name + "_tracks"]
+    nc, n = rows.shape[0], t_h.size
+    assert want.shape == (nc, n, 5) and nc > 0
+    out = np.zeros((nc, n, 5))
+    writer.ftb_host_track_points(float(info[0]), np.ascontiguousarray(t_h), n, np.ascontiguousarray(rows), nc, out)
+    assert np.array_equal(out, want)

@@ -1,7 +1,9 @@
 """The candidate file of a device search (ft_b200_result_candidates_csv,
 ft_b200_write_candidates_csv) is the reference's write_candidates_csv
-(io.cpp:82-115) text byte for byte: on the golden cases (the frames made again
-by the reference's simulate()), and against the live reference's file."""
+(io.cpp:82-115) text byte for byte, and its track points
+(ft_b200_result_track_point) are the reference's ft_get_track_point values: on
+the golden cases (the frames made again by the reference's simulate()), and
+against the live reference."""
 import json
 
 import numpy as np
@@ -26,6 +28,7 @@ def test_search_file_matches_golden(device, reference, case, tmp_path):
     got = device.search(frames, mjd, exp, csv_path=path, **setup["search"])
     assert got["candidates_csv"] == want
     assert path.read_text() == want
+    assert np.array_equal(got["track_points"], golden("candidates_csv_small.npz")[name + "_tracks"])
 
 
 def test_search_file_matches_live_reference(device, reference, tmp_path):
@@ -38,6 +41,7 @@ def test_search_file_matches_live_reference(device, reference, tmp_path):
     got = device.search(frames, mjd, exp, **kw)
     assert len(ref["candidates"]) > 0
     assert got["candidates_csv"] == ref["candidates_csv"]
+    assert np.array_equal(got["track_points"], ref["track_points"])
 
 
 def test_unwritable_path_is_an_error(device, tmp_path):
