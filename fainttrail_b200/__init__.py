@@ -70,6 +70,17 @@ class DriftCheck(C.Structure):
         return d
 
 
+def _set_fields(struct, kw, what):
+    """Set the named fields of a parameter struct; an unknown name is an error
+    (ctypes would otherwise keep it as a plain attribute and ignore it)."""
+    names = {f[0] for f in struct._fields_}
+    unknown = sorted(set(kw) - names)
+    if unknown:
+        raise TypeError(f"unknown {what} parameter(s) {unknown}; known: {sorted(names)}")
+    for k, v in kw.items():
+        setattr(struct, k, v)
+
+
 class Injection(C.Structure):
     """ft_b200_injection (Injection, validate.hpp:18-23)."""
     _fields_ = [(n, C.c_double) for n in ("x_ref", "y_ref", "vx_pxh", "vy_pxh", "flux")]
@@ -365,8 +376,7 @@ class Device:
         p = StageParams()
         self.L.ft_b200_stage_params_default(C.byref(p))
         p.fwhm_px = fwhm_px
-        for k, v in kw.items():
-            setattr(p, k, v)
+        _set_fields(p, kw, "stage")
         filt = np.empty_like(sub)
         sky = np.empty((h, w), np.float32)
         mask = np.empty((h, w), np.float32)
@@ -386,8 +396,7 @@ class Device:
         p = StageParams()
         self.L.ft_b200_stage_params_default(C.byref(p))
         p.fwhm_px = fwhm_px
-        for k, v in kw.items():
-            setattr(p, k, v)
+        _set_fields(p, kw, "stage")
         sigma = np.empty(nframes, np.float64)
         cr = np.empty(nframes, np.int32)
         rc = self.L.ft_b200_stage_dev(self.h, C.c_void_p(d_sub), width, height, pitch, nframes,
@@ -407,15 +416,15 @@ class Device:
     def _search_params(L, kw):
         p = SearchParams()
         L.ft_b200_search_params_default(C.byref(p))
-        for k, v in kw.items():
-            if k == "calibrated_tail":
-                v = (C.c_double * 4)(*v)
-            elif k == "align" and isinstance(v, str):
-                if v not in ALIGN_MODES:
-                    raise ValueError(f"align must be one of {sorted(ALIGN_MODES)} (this backend does not resample "
-                                     f"frames, so 'always' has no counterpart), not {v!r}")
-                v = ALIGN_MODES[v]
-            setattr(p, k, v)
+        kw = dict(kw)
+        if "calibrated_tail" in kw:
+            kw["calibrated_tail"] = (C.c_double * 4)(*kw["calibrated_tail"])
+        if isinstance(kw.get("align"), str):
+            if kw["align"] not in ALIGN_MODES:
+                raise ValueError(f"align must be one of {sorted(ALIGN_MODES)} (this backend does not resample "
+                                 f"frames, so 'always' has no counterpart), not {kw['align']!r}")
+            kw["align"] = ALIGN_MODES[kw["align"]]
+        _set_fields(p, kw, "search")
         return p
 
     def check_registration(self, frames, t_h):

@@ -117,3 +117,15 @@ def test_candidate_record_layout_and_checks():
     assert L.ft_b200_result_candidate(None, 0, C.byref(rec)) == ftb.FT_B200_ERROR
     d = C.c_double()
     assert L.ft_b200_result_track_point(None, 0, 0, *[C.byref(d)] * 5) == ftb.FT_B200_ERROR
+
+
+def test_unknown_parameters_are_errors():
+    """A misspelt search or stage parameter is refused, not silently ignored."""
+    import fainttrail_b200 as ftb
+    L = ftb.lib()
+    with pytest.raises(TypeError, match="nul_runs"):
+        ftb.Device._search_params(L, {"nul_runs": 3})
+    p = ftb.Device._search_params(L, {"null_runs": 5, "calibrated_tail": (1.0, 2.0, 3.0, 4.0), "align": "check"})
+    assert p.null_runs == 5 and list(p.calibrated_tail) == [1.0, 2.0, 3.0, 4.0] and p.align == 1
+    with pytest.raises(TypeError, match="clip"):
+        ftb._set_fields(ftb.StageParams(), {"clip": 3.0}, "stage")
