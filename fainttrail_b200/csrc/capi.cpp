@@ -87,9 +87,9 @@ int ft_b200_open(int device, double hbm_budget_bytes, ft_b200_ctx** out) {
     if (!out) return FT_B200_ERROR;
     *out = nullptr;
     try {
-        auto* h = new ft_b200_ctx;
+        auto h = std::make_unique<ft_b200_ctx>();
         h->c = std::make_unique<ftb::Context>(device, hbm_budget_bytes);
-        *out = h;
+        *out = h.release();
         return FT_B200_OK;
     } catch (const std::exception& e) {
         g_open_error = e.what();
