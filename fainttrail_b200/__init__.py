@@ -457,7 +457,10 @@ class Device:
         return self._result(r, width, height, maps)
 
     def search(self, frames, mjd, exptime, progress=None, maps=True, csv_path=None, **kw):
-        """A whole search (ft_b200_search) from raw frames; returns a dict. With
+        """A whole search (ft_b200_search) from raw frames; returns a dict
+        (threshold and tail fit, peaks, maps, null peaks, candidates with their
+        track points, the candidate file's text, the registration check). kw are
+        ft_b200_search_params fields (align: "off", "check" or "auto"). With
         csv_path, the candidate file is also written there
         (ft_b200_write_candidates_csv)."""
         frames = np.ascontiguousarray(frames, dtype=np.float32)
