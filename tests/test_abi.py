@@ -1,10 +1,13 @@
 """The C-ABI library loads and exports every entry point include/ft_b200.h
 declares; host-side argument checks. No GPU needed."""
 import ctypes as C
+import os
+
 import numpy as np
 import pytest
 
 import fainttrail_b200 as ftb
+from conftest import ROOT
 
 
 def test_library_exports_every_declared_symbol():
@@ -129,3 +132,39 @@ def test_unknown_parameters_are_errors():
     assert p.null_runs == 5 and list(p.calibrated_tail) == [1.0, 2.0, 3.0, 4.0] and p.align == 1
     with pytest.raises(TypeError, match="clip"):
         ftb._set_fields(ftb.StageParams(), {"clip": 3.0}, "stage")
+
+
+C_PROGRAM = r"""
+#include <stdio.h>
+#include "ft_b200.h"
+int main(void) {
+    ft_b200_search_params q;
+    ft_b200_stage_params s;
+    ft_b200_ctx* ctx = 0;
+    ft_b200_search_params_default(&q);
+    ft_b200_stage_params_default(&s);
+    printf("%s %d %g %d %g %d\n", ft_b200_version(), q.null_runs, q.vmax_pxh, q.align, s.clip_sigma,
+           ft_b200_open(0, 0.0, &ctx) == FT_B200_OK);
+    if (ctx) ft_b200_close(ctx);
+    return 0;
+}
+"""
+
+
+def test_header_is_plain_c(tmp_path):
+    """include/ft_b200.h compiles as strict C99 and a C program links against
+    the library and calls its host-side entries (no GPU work)."""
+    import shutil
+    import subprocess
+
+    gcc = shutil.which("gcc")
+    if not gcc:
+        pytest.skip("no C compiler")
+    src = tmp_path / "abi.c"
+    src.write_text(C_PROGRAM)
+    exe = tmp_path / "abi"
+    lib_dir = os.path.dirname(ftb.LIB_PATH)
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I" + os.path.join(ROOT, "include"),
+                    str(src), "-L" + lib_dir, "-lft_b200", "-Wl,-rpath," + lib_dir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    assert out[0].startswith("0.9.1") and out[1:5] == ["3", "40", "0", "8"]
