@@ -118,7 +118,10 @@ void ftref_sim_default(ftref_sim* s) {
     s->seed = d.seed;
 }
 
-int ftref_simulate(const ftref_sim* s, float* frames, double* mjd, double* exptime) {
+// simulate() with the given movers (movers[5 k ..] = x_ref, y_ref, vx_pxh, vy_pxh,
+// mag; none: the simulation draws its own).
+int ftref_simulate_movers(const ftref_sim* s, const double* movers, int nmovers, float* frames, double* mjd,
+                          double* exptime) {
     try {
         SimParams p;
         p.width = s->width;
@@ -143,7 +146,17 @@ int ftref_simulate(const ftref_sim* s, float* frames, double* mjd, double* expti
         p.star_mag_bright = s->star_mag_bright;
         p.star_mag_faint = s->star_mag_faint;
         p.seed = s->seed;
-        const SimResult r = simulate(p);
+        std::vector<SimMover> given(static_cast<std::size_t>(std::max(0, nmovers)));
+        for (int k = 0; k < nmovers; ++k) {
+            SimMover& m = given[static_cast<std::size_t>(k)];
+            m.id = "M" + std::to_string(k + 1);
+            m.x_ref = movers[5 * k];
+            m.y_ref = movers[5 * k + 1];
+            m.vx_pxh = movers[5 * k + 2];
+            m.vy_pxh = movers[5 * k + 3];
+            m.mag = movers[5 * k + 4];
+        }
+        const SimResult r = simulate(p, given);
         std::size_t o = 0;
         for (std::size_t i = 0; i < r.frames.size(); ++i) {
             const auto& f = r.frames[i];
@@ -157,6 +170,10 @@ int ftref_simulate(const ftref_sim* s, float* frames, double* mjd, double* expti
         g_err = e.what();
         return 1;
     }
+}
+
+int ftref_simulate(const ftref_sim* s, float* frames, double* mjd, double* exptime) {
+    return ftref_simulate_movers(s, nullptr, 0, frames, mjd, exptime);
 }
 
 // prepare(): returns an opaque Prepared*.

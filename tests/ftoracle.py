@@ -189,6 +189,7 @@ class Reference:
         L = self.L = C.CDLL(path, mode=C.RTLD_GLOBAL)
         L.ftref_last_error.restype = C.c_char_p
         L.ftref_simulate.argtypes = [C.POINTER(SimParams), _f32p, _f64p, _f64p]
+        L.ftref_simulate_movers.argtypes = [C.POINTER(SimParams), _f64p, C.c_int, _f32p, _f64p, _f64p]
         L.ftref_prepare.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f64p, _f64p, C.POINTER(FtParams)]
         L.ftref_prepare.restype = C.c_void_p
         L.ftref_prep_free.argtypes = [C.c_void_p]
@@ -251,12 +252,15 @@ class Reference:
             setattr(s, k, v)
         return s
 
-    def simulate(self, **kw):
+    def simulate(self, movers=None, **kw):
+        """simulate(); movers: rows of (x_ref, y_ref, vx_pxh, vy_pxh, mag) placed
+        instead of the simulation's own random movers."""
         s = self.sim_params(**kw)
         frames = np.empty((s.nframes, s.height, s.width), np.float32)
         mjd = np.empty(s.nframes)
         exp = np.empty(s.nframes)
-        if self.L.ftref_simulate(C.byref(s), frames, mjd, exp):
+        mv = _f64(np.asarray(movers if movers is not None else np.zeros((0, 5)), np.float64).reshape(-1, 5))
+        if self.L.ftref_simulate_movers(C.byref(s), mv.ravel(), mv.shape[0], frames, mjd, exp):
             raise RuntimeError(self.err())
         return frames, mjd, exp
 
