@@ -135,6 +135,8 @@ def _declare(L):
                                            C.POINTER(SearchParams), C.c_int, C.c_void_p, C.c_void_p,
                                            C.POINTER(C.c_void_p), C.c_void_p]
     L.ft_b200_result_free.argtypes = [C.c_void_p]
+    L.ft_b200_emulate_stack.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _i32p, _i32p, C.c_int, C.c_int, C.c_int,
+                                        _f32p, _i32p]
     L.ft_b200_check_registration.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p,
                                              C.POINTER(DriftCheck)]
     L.ft_b200_check_registration_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p,
@@ -263,6 +265,23 @@ def completeness(device, frames, mjd, exptime, snr_levels=(4.0, 5.0, 6.0, 7.0, 8
     out = [dict(target_snr=r.target_snr, injected=r.injected, recovered=r.recovered, detected=r.detected,
                 mean_snr=r.mean_snr, mean_dpos=r.mean_dpos, mean_dv=r.mean_dv) for r in rows[:lv.size]]
     return dict(rows=out, threshold=thr.value, method=meth.value.decode(), baseline_ok=ok.value, snr50=snr50.value)
+
+
+def emulate_stack(frames, dx, dy, min_count, shape=0):
+    """ft_b200_emulate_stack: one pass computed on the CPU as the device kernel
+    computes it over its plan (for checks without a GPU). frames (n, h, w);
+    dx/dy (m, n) motion-major shifts. Returns (max_snr, best_v)."""
+    L = lib()
+    frames = np.ascontiguousarray(frames, dtype=np.float32)
+    n, h, w = frames.shape
+    dx = np.ascontiguousarray(dx, dtype=np.int32)
+    dy = np.ascontiguousarray(dy, dtype=np.int32)
+    m = dx.size // n
+    ms = np.empty((h, w), np.float32)
+    bv = np.empty((h, w), np.int32)
+    if L.ft_b200_emulate_stack(frames, w, h, n, dx, dy, m, min_count, shape, ms, bv) != FT_B200_OK:
+        raise RuntimeError("emulate_stack: " + L.ft_b200_last_error(None).decode())
+    return ms, bv
 
 
 def set_tile_shape(shape):

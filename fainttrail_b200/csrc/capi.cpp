@@ -2,6 +2,7 @@
 // capture and status codes around the C++ engine.
 #include "ft_b200.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdint>
@@ -244,6 +245,36 @@ int ft_b200_stage_dev(ft_b200_ctx* ctx, const float* d_sub, int width, int heigh
         ftb::stage_device(c, d_sub, pitch, width, height, nframes, t_h, sp, d_filtered, d_static_sky, d_mask, sigma,
                           cr_pixels);
     });
+}
+
+int ft_b200_emulate_stack(const float* frames, int width, int height, int nframes, const int* dx, const int* dy,
+                          int motions, int min_count, int shape, float* max_snr, int* best_v) {
+    try {
+        check_pass(frames, width, height, nframes, motions, min_count);
+        if (!dx || !dy) throw std::runtime_error("stack pass: malformed shift table");
+        if (!max_snr || !best_v) throw std::runtime_error("stack pass: missing outputs");
+        if (shape < 0 || shape > ftb::kStackShapes) throw std::runtime_error("emulate: unknown tile shape");
+        const size_t pixels = static_cast<size_t>(width) * height;
+        if (min_count > nframes) {  // as the device entries: no S/N is defined anywhere
+            std::fill(max_snr, max_snr + pixels, 0.0f);
+            std::fill(best_v, best_v + pixels, -1);
+            return FT_B200_OK;
+        }
+        constexpr int kB200SmemOptin = 232448;  // 227 KB of shared memory per block
+        // a fixed shape whose windows do not fit falls back to the automatic
+        // choice, as ft_b200_set_tile_shape does for the device
+        ftb::StackConfig cfg = ftb::choose_stack_config(width, height, nframes, kB200SmemOptin);
+        if (shape > 0 && ftb::stack_shape_fits(ftb::stack_shape_config(shape, kB200SmemOptin), nframes))
+            cfg = ftb::stack_shape_config(shape, kB200SmemOptin);
+        const ftb::StackPlan plan =
+            ftb::make_stack_plan(width, height, nframes, dx, dy, motions, min_count,
+                                 ftb::motion_order(dx, dy, motions, nframes, 4.0, 4.0), cfg);
+        ftb::emulate_stack_pass(plan, frames, max_snr, best_v);
+        return FT_B200_OK;
+    } catch (const std::exception& e) {
+        g_open_error = e.what();
+        return FT_B200_ERROR;
+    }
 }
 
 void ft_b200_stage_params_default(ft_b200_stage_params* p) {

@@ -245,6 +245,14 @@ void run_plan(Context& c, const StackPlan& plan, const float* d_frames, float* d
 void stack_pass_device(Context& c, const float* d_frames, int pitch, int w, int h, int n, const int* dx,
                        const int* dy, int m, int min_count, const double* vel, double tmax, float* d_max_snr,
                        int* d_best_v, const Progress& progress) {
+    if (min_count > n) {
+        // no pixel is covered by min_count frames for any motion: every S/N is
+        // undefined, so max_snr is 0 and best_v -1 everywhere (the kernel's
+        // interior tiles take c = n without testing min_count)
+        fill_undefined_maps(d_max_snr, d_best_v, static_cast<size_t>(w) * h, c.stream());
+        FTB_CHECK(cudaStreamSynchronize(c.stream()));
+        return;
+    }
     const double t0 = wall_seconds();
     const StackConfig cfg = choose_stack_config(w, h, n, c.smem_optin());
     const std::vector<int> order = motion_order(dx, dy, m, n, 4.0, 4.0);
@@ -443,6 +451,20 @@ void clear_tuned_shapes() {
 
 void stack_passes_device(Context& c, std::vector<PassJob>& jobs) {
     if (jobs.empty()) return;
+    // a pass whose min_count exceeds its frame count (a search's min_coverage
+    // above 1) defines no S/N anywhere: its maps are filled, not stacked
+    if (std::any_of(jobs.begin(), jobs.end(), [](const PassJob& j) { return j.min_count > j.n; })) {
+        std::vector<PassJob> rest;
+        for (const PassJob& j : jobs) {
+            if (j.min_count > j.n)
+                fill_undefined_maps(j.d_max, j.d_bv, static_cast<size_t>(j.w) * j.h, c.stream());
+            else
+                rest.push_back(j);
+        }
+        stack_passes_device(c, rest);
+        FTB_CHECK(cudaStreamSynchronize(c.stream()));
+        return;
+    }
     // tile shapes first (probes run on the stream, before this batch's launches)
     std::vector<int> shapes_for(jobs.size(), 0);
     for (size_t k = 0; k < jobs.size(); ++k) shapes_for[k] = autotune_shape(c, jobs[k]);

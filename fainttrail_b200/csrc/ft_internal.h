@@ -81,6 +81,14 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
 
 StackConfig choose_stack_config(int w, int h, int n, int device_smem_optin);
 
+// The maps of a pass whose min_count exceeds its frame count, where no S/N is
+// defined: max_snr +0.0f and best_v -1 for `pixels` dense pixels.
+void fill_undefined_maps(float* d_max_snr, int* d_best_v, size_t pixels, cudaStream_t s);
+
+// The stacking kernel walked on the CPU over its plan (stack_emulate.cpp);
+// frames: n x h x w host floats; outputs h x w.
+void emulate_stack_pass(const StackPlan& plan, const float* frames, float* max_snr, int* best_v);
+
 // Raises a kernel's dynamic shared-memory limit on the current device to at
 // least `bytes`, never lowering it: the attribute is process-wide, so setting it
 // per launch from several threads (the server's workers) could lower it under

@@ -73,6 +73,11 @@ extern "C" int ft_b200_stack_dev_noalloc(const float* d_frames, int width, int h
         if (pitch < width || (pitch * 4) % 16 != 0 || reinterpret_cast<uintptr_t>(d_frames) % 16 != 0)
             throw std::runtime_error("stack pass: device frames need a 16-byte aligned base and row pitch");
         cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+        if (min_count > nframes) {  // no S/N is defined anywhere
+            fill_undefined_maps(d_max_snr, d_best_v, static_cast<size_t>(width) * height, s);
+            FTB_CHECK(cudaStreamSynchronize(s));
+            return FT_B200_OK;
+        }
         DeviceScratch& d = device_scratch();
         const StackConfig cfg = choose_stack_config(width, height, nframes, d.smem_optin);
         StackPlan plan = make_stack_plan(width, height, nframes, dx, dy, motions, min_count,

@@ -48,6 +48,11 @@ void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaError(std::string("CUDA: ") + what + ": " + cudaGetErrorString(e));
 }
 
+void fill_undefined_maps(float* d_max_snr, int* d_best_v, size_t pixels, cudaStream_t s) {
+    FTB_CHECK(cudaMemsetAsync(d_max_snr, 0, sizeof(float) * pixels, s));     // +0.0f
+    FTB_CHECK(cudaMemsetAsync(d_best_v, 0xff, sizeof(int) * pixels, s));     // -1
+}
+
 void allow_dynamic_smem(const void* func, size_t bytes) {
     static std::mutex mu;
     static std::map<std::pair<int, const void*>, size_t> limit;

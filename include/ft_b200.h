@@ -40,8 +40,8 @@ void ft_b200_close(ft_b200_ctx* ctx);
 /* Last error message of the context (ft_last_error, fainttrail.h:106); with a
  * NULL context, the last error on this thread of the entries that take no
  * context: ft_b200_open, ft_b200_server_open, ft_b200_stack_dev_noalloc,
- * ft_b200_set_tile_shape, ft_b200_null_threshold, ft_b200_pool_null_peaks and
- * ft_b200_write_candidates_csv. */
+ * ft_b200_set_tile_shape, ft_b200_null_threshold, ft_b200_pool_null_peaks,
+ * ft_b200_write_candidates_csv and ft_b200_emulate_stack. */
 const char* ft_b200_last_error(const ft_b200_ctx* ctx);
 /* Device name, SM count and memory; replaces SearchBackend::description()
  * (backend.hpp:113). name_len bytes are written to name, NUL-terminated. */
@@ -93,6 +93,19 @@ int ft_b200_stack_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int he
 int ft_b200_stack_dev_noalloc(const float* d_frames, int width, int height, int pitch, int nframes, const int* dx,
                               const int* dy, int motions, int min_count, float* d_max_snr, int* d_best_v,
                               void* cuda_stream);
+
+/* One stacking pass computed on the host exactly as the device kernel computes
+ * it, for checks of the pass planner on a machine without a GPU (the role of the
+ * reference's emulate_cuda_pass, cuda_plan.cpp:74-117): the pass is planned for
+ * kernel shape `shape` (1..7 as ft_b200_set_tile_shape; 0: the automatic choice)
+ * with a B200's 227 KB of shared memory per block, and the plan -- tiles, motion
+ * groups, frame windows zero-filled outside the frame, 16-bit window offsets,
+ * coverage counts with the interior-tile shortcut, float adds in ascending frame
+ * order, the maximum rule -- is walked on the CPU. Arguments and outputs as
+ * ft_b200_stack (host buffers); slow (one CPU thread). No device is used; error
+ * text in ft_b200_last_error(NULL). */
+int ft_b200_emulate_stack(const float* frames, int width, int height, int nframes, const int* dx, const int* dy,
+                          int motions, int min_count, int shape, float* max_snr, int* best_v);
 
 /* Parameters of the preprocessing stage; the defaults are SearchParams'
  * (include/fainttrail/search.hpp:18-90): static_exclude -1 (= max(1, lround(n/8))),

@@ -1,0 +1,82 @@
+"""The stacking kernel's plan checked without a GPU, as the reference checks its
+CUDA algorithm by host emulation (test_cuda_algorithm, test_main.cpp:553-622):
+ft_b200_emulate_stack plans a pass exactly as the device does for each kernel
+shape and walks the plan on the CPU (windows zero-filled outside the frame,
+16-bit offsets, coverage counts with the interior-tile shortcut, the maximum
+rule); its maps must equal the oracle's and the reference's golden maps bit for
+bit: the backend-contract passes (ties, far motions), NaN pixels, shift tables
+with +500 / -900 px jumps, random lattices up to 255 frames, every min_count
+including ones above the frame count."""
+import numpy as np
+import pytest
+
+import fainttrail_b200 as ftb
+from conftest import golden
+
+SHAPES = range(1, 8)
+
+
+def same(a, b):
+    return np.array_equal(a, b, equal_nan=True)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("name", ["stack_contract", "stack_constant", "stack_nan_table"])
+def test_golden_passes(oracle, name, shape):
+    g = golden(name + ".npz")
+    dx, dy = oracle.shift_table(g["t_h"], g["vel"])
+    ms, bv = ftb.emulate_stack(g["frames"], dx, dy, int(g["min_count"]), shape)
+    assert same(ms, g["max_snr"]) and np.array_equal(bv, g["best_v"])
+    if "dx" in g:  # the curved table with jumps
+        ms, bv = ftb.emulate_stack(g["frames"], g["dx"], g["dy"], int(g["min_count"]), shape)
+        assert same(ms, g["table_max_snr"]) and np.array_equal(bv, g["table_best_v"])
+
+
+def test_constant_frames_tie_to_motion_zero(oracle):
+    """The known answer of the reference's contract test (test_main.cpp:451-456):
+    constant frames tie every motion; pixel (18, 11) goes to motion 0 with S/N
+    sqrt(7), in every tile shape."""
+    g = golden("stack_constant.npz")
+    dx, dy = oracle.shift_table(g["t_h"], g["vel"])
+    for shape in SHAPES:
+        ms, bv = ftb.emulate_stack(g["frames"], dx, dy, int(g["min_count"]), shape)
+        assert bv[11, 18] == 0 and ms[11, 18] == np.float32(np.sqrt(7.0)), shape
+
+
+@pytest.mark.parametrize("n,w,h,m,seed,shape", [
+    (5, 37, 23, 30, 1, 1), (9, 41, 29, 60, 2, 2), (12, 70, 33, 45, 3, 3), (16, 65, 20, 40, 4, 4),
+    (7, 100, 50, 80, 5, 5), (11, 33, 47, 25, 6, 6), (6, 64, 36, 50, 7, 7), (40, 48, 24, 20, 8, 0),
+    (120, 40, 20, 12, 9, 0), (255, 36, 12, 6, 10, 0)])
+def test_random_lattices(oracle, n, w, h, m, seed, shape):
+    rng = np.random.default_rng(seed)
+    frames = rng.normal(0, 1, (n, h, w)).astype(np.float32)
+    frames[rng.integers(0, n), rng.integers(0, h), rng.integers(0, w)] = np.nan
+    frames[:, 3, :] = np.round(frames[:, 3, :])  # integer values: exact ties
+    span = rng.integers(1, 60)
+    dx = rng.integers(-span, span + 1, (m, n)).astype(np.int32)
+    dy = rng.integers(-span, span + 1, (m, n)).astype(np.int32)
+    dx[0, :] = 0
+    dy[0, :] = 0
+    for min_count in sorted({1, max(1, n // 2), n, n + 1}):
+        want = oracle.stack(frames, dx, dy, min_count)
+        got = ftb.emulate_stack(frames, dx, dy, min_count, shape)
+        assert same(got[0], want[0]) and np.array_equal(got[1], want[1]), min_count
+
+
+def test_min_count_above_frame_count_defines_nothing(oracle):
+    rng = np.random.default_rng(11)
+    frames = rng.normal(0, 1, (5, 23, 37)).astype(np.float32)
+    d = np.zeros((3, 5), np.int32)
+    ms, bv = ftb.emulate_stack(frames, d, d, 6, 1)
+    assert not ms.any() and np.all(bv == -1)
+    want = oracle.stack(frames, d, d, 6)
+    assert same(ms, want[0]) and np.array_equal(bv, want[1])
+
+
+def test_bad_arguments_are_errors():
+    f = np.zeros((3, 8, 8), np.float32)
+    d = np.zeros((1, 3), np.int32)
+    with pytest.raises(RuntimeError, match="min_count"):
+        ftb.emulate_stack(f, d, d, 0)
+    with pytest.raises(RuntimeError, match="tile shape"):
+        ftb.emulate_stack(f, d, d, 1, shape=9)

@@ -92,3 +92,16 @@ def test_progress_and_cancel(backend, oracle):
     # the context stays usable after a cancel
     ms3, bv3 = run(backend, frames, t_h=t, velocities=grid, min_count=5)
     assert same(ms3, ms) and same(bv3, bv)
+
+
+def test_min_count_above_frame_count(backend, oracle):
+    """min_count above the frame count (allowed by validate_pass,
+    backend.cpp:89-108): no S/N is defined, so max_snr is 0 and best_v -1
+    everywhere, as the reference's CPU backend gives (the pass is not stacked)."""
+    g = golden("stack_contract.npz")
+    n = g["frames"].shape[0]
+    dx, dy = oracle.shift_table(g["t_h"], g["vel"])
+    for mc in (n + 1, n + 5):
+        ms, bv = run(backend, g["frames"], t_h=g["t_h"], velocities=g["vel"], min_count=mc)
+        want = oracle.stack(g["frames"], dx, dy, mc)
+        assert same(ms, want[0]) and same(bv, want[1]) and not ms.any() and np.all(bv == -1)
