@@ -80,3 +80,19 @@ def test_bad_arguments_are_errors():
         ftb.emulate_stack(f, d, d, 0)
     with pytest.raises(RuntimeError, match="tile shape"):
         ftb.emulate_stack(f, d, d, 1, shape=9)
+
+
+def test_headline_motion_grid(oracle):
+    """The motion grid of the 40-frame full-frame benchmark (0.325 h span, 6-120
+    px/h, 0.125 px tolerance: 19,328 motions) on a 64 x 64 crop: the large
+    groups the planner builds for it reproduce the oracle's maps."""
+    n = 40
+    t = np.linspace(-0.1625, 0.1625, n)
+    grid, _ = oracle.velocity_grid(0.325, 6.0, 120.0, 0.125)
+    assert grid.shape[0] == 19328
+    dx, dy = oracle.shift_table(t, grid)
+    frames = np.random.default_rng(12).normal(0, 1, (n, 64, 64)).astype(np.float32)
+    mc = oracle.min_count(0.7, n)
+    got = ftb.emulate_stack(frames, dx, dy, mc)
+    want = oracle.stack(frames, dx, dy, mc)
+    assert same(got[0], want[0]) and np.array_equal(got[1], want[1])
