@@ -96,3 +96,35 @@ def test_headline_motion_grid(oracle):
     got = ftb.emulate_stack(frames, dx, dy, mc)
     want = oracle.stack(frames, dx, dy, mc)
     assert same(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
+def test_seeded_random_passes(oracle):
+    """400 seeded random passes: 1-255 frames, 1-119 x 1-79 pixels, up to 300
+    motions with shifts of 3 to 1000 px (random or straight-track tables),
+    integer-valued ties, NaN, +-inf and near-overflow pixels, every min_count up
+    to n + 1 and every tile shape."""
+    rng = np.random.default_rng(2026)
+    for case in range(400):
+        n = int(rng.choice([1, 2, 3, 5, 8, 13, 30, 64, 100, 255]))
+        w, h = int(rng.integers(1, 120)), int(rng.integers(1, 80))
+        m = int(rng.integers(1, 300 if n * w * h < 20000 else 40))
+        span = int(rng.choice([3, 40, 400, 1000]))
+        if rng.random() < 0.3:  # straight tracks: round(v t) half away from zero
+            t = np.sort(rng.uniform(-0.5, 0.5, n))
+            f = rng.uniform(-span, span, (m, 2))[:, None, :] * t[None, :, None]
+            r = (np.sign(f) * np.floor(np.abs(f) + 0.5)).astype(np.int32)
+            dx, dy = np.ascontiguousarray(r[:, :, 0]), np.ascontiguousarray(r[:, :, 1])
+        else:
+            dx = rng.integers(-span, span + 1, (m, n)).astype(np.int32)
+            dy = rng.integers(-span, span + 1, (m, n)).astype(np.int32)
+        frames = rng.normal(0, 1, (n, h, w)).astype(np.float32)
+        if rng.random() < 0.5:
+            frames = np.round(frames)
+        if rng.random() < 0.4:
+            k = int(rng.integers(1, 6))
+            frames.flat[rng.integers(0, frames.size, k)] = rng.choice(
+                [np.inf, -np.inf, np.nan, 3e38, -3e38], k).astype(np.float32)
+        mc, shape = int(rng.integers(1, n + 2)), int(rng.integers(0, 8))
+        got = ftb.emulate_stack(frames, dx, dy, mc, shape)
+        want = oracle.stack(frames, dx, dy, mc)
+        assert same(got[0], want[0]) and np.array_equal(got[1], want[1]), (case, n, w, h, m, span, mc, shape)
