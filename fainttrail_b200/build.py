@@ -76,10 +76,17 @@ def build(verbose=False, ptxas_info=False):
     return LIB
 
 
-def build_adapter(ref_root="/root/reference", ref_lib_dir=None):
+def reference_root():
+    """The FaintTrail source tree the checkers are built from: $FAINTTRAIL_REF, or
+    a `reference` directory beside the repository."""
+    return os.environ.get("FAINTTRAIL_REF") or os.path.join(os.path.dirname(ROOT), "reference")
+
+
+def build_adapter(ref_root=None, ref_lib_dir=None):
     """SearchBackend adapter ("b200") for the reference library. Needs the
     reference headers (only where the reference tree is present) and links
     libft_b200.so; the reference library itself is resolved at load time."""
+    ref_root = ref_root or reference_root()
     inc = os.path.join(ref_root, "include")
     if not os.path.isdir(inc) or not os.path.exists(ADAPTER_SRC):
         return None

@@ -1,12 +1,13 @@
 // An allocation-free stacking pass, for callers that cannot allocate device
-// memory: code that runs while a CUDA graph is being captured (a cudaMalloc
-// there breaks the capture), host applications that hand every byte of HBM to
-// their own arena or memory pool and forbid the library from growing it, and
-// real-time loops that must not block on the allocator. The caller owns the
-// frames and the two output maps; the pass's only scratch -- its plan tables
-// (motion groups, per-frame windows, shared-memory offsets, shifts, 1/sqrt(c))
-// -- lives in a file-scope device array of fixed size that every GPU loading
-// this library holds until the process exits.
+// memory: host applications that hand every byte of HBM to their own arena or
+// memory pool and forbid a library from growing it, and latency-bound loops
+// that must not block on the allocator. The caller owns the frames and the two
+// output maps; the pass's only scratch -- its plan tables (motion groups,
+// per-frame windows, shared-memory offsets, shifts, 1/sqrt(c)) and the launch
+// descriptors -- lives in a file-scope device array of fixed size that every GPU
+// loading this library holds until the process exits. The call copies the
+// tables from host memory, launches the pass on the caller's stream,
+// synchronises that stream and returns when the pass is complete.
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -40,9 +41,18 @@ DeviceScratch g_devices[64];
 
 // Once per device, with that device current: the device addresses of the arrays
 // (the names are host-side stand-ins in host code and cannot be passed to a kernel).
-DeviceScratch& device_scratch() {
+// The stream must belong to the current device, or the copies and the kernel
+// would use another device's arrays.
+DeviceScratch& device_scratch(cudaStream_t s) {
     int dev = 0;
     FTB_CHECK(cudaGetDevice(&dev));
+    if (s) {
+        int sdev = -1;
+        FTB_CHECK(cudaStreamGetDevice(s, &sdev));
+        if (sdev != dev)
+            throw std::runtime_error("stack pass: the stream belongs to device " + std::to_string(sdev) +
+                                     ", not to the current device " + std::to_string(dev));
+    }
     if (dev < 0 || dev >= 64) throw std::runtime_error("device index out of range");
     std::lock_guard<std::mutex> lk(g_mu);
     DeviceScratch& d = g_devices[dev];
@@ -73,12 +83,12 @@ extern "C" int ft_b200_stack_dev_noalloc(const float* d_frames, int width, int h
         if (pitch < width || (pitch * 4) % 16 != 0 || reinterpret_cast<uintptr_t>(d_frames) % 16 != 0)
             throw std::runtime_error("stack pass: device frames need a 16-byte aligned base and row pitch");
         cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
+        DeviceScratch& d = device_scratch(s);
         if (min_count > nframes) {  // no S/N is defined anywhere
             fill_undefined_maps(d_max_snr, d_best_v, static_cast<size_t>(width) * height, s);
             FTB_CHECK(cudaStreamSynchronize(s));
             return FT_B200_OK;
         }
-        DeviceScratch& d = device_scratch();
         const StackConfig cfg = choose_stack_config(width, height, nframes, d.smem_optin);
         StackPlan plan = make_stack_plan(width, height, nframes, dx, dy, motions, min_count,
                                          motion_order(dx, dy, motions, nframes, 4.0, 4.0), cfg);

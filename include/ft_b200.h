@@ -71,25 +71,27 @@ int ft_b200_stack_linear(ft_b200_ctx* ctx, const float* frames, int width, int h
 int ft_b200_stack_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int height, int pitch, int nframes,
                       const int* dx, const int* dy, int motions, int min_count, float* d_max_snr, int* d_best_v);
 
-/* A stacking pass that allocates no device memory, for callers that cannot: code
- * running while a CUDA graph is being captured (an allocation there breaks the
- * capture), applications whose own arena or pool owns the GPU's memory and does
- * not let a library grow it, and latency-bound loops that must not wait on the
- * allocator. This entry point has no counterpart in FaintTrail; it is the
- * device-resident pass of ft_b200_stack_dev with the same arguments and results,
- * needing no context. The caller owns d_frames (nframes x height rows of `pitch`
- * floats, pitch >= width, pitch * 4 a multiple of 16, base 16-byte aligned) and
- * the outputs d_max_snr / d_best_v (height x width). dx/dy are host tables.
- * cuda_stream: a cudaStream_t, or NULL for the default stream; the call returns
- * when the pass is complete.
- * The pass's scratch -- its plan tables -- lives in one 32 MiB device array
- * built into this library (every GPU that loads the library holds it until the
- * process exits); a pass whose tables need more (about 5 million motion x frame
- * pairs) is refused with an error, nothing else is limited. The first call on a
- * device looks up that array's device address, so make it before any stream
- * capture. All calls share the array and it keeps the last call's tables: calls
- * that overlap on the GPU (other host threads, other streams) race and must be
- * serialised by the caller. Error text: ft_b200_last_error(NULL). */
+/* A stacking pass that allocates no device memory, for callers that cannot:
+ * applications whose own arena or pool owns the GPU's memory and does not let a
+ * library grow it, and latency-bound loops that must not wait on the allocator.
+ * This entry point has no counterpart in FaintTrail; it is the device-resident
+ * pass of ft_b200_stack_dev with the same arguments and results, needing no
+ * context. The caller owns d_frames (nframes x height rows of `pitch` floats,
+ * pitch >= width, pitch * 4 a multiple of 16, base 16-byte aligned) and the
+ * outputs d_max_snr / d_best_v (height x width). dx/dy are host tables.
+ * cuda_stream: a cudaStream_t of the current device (another device's stream is
+ * refused), or NULL for the default stream. The call copies the pass's tables
+ * from host memory, launches the pass, synchronises the stream and returns when
+ * the pass is complete.
+ * The pass's scratch -- its plan tables and launch descriptors -- lives in one
+ * 32 MiB device array built into this library (every GPU that loads the library
+ * holds it until the process exits); a pass whose tables need more (about 5
+ * million motion x frame pairs) is refused with an error, nothing else is
+ * limited. The first call on a device does a one-time set-up (it looks up that
+ * array's device address on the device), so make the first call before any
+ * stream capture begins. All calls share the array and it keeps the last call's
+ * tables: calls that overlap on the GPU (other host threads, other streams) race
+ * and must be serialised by the caller. Error text: ft_b200_last_error(NULL). */
 int ft_b200_stack_dev_noalloc(const float* d_frames, int width, int height, int pitch, int nframes, const int* dx,
                               const int* dy, int motions, int min_count, float* d_max_snr, int* d_best_v,
                               void* cuda_stream);
