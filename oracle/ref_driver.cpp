@@ -296,6 +296,37 @@ int ftref_stack(const float* frames, int w, int h, int n, const int* dx, const i
     }
 }
 
+// The reference CUDA backend's pass (CudaBackend::run, backend_cuda.cu:99-195)
+// with straight-line shifts, and its own timing breakdown: timings[0..3] =
+// upload, kernel, download, setup seconds (the StageTime entries it reports).
+int ftref_stack_cuda_timed(const float* frames, int w, int h, int n, const double* t_h, const double* vel, int m,
+                           int min_count, float* max_snr, int* best_v, double* timings) {
+    try {
+        const std::vector<Image> fr = images_from(frames, n, w, h);
+        std::vector<double> t(t_h, t_h + n);
+        std::vector<std::pair<double, double>> v;
+        for (int j = 0; j < m; ++j) v.emplace_back(vel[2 * j], vel[2 * j + 1]);
+        StackPass pass;
+        pass.frames = &fr;
+        pass.t_h = &t;
+        pass.velocities = &v;
+        pass.min_count = min_count;
+        const StackResult r = make_backend("cuda")->run(pass);
+        std::memcpy(max_snr, r.max_snr.data.data(), r.max_snr.data.size() * sizeof(float));
+        std::memcpy(best_v, r.best_v.data(), r.best_v.size() * sizeof(int));
+        const char* names[4] = {"upload", "kernel", "download", "setup"};
+        for (int k = 0; k < 4; ++k) {
+            timings[k] = 0.0;
+            for (const auto& st : r.timings)
+                if (st.name == names[k]) timings[k] = st.seconds;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 int ftref_cuda_available(void) { return cuda_backend_available(nullptr) ? 1 : 0; }
 
 // velocity_grid for a sequence of the given span. Returns the count (or -1);

@@ -200,6 +200,8 @@ class Reference:
                                         _f32p, _f32p, _f32p, _f64p, _i32p, C.c_void_p]
         L.ftref_stack.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _i32p]
+        L.ftref_stack_cuda_timed.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_int, C.c_int,
+                                             _f32p, _i32p, _f64p]
         L.ftref_velocity_grid.argtypes = [C.c_double, C.POINTER(FtParams), C.c_void_p, C.c_int,
                                           C.POINTER(C.c_double)]
         L.ftref_null_orders.argtypes = [_f64p, C.c_int, C.c_int, C.c_ulonglong, _f64p]
@@ -302,6 +304,22 @@ class Reference:
         if rc:
             raise RuntimeError(self.err())
         return ms, bv
+
+    def cuda_available(self):
+        return bool(self.L.ftref_cuda_available())
+
+    def stack_cuda_timed(self, frames, t_h, vel, min_count):
+        """The reference CUDA backend's pass (straight-line shifts) and its own
+        timings: dict(max_snr, best_v, upload, kernel, download, setup)."""
+        frames = _f32(frames)
+        n, h, w = frames.shape
+        vel = _f64(vel)
+        ms = np.empty((h, w), np.float32)
+        bv = np.empty((h, w), np.int32)
+        tm = np.zeros(4)
+        if self.L.ftref_stack_cuda_timed(frames, w, h, n, _f64(t_h), vel.ravel(), vel.shape[0], min_count, ms, bv, tm):
+            raise RuntimeError(self.err())
+        return dict(max_snr=ms, best_v=bv, upload=tm[0], kernel=tm[1], download=tm[2], setup=tm[3])
 
     def velocity_grid(self, span_h, **kw):
         p = self.params(**kw)
