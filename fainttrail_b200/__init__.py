@@ -135,6 +135,8 @@ def _declare(L):
                                            C.POINTER(SearchParams), C.c_int, C.c_void_p, C.c_void_p,
                                            C.POINTER(C.c_void_p), C.c_void_p]
     L.ft_b200_result_free.argtypes = [C.c_void_p]
+    L.ft_b200_plan_stats.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, C.c_int, C.c_int,
+                                     np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")]
     L.ft_b200_emulate_stack.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _i32p, _i32p, C.c_int, C.c_int, C.c_int,
                                         _f32p, _i32p]
     L.ft_b200_check_registration.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p,
@@ -265,6 +267,18 @@ def completeness(device, frames, mjd, exptime, snr_levels=(4.0, 5.0, 6.0, 7.0, 8
     out = [dict(target_snr=r.target_snr, injected=r.injected, recovered=r.recovered, detected=r.detected,
                 mean_snr=r.mean_snr, mean_dpos=r.mean_dpos, mean_dv=r.mean_dv) for r in rows[:lv.size]]
     return dict(rows=out, threshold=thr.value, method=meth.value.decode(), baseline_ok=ok.value, snr50=snr50.value)
+
+
+def plan_stats(w, h, n, dx, dy, shape=0):
+    """ft_b200_plan_stats: the planner's motion groups for a pass (host only):
+    dict(groups, row_groups, slots, pads, row_slots, max_group_bytes)."""
+    L = lib()
+    dx = np.ascontiguousarray(dx, dtype=np.int32)
+    dy = np.ascontiguousarray(dy, dtype=np.int32)
+    out = np.zeros(6, np.int64)
+    if L.ft_b200_plan_stats(w, h, n, dx, dy, dx.size // n, shape, out) != FT_B200_OK:
+        raise RuntimeError("plan_stats: " + L.ft_b200_last_error(None).decode())
+    return dict(zip(("groups", "row_groups", "slots", "pads", "row_slots", "max_group_bytes"), map(int, out)))
 
 
 def emulate_stack(frames, dx, dy, min_count, shape=0):

@@ -277,6 +277,37 @@ int ft_b200_emulate_stack(const float* frames, int width, int height, int nframe
     }
 }
 
+int ft_b200_plan_stats(int width, int height, int nframes, const int* dx, const int* dy, int motions, int shape,
+                       long long* stats) {
+    try {
+        if (!dx || !dy || !stats || width < 1 || height < 1 || nframes < 1 || motions < 1)
+            throw std::runtime_error("plan_stats: malformed pass");
+        if (shape < 0 || shape > ftb::kStackShapes) throw std::runtime_error("plan_stats: unknown tile shape");
+        constexpr int kB200SmemOptin = 232448;
+        ftb::StackConfig cfg = ftb::choose_stack_config(width, height, nframes, kB200SmemOptin);
+        if (shape > 0 && ftb::stack_shape_fits(ftb::stack_shape_config(shape, kB200SmemOptin), nframes))
+            cfg = ftb::stack_shape_config(shape, kB200SmemOptin);
+        const ftb::StackPlan plan = ftb::make_stack_plan(width, height, nframes, dx, dy, motions, 1,
+                                                         ftb::motion_order(dx, dy, motions, nframes, 4.0, 4.0), cfg);
+        long long fast = 0, pads = 0, fast_slots = 0;
+        for (const auto& g : plan.groups) {
+            fast += g.rows_fast;
+            fast_slots += g.rows_fast ? g.nslots : 0;
+        }
+        for (int j : plan.slot_motion) pads += j < 0;
+        stats[0] = static_cast<long long>(plan.groups.size());
+        stats[1] = fast;
+        stats[2] = static_cast<long long>(plan.slot_motion.size());
+        stats[3] = pads;
+        stats[4] = fast_slots;
+        stats[5] = plan.max_group_bytes;
+        return FT_B200_OK;
+    } catch (const std::exception& e) {
+        g_open_error = e.what();
+        return FT_B200_ERROR;
+    }
+}
+
 void ft_b200_stage_params_default(ft_b200_stage_params* p) {
     if (!p) return;
     const ftb::StageParams d;

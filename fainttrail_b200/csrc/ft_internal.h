@@ -33,7 +33,17 @@ struct StackGroup {
     int gdxmin = 0, gdxmax = 0, gdymin = 0, gdymax = 0;  // shift extremes over the group
     int rows_total = 0;      // window rows in shared memory (sum over frames)
     int win0 = 0;            // first per-frame window descriptor of the group
+    int rows_fast = 0;       // 1: every block shares its column in every frame (row descriptors)
+    int tab_bytes = 0;       // bytes of the group's offset table (a multiple of 16)
 };
+
+// Motions are planned in blocks of kMotionBlock slots (one register block of
+// the kernel). A block whose motions, in every frame, share the column shift and
+// lie within kRowSpread rows of one another is described per frame by one
+// 32-bit word: bits 0-15 the window offset of its lowest row, bits 16-23 each
+// slot's row above it (2 bits a slot), bits 24-25 the largest of those.
+constexpr int kMotionBlock = 4;
+constexpr int kRowSpread = 3;
 
 struct StackWin {            // one frame's window for a group
     int dx0 = 0;             // window x origin relative to the tile (a multiple of 4)
@@ -52,6 +62,7 @@ struct StackConfig {         // one compiled kernel variant
     int bh = 4;              // TMA box height (rows)
     int mblock = 4;          // motions accumulated together in registers
     int merge = 0;           // 0: best/argmax per thread; 1: one shared maximum per tile (atomicMax)
+    int rows = 0;            // 1: the kernel reads row descriptors (blocks sharing a column)
     int smem_bytes = 200 * 1024;
 };
 
@@ -61,7 +72,8 @@ struct StackPlan {
     std::vector<StackGroup> groups;
     std::vector<StackWin> wins;               // groups x frames
     std::vector<int> slot_motion;             // motion index per slot, -1 = pad
-    std::vector<uint16_t> slot_off;           // per group: [frame][slot] shared-memory offsets
+    std::vector<uint16_t> slot_off;           // per group: [frame][slot] shared-memory offsets, or for a
+                                              // rows_fast group [frame][block] 32-bit row descriptors
     std::vector<int> slot_off_base;           // per group: start in slot_off (elements)
     std::vector<short2> slot_shift;           // [slot][frame] clamped (dx, dy), for coverage counts
     std::vector<float> inv_sqrt;              // float(1 / sqrt(c)), c = 0..n
@@ -71,8 +83,11 @@ struct StackPlan {
     double adds = 0;                          // m * n * w * h
 };
 
-// Motion visiting order for the planner: motions whose shifts are close come
-// together (patches of about sx x sy pixels at the frame of widest spread).
+// Motion blocks for the planner, flattened: kMotionBlock slots a block, -1 for a
+// pad. Motions whose column shifts agree in every frame form a class; a class is
+// cut, in index order, into blocks whose rows stay within kRowSpread of one
+// another in every frame; blocks whose shifts are close come together (patches
+// of about sx x sy pixels at the frame of widest spread).
 std::vector<int> motion_order(const int* dx, const int* dy, int m, int n, double sx_px, double sy_px);
 
 // Build a plan for a pass; dx/dy are motion-major (j * n + i) host tables.

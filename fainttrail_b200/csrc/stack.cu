@@ -31,6 +31,7 @@
 #include <math_constants.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -39,6 +40,7 @@
 #include <map>
 #include <mutex>
 #include <numeric>
+#include <unordered_map>
 
 #include "ft_internal.h"
 
@@ -68,42 +70,121 @@ void allow_dynamic_smem(const void* func, size_t bytes) {
 // ------------------------------------------------------------------ host plan
 
 std::vector<int> motion_order(const int* dx, const int* dy, int m, int n, double sx_px, double sy_px) {
-    std::vector<int> order(static_cast<size_t>(m));
-    std::iota(order.begin(), order.end(), 0);
-    if (m < 2) return order;
+    constexpr int M = kMotionBlock;
+    std::vector<int> out;
+    if (m <= 0 || n <= 0) return out;
+    auto DX = [&](int j, int i) { return dx[static_cast<size_t>(j) * n + i]; };
+    auto DY = [&](int j, int i) { return dy[static_cast<size_t>(j) * n + i]; };
     // the frame whose shifts spread most (for straight tracks: the frame furthest
-    // from the reference epoch) decides the grouping: motions are bucketed into
-    // patches of about sx x sy pixels of shift there, row-major inside a patch
-    // (equal dy first), so that the planner's groups are compact in both axes
+    // from the reference epoch) decides the order of the blocks
     int ie = 0;
     long long best = -1;
     for (int i = 0; i < n; ++i) {
         int lo = INT32_MAX, hi = INT32_MIN;
         for (int j = 0; j < m; ++j) {
-            lo = std::min(lo, dx[static_cast<size_t>(j) * n + i]);
-            hi = std::max(hi, dx[static_cast<size_t>(j) * n + i]);
-            lo = std::min(lo, dy[static_cast<size_t>(j) * n + i]);
-            hi = std::max(hi, dy[static_cast<size_t>(j) * n + i]);
+            lo = std::min({lo, DX(j, i), DY(j, i)});
+            hi = std::max({hi, DX(j, i), DY(j, i)});
         }
         if (static_cast<long long>(hi) - lo > best) {
             best = static_cast<long long>(hi) - lo;
             ie = i;
         }
     }
-    auto ex = [&](int j) { return dx[static_cast<size_t>(j) * n + ie]; };
-    auto ey = [&](int j) { return dy[static_cast<size_t>(j) * n + ie]; };
-    auto kx = [&](int j) { return static_cast<long long>(std::floor(ex(j) / sx_px)); };
-    auto ky = [&](int j) { return static_cast<long long>(std::floor(ey(j) / sy_px)); };
-    // patches are visited column by column: a group then grows in dy (more
-    // window rows, limited only by shared memory) while its dx spread stays
-    // within the window pitch
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    // classes of motions whose column shifts agree in every frame (for the
+    // velocity lattice: equal vx), by a hash of the dx row, checked row by row
+    std::vector<int> cls(static_cast<size_t>(m)), rep, chain;
+    std::unordered_map<uint64_t, int> by_hash;
+    for (int j = 0; j < m; ++j) {
+        uint64_t hsh = 1469598103934665603ull;
+        for (int i = 0; i < n; ++i) {
+            hsh ^= static_cast<uint32_t>(DX(j, i));
+            hsh *= 1099511628211ull;
+        }
+        auto it = by_hash.find(hsh);
+        int c = -1;
+        if (it != by_hash.end())
+            for (int k = it->second; k >= 0 && c < 0; k = chain[static_cast<size_t>(k)])
+                if (std::memcmp(dx + static_cast<size_t>(rep[static_cast<size_t>(k)]) * n, dx + static_cast<size_t>(j) * n,
+                                sizeof(int) * static_cast<size_t>(n)) == 0)
+                    c = k;
+        if (c < 0) {
+            c = static_cast<int>(rep.size());
+            rep.push_back(j);
+            chain.push_back(it != by_hash.end() ? it->second : -1);
+            by_hash[hsh] = c;
+        }
+        cls[static_cast<size_t>(j)] = c;
+    }
+    std::vector<std::vector<int>> members(rep.size());
+    for (int j = 0; j < m; ++j) members[static_cast<size_t>(cls[static_cast<size_t>(j)])].push_back(j);
+    // each class in index order (for the lattice: ascending vy), cut into blocks
+    // whose rows stay within kRowSpread of one another in every frame
+    std::vector<std::array<int, M>> blocks;
+    std::vector<int> lo(static_cast<size_t>(n)), hi(static_cast<size_t>(n));
+    for (const std::vector<int>& mem : members) {
+        std::array<int, M> cur;
+        int cnt = 0;
+        auto close = [&]() {
+            for (int k = cnt; k < M; ++k) cur[static_cast<size_t>(k)] = -1;
+            blocks.push_back(cur);
+            cnt = 0;
+        };
+        for (int j : mem) {
+            bool fits = cnt > 0 && cnt < M;
+            for (int i = 0; i < n && fits; ++i) {
+                const int v = DY(j, i);
+                fits = std::max(hi[static_cast<size_t>(i)], v) - std::min(lo[static_cast<size_t>(i)], v) <= kRowSpread;
+            }
+            if (!fits && cnt > 0) close();
+            if (cnt == 0)
+                for (int i = 0; i < n; ++i) lo[static_cast<size_t>(i)] = hi[static_cast<size_t>(i)] = DY(j, i);
+            for (int i = 0; i < n; ++i) {
+                lo[static_cast<size_t>(i)] = std::min(lo[static_cast<size_t>(i)], DY(j, i));
+                hi[static_cast<size_t>(i)] = std::max(hi[static_cast<size_t>(i)], DY(j, i));
+            }
+            cur[static_cast<size_t>(cnt++)] = j;
+        }
+        if (cnt > 0) close();
+    }
+    // tables without that structure (few motions share a column, so most blocks
+    // would be padding) are packed densely instead: consecutive motions of the
+    // patch order below form the blocks, whose frames then read four offsets each
+    const size_t slots = blocks.size() * M;
+    if (slots - static_cast<size_t>(m) > static_cast<size_t>(m) / 10) {
+        std::vector<int> ord(static_cast<size_t>(m));
+        std::iota(ord.begin(), ord.end(), 0);
+        auto kxm = [&](int j) { return static_cast<long long>(std::floor(DX(j, ie) / sx_px)); };
+        auto kym = [&](int j) { return static_cast<long long>(std::floor(DY(j, ie) / sy_px)); };
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+            if (kxm(a) != kxm(b)) return kxm(a) < kxm(b);
+            if (kym(a) != kym(b)) return kym(a) < kym(b);
+            if (DY(a, ie) != DY(b, ie)) return DY(a, ie) < DY(b, ie);
+            return DX(a, ie) < DX(b, ie);
+        });
+        blocks.clear();
+        for (size_t q = 0; q < ord.size(); q += M) {
+            std::array<int, M> b;
+            for (int k = 0; k < M; ++k) b[static_cast<size_t>(k)] = q + k < ord.size() ? ord[q + k] : -1;
+            blocks.push_back(b);
+        }
+    }
+    // blocks whose shifts are close come together: patches of about sx x sy
+    // pixels at frame ie, visited column by column (a group then grows in dy,
+    // limited only by shared memory, while its dx spread stays within the window
+    // pitch), row-major inside a patch
+    auto ex = [&](const std::array<int, M>& b) { return DX(b[0], ie); };
+    auto ey = [&](const std::array<int, M>& b) { return DY(b[0], ie); };
+    auto kx = [&](const std::array<int, M>& b) { return static_cast<long long>(std::floor(ex(b) / sx_px)); };
+    auto ky = [&](const std::array<int, M>& b) { return static_cast<long long>(std::floor(ey(b) / sy_px)); };
+    std::stable_sort(blocks.begin(), blocks.end(), [&](const std::array<int, M>& a, const std::array<int, M>& b) {
         if (kx(a) != kx(b)) return kx(a) < kx(b);
         if (ky(a) != ky(b)) return ky(a) < ky(b);
         if (ey(a) != ey(b)) return ey(a) < ey(b);
         return ex(a) < ex(b);
     });
-    return order;
+    out.reserve(blocks.size() * M);
+    for (const auto& b : blocks) out.insert(out.end(), b.begin(), b.end());
+    return out;
 }
 
 namespace {
@@ -128,10 +209,10 @@ StackConfig stack_shape_config(int shape, int smem_optin) {
     c.bh = 4;
     c.smem_bytes = std::min(smem_optin - 1024, 224 * 1024);
     switch (shape) {
-        case 1: c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 12; break;
+        case 1: c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 12; c.rows = 1; break;
         case 2: c.tile_w = 64; c.wp = 72; c.p = 8; c.ty = 12; break;
-        case 3: c.tile_w = 32; c.wp = 40; c.p = 8; c.ty = 16; break;
-        case 4: c.tile_w = 32; c.wp = 40; c.p = 4; c.ty = 16; break;
+        case 3: c.tile_w = 32; c.wp = 40; c.p = 8; c.ty = 16; c.rows = 1; break;
+        case 4: c.tile_w = 32; c.wp = 40; c.p = 4; c.ty = 16; c.rows = 1; break;
         case 5:  // 32 x 16 with the shared maximum: 16 warps
             c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 16; c.merge = 1;
             c.smem_bytes -= 32 * 16 * 8;  // the keys sit ahead of the windows
@@ -140,7 +221,7 @@ StackConfig stack_shape_config(int shape, int smem_optin) {
             c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 14; c.merge = 1;
             c.smem_bytes -= 32 * 16 * 8;
             break;
-        case 7: c.tile_w = 32; c.wp = 40; c.p = 12; c.ty = 16; break;
+        case 7: c.tile_w = 32; c.wp = 40; c.p = 12; c.ty = 16; c.rows = 1; break;
         default: throw std::runtime_error("stack: unknown tile shape");
     }
     return c;
@@ -174,6 +255,8 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
                           const std::vector<int>& order, const StackConfig& cfg) {
     if (w <= 0 || h <= 0 || n <= 0 || m <= 0) throw std::runtime_error("stack pass: empty frames or motions");
     if (min_count < 1) throw std::runtime_error("stack pass: min_count must be at least 1");
+    constexpr int M = kMotionBlock;
+    if (cfg.mblock != M || order.size() % M != 0) throw std::runtime_error("stack plan: motions not in blocks");
     StackPlan P;
     P.w = w;
     P.h = h;
@@ -183,7 +266,7 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
     P.pitch = frame_pitch(w);
     P.cfg = cfg;
     P.adds = static_cast<double>(m) * n * w * h;
-    const int TW = cfg.tile_w, TH = cfg.tile_h(), WP = cfg.wp, BH = cfg.bh, M = cfg.mblock;
+    const int TW = cfg.tile_w, TH = cfg.tile_h(), WP = cfg.wp, BH = cfg.bh;
     // shared memory in floats after the barrier and alignment slack
     const long long budget = (cfg.smem_bytes - 256) / 4;
 
@@ -193,19 +276,63 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
     // clamped shifts: beyond +-w / +-h a frame never covers, as within
     auto cdx = [&](int j, int i) { return std::clamp(dx[static_cast<size_t>(j) * n + i], -w, w); };
     auto cdy = [&](int j, int i) { return std::clamp(dy[static_cast<size_t>(j) * n + i], -h, h); };
+    for (size_t e = 0; e < order.size(); ++e) {
+        if (order[e] >= m || (e % M == 0 && order[e] < 0))
+            throw std::runtime_error("stack plan: motion blocks out of range or without motions");
+    }
+    // a block whose windows (the tile plus its motions' row spread, in every
+    // frame) do not fit in shared memory on their own is split into single motions
+    std::vector<int> blocks;
+    blocks.reserve(order.size());
+    for (size_t b = 0; b < order.size(); b += M) {
+        long long rows = 0;
+        int real = 0;
+        bool fits = true;
+        for (int k = 0; k < M; ++k) real += order[b + k] >= 0;
+        for (int i = 0; i < n && real > 1; ++i) {
+            int lx = INT32_MAX, hx = INT32_MIN, ly = INT32_MAX, hy = INT32_MIN;
+            for (int k = 0; k < M; ++k) {
+                const int j = order[b + k];
+                if (j < 0) continue;
+                lx = std::min(lx, cdx(j, i));
+                hx = std::max(hx, cdx(j, i));
+                ly = std::min(ly, cdy(j, i));
+                hy = std::max(hy, cdy(j, i));
+            }
+            if (hx - floor4(lx) + TW > WP) fits = false;
+            rows += roundup(TH + hy - ly, BH);
+        }
+        if (real > 1 && (!fits || rows * WP + static_cast<long long>(roundup(M * n, 8)) / 2 > budget)) {
+            for (int k = 0; k < M; ++k)
+                if (order[b + k] >= 0) blocks.insert(blocks.end(), {order[b + k], -1, -1, -1});
+        } else {
+            blocks.insert(blocks.end(), order.begin() + static_cast<long long>(b),
+                          order.begin() + static_cast<long long>(b) + M);
+        }
+    }
+    const int nblk = static_cast<int>(blocks.size()) / M;
+    // slot k of block b, pads standing for the block's last motion (their
+    // windows and offsets repeat it; their slot_motion is -1)
+    auto slot = [&](int b, int k) {
+        int j = -1;
+        for (int q = 0; q <= k; ++q)
+            if (blocks[static_cast<size_t>(b) * M + q] >= 0) j = blocks[static_cast<size_t>(b) * M + q];
+        return j;
+    };
 
     std::vector<int> mnx(static_cast<size_t>(n)), mxx(static_cast<size_t>(n)), mny(static_cast<size_t>(n)),
         mxy(static_cast<size_t>(n));
     std::vector<int> tnx(mnx), txx(mxx), tny(mny), txy(mxy);
-    std::vector<int> members;
+    std::vector<int> members;  // blocks of the open group
 
-    // offset table of a group of `count` motions, in floats
-    auto table_floats = [&](int count) { return static_cast<long long>(roundup(roundup(count, M) * n, 8)) / 2; };
+    // offset table of a group of `nb` blocks, in floats (the 16-bit slot table,
+    // the larger of the two forms)
+    auto table_floats = [&](int nb) { return static_cast<long long>(roundup(nb * M * n, 8)) / 2; };
     auto flush = [&]() {
         StackGroup g;
         g.slot0 = static_cast<int>(P.slot_motion.size());
-        const int cnt = static_cast<int>(members.size());
-        g.nslots = roundup(cnt, M);
+        const int nb = static_cast<int>(members.size());
+        g.nslots = nb * M;
         g.win0 = static_cast<int>(P.wins.size());
         g.gdxmin = g.gdymin = std::numeric_limits<int>::max();
         g.gdxmax = g.gdymax = std::numeric_limits<int>::min();
@@ -224,126 +351,156 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
             g.gdymax = std::max(g.gdymax, mxy[static_cast<size_t>(i)]);
         }
         g.rows_total = row;
+        // window offset of slot (q, k) in frame i
+        auto offset = [&](int q, int k, int i) {
+            const int j = slot(members[static_cast<size_t>(q)], k);
+            const StackWin& wv = P.wins[static_cast<size_t>(g.win0 + i)];
+            const long long off =
+                static_cast<long long>(wv.row0 + cdy(j, i) - wv.dy0) * WP + (cdx(j, i) - wv.dx0);
+            if (off < 0 || off > 65535) throw std::runtime_error("stack plan: window offset out of range");
+            return static_cast<int>(off);
+        };
+        // row descriptors when every block shares its column in every frame
+        bool fast = cfg.rows != 0;
+        for (int q = 0; q < nb && fast; ++q)
+            for (int i = 0; i < n && fast; ++i) {
+                const int j0 = slot(members[static_cast<size_t>(q)], 0);
+                int lo = cdy(j0, i), hi = lo;
+                for (int k = 1; k < M && fast; ++k) {
+                    const int j = slot(members[static_cast<size_t>(q)], k);
+                    fast = cdx(j, i) == cdx(j0, i);
+                    lo = std::min(lo, cdy(j, i));
+                    hi = std::max(hi, cdy(j, i));
+                }
+                fast = fast && hi - lo <= kRowSpread;
+            }
+        g.rows_fast = fast ? 1 : 0;
+        g.tab_bytes = fast ? roundup(nb * n * 4, 16) : roundup(g.nslots * n * 2, 16);
         P.max_rows = std::max(P.max_rows, row);
-        P.max_group_bytes = std::max(P.max_group_bytes, static_cast<long long>(row) * WP * 4 + table_floats(cnt) * 4);
+        P.max_group_bytes = std::max(P.max_group_bytes, static_cast<long long>(row) * WP * 4 + g.tab_bytes);
         P.max_slots = std::max(P.max_slots, g.nslots);
         P.slot_off_base.push_back(static_cast<int>(P.slot_off.size()));
-        // [frame][slot] 16-bit offsets, padded to a multiple of 16 bytes
-        const size_t tab = static_cast<size_t>(roundup(g.nslots * n, 8));
         const size_t base = P.slot_off.size();
-        P.slot_off.resize(base + tab, 0);
-        for (int s = 0; s < g.nslots; ++s) {
-            const int j = members[static_cast<size_t>(std::min(s, cnt - 1))];  // pads repeat the last motion
-            P.slot_motion.push_back(s < cnt ? j : -1);
-            for (int i = 0; i < n; ++i) {
-                const StackWin& wv = P.wins[static_cast<size_t>(g.win0 + i)];
-                const int ddx = cdx(j, i), ddy = cdy(j, i);
-                const long long off = static_cast<long long>(wv.row0 + ddy - wv.dy0) * WP + (ddx - wv.dx0);
-                if (off < 0 || off > 65535) throw std::runtime_error("stack plan: window offset out of range");
-                P.slot_off[base + static_cast<size_t>(i) * g.nslots + static_cast<size_t>(s)] = static_cast<uint16_t>(off);
-                P.slot_shift.push_back(make_short2(static_cast<short>(ddx), static_cast<short>(ddy)));
-            }
+        P.slot_off.resize(base + static_cast<size_t>(g.tab_bytes) / 2, 0);
+        if (fast) {
+            // [frame][block] descriptors: lowest row's offset, each slot's row above it
+            for (int i = 0; i < n; ++i)
+                for (int q = 0; q < nb; ++q) {
+                    int o[M];
+                    int omin = 1 << 30;
+                    for (int k = 0; k < M; ++k) {
+                        o[k] = offset(q, k, i);
+                        omin = std::min(omin, o[k]);
+                    }
+                    uint32_t d = static_cast<uint32_t>(omin), smax = 0;
+                    for (int k = 0; k < M; ++k) {
+                        const uint32_t dk = static_cast<uint32_t>((o[k] - omin) / WP);
+                        d |= dk << (16 + 2 * k);
+                        smax = std::max(smax, dk);
+                    }
+                    d |= smax << 24;
+                    const size_t e = base + 2 * (static_cast<size_t>(i) * nb + static_cast<size_t>(q));
+                    P.slot_off[e] = static_cast<uint16_t>(d & 0xffffu);
+                    P.slot_off[e + 1] = static_cast<uint16_t>(d >> 16);
+                }
+        } else {
+            // [frame][slot] 16-bit offsets
+            for (int q = 0; q < nb; ++q)
+                for (int k = 0; k < M; ++k)
+                    for (int i = 0; i < n; ++i)
+                        P.slot_off[base + static_cast<size_t>(i) * g.nslots + static_cast<size_t>(q * M + k)] =
+                            static_cast<uint16_t>(offset(q, k, i));
         }
+        for (int q = 0; q < nb; ++q)
+            for (int k = 0; k < M; ++k) {
+                const int b = members[static_cast<size_t>(q)];
+                P.slot_motion.push_back(blocks[static_cast<size_t>(b) * M + k]);
+                const int j = slot(b, k);
+                for (int i = 0; i < n; ++i)
+                    P.slot_shift.push_back(make_short2(static_cast<short>(cdx(j, i)), static_cast<short>(cdy(j, i))));
+            }
         P.groups.push_back(g);
         members.clear();
     };
 
-    auto start_group = [&](int j) {
-        for (int i = 0; i < n; ++i) {
-            const size_t k = static_cast<size_t>(i);
-            mnx[k] = mxx[k] = cdx(j, i);
-            mny[k] = mxy[k] = cdy(j, i);
-        }
-        if (TW + 3 > WP || static_cast<long long>(n) * roundup(TH, BH) * WP + table_floats(1) > budget)
-            throw std::runtime_error("stack plan: one motion's frame windows exceed shared memory");
-        members.push_back(j);
-    };
-    // bounds of a member list, recomputed after a cut
-    auto recompute = [&](const std::vector<int>& mem) {
-        for (int i = 0; i < n; ++i) {
-            const size_t k = static_cast<size_t>(i);
-            mnx[k] = mny[k] = std::numeric_limits<int>::max();
-            mxx[k] = mxy[k] = std::numeric_limits<int>::min();
-            for (int jj : mem) {
-                mnx[k] = std::min(mnx[k], cdx(jj, i));
-                mxx[k] = std::max(mxx[k], cdx(jj, i));
-                mny[k] = std::min(mny[k], cdy(jj, i));
-                mxy[k] = std::max(mxy[k], cdy(jj, i));
-            }
-        }
-    };
-    // try to add motion j to the open group; returns false (and changes nothing)
+    // the bounds of the open group extended by block b (into tnx..txy); false
     // when its windows would not fit
-    auto try_add = [&](int j) {
-        if (members.empty()) {
-            start_group(j);
-            return true;
-        }
-        bool fits = true;
+    auto extend = [&](int b) {
         long long rows = 0;
+        bool fits = true;
         for (int i = 0; i < n && fits; ++i) {
             const size_t k = static_cast<size_t>(i);
-            const int ddx = cdx(j, i), ddy = cdy(j, i);
-            tnx[k] = std::min(mnx[k], ddx);
-            txx[k] = std::max(mxx[k], ddx);
-            tny[k] = std::min(mny[k], ddy);
-            txy[k] = std::max(mxy[k], ddy);
-            if (txx[k] - floor4(tnx[k]) + TW > WP) fits = false;
-            rows += roundup(TH + txy[k] - tny[k], BH);
-        }
-        const int cnt = static_cast<int>(members.size()) + 1;
-        if (fits && rows * WP + table_floats(cnt) > budget) fits = false;
-        if (!fits) return false;
-        mnx.swap(tnx);
-        mxx.swap(txx);
-        mny.swap(tny);
-        mxy.swap(txy);
-        members.push_back(j);
-        return true;
-    };
-    std::function<void(int)> add_or_flush = [&](int j) {
-        if (try_add(j)) return;
-        flush();
-        start_group(j);
-    };
-    for (const int j : order) {
-        if (members.empty()) {
-            start_group(j);
-            continue;
-        }
-        bool fits = true;
-        long long rows = 0;
-        for (int i = 0; i < n && fits; ++i) {
-            const size_t k = static_cast<size_t>(i);
-            const int ddx = cdx(j, i), ddy = cdy(j, i);
-            tnx[k] = std::min(mnx[k], ddx);
-            txx[k] = std::max(mxx[k], ddx);
-            tny[k] = std::min(mny[k], ddy);
-            txy[k] = std::max(mxy[k], ddy);
-            if (txx[k] - floor4(tnx[k]) + TW > WP) fits = false;
-            rows += roundup(TH + txy[k] - tny[k], BH);
-        }
-        const int cnt = static_cast<int>(members.size()) + 1;
-        if (fits && rows * WP + table_floats(cnt) > budget) fits = false;
-        if (!fits) {
-            const int share = cfg.ty * M;  // one block for every warp
-            const int keep = static_cast<int>(members.size()) / share * share;
-            std::vector<int> carry;
-            if (keep > 0 && keep < static_cast<int>(members.size())) {
-                carry.assign(members.begin() + keep, members.end());
-                members.resize(static_cast<size_t>(keep));
-                recompute(members);
+            int lx = members.empty() ? INT32_MAX : mnx[k], hx = members.empty() ? INT32_MIN : mxx[k];
+            int ly = members.empty() ? INT32_MAX : mny[k], hy = members.empty() ? INT32_MIN : mxy[k];
+            for (int q = 0; q < M; ++q) {
+                const int j = blocks[static_cast<size_t>(b) * M + q];
+                if (j < 0) continue;
+                lx = std::min(lx, cdx(j, i));
+                hx = std::max(hx, cdx(j, i));
+                ly = std::min(ly, cdy(j, i));
+                hy = std::max(hy, cdy(j, i));
             }
-            flush();
-            for (int c : carry) add_or_flush(c);
-            add_or_flush(j);
-            continue;
+            tnx[k] = lx;
+            txx[k] = hx;
+            tny[k] = ly;
+            txy[k] = hy;
+            if (hx - floor4(lx) + TW > WP) fits = false;
+            rows += roundup(TH + hy - ly, BH);
         }
+        const int nb = static_cast<int>(members.size()) + 1;
+        return fits && rows * WP + table_floats(nb) <= budget;
+    };
+    auto accept = [&](int b) {
         mnx.swap(tnx);
         mxx.swap(txx);
         mny.swap(tny);
         mxy.swap(txy);
-        members.push_back(j);
+        members.push_back(b);
+    };
+    auto start_group = [&](int b) {
+        if (!extend(b)) throw std::runtime_error("stack plan: one motion block's frame windows exceed shared memory");
+        accept(b);
+    };
+    auto recompute = [&]() {
+        std::vector<int> keep;
+        keep.swap(members);
+        for (int b : keep) {
+            extend(b);
+            accept(b);
+        }
+    };
+    std::function<void(int)> add_or_flush = [&](int b) {
+        if (members.empty()) {
+            start_group(b);
+        } else if (extend(b)) {
+            accept(b);
+        } else {
+            flush();
+            start_group(b);
+        }
+    };
+    for (int b = 0; b < nblk; ++b) {
+        if (members.empty()) {
+            start_group(b);
+            continue;
+        }
+        if (extend(b)) {
+            accept(b);
+            continue;
+        }
+        // a full group: keep a whole number of blocks for every warp and carry
+        // the rest into the next group
+        const int share = cfg.ty;
+        const int keep = static_cast<int>(members.size()) / share * share;
+        std::vector<int> carry;
+        if (keep > 0 && keep < static_cast<int>(members.size())) {
+            carry.assign(members.begin() + keep, members.end());
+            members.resize(static_cast<size_t>(keep));
+            recompute();
+        }
+        flush();
+        for (int c : carry) add_or_flush(c);
+        add_or_flush(b);
     }
     if (!members.empty()) flush();
     return P;
@@ -483,7 +640,22 @@ __device__ __forceinline__ void add_column(float (&acc)[P], const float (&v)[P])
 // BORDER: coverage counts. A frame that covers the whole tile for a motion (the
 // common case; a warp-uniform test) adds 1 to the motion's count, a frame that
 // covers part of it is counted per pixel (8-bit counters, 4 per register).
-template <int P, int WP, bool BORDER>
+// ROWS: the group's table holds row descriptors ([frame][block] 32-bit words)
+// instead of 16-bit slot offsets; the four offsets follow from the descriptor.
+template <bool ROWS, int WP>
+__device__ __forceinline__ uint2 block_offsets(const uint16_t* __restrict__ offs, const StackGroup& G, int s0, int i) {
+    if constexpr (ROWS) {
+        const uint32_t d = reinterpret_cast<const uint32_t*>(offs)[i * (G.nslots >> 2) + (s0 >> 2)];
+        const uint32_t o = d & 0xffffu;
+        const uint32_t o0 = o + ((d >> 16) & 3u) * WP, o1 = o + ((d >> 18) & 3u) * WP;
+        const uint32_t o2 = o + ((d >> 20) & 3u) * WP, o3 = o + ((d >> 22) & 3u) * WP;
+        return make_uint2(o0 | (o1 << 16), o2 | (o3 << 16));
+    } else {
+        return *reinterpret_cast<const uint2*>(offs + i * G.nslots + s0);
+    }
+}
+
+template <int P, int WP, bool BORDER, bool ROWS>
 __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup& G, int s0,
                                             const float* __restrict__ win, const uint16_t* __restrict__ offs, int tb,
                                             int x, int x0, int y0, float inv_n, float (&best)[P], int (&arg)[P]) {
@@ -502,11 +674,10 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
         for (int w = 0; w < PW; ++w) cpart[k][w] = 0;
     // the next frame's four offsets are loaded one frame ahead, so the reuse
     // tests below do not wait on a shared-memory load
-    const uint16_t* op = offs + s0;
-    uint2 qn = *reinterpret_cast<const uint2*>(op);
+    uint2 qn = block_offsets<ROWS, WP>(offs, G, s0, 0);
     for (int i = 0; i < a.n; ++i) {
         const uint2 q = qn;
-        if (i + 1 < a.n) qn = *reinterpret_cast<const uint2*>(op + (i + 1) * G.nslots);
+        if (i + 1 < a.n) qn = block_offsets<ROWS, WP>(offs, G, s0, i + 1);
         const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
         float v[P];
         load_column<P, WP>(v, win + o0 + tb);
@@ -555,6 +726,104 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
     }
 }
 
+// Packed pairs of floats: add.rn.f32x2 / mul.rn.f32x2 are two independent
+// round-to-nearest operations, bit-identical to two scalar ones.
+__device__ __forceinline__ uint64_t pack2(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+__device__ __forceinline__ void unpack2(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+// One block of 4 motions of a rows_fast group for this thread's P pixels (one
+// column, P rows), frames in ascending order, on an interior tile. In every
+// frame the block's motions read one column of the window at row offsets
+// 0..3 above the descriptor's base, so the thread loads that column once
+// (P + S rows, S = the largest row offset) and every motion adds its P rows
+// from registers. Rows are paired across the two halves of the tile, row q with
+// row q + P/2, and each pair is one add.rn.f32x2: register pair A[r] holds rows
+// (r, r + P/2), so motion k adds A[q + row offset] to its accumulator pair q
+// (rows P/2 .. P/2 + S - 1 are loaded twice, once for each pairing).
+template <int P, int WP>
+__device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const StackGroup& G, int s0,
+                                                 const float* __restrict__ win, const uint16_t* __restrict__ offs,
+                                                 int tb, float inv_n, float (&best)[P], int (&arg)[P]) {
+    constexpr int M = 4;
+    constexpr int H = P / 2;
+    static_assert(P % 2 == 0, "rows are paired");
+    uint64_t acc[M][H];
+#pragma unroll
+    for (int k = 0; k < M; ++k)
+#pragma unroll
+        for (int q = 0; q < H; ++q) acc[k][q] = 0ull;  // (+0.0f, +0.0f)
+    const int nb = G.nslots >> 2;
+    const uint32_t* dp = reinterpret_cast<const uint32_t*>(offs) + (s0 >> 2);
+    uint32_t dn = dp[0];
+    for (int i = 0; i < a.n; ++i) {
+        const uint32_t d = dn;
+        if (i + 1 < a.n) dn = dp[(i + 1) * nb];
+        const float* src = win + (d & 0xffffu) + tb;
+        const uint32_t S = (d >> 24) & 3u;
+        uint64_t A[H + kRowSpread];
+#pragma unroll
+        for (int r = 0; r < H; ++r) A[r] = pack2(src[r * WP], src[(r + H) * WP]);
+        if (S >= 1u) A[H] = pack2(src[H * WP], src[P * WP]);
+        if (S >= 2u) A[H + 1] = pack2(src[(H + 1) * WP], src[(P + 1) * WP]);
+        if (S >= 3u) A[H + 2] = pack2(src[(H + 2) * WP], src[(P + 2) * WP]);
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            const uint32_t dk = (d >> (16 + 2 * k)) & 3u;
+            if (dk == 0u) {
+#pragma unroll
+                for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q]);
+            } else if (dk == 1u) {
+#pragma unroll
+                for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q + 1]);
+            } else if (dk == 2u) {
+#pragma unroll
+                for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q + 2]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q + 3]);
+            }
+        }
+    }
+    const uint64_t inv2 = pack2(inv_n, inv_n);
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        const int j = a.slot_motion[G.slot0 + s0 + k];
+        if (j < 0) continue;
+#pragma unroll
+        for (int q = 0; q < H; ++q) {
+            float lo, hi;
+            unpack2(mul2(acc[k][q], inv2), lo, hi);
+            if (lo > best[q] || (lo == best[q] && j < arg[q])) {
+                best[q] = lo;
+                arg[q] = j;
+            }
+            if (hi > best[q + H] || (hi == best[q + H] && j < arg[q + H])) {
+                best[q + H] = hi;
+                arg[q + H] = j;
+            }
+        }
+    }
+}
+
 // Stages group g for the tile at (x0, y0): every frame's window by TMA (the
 // lanes of warp 0 share the copies) and the group's 16-bit offset table by one
 // bulk copy, all completing on the one mbarrier; resets the block counter the
@@ -570,7 +839,7 @@ __device__ __forceinline__ bool stage_group(const StackArgs& a, const StackGroup
     fence_proxy_async();
     __syncthreads();
     if (tid < 32) {
-        const uint32_t tab_bytes = static_cast<uint32_t>((G.nslots * a.n + 7) / 8) * 16u;
+        const uint32_t tab_bytes = static_cast<uint32_t>(G.tab_bytes);
         if (lane == 0) {
             *block_next = NW;  // blocks 0 .. NW-1 go to the warps in order
             mbar_expect_tx(bar, static_cast<uint32_t>(G.rows_total * WP * 4) + tab_bytes);
@@ -623,12 +892,20 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
         const bool interior = full && x0 + G.gdxmin >= 0 && x0 + 31 + G.gdxmax < a.w && y0 + G.gdymin >= 0 &&
                               y0 + P - 1 + G.gdymax < a.h;
         // blocks by a shared counter: a warp whose blocks reuse more loads takes more of them
-        if (interior) {
+        if (G.rows_fast) {
+            if (interior) {
+                for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
+                    motion_quad_rows<P, WP>(a, G, s0, win, offs, tb, inv_n, best, arg);
+            } else {
+                for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
+                    motion_quad<P, WP, true, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+            }
+        } else if (interior) {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                motion_quad<P, WP, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+                motion_quad<P, WP, false, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
         } else {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                motion_quad<P, WP, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+                motion_quad<P, WP, true, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
         }
     }
     // merge the warps' maxima (and, for a continued pass, the stored running ones)
@@ -827,28 +1104,6 @@ __device__ bool stack_tile_atom(const StackArgs& a, const CUtensorMap* tmap, int
 // (two independent round-to-nearest float adds, bit-identical to two scalar
 // adds), which halves the add instructions; a window offset that is even loads
 // both columns with one 64-bit shared load, an odd one with two 32-bit loads.
-
-__device__ __forceinline__ uint64_t pack2(float lo, float hi) {
-    uint64_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-
-__device__ __forceinline__ void unpack2(uint64_t v, float& lo, float& hi) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-
-__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
-    uint64_t r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-
-__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
-    uint64_t r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
 
 template <int P, int WP>
 __device__ __forceinline__ void load_pairs(uint64_t (&v)[P], const float* __restrict__ src, uint32_t odd) {

@@ -3,7 +3,8 @@
 // the TMA copies fill them), 16-bit window offsets, clamped shifts for the
 // coverage counts, float adds in ascending frame order, the 1/sqrt(c) scale and
 // the maximum rule (larger S/N, or equal S/N and lower motion index), walked on
-// the CPU. It lets the planner be checked against the stacking contract on a
+// the CPU; groups of blocks that share their column read the row descriptors
+// the kernel reads. It lets the planner be checked against the stacking contract on a
 // machine without a GPU, as the reference checks its CUDA algorithm with
 // emulate_cuda_pass (cuda_plan.cpp:74-117).
 #include <cmath>
@@ -49,6 +50,15 @@ void emulate_stack_pass(const StackPlan& P, const float* frames, float* max_snr,
                                       x0 + TW - 1 + G.gdxmax < w && y0 + G.gdymin >= 0 &&
                                       y0 + TH - 1 + G.gdymax < h;
                 const uint16_t* offs = P.slot_off.data() + P.slot_off_base[g];
+                // window offset of slot s in frame i: from the group's row
+                // descriptors ([frame][block] words: lowest row's offset, each
+                // slot's row above it) or its 16-bit slot table
+                auto slot_offset = [&](int s, int i) -> size_t {
+                    if (!G.rows_fast) return offs[static_cast<size_t>(i) * G.nslots + s];
+                    const size_t e = 2 * (static_cast<size_t>(i) * (G.nslots / kMotionBlock) + s / kMotionBlock);
+                    const uint32_t d = offs[e] | (static_cast<uint32_t>(offs[e + 1]) << 16);
+                    return (d & 0xffffu) + ((d >> (16 + 2 * (s % kMotionBlock))) & 3u) * static_cast<size_t>(WP);
+                };
                 for (int s = 0; s < G.nslots; ++s) {
                     const int j = P.slot_motion[static_cast<size_t>(G.slot0 + s)];
                     if (j < 0) continue;  // a pad slot
@@ -58,7 +68,7 @@ void emulate_stack_pass(const StackPlan& P, const float* frames, float* max_snr,
                             float acc = 0.0f;
                             int c = 0;
                             for (int i = 0; i < n; ++i) {
-                                const size_t o = offs[static_cast<size_t>(i) * G.nslots + s];
+                                const size_t o = slot_offset(s, i);
                                 acc = acc + win[o + static_cast<size_t>(yl) * WP + xl];
                                 const int cx = x0 + xl + sh[i].x, cy = y0 + yl + sh[i].y;
                                 if (cx >= 0 && cx < w && cy >= 0 && cy < h) ++c;

@@ -65,6 +65,56 @@ __device__ __forceinline__ int sky_toggle(uint32_t (&ex)[W], int p) {
     return 1;
 }
 
+// The static sky and the leave-out residuals of one pixel from its values by
+// time rank (V, +inf where not finite), its m_all finite values in sorted order
+// (S) and each rank's sorted position (PF, 255 where not finite).
+template <int W>
+__device__ __forceinline__ void sky_finish(const SkyArgs& a, const float* V, const float* S, const unsigned char* PF,
+                                           int T, int t, int m_all, size_t pix, size_t plane) {
+    const int n = a.n;
+    // global median: the two middle floats are added in float (preprocess.cpp:171)
+    const float mid_sum = __fadd_rn(S[((m_all - 1) / 2) * T + t], S[(m_all / 2) * T + t]);
+    const double global = 0.5 * static_cast<double>(mid_sum);
+    a.sky[pix] = __double2float_rn(global);
+    uint32_t ex[W];
+#pragma unroll
+    for (int wd = 0; wd < W; ++wd) ex[wd] = 0;
+    int excluded = 0;
+    if (a.exclude > 0)
+        for (int r = 0; r <= min(a.exclude, n - 1); ++r) excluded += sky_toggle<W>(ex, PF[r * T + t]);  // rank 0's window
+    for (int r = 0; r < n; ++r) {
+        if (a.exclude > 0 && r > 0) {
+            if (r - 1 - a.exclude >= 0) excluded -= sky_toggle<W>(ex, PF[(r - 1 - a.exclude) * T + t]);
+            if (r + a.exclude < n) excluded += sky_toggle<W>(ex, PF[(r + a.exclude) * T + t]);
+        }
+        const float v = V[r * T + t];
+        float* out = a.residual + a.frame_of[r] * plane + pix;
+        if (v == CUDART_INF_F) {
+            *out = CUDART_NAN_F;
+            continue;
+        }
+        double st = global;
+        const int m = m_all - excluded;
+        if (a.exclude > 0 && m >= 5) {
+            const int lo = (m - 1) / 2, hi = m / 2;
+            int plo = -1, phi = -1, seen = 0;
+#pragma unroll
+            for (int wd = 0; wd < W; ++wd) {
+                const int nb = min(32, max(0, m_all - wd * 32));
+                const uint32_t valid = nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u);
+                const uint32_t keep = ~ex[wd] & valid;
+                const int c = __popc(keep);
+                if (plo < 0 && lo < seen + c) plo = wd * 32 + static_cast<int>(__fns(keep, 0, lo - seen + 1));
+                if (phi < 0 && hi < seen + c) phi = wd * 32 + static_cast<int>(__fns(keep, 0, hi - seen + 1));
+                seen += c;
+            }
+            // double add of the two middle values (preprocess.cpp:198)
+            st = 0.5 * (static_cast<double>(S[plo * T + t]) + static_cast<double>(S[phi * T + t]));
+        }
+        *out = __double2float_rn(static_cast<double>(v) - st);
+    }
+}
+
 template <int W>
 __global__ void __launch_bounds__(64) sky_kernel(const SkyArgs a) {
     extern __shared__ unsigned char sm[];
@@ -123,47 +173,102 @@ __global__ void __launch_bounds__(64) sky_kernel(const SkyArgs a) {
             PF[(e0 + b) * T + t] = fin ? static_cast<unsigned char>(pos[b]) : 255;
         }
     }
-    // global median: the two middle floats are added in float (preprocess.cpp:171)
-    const float mid_sum = __fadd_rn(S[((m_all - 1) / 2) * T + t], S[(m_all / 2) * T + t]);
-    const double global = 0.5 * static_cast<double>(mid_sum);
-    a.sky[pix] = __double2float_rn(global);
-    uint32_t ex[W];
+    sky_finish<W>(a, V, S, PF, T, t, m_all, pix, plane);
+}
+
+// The same for n <= N <= 64 with the sorted order from a bitonic network in
+// registers instead of counting ranks: the pixel's values (non-finite ones as
+// +inf) are sorted with float min / max, which orders everything but the two
+// zeros; where a -0.0 is present the zero run is rewritten with the zeros in
+// time-rank order, which is the reference's order of equal (value, rank) pairs.
+// Each rank's sorted position is then the lower bound of its value in the
+// sorted values plus the number of equal values of lower rank.
+template <int N>
+__global__ void __launch_bounds__(128) sky_net_kernel(const SkyArgs a) {
+    constexpr int W = (N + 31) / 32;
+    extern __shared__ unsigned char sm[];
+    const int T = blockDim.x, t = threadIdx.x;
+    const int n = a.n;
+    float* V = reinterpret_cast<float*>(sm);                            // [n][T] values by time rank, +inf if not finite
+    float* S = V + n * T;                                               // [n][T] finite values in sorted order
+    unsigned char* PF = reinterpret_cast<unsigned char*>(S + n * T);    // [n][T] sorted position by rank, 255: none
+    const long long q = static_cast<long long>(blockIdx.x) * T + t;
+    const int x = static_cast<int>(q % a.w), y = static_cast<int>(q / a.w);
+    if (y >= a.h) return;
+    const size_t plane = static_cast<size_t>(a.pitch) * a.h;
+    const size_t pix = static_cast<size_t>(y) * a.pitch + x;
+    float sv[N];
+    int m_all = 0;
+    bool negzero = false;
 #pragma unroll
-    for (int wd = 0; wd < W; ++wd) ex[wd] = 0;
-    int excluded = 0;
-    if (a.exclude > 0)
-        for (int r = 0; r <= min(a.exclude, n - 1); ++r) excluded += sky_toggle<W>(ex, PF[r * T + t]);  // rank 0's window
-    for (int r = 0; r < n; ++r) {
-        if (a.exclude > 0 && r > 0) {
-            if (r - 1 - a.exclude >= 0) excluded -= sky_toggle<W>(ex, PF[(r - 1 - a.exclude) * T + t]);
-            if (r + a.exclude < n) excluded += sky_toggle<W>(ex, PF[(r + a.exclude) * T + t]);
+    for (int r = 0; r < N; ++r) {
+        float v = CUDART_INF_F;
+        if (r < n) {
+            const float u = a.sub[a.frame_of[r] * plane + pix];
+            const bool fin = finitef(u);
+            v = fin ? u : CUDART_INF_F;
+            m_all += fin;
+            negzero |= __float_as_uint(u) == 0x80000000u;
+            V[r * T + t] = v;
         }
+        sv[r] = v;
+    }
+    if (m_all < a.need) {
+        a.sky[pix] = CUDART_NAN_F;
+        for (int i = 0; i < n; ++i) a.residual[i * plane + pix] = CUDART_NAN_F;
+        return;
+    }
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const float lo = fminf(sv[i], sv[l]), hi = fmaxf(sv[i], sv[l]);
+                    if ((i & k) == 0) {
+                        sv[i] = lo;
+                        sv[l] = hi;
+                    } else {
+                        sv[i] = hi;
+                        sv[l] = lo;
+                    }
+                }
+            }
+#pragma unroll
+    for (int p = 0; p < N; ++p)
+        if (p < m_all) S[p * T + t] = sv[p];
+    if (negzero) {
+        int p = 0;
+        while (p < m_all && S[p * T + t] < 0.0f) ++p;
+        for (int r = 0; r < n; ++r) {
+            const float v = V[r * T + t];
+            if (v == 0.0f) S[(p++) * T + t] = v;
+        }
+    }
+    for (int r = 0; r < n; ++r) {
         const float v = V[r * T + t];
-        float* out = a.residual + a.frame_of[r] * plane + pix;
         if (v == CUDART_INF_F) {
-            *out = CUDART_NAN_F;
+            PF[r * T + t] = 255;
             continue;
         }
-        double st = global;
-        const int m = m_all - excluded;
-        if (a.exclude > 0 && m >= 5) {
-            const int lo = (m - 1) / 2, hi = m / 2;
-            int plo = -1, phi = -1, seen = 0;
-#pragma unroll
-            for (int wd = 0; wd < W; ++wd) {
-                const int nb = min(32, max(0, m_all - wd * 32));
-                const uint32_t valid = nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u);
-                const uint32_t keep = ~ex[wd] & valid;
-                const int c = __popc(keep);
-                if (plo < 0 && lo < seen + c) plo = wd * 32 + static_cast<int>(__fns(keep, 0, lo - seen + 1));
-                if (phi < 0 && hi < seen + c) phi = wd * 32 + static_cast<int>(__fns(keep, 0, hi - seen + 1));
-                seen += c;
+        int lo = 0, len = m_all;
+        while (len > 0) {
+            const int half = len >> 1;
+            if (S[(lo + half) * T + t] < v) {
+                lo += half + 1;
+                len -= half + 1;
+            } else {
+                len = half;
             }
-            // double add of the two middle values (preprocess.cpp:198)
-            st = 0.5 * (static_cast<double>(S[plo * T + t]) + static_cast<double>(S[phi * T + t]));
         }
-        *out = __double2float_rn(static_cast<double>(v) - st);
+        int p = lo;
+        if (lo + 1 < m_all && S[(lo + 1) * T + t] == v)
+            for (int f = 0; f < r; ++f) p += V[f * T + t] == v;
+        PF[r * T + t] = static_cast<unsigned char>(p);
     }
+    sky_finish<W>(a, V, S, PF, T, t, m_all, pix, plane);
 }
 
 // ------------------------------------------------------------------ samples + exact medians
@@ -491,6 +596,159 @@ __global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
     if (threadIdx.x == 0 && cr_tile) atomicAdd(&a.cr[f], cr_tile);
 }
 
+// 4-byte asynchronous copy global -> shared; a source outside the image copies
+// nothing and fills zero (src-size 0).
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// The filter of filter_kernel for a run of frames per CTA (fixed radius RT):
+// the tile's mask and scatter weight are read once for all its frames (one
+// float per pixel: NaN where masked or outside the image, else the divisor,
+// 1 for none), and the next frame's residual tile plus halo is copied
+// asynchronously into a second buffer while the current one is filtered, so
+// the loads of frame f + 1 overlap the arithmetic of frame f. Per frame the
+// steps, their arithmetic and their order are filter_kernel's.
+template <int RT, int TWc, int THc>
+__global__ void __launch_bounds__(256) filter_frames_kernel(const FilterArgs a, int n, int fpc) {
+    extern __shared__ float fs[];
+    constexpr int R = RT, H = R + 2, ZW = TWc + 2 * H, ZH = THc + 2 * H, ZN = ZW * ZH, KN = 2 * RT + 1;
+    constexpr int TR = THc + 2 * R;
+    float* const Rb0 = fs;                  // residual tile + halo, double-buffered
+    float* const Rb1 = fs + ZN;
+    float* E = fs + 2 * ZN;                 // weight divisor, NaN: masked or outside
+    float* Z = fs + 3 * ZN;                 // z, then cleaned and clipped z
+    float* Tt = fs + 4 * ZN;                // TR x TWc horizontal pass
+    unsigned char* F = reinterpret_cast<unsigned char*>(Tt + TR * TWc);  // ZN cosmic-ray centre flags
+    __shared__ int cr_tile;
+    float kr[KN], kn[KN];
+#pragma unroll
+    for (int j = 0; j < KN; ++j) {
+        kr[j] = a.k[j];
+        kn[j] = __fmul_rn(kr[j], a.norm);
+    }
+    const int x0 = blockIdx.x * TWc, y0 = blockIdx.y * THc;
+    const int fa = blockIdx.z * fpc, fb = min(n, fa + fpc);
+    const size_t plane = static_cast<size_t>(a.pitch) * a.h;
+    const int tid = threadIdx.x;
+    auto issue = [&](float* dst, int f) {
+        const float* base = a.residual + f * plane;
+        for (int e = tid; e < ZN; e += blockDim.x) {
+            const int gx = x0 - H + e % ZW, gy = y0 - H + e / ZW;
+            const bool in = gx >= 0 && gy >= 0 && gx < a.w && gy < a.h;
+            cp_async4(dst + e, in ? base + static_cast<size_t>(gy) * a.pitch + gx : base, in);
+        }
+        cp_async_commit();
+    };
+    if (fa < fb) issue(Rb0, fa);
+    for (int e = tid; e < ZN; e += blockDim.x) {
+        const int gx = x0 - H + e % ZW, gy = y0 - H + e / ZW;
+        float ev = CUDART_NAN_F;
+        if (gx >= 0 && gy >= 0 && gx < a.w && gy < a.h) {
+            const size_t pix = static_cast<size_t>(gy) * a.pitch + gx;
+            const float mk = __ldg(a.mask + pix), sc = __ldg(a.scatter + pix);
+            if (mk != 0.0f) ev = sc > a.wscat ? sc : 1.0f;
+        }
+        E[e] = ev;
+    }
+    for (int f = fa; f < fb; ++f) {
+        const float* cur = ((f - fa) & 1) ? Rb1 : Rb0;
+        cp_async_wait_all();
+        __syncthreads();  // cur is complete; every thread is past its last read of the other buffer
+        if (f + 1 < fb) issue(((f - fa) & 1) ? Rb0 : Rb1, f + 1);
+        if (tid == 0) cr_tile = 0;
+        const float inv = __double2float_rn(__ddiv_rn(1.0, a.sigma[f]));
+        for (int e = tid; e < ZN; e += blockDim.x) {
+            const float v = cur[e], ev = E[e];
+            float z = 0.0f;
+            if (ev == ev && finitef(v)) {
+                const float vm = __fmul_rn(v, inv);
+                // (v / sigma) / e, e = scatter above weight_scatter, else 1 (an exact division)
+                z = ev != 1.0f ? __fdiv_rn(vm, ev) : vm;
+            }
+            Z[e] = z;
+        }
+        __syncthreads();
+        // cosmic-ray centres (preprocess.cpp:433-447): inside [1, w-2] x [1, h-2]
+        for (int e = tid; e < ZN; e += blockDim.x) {
+            const int lx = e % ZW, ly = e / ZW;
+            const int gx = x0 - H + lx, gy = y0 - H + ly;
+            unsigned char flag = 0;
+            if (lx >= 1 && ly >= 1 && lx < ZW - 1 && ly < ZH - 1 && gx >= 1 && gy >= 1 && gx < a.w - 1 &&
+                gy < a.h - 1) {
+                const float v = Z[e];
+                if (v >= a.hit) {
+                    const float s4 = __fadd_rn(__fadd_rn(__fadd_rn(Z[e - 1], Z[e + 1]), Z[e - ZW]), Z[e + ZW]);
+                    const float n4 = __fmul_rn(0.25f, s4);
+                    if (!(n4 >= __fmul_rn(a.ratio, v))) {
+                        flag = 1;
+                        if (gx >= x0 && gx < x0 + TWc && gy >= y0 && gy < y0 + THc) atomicAdd(&cr_tile, 1);
+                    }
+                }
+            }
+            F[e] = flag;
+        }
+        __syncthreads();
+        // cleaned, clipped z over the tile plus R (kills applied after the scan)
+        for (int e = tid; e < ZN; e += blockDim.x) {
+            const int lx = e % ZW, ly = e / ZW;
+            if (lx < 2 || ly < 2 || lx >= ZW - 2 || ly >= ZH - 2) continue;
+            const float v = Z[e];
+            bool kill = F[e] != 0;
+            if (!kill && v > 2.5f)
+                for (int dy = -1; dy <= 1 && !kill; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx)
+                        if (F[e + dy * ZW + dx]) {
+                            kill = true;
+                            break;
+                        }
+            const float zc = kill ? 0.0f : v;
+            Z[e] = zc < -a.clip ? -a.clip : (a.clip < zc ? a.clip : zc);
+        }
+        __syncthreads();
+        // horizontal pass over rows y0-R .. y0+THc+R-1, the tile's columns
+        for (int e = tid; e < TR * TWc; e += blockDim.x) {
+            const int c = e % TWc, r = e / TWc;
+            const float* row = Z + (r + 2) * ZW + (c + 2);
+            float acc = 0.0f;
+#pragma unroll
+            for (int j = 0; j < KN; ++j) acc = __fadd_rn(acc, __fmul_rn(row[j], kr[j]));
+            const int gy = y0 - R + r;
+            Tt[e] = (gy >= 0 && gy < a.h) ? acc : 0.0f;
+        }
+        __syncthreads();
+        float* out = a.out + f * plane;
+        for (int e = tid; e < TWc * THc; e += blockDim.x) {
+            const int c = e % TWc, r = e / TWc;
+            const int gx = x0 + c, gy = y0 + r;
+            if (gx >= a.w || gy >= a.h) continue;
+            float acc = 0.0f;
+#pragma unroll
+            for (int j = 0; j < KN; ++j) acc = __fadd_rn(acc, __fmul_rn(kn[j], Tt[(r + j) * TWc + c]));
+            out[static_cast<size_t>(gy) * a.pitch + gx] = acc;
+        }
+        if (tid == 0 && cr_tile) atomicAdd(&a.cr[f], cr_tile);
+    }
+}
+
+template <int RT, int TWc, int THc>
+void launch_filter_frames(const FilterArgs& a, int n, int sms, cudaStream_t s) {
+    constexpr int H = RT + 2, ZW = TWc + 2 * H, ZH = THc + 2 * H, ZN = ZW * ZH;
+    const size_t smem = sizeof(float) * (4 * ZN + (THc + 2 * RT) * TWc) + ((ZN + 15) / 16) * 16;
+    const int tx = (a.w + TWc - 1) / TWc, ty = (a.h + THc - 1) / THc;
+    // frames split over CTAs only when the tiles alone leave SMs idle
+    const long long tiles = static_cast<long long>(tx) * ty;
+    const int groups = static_cast<int>(std::min<long long>(n, std::max<long long>(1, (4LL * sms + tiles - 1) / tiles)));
+    const int fpc = (n + groups - 1) / groups;
+    auto kern = filter_frames_kernel<RT, TWc, THc>;
+    allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
+    kern<<<dim3(tx, ty, (n + fpc - 1) / fpc), 256, smem, s>>>(a, n, fpc);
+    FTB_CHECK(cudaGetLastError());
+}
+
 // one launch of the filter kernel for radius R (compile-time radius up to 8)
 template <int RT, int TWc, int THc>
 void launch_filter(const FilterArgs& a, int n, cudaStream_t s) {
@@ -502,16 +760,16 @@ void launch_filter(const FilterArgs& a, int n, cudaStream_t s) {
     FTB_CHECK(cudaGetLastError());
 }
 
-void launch_filter_any(const FilterArgs& a, int n, cudaStream_t s) {
+void launch_filter_any(const FilterArgs& a, int n, int sms, cudaStream_t s) {
     switch (a.R) {
-        case 1: launch_filter<1, 64, 32>(a, n, s); break;
-        case 2: launch_filter<2, 64, 32>(a, n, s); break;
-        case 3: launch_filter<3, 64, 32>(a, n, s); break;
-        case 4: launch_filter<4, 64, 32>(a, n, s); break;
-        case 5: launch_filter<5, 64, 32>(a, n, s); break;
-        case 6: launch_filter<6, 64, 32>(a, n, s); break;
-        case 7: launch_filter<7, 64, 32>(a, n, s); break;
-        case 8: launch_filter<8, 64, 32>(a, n, s); break;
+        case 1: launch_filter_frames<1, 64, 32>(a, n, sms, s); break;
+        case 2: launch_filter_frames<2, 64, 32>(a, n, sms, s); break;
+        case 3: launch_filter_frames<3, 64, 32>(a, n, sms, s); break;
+        case 4: launch_filter_frames<4, 64, 32>(a, n, sms, s); break;
+        case 5: launch_filter_frames<5, 64, 32>(a, n, sms, s); break;
+        case 6: launch_filter_frames<6, 64, 32>(a, n, sms, s); break;
+        case 7: launch_filter_frames<7, 64, 32>(a, n, sms, s); break;
+        case 8: launch_filter_frames<8, 64, 32>(a, n, sms, s); break;
         default: launch_filter<0, 32, 16>(a, n, s); break;
     }
 }
@@ -652,9 +910,13 @@ void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h,
         const int span = c.span_begin("static sky + residuals");
         SkyArgs a{d_sub, sc.residual.as<float>(), d_sky, tb.tab, tb.tab + n, w, h, pitch, n, exclude,
                   std::max(5, static_cast<int>(0.6 * n))};
-        const int T = 64;
+        // up to 64 frames: the sorting network; beyond: counted ranks
+        const int T = n <= 64 ? 128 : 64;
         const size_t smem = static_cast<size_t>(T) * n * 9;
-        auto kern = n <= 32 ? sky_kernel<1> : n <= 64 ? sky_kernel<2> : n <= 128 ? sky_kernel<4> : sky_kernel<8>;
+        auto kern = n <= 16   ? sky_net_kernel<16>
+                    : n <= 32 ? sky_net_kernel<32>
+                    : n <= 64 ? sky_net_kernel<64>
+                    : n <= 128 ? sky_kernel<4> : sky_kernel<8>;
         allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
         kern<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
         FTB_CHECK(cudaGetLastError());
@@ -744,7 +1006,7 @@ void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const Stage
         a.h = h;
         a.pitch = pitch;
         a.R = R;
-        launch_filter_any(a, n, s);
+        launch_filter_any(a, n, c.sms(), s);
         ++c.launches;
         c.span_end(span);
     }

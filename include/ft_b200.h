@@ -109,6 +109,15 @@ int ft_b200_stack_dev_noalloc(const float* d_frames, int width, int height, int 
 int ft_b200_emulate_stack(const float* frames, int width, int height, int nframes, const int* dx, const int* dy,
                           int motions, int min_count, int shape, float* max_snr, int* best_v);
 
+/* The planner's view of a pass, for checks without a GPU (host only; no
+ * counterpart in FaintTrail, whose CUDA plan has no motion groups): stats[0]
+ * motion groups, [1] groups whose blocks share their column in every frame (the
+ * kernel's row-descriptor path), [2] slots, [3] pad slots, [4] slots in those
+ * groups, [5] the largest group's shared-memory bytes. shape as
+ * ft_b200_emulate_stack. */
+int ft_b200_plan_stats(int width, int height, int nframes, const int* dx, const int* dy, int motions, int shape,
+                       long long* stats);
+
 /* Parameters of the preprocessing stage; the defaults are SearchParams'
  * (include/fainttrail/search.hpp:18-90): static_exclude -1 (= max(1, lround(n/8))),
  * clip 8, cosmic-ray level 5, mask scatter 2.5, weight scatter 1.5. fwhm_px is the

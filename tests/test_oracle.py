@@ -95,3 +95,25 @@ def test_null_orders_and_peaks_against_reference(oracle, reference):
     a = oracle.find_peaks(flat, np.zeros_like(flat, np.int32), 3.0, 2, 1, 100)
     b = reference.find_peaks(flat, np.zeros_like(flat, np.int32), 3.0, 2, 1, 100)
     assert all(same(x, y) for x, y in zip(a, b)) and len(a[0]) == 2
+
+
+def _bits_equal(a, b):
+    a, b = np.asarray(a, np.float32), np.asarray(b, np.float32)
+    na, nb = np.isnan(a), np.isnan(b)
+    return np.array_equal(na, nb) and np.array_equal(a.view(np.uint32)[~na], b.view(np.uint32)[~nb])
+
+
+@pytest.mark.parametrize("n,seed", [(9, 1), (40, 4), (65, 6)])
+def test_oracle_stage_signed_zeros_against_reference(oracle, reference, n, seed):
+    """Integer-valued frames with +0.0 and -0.0: the restatement's static sky and
+    filtered frames equal the reference's bit for bit (equal values ordered by
+    time rank, preprocess.cpp:154-204), so the device stage can be held to bits."""
+    rng = np.random.default_rng(seed)
+    sub = rng.integers(-2, 3, (n, 24, 70)).astype(np.float32)
+    sub[(sub == 0) & (rng.random(sub.shape) < 0.5)] = -0.0
+    sub[:, :, :2] = np.nan
+    t = np.sort(rng.uniform(-0.3, 0.3, n))
+    rng.shuffle(t)
+    o, r = oracle.build_stage(sub, t, 2.5), reference.build_stage(sub, t, 2.5)
+    assert np.signbit(r["static_sky"]).any()
+    assert _bits_equal(o["static_sky"], r["static_sky"]) and _bits_equal(o["filtered"], r["filtered"])

@@ -128,3 +128,38 @@ def test_seeded_random_passes(oracle):
         got = ftb.emulate_stack(frames, dx, dy, mc, shape)
         want = oracle.stack(frames, dx, dy, mc)
         assert same(got[0], want[0]) and np.array_equal(got[1], want[1]), (case, n, w, h, m, span, mc, shape)
+
+
+@pytest.mark.parametrize("grid_tol,n,w,h,shape", [(0.125, 20, 96, 70, 1), (0.125, 40, 70, 50, 7), (0.5, 12, 80, 64, 3),
+                                                  (0.5, 30, 64, 40, 4), (0.3, 25, 90, 45, 0)])
+def test_lattice_blocks_share_columns(oracle, grid_tol, n, w, h, shape):
+    """Velocity lattices (the search's own grids, velocity_grid's rule) are
+    planned in blocks of motions that share their column in every frame, read
+    through row descriptors with row offsets up to 3 (grid_tol 0.5 spreads four
+    motions over three rows at the ends of the sequence); the plan, walked on
+    the CPU, equals the oracle bit for bit, border tiles included."""
+    rng = np.random.default_rng(n)
+    t = np.sort(rng.uniform(0.0, 1.5, n))
+    t = t - 0.5 * (t[0] + t[-1])
+    grid, _ = oracle.velocity_grid(t[-1] - t[0], 2.0, 24.0, grid_tol)
+    dx, dy = oracle.shift_table(t, grid)
+    st = ftb.plan_stats(w, h, n, dx, dy, shape)
+    assert st["row_groups"] == st["groups"] and st["pads"] * 10 < st["slots"]
+    frames = rng.normal(0, 1, (n, h, w)).astype(np.float32)
+    frames[:, 5, :] = np.round(frames[:, 5, :])  # exact ties
+    frames[1, 7, 9] = np.nan
+    for mc in (max(1, int(np.ceil(0.7 * n))), n):
+        ms, bv = ftb.emulate_stack(frames, dx, dy, mc, shape)
+        want_ms, want_bv = oracle.stack(frames, dx, dy, mc)
+        assert same(ms, want_ms) and np.array_equal(bv, want_bv)
+
+
+def test_unstructured_tables_are_packed_densely():
+    """A random table whose motions never share a column in every frame is packed
+    four motions a block, not one motion and three pads."""
+    rng = np.random.default_rng(2)
+    n, m = 9, 200
+    dx = rng.integers(-2, 3, (m, n)).astype(np.int32)
+    dy = rng.integers(-20, 21, (m, n)).astype(np.int32)
+    st = ftb.plan_stats(64, 48, n, dx, dy, 1)
+    assert st["pads"] < 4 and st["row_groups"] == 0
