@@ -27,6 +27,15 @@ serving loop (ft_b200_server_*); reports throughput, served searches/s and
 p50 / p99 latency, beside the same requests run one after another through
 ft_b200_search under the same arrival times.
 
+The default run (N=1) adds to its one JSON line: `batched` (the batched
+calibration workload, all passes batched, beside one pass per launch),
+`serving` (a request stream drawn from the serving configuration, served beside
+the same requests run one after another), `reference_cuda` (the reference's own
+CUDA backend built for sm_100a on one pass of the full-frame frames, beside this
+backend's pass of the same frames, compared bit for bit) and
+`parity_vs_reference` (the device search on the crop the CPU baseline times,
+compared with the reference's search() of that crop). --no-extras skips them.
+
 --impl reference times the reference's own CPU implementation (FaintTrail
 0.9.1 built from its sources, oracle/_ref) on the host's cores with all
 threads, each step a bounded crop of the same workload (all frames, the full
@@ -64,6 +73,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-shape", type=int, default=0, help="stack kernel tile shape (0: autotuned)")
     ap.add_argument("--workers", type=int, default=2, help="serving: rounds in flight at once")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched, serving and reference-CUDA parts")
+    ap.add_argument("--serve-requests", type=int, default=16)
+    ap.add_argument("--serve-max-adds", type=float, default=5.0e13)
     return ap.parse_args()
 
 
@@ -164,11 +176,14 @@ def reference_search_rate(wl, frames_np, mjd, exptime, target_s=15.0, steps=1):
                               grid_tol_px=params["grid_tol_px"])
     m = grid.shape[0]
 
+    last = {}
+
     def run(side):
         crop = np.ascontiguousarray(frames_np[:, :side, :side])
         t0 = time.perf_counter()
         prep = R.prepare(crop, mjd, exptime, fwhm_px=params["fwhm_px"], null_runs=params["null_runs"])
-        prep.search(backend="cpu", **params)
+        last["result"] = prep.search(backend="cpu", **params)
+        last["crop"] = crop
         dt = time.perf_counter() - t0
         return m * wl.nframes * side * side * (1 + params["null_runs"]) / dt, dt
     side = 128
@@ -178,7 +193,125 @@ def reference_search_rate(wl, frames_np, mjd, exptime, target_s=15.0, steps=1):
         side *= 2
         rate, dt = run(side)
     rates = [rate] + [run(side)[0] for _ in range(steps - 1)]
-    return statistics.median(rates), side, dt, m
+    return statistics.median(rates), side, dt, m, last
+
+
+# --------------------------------------------------------------------------- parts of the default line
+def crop_parity(dev, last, mjd, exptime, params, side):
+    """The device search of the crop the CPU baseline timed, against the
+    reference's search() result of that crop: threshold, tail fit, pooled null
+    peaks, detection map and refined candidates, bit for bit."""
+    ref, crop = last["result"], last["crop"]
+    got = dev.search(crop, mjd, exptime, **params)
+    cands = len(got["candidates"]) == len(ref["candidates"]) and all(
+        np.array_equal(a, b) and fa == fb for (a, fa), (b, fb) in zip(got["candidates"], ref["candidates"]))
+    checks = {"threshold": got["threshold"] == ref["threshold"] and got["method"] == ref["method"] and
+              (got["null_a"], got["null_k"], got["null_inv_s2"]) == (ref["null_a"], ref["null_k"], ref["null_inv_s2"]),
+              "null_peaks": bool(np.array_equal(got["null_peaks"], ref["null_peaks"])),
+              "max_snr": bool(np.array_equal(got["max_snr"], ref["max_snr"], equal_nan=True)),
+              "candidates": bool(cands)}
+    return {"equal": all(checks.values()), "crop": f"{side}x{side} of all {crop.shape[0]} frames",
+            "threshold": ref["threshold"], "null_peaks": int(len(ref["null_peaks"])),
+            "candidates": int(len(ref["candidates"])), "checks": checks}
+
+
+def lround(x):
+    """std::lround of doubles (halves away from zero), exactly."""
+    t = np.trunc(x)
+    return (t + np.sign(x) * (np.abs(x - t) >= 0.5)).astype(np.int32)
+
+
+def reference_cuda_measure(dev, frames, mjd, wl, grid):
+    """The reference's own CUDA backend (CudaBackend::run, backend_cuda.cu:99-195,
+    built for sm_100a from its sources) on one pass of the workload's frames with
+    the full motion grid, beside this backend's pass of the same frames
+    (ft_b200_stack_dev on the frames in HBM); both maps compared bit for bit.
+    Rates are adds per second of kernel time (the reference's own timing of its
+    kernel launches; CUDA events on the library stream here)."""
+    import math
+    import torch
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from ftoracle import Reference
+        R = Reference()
+        if not R.cuda_available():
+            return {"unavailable": "the reference CUDA backend sees no device"}
+    except Exception as e:  # the reference build is test infrastructure; report, do not fail the bench
+        return {"unavailable": f"reference build: {e}"}
+    n, h, w = frames.shape
+    mjd = np.asarray(mjd, np.float64)
+    t_h = (mjd - 0.5 * (mjd[0] + mjd[-1])) * 24.0
+    grid = np.ascontiguousarray(grid, np.float64)
+    m = grid.shape[0]
+    mc = max(3, int(math.ceil(0.7 * n)))
+    dx = np.ascontiguousarray(lround(grid[:, :1] * t_h[None, :]))
+    dy = np.ascontiguousarray(lround(grid[:, 1:] * t_h[None, :]))
+    ms = torch.empty((h, w), dtype=torch.float32, device=frames.device)
+    bv = torch.empty((h, w), dtype=torch.int32, device=frames.device)
+    dev.stack_dev(frames.data_ptr(), w, h, w, n, dx, dy, mc, ms.data_ptr(), bv.data_ptr())
+    dev.stack_dev(frames.data_ptr(), w, h, w, n, dx, dy, mc, ms.data_ptr(), bv.data_ptr())
+    ours = dict(dev.timings()).get("kernel")
+    host = frames.cpu().numpy()
+    t0 = time.perf_counter()
+    ref = R.stack_cuda_timed(host, t_h, grid, mc)
+    wall = time.perf_counter() - t0
+    equal = bool(np.array_equal(ref["max_snr"], ms.cpu().numpy(), equal_nan=True) and
+                 np.array_equal(ref["best_v"], bv.cpu().numpy()))
+    adds = float(m) * n * w * h
+    return {"kernel": "reference stack_kernel (backend_cuda.cu:55-72, cuda_stack_core.hpp:46-80), sm_100a",
+            "pass": f"{n} x {w} x {h} frames, {m} motions, min_count {mc} (one stacking pass)",
+            "value": adds / ref["kernel"], "unit": METRIC + " (kernel time)",
+            "seconds": {k: ref[k] for k in ("upload", "kernel", "download", "setup")}, "wall_s": wall,
+            "b200_value": adds / ours if ours else None, "b200_kernel_s": ours,
+            "speedup": ref["kernel"] / ours if ours else None, "bit_identical": equal}
+
+
+def batched_measure(dev, local_rank):
+    """The batched calibration workload: 30 x 2048^2 frames, 64 time-shuffled
+    null runs and 16 injection copies of 50 objects, all 81 passes batched into
+    persistent launches (ft_b200_search_batch_dev), beside the same search with
+    one pass per launch (passes_per_launch 1); one warm-up, then one of each."""
+    import torch
+    from fainttrail_b200 import synthetic
+    wl = synthetic.WORKLOADS["batched-2k"]
+    frames, mjd, exptime, _ = synthetic.generate(wl, seed=7, device=f"cuda:{local_rank}")
+    torch.cuda.synchronize()
+    n, h, w = frames.shape
+    copies = synthetic.injection_copies(wl, frames.shape, seed=11)
+    params = wl.search_params()
+
+    def run(**over):
+        r, _ = dev.search_batch_dev(frames.data_ptr(), w, h, w, n, mjd, exptime, copies, maps=False,
+                                    **dict(params, **over))
+        return r, dict(dev.timings()), dev.launches()
+    run()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    r, tm, nl = run()
+    rp, tmp, nlp = run(passes_per_launch=1)
+    clk = clocks.stop()
+    m = r["n_velocities"]
+    passes = 1 + wl.null_runs + len(copies)
+    adds = float(m) * n * w * h * passes
+    peaks, _ = measured_peaks()
+    fp32_peak = dev.info()[1] * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    achieved = adds / tm["kernel"] / 1e12
+    same = (r["threshold"] == rp["threshold"] and np.array_equal(r["null_peaks"], rp["null_peaks"]) and
+            r["peaks"] == rp["peaks"])
+    del frames
+    torch.cuda.empty_cache()
+    return {"workload": (f"batched-2k: {n} x {w} x {h} float32 frames, {wl.cadence_s:g} s cadence, rates "
+                         f"{wl.rate_px_min[0]:g}-{wl.rate_px_min[1]:g} px/min ({m} trial motions), {wl.null_runs} null "
+                         f"runs + {len(copies)} injection copies x {len(copies[0])} objects ({passes} searches)"),
+            "value": adds / tm["total"], "unit": METRIC, "ms_per_step": 1000.0 * tm["total"],
+            "searches_per_s": passes / tm["total"], "gpu_launches": nl, "threshold_snr": r["threshold"],
+            "plain": {"value": adds / tmp["total"], "ms_per_step": 1000.0 * tmp["total"],
+                      "searches_per_s": passes / tmp["total"], "gpu_launches": nlp,
+                      "path": "the same search, one pass per launch"},
+            "speedup_vs_plain": tmp["total"] / tm["total"], "bit_identical_to_plain": bool(same),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak, "kernel": "stack_batch_kernel"},
+            "clocks": clk}
 
 
 # --------------------------------------------------------------------------- arms
@@ -195,7 +328,7 @@ def reference_arm(args):
     frames_np = frames[:, :side_max, :side_max].cpu().numpy()
     del frames
     t0 = time.perf_counter()
-    rate, side, dt, m = reference_search_rate(wl, frames_np, mjd, exptime, steps=max(1, args.steps))
+    rate, side, dt, m, _ = reference_search_rate(wl, frames_np, mjd, exptime, steps=max(1, args.steps))
     cores = os.cpu_count()
     sample = (f"reference search() (prepare + real pass + {wl.null_runs} null runs, backend cpu) on a "
               f"{side} x {side} crop of all {wl.nframes} frames, full motion grid; {dt:.1f} s per step")
@@ -330,17 +463,25 @@ def b200_arm(args):
                "ms_per_step": 1000.0 * wall / args.e2e_steps}
         del host, host_np
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             frames_np = frames[:, :1024, :1024].cpu().numpy()
-            rate, side, dt, _ = reference_search_rate(wl, frames_np, mjd, exptime)
+            rate, side, dt, _, last = reference_search_rate(wl, frames_np, mjd, exptime)
             cpu = {"value": rate, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"reference search() with backend cpu on a {side} x {side} crop of all {n} frames, "
                              f"full motion grid, {wl.null_runs} null runs ({dt:.1f} s)"}
+            parity = crop_parity(dev, last, mjd, exptime, params, side)
         except Exception as e:  # the reference build is test infrastructure; report, do not fail the bench
             cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {e}"}
+    extras = {}
+    if world == 1 and not args.no_extras and not batched:
+        extras["reference_cuda"] = reference_cuda_measure(dev, frames, mjd, wl, r["grid"])
+        del frames
+        torch.cuda.empty_cache()
+        extras["batched"] = batched_measure(dev, local_rank)
+        extras["serving"] = serving_measure(args, local_rank)
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                "warmup": max(3, args.warmup), "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
@@ -359,6 +500,9 @@ def b200_arm(args):
                "stage_seconds_per_step": {k: v / args.steps for k, v in stage.items()},
                "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "gpu_launches": launches,
                "threshold_snr": r["threshold"], "threshold_method": r["method"]}
+        if parity is not None:
+            out["parity_vs_reference"] = parity
+        out.update(extras)
         if batched:
             out["config"]["batch"] = (f"{wl.null_runs} null runs + {len(copies)} injection copies x "
                                       f"{len(copies[0])} objects (S/N {wl.snr[0]:g}-{wl.snr[1]:g}); "
@@ -381,24 +525,28 @@ def result_digest(r):
     return (r["threshold"], r["method"], tuple(r["peaks"]), hs.hexdigest())
 
 
-def serving_arm(args, rank, local_rank, world, dist):
-    """The serving loop under a Poisson stream of uneven requests, beside the same
-    requests run one after another (first come, first served) through ft_b200_search."""
+def serving_measure(args, local_rank, rank=0, world=1, dist=None):
+    """The serving loop under a Poisson stream of uneven requests drawn from the
+    serving configuration (synthetic.serving_requests), beside the same requests
+    run one after another (first come, first served) through ft_b200_search.
+    Returns the measurements as a dict."""
     import torch
     import fainttrail_b200 as ftb
     from fainttrail_b200 import synthetic
-    reqs = synthetic.serving_requests(count=40, rate_per_s=20.0, seed=2024 + rank)
+    reqs, draws = synthetic.serving_requests(count=args.serve_requests, rate_per_s=20.0, seed=2024 + rank,
+                                             max_adds=args.serve_max_adds)
     inputs = []
     for k, (t_arr, wl) in enumerate(reqs):
         f, mjd, exptime, _ = synthetic.generate(wl, seed=100 + k, device=f"cuda:{local_rank}")
         inputs.append((t_arr, wl, f.cpu().numpy(), mjd, exptime))
         del f
+    torch.cuda.empty_cache()
     torch.cuda.synchronize()
     dev = ftb.Device(local_rank)
     # warm-up, then the plain sequential pass: each request alone, in arrival
     # order; its latency under the same arrival times follows from the measured
     # service times (one server, first come first served)
-    for t_arr, wl, f, mjd, exptime in inputs[:3]:
+    for t_arr, wl, f, mjd, exptime in inputs[:2]:
         dev.search(f, mjd, exptime, maps=True, **wl.search_params())
     service, alone, adds, phases = [], [], [], {}
     for t_arr, wl, f, mjd, exptime in inputs:
@@ -416,13 +564,15 @@ def serving_arm(args, rank, local_rank, world, dist):
         finish = max(finish, t_arr) + sv
         lat.append(finish - t_arr)
     plain_makespan = finish  # from the stream's start, as the served run
-    srv = ftb.Server(local_rank, 0.0, max_batch=16, workers=args.workers)
-    tk = [srv.submit(f, mjd, exptime, **wl.search_params()) for _, wl, f, mjd, exptime in inputs[:3]]
-    for t in tk:  # warm-up round on the server's own context
+    budget = 150.0e9
+    srv = ftb.Server(local_rank, budget, max_batch=16, workers=args.workers)
+    tk = [srv.submit(f, mjd, exptime, **wl.search_params()) for _, wl, f, mjd, exptime in inputs[:2]]
+    for t in tk:  # warm-up round on the server's own contexts
         srv.poll(t)
     srv.close()
+
     def served_run():
-        srv = ftb.Server(local_rank, 0.0, max_batch=16, workers=args.workers)
+        srv = ftb.Server(local_rank, budget, max_batch=16, workers=args.workers)
         if dist:
             dist.barrier()
         tickets = [None] * len(inputs)
@@ -464,32 +614,41 @@ def serving_arm(args, rank, local_rank, world, dist):
     def pct(v, q):
         k = max(1, int(np.ceil(q * len(v))))
         return v[min(len(v), k) - 1]
+    cap = args.serve_max_adds
+    return {"workload": (f"serving: {len(inputs)} requests, Poisson arrivals at 20/s, frames "
+                         f"{min(i[1].nframes for i in inputs)}-{max(i[1].nframes for i in inputs)}, sizes "
+                         f"{min(i[1].width for i in inputs)}x{min(i[1].height for i in inputs)} to "
+                         f"{max(i[1].width for i in inputs)}x{max(i[1].height for i in inputs)}, rate ranges inside "
+                         f"0.1-3 px/min, 8-32 null runs, 30 s cadence, HBM budget 150 GB; drawn from the serving "
+                         f"configuration with requests above {cap:.0e} pixel-frame-motion adds drawn again "
+                         f"({draws - len(inputs)} of {draws} draws, {100.0 * (draws - len(inputs)) / draws:.0f} %, "
+                         f"redrawn)"),
+            "value": world * total_adds / makespan, "unit": METRIC, "ms_per_step": 1000.0 * makespan,
+            "searches_per_s": world * len(inputs) / makespan, "p50_s": st["p50_s"], "p99_s": st["p99_s"],
+            "rounds": st["rounds"], "mean_batch": st["mean_batch"], "workers": args.workers, "max_batch": 16,
+            "plain": {"value": total_adds / plain_makespan, "unit": METRIC,
+                      "searches_per_s": len(inputs) / plain_makespan, "p50_s": pct(lat_sorted, 0.5),
+                      "p99_s": pct(lat_sorted, 0.99), "service_s_sum": sum(service), "phase_seconds": phases,
+                      "path": "ft_b200_search per request, in arrival order"},
+            "speedup_vs_plain": plain_makespan / makespan,
+            "e2e": {"value": world * total_adds / makespan, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "clocks": clk, "completed": st["completed"], "gpu_launches": st["launches"],
+            "bit_identical_to_alone": min(sum(a == b for a, b in zip(r[2], alone)) for r in runs),
+            "requests": len(inputs), "served_makespans_s": spread}
+
+
+def serving_arm(args, rank, local_rank, world, dist):
+    """--workload serving: the serving measurement as its own line."""
+    out = serving_measure(args, local_rank, rank, world, dist)
     if rank == 0:
-        out = {"metric": METRIC, "value": world * total_adds / makespan, "unit": METRIC, "n_gpus": world,
-               "steps": 1, "warmup": 3, "ms_per_step": 1000.0 * makespan, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-               "data": "synthetic (seeded requests; sky/read/photon noise, stars, movers)",
-               "config": {"workload": (f"serving: {len(inputs)} requests, Poisson arrivals at 20/s, frames "
-                                       f"{min(i[1].nframes for i in inputs)}-{max(i[1].nframes for i in inputs)}, "
-                                       f"sizes up to {max(i[1].width for i in inputs)} x "
-                                       f"{max(i[1].height for i in inputs)}, rates 0.1-3 px/min, 8-32 null runs, "
-                                       f"each request at most 2e12 pixel-frame-motion adds"),
-                          "parallelism": f"independent request streams x{world}", "max_batch": 16,
-                          "workers": args.workers},
-               "searches_per_s": world * len(inputs) / makespan,
-               "p50_s": st["p50_s"], "p99_s": st["p99_s"], "rounds": st["rounds"], "mean_batch": st["mean_batch"],
-               "plain": {"value": total_adds / plain_makespan, "unit": METRIC,
-                         "searches_per_s": len(inputs) / plain_makespan, "p50_s": pct(lat_sorted, 0.5),
-                         "p99_s": pct(lat_sorted, 0.99), "service_s_sum": sum(service),
-                         "phase_seconds": phases,
-                         "path": "ft_b200_search per request, in arrival order"},
-               "speedup_vs_plain": plain_makespan / makespan,
-               "e2e": {"value": world * total_adds / makespan, "unit": METRIC, "h2d_bytes_per_step": h2d,
-                       "d2h_bytes_per_step": d2h},
-               "clocks": clk, "completed": st["completed"], "gpu_launches": st["launches"],
-               "bit_identical_to_alone": min(sum(a == b for a, b in zip(r[2], alone)) for r in runs),
-               "served_makespans_s": spread}
-        print(json.dumps(out), flush=True)
+        line = {"metric": METRIC, "value": out["value"], "unit": METRIC, "n_gpus": world, "steps": 1, "warmup": 2,
+                "ms_per_step": out["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded requests; sky/read/photon noise, stars, movers)",
+                "config": {"workload": out["workload"], "parallelism": f"independent request streams x{world}",
+                           "max_batch": 16, "workers": args.workers}}
+        line.update({k: v for k, v in out.items() if k not in ("workload", "value", "unit", "ms_per_step")})
+        print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
 

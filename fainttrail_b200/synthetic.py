@@ -152,16 +152,18 @@ def motion_count(span_h, vmin_pxh, vmax_pxh, grid_tol_px):
     return int(np.count_nonzero((v >= lo) & (v <= hi)))
 
 
-def serving_requests(count=40, rate_per_s=20.0, seed=2024, max_adds=2.0e12, max_frame_bytes=1 << 30):
-    """A seeded stream of search requests: Poisson arrivals at rate_per_s; frame
-    counts 8-120, sizes from 512 x 512 to 6000 x 4000, rate ranges inside
-    0.1-3 px/min, 8-32 null runs, 30 s cadence. Draws whose work (motions x
-    frames x pixels x passes) exceeds max_adds, or whose frames exceed
-    max_frame_bytes, are drawn again, which keeps the request mix servable on one
-    GPU (the unbounded mix reaches 1e17 adds for one request). Returns a list of
-    (arrival_s, Workload)."""
+def serving_requests(count=16, rate_per_s=20.0, seed=2024, max_adds=5.0e13):
+    """A seeded stream of search requests drawn from the serving configuration:
+    Poisson arrivals at rate_per_s; frame counts 8-120, widths 512-6000 and
+    heights 512-4000 (multiples of 16), a rate range [lo, hi] inside 0.1-3
+    px/min, 8-32 null runs; 30 s cadence and the half-pixel motion grid of the
+    other configurations. Draws whose work (motions x frames x pixels x passes)
+    exceeds max_adds are drawn again (max_adds None keeps every draw): the
+    unbounded mix has a median of about 2e14 and a tail to 2e16 adds per request,
+    over a thousand times what one GPU serves at 20 requests per second. Returns
+    ([(arrival_s, Workload)], draws made)."""
     rng = np.random.default_rng(seed)
-    out, t = [], 0.0
+    out, t, draws = [], 0.0, 0
     while len(out) < count:
         n = int(rng.integers(8, 121))
         w = int(rng.integers(512, 6001)) // 16 * 16
@@ -169,14 +171,13 @@ def serving_requests(count=40, rate_per_s=20.0, seed=2024, max_adds=2.0e12, max_
         lo = float(rng.uniform(0.1, 2.5))
         hi = float(rng.uniform(lo + 0.2, 3.0))
         runs = int(rng.integers(8, 33))
-        if 4.0 * n * w * h > max_frame_bytes:
-            continue
+        draws += 1
         span_h = (n - 1) * 30.0 / 3600.0
         m = motion_count(span_h, lo * 60.0, hi * 60.0, 0.125)
-        if float(m) * n * w * h * (1 + runs) > max_adds:
+        if max_adds is not None and float(m) * n * w * h * (1 + runs) > max_adds:
             continue
         t += float(rng.exponential(1.0 / rate_per_s))
         k = len(out)
         out.append((t, Workload(f"serve-{k}", w, h, n, 30.0, 30.0, max(20, w * h // 20000), 3, (5.0, 10.0),
                                 (lo, hi), runs)))
-    return out
+    return out, draws

@@ -21,8 +21,9 @@ def test_motion_count_equals_velocity_grid(oracle, span_h, vmin, vmax, tol):
 
 
 def test_serving_stream_is_seeded_and_bounded():
-    a = synthetic.serving_requests(count=12, seed=5)
-    b = synthetic.serving_requests(count=12, seed=5)
+    a, da = synthetic.serving_requests(count=12, seed=5)
+    b, db = synthetic.serving_requests(count=12, seed=5)
+    assert da == db >= 12
     assert [(t, w.width, w.height, w.nframes, w.rate_px_min, w.null_runs) for t, w in a] == \
            [(t, w.width, w.height, w.nframes, w.rate_px_min, w.null_runs) for t, w in b]
     times = [t for t, _ in a]
@@ -32,7 +33,10 @@ def test_serving_stream_is_seeded_and_bounded():
         assert 0.1 <= w.rate_px_min[0] < w.rate_px_min[1] <= 3.0 and 8 <= w.null_runs <= 32
         span = (w.nframes - 1) * 30.0 / 3600.0
         m = synthetic.motion_count(span, w.rate_px_min[0] * 60, w.rate_px_min[1] * 60, 0.125)
-        assert m * w.nframes * w.width * w.height * (1 + w.null_runs) <= 2.0e12
+        assert m * w.nframes * w.width * w.height * (1 + w.null_runs) <= 5.0e13
+    # without the work bound every draw is kept, in the same order
+    c, dc = synthetic.serving_requests(count=5, seed=5, max_adds=None)
+    assert dc == 5
 
 
 def test_bench_reads_profiled_traffic():
