@@ -1,13 +1,20 @@
 // The serving loop: search requests of any frame count, image size and motion
-// range arrive at any time; a worker thread admits them by the HBM budget and
-// runs them in rounds. A round prepares every admitted request (upload,
-// background, preprocessing, grid), rebuilds all their null runs, and stacks the
-// real and null passes of all of them together in persistent launches (one per
-// kernel shape), so their work shares the device; then each request's peaks,
-// artefact screen and threshold are finished and its result published. Requests
-// that arrive during a round are admitted at the next one, as memory frees up.
-// Every result is bit-identical to the same search run alone.
+// range arrive at any time. At submit a request's frames are copied into HBM
+// and stay resident there while it waits (as long as the resident stacks take
+// at most half of the HBM budget; beyond that a request waits in host memory).
+// Worker threads, each with its own context and stream, run steps: at every
+// step a worker first admits queued requests whose estimated device memory fits
+// what the admitted ones leave of the budget and prepares them (background,
+// preprocessing, grid), then takes up to max_batch passes -- real passes, null
+// runs with their rebuilt preprocessing -- from all its admitted requests in
+// turn and stacks them together in persistent launches, and finally publishes
+// every request whose passes are all done (peaks, artefact screen, threshold,
+// candidates) and frees its memory. A request that arrives while others are on
+// the GPU is admitted at the next step boundary, as memory frees up, and its
+// passes share launches with theirs. Every result is bit-identical to the same
+// search run alone.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -29,19 +36,32 @@ double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock:
 struct Server::Req {
     long long id = 0;
     int w = 0, h = 0, n = 0;
-    std::vector<float> frames;
+    std::vector<float> frames;  // host copy, when the frames are not resident
+    DevBuf resident;            // the frames in HBM (n x h x w), from submit until prepared
     std::vector<double> mjd, exptime;
     SearchParams p;
-    double t_submit = 0, t_done = 0;
-    bool done = false;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    bool done = false, failed = false;
     std::string error;
     SearchOut out;
-    size_t bytes() const {
-        const int runs = p.threshold_snr <= 0.0 ? std::max(0, p.null_runs) : 0;
+    int runs() const { return p.threshold_snr <= 0.0 ? std::max(0, p.null_runs) : 0; }
+    size_t item_bytes() const {
         const size_t plane = static_cast<size_t>(frame_pitch(w)) * h;
-        return SearchRequest::base_bytes(w, h, n) +
-               static_cast<size_t>(runs) * (sizeof(float) * (plane * n + 2 * plane) + 8 * static_cast<size_t>(w) * h);
+        return sizeof(float) * (plane * n + 2 * plane) + 8 * static_cast<size_t>(w) * h;
     }
+    // device bytes while admitted: the prepared request and up to `items` passes in flight
+    size_t bytes(int items) const {
+        return SearchRequest::base_bytes(w, h, n) + static_cast<size_t>(std::min(runs(), items)) * item_bytes();
+    }
+};
+
+// An admitted request on a worker: its search state and the next pass to stack.
+struct Server::Active {
+    std::shared_ptr<Req> r;
+    std::unique_ptr<SearchRequest> s;
+    int next = 0;
+    bool real_staged = false;
+    size_t reserved = 0;
 };
 
 Server::Server(int device, double budget_bytes, int max_batch, int workers) : max_batch_(std::max(1, max_batch)) {
@@ -51,6 +71,8 @@ Server::Server(int device, double budget_bytes, int max_batch, int workers) : ma
     ctx_.push_back(std::make_unique<Context>(device, budget_bytes));
     for (int k = 1; k < workers; ++k)
         ctx_.push_back(std::make_unique<Context>(ctx_[0]->device(), ctx_[0]->account()));
+    // the context of the uploads at submit (its own stream), charging the same account
+    upload_ = std::make_unique<Context>(ctx_[0]->device(), ctx_[0]->account());
     for (auto& c : ctx_) {
         Context* cp = c.get();
         workers_.emplace_back([this, cp] { loop(*cp); });
@@ -74,7 +96,32 @@ long long Server::submit(const float* frames, int w, int h, int n, const double*
     r->w = w;
     r->h = h;
     r->n = n;
-    r->frames.assign(frames, frames + static_cast<size_t>(w) * h * n);
+    const size_t bytes = sizeof(float) * static_cast<size_t>(w) * h * n;
+    bool keep = false;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (resident_ + bytes <= upload_->budget() / 2) {
+            resident_ += bytes;
+            keep = true;
+        }
+    }
+    if (keep) {
+        // resident in HBM from now on; host memory if the device has no room after all
+        try {
+            std::lock_guard<std::mutex> ul(upload_mu_);
+            upload_->bind();
+            r->resident = DevBuf(upload_.get(), bytes, "resident frames");
+            FTB_CHECK(cudaMemcpyAsync(r->resident.as<float>(), frames, bytes, cudaMemcpyHostToDevice,
+                                      upload_->stream()));
+            FTB_CHECK(cudaStreamSynchronize(upload_->stream()));
+        } catch (const std::exception&) {
+            r->resident.reset();
+            std::lock_guard<std::mutex> lk(mu_);
+            resident_ -= bytes;
+            keep = false;
+        }
+    }
+    if (!keep) r->frames.assign(frames, frames + static_cast<size_t>(w) * h * n);
     r->mjd.assign(mjd, mjd + n);
     if (exptime) r->exptime.assign(exptime, exptime + n);
     r->p = p;
@@ -148,109 +195,160 @@ void Server::loop(Context& c) {
         c.bind();
     } catch (...) {
     }
+    std::vector<Active> active;
     for (;;) {
-        std::vector<std::shared_ptr<Req>> round;
-        size_t round_bytes = 0;
+        std::vector<std::shared_ptr<Req>> admitted;
         {
             std::unique_lock<std::mutex> lk(mu_);
             ++idle_;
-            cv_.wait(lk, [&] { return stop_ || (!paused_ && !queue_.empty()); });
-            if (stop_ && (queue_.empty() || paused_)) {
-                --idle_;
-                break;
-            }
-            // admission: the oldest requests whose device memory fits what the
-            // rounds in flight leave of the budget, the queue shared out among the
-            // idle workers; a request is admitted alone when nothing else runs
-            const int share = static_cast<int>((queue_.size() + idle_ - 1) / std::max(1, idle_));
-            const int cap = std::max(1, std::min(max_batch_, share));
-            const size_t budget = c.budget() > reserved_ ? c.budget() - reserved_ : 0;
-            size_t need = 0;
-            while (!queue_.empty() && static_cast<int>(round.size()) < cap) {
-                const size_t b = queue_.front()->bytes();
-                if (need + b > budget && !(round.empty() && reserved_ == 0)) break;
-                need += b;
-                round.push_back(queue_.front());
+            cv_.wait(lk, [&] { return stop_ || !active.empty() || (!paused_ && !queue_.empty()); });
+            --idle_;
+            if (stop_ && active.empty() && (queue_.empty() || paused_)) break;
+            // admission at every step: the oldest requests whose memory (prepared
+            // request plus a step's passes) fits what the admitted ones leave of
+            // the budget; a request is admitted alone when nothing else is
+            // the queue is shared out among this worker and the idle ones (at least one each)
+            const int share = static_cast<int>((queue_.size() + idle_) / (idle_ + 1));
+            int taken = 0;
+            while (!paused_ && !queue_.empty() && static_cast<int>(active.size() + admitted.size()) < max_batch_ &&
+                   taken < share) {
+                ++taken;
+                const size_t need = queue_.front()->bytes(max_batch_);
+                const size_t held = reserved_ + resident_;
+                const bool alone = reserved_ == 0 && active.empty() && admitted.empty();
+                if (held + need > c.budget() && !alone) break;
+                reserved_ += need;
+                admitted.push_back(queue_.front());
+                admitted.back()->t_admit = now_s();
                 queue_.pop_front();
             }
-            if (round.empty()) {  // waits for a round in flight to end
-                cv_.wait(lk);
-                --idle_;
+            if (active.empty() && admitted.empty()) {
+                cv_.wait(lk);  // memory held by other workers: wait for a step to end
                 continue;
             }
-            --idle_;
-            reserved_ += need;
-            round_bytes = need;
         }
-        run_round(c, round);
+        c.timing_reset();
+        // prepare the admitted requests (frames from HBM where resident)
+        for (auto& r : admitted) {
+            Active a;
+            a.r = r;
+            a.reserved = r->bytes(max_batch_);
+            try {
+                a.s = std::make_unique<SearchRequest>(c, r->p, r->w, r->h, r->n);
+                if (r->resident)
+                    a.s->prepare(r->resident.as<float>(), r->mjd.data(), r->exptime.empty() ? nullptr : r->exptime.data(),
+                                 true, r->w, false, {});
+                else
+                    a.s->prepare(r->frames.data(), r->mjd.data(), r->exptime.empty() ? nullptr : r->exptime.data(),
+                                 false, 0, false, {});
+                FTB_CHECK(cudaStreamSynchronize(c.stream()));
+            } catch (const std::exception& e) {
+                r->error = e.what();
+                a.s.reset();
+                cudaStreamSynchronize(c.stream());
+            }
+            release_frames(*r);
+            active.push_back(std::move(a));
+        }
+        // one step: up to max_batch passes from the admitted requests in turn,
+        // stacked together; each request's real pass goes with its first passes
+        std::vector<PassJob> jobs;
+        std::vector<std::array<int, 3>> ranges;  // (active index, k0, k1)
+        int quota = max_batch_;
+        const size_t margin = size_t{256} << 20;
+        bool progress = true;
+        std::vector<int> take(active.size(), 0);
+        while (quota > 0 && progress) {  // round-robin, one pass per request per turn
+            progress = false;
+            for (size_t k = 0; k < active.size() && quota > 0; ++k) {
+                Active& a = active[k];
+                if (!a.s || a.next + take[k] >= a.s->runs()) continue;
+                const size_t avail = c.budget() > c.used() + margin ? c.budget() - c.used() - margin : 0;
+                if (take[k] + 1 > 1 && (static_cast<size_t>(take[k]) + 1) * a.s->item_bytes() > avail) continue;
+                ++take[k];
+                --quota;
+                progress = true;
+            }
+        }
+        int requests_in_step = 0;
+        try {
+            for (size_t k = 0; k < active.size(); ++k) {
+                Active& a = active[k];
+                if (!a.s || a.r->failed) continue;
+                if (take[k] == 0 && a.real_staged) continue;
+                a.s->stage_items(a.next, a.next + take[k], {}, jobs);
+                ranges.push_back({static_cast<int>(k), a.next, a.next + take[k]});
+                a.real_staged = true;
+                ++requests_in_step;
+            }
+            if (!jobs.empty()) stack_passes_device(c, jobs);
+            for (const auto& rg : ranges) {
+                Active& a = active[static_cast<size_t>(rg[0])];
+                a.s->finish_items(rg[1], rg[2]);
+                a.next = rg[2];
+            }
+        } catch (const std::exception& e) {
+            cudaStreamSynchronize(c.stream());
+            for (const auto& rg : ranges) {
+                Active& a = active[static_cast<size_t>(rg[0])];
+                if (a.r->error.empty()) a.r->error = e.what();
+                a.r->failed = true;
+            }
+        }
+        // publish every request whose passes are all done (or that failed)
+        std::vector<Active> keep;
+        std::vector<std::shared_ptr<Req>> done;
+        size_t freed = 0;
+        for (auto& a : active) {
+            const bool finished = !a.s || a.r->failed || (a.real_staged && a.next >= a.s->runs());
+            if (!finished) {
+                keep.push_back(std::move(a));
+                continue;
+            }
+            if (a.s && !a.r->failed) {
+                try {
+                    a.r->out = a.s->finalize(nullptr);
+                } catch (const std::exception& e) {
+                    a.r->error = e.what();
+                }
+            }
+            a.s.reset();
+            cudaStreamSynchronize(c.stream());
+            freed += a.reserved;
+            done.push_back(a.r);
+        }
+        active.swap(keep);
         {
             std::lock_guard<std::mutex> lk(mu_);
             const double t = now_s();
-            for (auto& r : round) {
+            for (auto& r : done) {
                 r->t_done = t;
                 r->done = true;
                 if (r->error.empty()) latencies_.push_back(r->t_done - r->t_submit);
             }
-            last_done_ = t;
+            if (!done.empty()) last_done_ = t;
             launches_ += c.launches;
-            reserved_ -= round_bytes;
+            reserved_ -= freed;
             ++rounds_;
-            batched_ += static_cast<long long>(round.size());
+            batched_ += requests_in_step;
         }
-        done_cv_.notify_all();
-        cv_.notify_all();  // memory freed: a waiting worker may admit now
+        if (!done.empty()) done_cv_.notify_all();
+        cv_.notify_all();  // memory freed or a step ended: a waiting worker may admit now
     }
 }
 
-void Server::run_round(Context& c, std::vector<std::shared_ptr<Req>>& round) {
-    c.timing_reset();
-    std::vector<std::unique_ptr<SearchRequest>> rs(round.size());
-    for (size_t k = 0; k < round.size(); ++k) {
-        Req& r = *round[k];
-        try {
-            rs[k] = std::make_unique<SearchRequest>(c, r.p, r.w, r.h, r.n);
-            rs[k]->prepare(r.frames.data(), r.mjd.data(), r.exptime.empty() ? nullptr : r.exptime.data(), false, 0,
-                           false, {});
-        } catch (const std::exception& e) {
-            r.error = e.what();
-            rs[k].reset();
-            cudaStreamSynchronize(c.stream());
+void Server::release_frames(Req& r) {
+    if (r.resident) {
+        const size_t b = r.resident.bytes();
+        {
+            std::lock_guard<std::mutex> ul(upload_mu_);
+            r.resident.reset();
         }
+        std::lock_guard<std::mutex> lk(mu_);
+        resident_ -= b;
     }
-    try {
-        if (round.size() == 1 && rs[0]) {
-            // one request alone: its null runs in as many batches as the budget needs
-            SearchRequest& s = *rs[0];
-            const int items = s.runs();
-            const size_t avail = c.budget() > c.used() + (size_t{256} << 20) ? c.budget() - c.used() - (size_t{256} << 20) : 0;
-            const int per = static_cast<int>(std::max<size_t>(1, std::min<size_t>(std::max(items, 1), avail / s.item_bytes())));
-            for (int k0 = 0; k0 < std::max(items, 1); k0 += per) {
-                const int k1 = std::min(items, k0 + per);
-                std::vector<PassJob> jobs;
-                s.stage_items(k0, k1, {}, jobs);
-                stack_passes_device(c, jobs);
-                s.finish_items(k0, k1);
-            }
-        } else {
-            std::vector<PassJob> jobs;
-            for (auto& s : rs)
-                if (s) s->stage_items(0, s->runs(), {}, jobs);
-            stack_passes_device(c, jobs);  // every request's passes in shared launches
-            for (auto& s : rs)
-                if (s) s->finish_items(0, s->runs());
-        }
-        for (size_t k = 0; k < round.size(); ++k)
-            if (rs[k]) round[k]->out = rs[k]->finalize(nullptr);
-    } catch (const std::exception& e) {
-        cudaStreamSynchronize(c.stream());
-        for (size_t k = 0; k < round.size(); ++k)
-            if (rs[k] && round[k]->error.empty()) round[k]->error = e.what();
-    }
-    rs.clear();
-    for (auto& r : round) {
-        r->frames.clear();
-        r->frames.shrink_to_fit();
-    }
+    r.frames.clear();
+    r.frames.shrink_to_fit();
 }
 
 }  // namespace ftb

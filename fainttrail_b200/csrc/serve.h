@@ -1,5 +1,6 @@
-// The serving loop (serve.cu): a request queue, admission by the HBM budget,
-// and rounds in which all admitted requests' passes share persistent launches.
+// The serving loop (serve.cu): frames resident in HBM from submit, admission by
+// the HBM budget at every step, and steps in which the passes of all admitted
+// requests share persistent launches.
 #pragma once
 
 #include <condition_variable>
@@ -22,12 +23,14 @@ struct ServerStats {
 
 class Server {
 public:
-    // workers: rounds in flight at once, each on its own stream with an equal
-    // share of the budget, so one round's host phases (plans, peak sorting, the
-    // threshold fit) overlap another's kernels
+    // workers: steps in flight at once, each worker on its own stream charging
+    // the one budget, so one step's host phases (plans, peak sorting, the
+    // threshold fit) overlap another's kernels; max_batch: passes per step (and
+    // requests admitted per worker)
     Server(int device, double budget_bytes, int max_batch, int workers = 2);
     ~Server();
-    // copies the request; returns its id
+    // copies the request's frames into HBM (host memory when the resident stacks
+    // would take more than half the budget); returns its id
     long long submit(const float* frames, int w, int h, int n, const double* mjd, const double* exptime,
                      const SearchParams& p);
     // 0: done (out filled), 3: not done yet, 1: failed or unknown id (err filled).
@@ -38,11 +41,15 @@ public:
 
 private:
     struct Req;
+    struct Active;
     void loop(Context& c);
-    void run_round(Context& c, std::vector<std::shared_ptr<Req>>& round);
+    void release_frames(Req& r);
     std::vector<std::unique_ptr<Context>> ctx_;
+    std::unique_ptr<Context> upload_;  // uploads at submit, on their own stream
+    std::mutex upload_mu_;
+    size_t resident_ = 0;  // bytes of frames held in HBM for requests not yet prepared
     int max_batch_ = 16, idle_ = 0;
-    size_t reserved_ = 0;  // estimated device bytes of the rounds in flight
+    size_t reserved_ = 0;  // estimated device bytes of the admitted requests
     std::vector<std::thread> workers_;
     std::mutex mu_;
     std::condition_variable cv_, done_cv_;

@@ -401,21 +401,27 @@ int ft_b200_tile_shape(void);
 int ft_b200_tuned_shapes(int* keys, int* shapes, int cap);
 void ft_b200_clear_tuned_shapes(void);
 
-/* The serving loop. A server owns a device context and a worker thread; requests
- * (frames of any count and size, any motion range) are copied on submission,
- * admitted in arrival order as the HBM budget allows, and run in rounds: every
- * admitted request is prepared, its null runs rebuilt, and the real and null
- * passes of all of them are stacked together in shared persistent launches; a
- * request that arrives during a round joins the next one. Each result equals
- * ft_b200_search on the same request. This has no counterpart in the reference,
- * which runs one search at a time (search.cpp:716). max_batch caps the requests
- * per round. */
+/* The serving loop. A server owns worker threads, each with its own device
+ * context and stream; requests (frames of any count and size, any motion range)
+ * are copied into HBM on submission and stay resident there until they are
+ * prepared (in host memory instead while the resident frames would take more
+ * than half the HBM budget). Workers run steps: at every step a worker admits
+ * queued requests in arrival order as the HBM budget allows and prepares them,
+ * then stacks up to max_batch passes (real passes and null runs with their
+ * rebuilt preprocessing) taken in turn from all its admitted requests in shared
+ * persistent launches, and publishes the requests whose passes are all done. A
+ * request that arrives while others are on the GPU is admitted at the next step
+ * and its passes share launches with theirs. Each result equals ft_b200_search
+ * on the same request. This has no counterpart in the reference, which runs one
+ * search at a time (search.cpp:716). max_batch caps the passes per step and the
+ * requests a worker holds. */
 typedef struct ft_b200_server ft_b200_server;
 
-/* workers: rounds in flight at once (each on its own stream; <= 0: 2), so one
- * round's host work overlaps another's kernels. The workers share the HBM budget:
- * requests are admitted while their estimated memory fits what the rounds in
- * flight leave, and one that needs the whole budget runs alone. */
+/* workers: steps in flight at once (each on its own stream; <= 0: 2), so one
+ * step's host work overlaps another's kernels. The workers share the HBM budget:
+ * requests are admitted while their estimated memory (prepared frames plus a
+ * step's passes) fits what the admitted ones and the resident frames leave, and
+ * one that needs the whole budget runs alone. */
 int ft_b200_server_open(int device, double hbm_budget_bytes, int max_batch, int workers, ft_b200_server** out);
 /* Finishes the queued requests, then stops the worker. */
 void ft_b200_server_close(ft_b200_server* s);
@@ -431,8 +437,8 @@ const char* ft_b200_server_error(const ft_b200_server* s);
 /* Hold (1) or resume (0) admission; held requests queue up and start together. */
 int ft_b200_server_pause(ft_b200_server* s, int paused);
 /* Completed requests, their p50 / p99 latency (submit to done, seconds),
- * throughput (completed / time from first submit to last completion), rounds,
- * mean requests per round and kernels launched. */
+ * throughput (completed / time from first submit to last completion), steps
+ * (rounds), mean requests per step and kernels launched. */
 int ft_b200_server_stats(ft_b200_server* s, long long* completed, double* p50_s, double* p99_s,
                          double* searches_per_s, long long* rounds, double* mean_batch, long long* launches);
 

@@ -67,8 +67,8 @@ def test_server_batch_matches_standalone(device):
 
 
 def test_server_two_workers_share_the_queue(device):
-    """Two rounds in flight on two streams: the held queue is shared out, and
-    every result still equals the search run alone."""
+    """Two workers' steps in flight on two streams: the held queue is shared
+    out, and every result still equals the search run alone."""
     import fainttrail_b200 as ftb
     reqs = _requests()
     alone = [device.search(f, m, e, **kw) for f, m, e, kw in reqs]
@@ -124,4 +124,37 @@ def test_server_shared_budget_admits_as_memory_frees(device):
         srv.close()
     for a, b in zip(got, alone):
         _same(a, b)
-    assert st["completed"] == len(reqs) and st["rounds"] == len(reqs)
+    assert st["completed"] == len(reqs) and st["rounds"] >= len(reqs)
+
+
+def test_server_admits_during_a_long_request(device):
+    """Continuous batching: a short request submitted while a long one is being
+    stacked (thirty null runs, two passes per step) is admitted at the next step
+    boundary, its pass shares a launch with the long one's, and it is published
+    first; both results equal the searches run alone."""
+    import time
+    import fainttrail_b200 as ftb
+    g = golden("search_small.npz")
+    raw, mjd, exp = g["raw"], g["mjd"], g["exptime"]
+    long_kw = dict(fwhm_px=2.5, null_runs=30)
+    short_kw = dict(fwhm_px=2.5, threshold_snr=4.5)
+    short = raw[:, 10:, 10:].copy()
+    alone_long = device.search(raw, mjd, exp, **long_kw)
+    alone_short = device.search(short, mjd, exp, **short_kw)
+    srv = ftb.Server(0, 0.0, max_batch=2, workers=1)
+    try:
+        t_long = srv.submit(raw, mjd, exp, **long_kw)
+        t0 = time.perf_counter()
+        while srv.stats()["rounds"] < 1 and time.perf_counter() - t0 < 30:
+            time.sleep(0.001)
+        t_short = srv.submit(short, mjd, exp, **short_kw)
+        got_short = srv.poll(t_short)
+        long_pending = srv.poll(t_long, wait_ms=0)
+        got_long = long_pending if long_pending is not None else srv.poll(t_long)
+        st = srv.stats()
+    finally:
+        srv.close()
+    _same(got_long, alone_long)
+    _same(got_short, alone_short)
+    assert long_pending is None  # the short request finished while the long one was still stacking
+    assert st["completed"] == 2 and st["rounds"] >= 15
