@@ -327,6 +327,76 @@ int ftref_stack_cuda_timed(const float* frames, int w, int h, int n, const doubl
     }
 }
 
+// The reference's backend conformance procedure (the CLI's check-backend,
+// cli/main.cpp:697-741) for a registered backend `name`: a simulated 72 x 52 x 12
+// sequence against run_pass_naive, the same frames with a curved shift table,
+// and a 384 x 320 x 40 sequence against run_pass_simple, each judged by
+// check_backend (backend.cpp:281-314). Writes one line per check into `report`;
+// returns the number of checks that conform; *identical counts those whose maps
+// are also bit-identical; -1 on error.
+int ftref_check_backend(const char* name, char* report, int cap, int* checks, int* identical) {
+    try {
+        const std::unique_ptr<SearchBackend> cand = make_backend(name);
+        std::string text;
+        int ok = 0, same = 0, total = 0;
+        auto judge = [&](const char* what, const StackPass& pass, const StackResult& ref, const StackResult& got) {
+            const BackendCheck c = check_backend(pass, ref, got);
+            const bool bits = ref.best_v == got.best_v && ref.max_snr.data.size() == got.max_snr.data.size() &&
+                              std::memcmp(ref.max_snr.data.data(), got.max_snr.data.data(),
+                                          ref.max_snr.data.size() * sizeof(float)) == 0;
+            ++total;
+            ok += c.ok;
+            same += c.ok && bits;
+            text += std::string(what) + ": " + c.message + (bits ? ", bit-identical" : "") + "\n";
+        };
+        for (int round = 0; round < 2; ++round) {
+            SimParams sp;
+            sp.width = round == 0 ? 72 : 384;
+            sp.height = round == 0 ? 52 : 320;
+            sp.nframes = round == 0 ? 12 : 40;
+            sp.nstars = round == 0 ? 20 : 400;
+            sp.seed = 77 + static_cast<std::uint64_t>(round);
+            const SimResult sim = simulate(sp);
+            SearchParams p;
+            p.vmin_pxh = 2;
+            p.vmax_pxh = round == 0 ? 20 : 45;
+            const Prepared prep = prepare(sim.frames, p);
+            const auto grid = velocity_grid(prep, p);
+            StackPass pass;
+            pass.frames = &prep.filtered;
+            pass.t_h = &prep.t_h;
+            pass.velocities = &grid;
+            pass.min_count = std::max(3, static_cast<int>(std::ceil(p.min_coverage * prep.nframes)));
+            const StackResult got = cand->run(pass);
+            if (round == 0) {
+                judge("vs naive contract (72x52, 12 fr)", pass, run_pass_naive(pass), got);
+                ShiftTable curved = linear_shift_table(prep.t_h, grid);
+                for (int j = 0; j < curved.motions; ++j)
+                    for (int i = 0; i < curved.frames; ++i) {
+                        const double ti = prep.t_h[static_cast<std::size_t>(i)];
+                        curved.x(j, i) += static_cast<int>(std::lround(((j % 9) - 4) * 2.0 * ti * ti));
+                        curved.y(j, i) += static_cast<int>(std::lround(((j % 7) - 3) * 2.0 * ti * ti));
+                    }
+                StackPass cp = pass;
+                cp.shifts = &curved;
+                judge("curved shift table vs naive", cp, run_pass_naive(cp), cand->run(cp));
+            } else {
+                judge("vs simple reference (384x320, 40 fr)", pass, run_pass_simple(pass), got);
+            }
+        }
+        if (report && cap > 0) {
+            std::strncpy(report, text.c_str(), static_cast<std::size_t>(cap) - 1);
+            report[cap - 1] = 0;
+        }
+        if (checks) *checks = total;
+        if (identical) *identical = same;
+        return ok;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
 int ftref_cuda_available(void) { return cuda_backend_available(nullptr) ? 1 : 0; }
 
 // velocity_grid for a sequence of the given span. Returns the count (or -1);

@@ -202,6 +202,7 @@ class Reference:
                                   C.c_int, C.c_int, C.c_int, C.c_int, _f32p, _i32p]
         L.ftref_stack_cuda_timed.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.c_int, C.c_int,
                                              _f32p, _i32p, _f64p]
+        L.ftref_check_backend.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.ftref_velocity_grid.argtypes = [C.c_double, C.POINTER(FtParams), C.c_void_p, C.c_int,
                                           C.POINTER(C.c_double)]
         L.ftref_null_orders.argtypes = [_f64p, C.c_int, C.c_int, C.c_ulonglong, _f64p]
@@ -304,6 +305,16 @@ class Reference:
         if rc:
             raise RuntimeError(self.err())
         return ms, bv
+
+    def check_backend(self, name):
+        """The reference's check-backend procedure for backend `name`:
+        (conforming checks, checks, bit-identical checks, report text)."""
+        buf = C.create_string_buffer(4096)
+        total, same = C.c_int(), C.c_int()
+        ok = self.L.ftref_check_backend(name.encode(), buf, 4096, C.byref(total), C.byref(same))
+        if ok < 0:
+            raise RuntimeError(self.err())
+        return ok, total.value, same.value, buf.value.decode()
 
     def cuda_available(self):
         return bool(self.L.ftref_cuda_available())

@@ -48,3 +48,16 @@ def test_reference_search_with_b200_backend(ref_b200, seed, w, h, n, nmovers):
     compare(cpu, gpu)
     if n >= 24:
         assert len(cpu["candidates"]) > 0
+
+
+def test_reference_check_backend_conformance(ref_b200):
+    """The reference's own conformance procedure (check-backend: a 72 x 52 x 12
+    sequence against the naive contract, the same frames with a curved shift
+    table, a 384 x 320 x 40 sequence against the simple reference;
+    cli/main.cpp:697-741, backend.cpp:281-314) run on the "b200" backend: every
+    check conforms, and every map is bit-identical, not merely within the
+    contract's 1e-4 tolerance."""
+    ok, total, same, text = ref_b200.check_backend("b200")
+    assert total == 3 and ok == total and same == total, text
+    ok, total, same, text = ref_b200.check_backend("cpu")
+    assert ok == total == same == 3, text
