@@ -44,7 +44,8 @@ class SearchParams(C.Structure):
         ("static_exclude", C.c_int), ("null_runs", C.c_int), ("max_candidates", C.c_int), ("edge_px", C.c_int),
         ("threads", C.c_int), ("seed", C.c_ulonglong), ("null_tested", C.c_int), ("null_model_gauss", C.c_int),
         ("passes_per_launch", C.c_int), ("shard_index", C.c_int), ("shard_count", C.c_int),
-        ("calibrated_threshold", C.c_double), ("calibrated_tail", C.c_double * 4), ("align", C.c_int)]
+        ("calibrated_threshold", C.c_double), ("calibrated_tail", C.c_double * 4), ("align", C.c_int),
+        ("reg_dx", C.c_void_p), ("reg_dy", C.c_void_p)]
 
 
 ALIGN_MODES = {"off": 0, "check": 1, "auto": 2}
@@ -457,7 +458,15 @@ class Device:
                 raise ValueError(f"align must be one of {sorted(ALIGN_MODES)} (this backend does not resample "
                                  f"frames, so 'always' has no counterpart), not {kw['align']!r}")
             kw["align"] = ALIGN_MODES[kw["align"]]
+        # per-frame registration offsets: arrays kept alive with the parameters
+        reg = [kw.pop(k, None) for k in ("reg_dx", "reg_dy")]
+        if (reg[0] is None) != (reg[1] is None):
+            raise ValueError("registration offsets need both reg_dx and reg_dy")
         _set_fields(p, kw, "search")
+        if reg[0] is not None:
+            p._reg = [np.ascontiguousarray(a, dtype=np.float64) for a in reg]
+            p.reg_dx = p._reg[0].ctypes.data_as(C.c_void_p)
+            p.reg_dy = p._reg[1].ctypes.data_as(C.c_void_p)
         return p
 
     def check_registration(self, frames, t_h):

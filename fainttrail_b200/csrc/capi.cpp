@@ -370,7 +370,9 @@ void ft_b200_search_params_default(ft_b200_search_params* p) {
 }
 
 namespace {
-static ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
+// nframes: the frames of the search (for the per-frame registration offsets;
+// 0 where a call has no frames)
+static ftb::SearchParams to_search_params(const ft_b200_search_params* params, int nframes) {
     ft_b200_search_params d;
     ft_b200_search_params_default(&d);
     const ft_b200_search_params& q = params ? *params : d;
@@ -408,6 +410,12 @@ static ftb::SearchParams to_search_params(const ft_b200_search_params* params) {
     p.seed = q.seed;
     p.align = q.align;
     if (p.align < 0 || p.align > 2) throw std::runtime_error("search: align must be 0 (off), 1 (check) or 2 (auto)");
+    if ((q.reg_dx != nullptr) != (q.reg_dy != nullptr))
+        throw std::runtime_error("search: registration offsets need both reg_dx and reg_dy");
+    if (q.reg_dx && nframes > 0) {
+        p.reg_dx.assign(q.reg_dx, q.reg_dx + nframes);
+        p.reg_dy.assign(q.reg_dy, q.reg_dy + nframes);
+    }
     return p;
 }
 }  // namespace
@@ -419,7 +427,7 @@ int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height,
     return guarded(ctx, [&](ftb::Context& c) {
         if (!frames || !mjd || !out) throw std::runtime_error("search: missing frames, times or result pointer");
         auto r = std::make_unique<ft_b200_result>();
-        r->o = ftb::search_host(c, frames, width, height, nframes, mjd, exptime, to_search_params(params),
+        r->o = ftb::search_host(c, frames, width, height, nframes, mjd, exptime, to_search_params(params, nframes),
                                 wrap(progress, user));
         *out = r.release();
     });
@@ -448,7 +456,7 @@ static int search_batch_common(ft_b200_ctx* ctx, const float* frames, bool on_de
         }
         std::vector<ftb::SearchOut> outs;
         auto r = std::make_unique<ft_b200_result>();
-        r->o = ftb::search_batch_host(c, frames, width, height, nframes, mjd, exptime, to_search_params(params), sets,
+        r->o = ftb::search_batch_host(c, frames, width, height, nframes, mjd, exptime, to_search_params(params, nframes), sets,
                                       outs, wrap(progress, user), on_device, on_device ? pitch : width);
         std::vector<std::unique_ptr<ft_b200_result>> rs;
         for (auto& o : outs) {
@@ -485,7 +493,7 @@ int ft_b200_search_dev(ft_b200_ctx* ctx, const float* d_frames, int width, int h
         if (!d_frames || !mjd || !out) throw std::runtime_error("search: missing frames, times or result pointer");
         if (pitch < width) throw std::runtime_error("search: row pitch below the width");
         auto r = std::make_unique<ft_b200_result>();
-        r->o = ftb::search_host(c, d_frames, width, height, nframes, mjd, exptime, to_search_params(params), {}, true,
+        r->o = ftb::search_host(c, d_frames, width, height, nframes, mjd, exptime, to_search_params(params, nframes), {}, true,
                                 pitch);
         *out = r.release();
     });
@@ -536,7 +544,7 @@ int ft_b200_server_submit(ft_b200_server* s, const float* frames, int width, int
                           long long* request_id) {
     if (!s || !request_id) return FT_B200_ERROR;
     try {
-        *request_id = s->s->submit(frames, width, height, nframes, mjd, exptime, to_search_params(params));
+        *request_id = s->s->submit(frames, width, height, nframes, mjd, exptime, to_search_params(params, nframes));
         return FT_B200_OK;
     } catch (const std::exception& e) {
         s->error = e.what();
@@ -633,7 +641,7 @@ int ft_b200_completeness(ft_b200_ctx* ctx, const float* frames, int width, int h
             throw std::runtime_error("completeness: missing or malformed arguments");
         const std::vector<double> levels(snr_levels, snr_levels + nlevels);
         const ftb::CompletenessOut r = ftb::completeness_host(c, frames, width, height, nframes, mjd, exptime,
-                                                               to_search_params(params), levels, per_level,
+                                                               to_search_params(params, nframes), levels, per_level,
                                                                min_separation, seed);
         for (int k = 0; k < nlevels; ++k) {
             const ftb::CompletenessRow& q = r.rows[static_cast<size_t>(k)];
@@ -689,7 +697,7 @@ int ft_b200_null_threshold(const double* pooled, long long count, int runs, doub
     try {
         if (count < 0 || (count > 0 && !pooled)) throw std::runtime_error("null threshold: missing pooled peaks");
         if (runs < 0 || width < 1 || height < 1 || motions < 0) throw std::runtime_error("null threshold: bad sizes");
-        ftb::SearchParams p = to_search_params(params);
+        ftb::SearchParams p = to_search_params(params, 0);
         p.shard_index = 0;
         p.shard_count = 1;
         // the engine pools the S/N values as float; doubles that came from a result convert back exactly

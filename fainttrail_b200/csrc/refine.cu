@@ -91,6 +91,18 @@ __global__ void cutout_kernel(const double4* track, int K, int half, RefineDev d
     out[idx] = cnt == 0 ? CUDART_NAN_F : __fdiv_rn(acc, static_cast<float>(cnt));
 }
 
+// detector_flag (search.cpp:196-225): one warp per candidate, the largest S/N
+// of a source fixed on the detector near the track (track.cuh)
+__global__ void detector_kernel(const double4* track, int K, RefineDev d, const double* reg, const double* steps,
+                                int nsteps, double* best) {
+    const int k = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (k >= K) return;  // the whole warp
+    const double4 t = track[k];
+    const double b = detector_best_fixed(d.filt, d.plane, d.w, d.h, d.pitch, d.n, d.t, reg, reg + d.n, steps, nsteps,
+                                         t.x, t.y, t.z, t.w);
+    if ((threadIdx.x & 31) == 0) best[k] = b;
+}
+
 // field edge: frames whose track pixel has a blank (non-finite sub or static
 // sky, or outside) pixel within r; one thread per (candidate, frame)
 __global__ void edge_kernel(const double4* track, int K, int r, RefineDev d, int* near_blank) {
@@ -290,9 +302,15 @@ std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const S
     const int r_edge = static_cast<int>(std::ceil(2.0 * o.fwhm_px)) + 1;
     std::vector<float> cut(static_cast<size_t>(K) * size * size);
     std::vector<int> near_blank(static_cast<size_t>(K), 0);
+    // with registration offsets, the detector test's best fixed-position S/N
+    const bool reg = static_cast<int>(o.reg_dx.size()) == n && static_cast<int>(o.reg_dy.size()) == n;
+    const std::vector<double> steps = reg ? detector_steps(o.fwhm_px) : std::vector<double>();
+    std::vector<double> best_fixed(static_cast<size_t>(K), 0.0);
     {
         const size_t trb = align(sizeof(double4) * K), cb = align(sizeof(float) * cut.size()), eb = align(sizeof(int) * K);
-        DevBuf& buf = c.scratch(26, trb + cb + eb, "refine cutouts");
+        const size_t rb = reg ? align(sizeof(double) * (2 * static_cast<size_t>(n) + steps.size())) : 0;
+        const size_t bb = reg ? align(sizeof(double) * K) : 0;
+        DevBuf& buf = c.scratch(26, trb + cb + eb + rb + bb, "refine cutouts");
         unsigned char* base = buf.as<unsigned char>();
         std::vector<double4> tr(static_cast<size_t>(K));
         for (int k = 0; k < K; ++k) {
@@ -312,6 +330,20 @@ std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const S
         edge_kernel<<<static_cast<unsigned>((nedge + 127) / 128), 128, 0, s>>>(d_tr, K, r_edge, d, d_nb);
         FTB_CHECK(cudaGetLastError());
         ++c.launches;
+        if (reg) {
+            std::vector<double> rv(o.reg_dx);
+            rv.insert(rv.end(), o.reg_dy.begin(), o.reg_dy.end());
+            rv.insert(rv.end(), steps.begin(), steps.end());
+            double* d_reg = reinterpret_cast<double*>(base + trb + cb + eb);
+            double* d_best = reinterpret_cast<double*>(base + trb + cb + eb + rb);
+            FTB_CHECK(cudaMemcpyAsync(d_reg, rv.data(), sizeof(double) * rv.size(), cudaMemcpyHostToDevice, s));
+            const long long threads = 32LL * K;
+            detector_kernel<<<static_cast<unsigned>((threads + 127) / 128), 128, 0, s>>>(
+                d_tr, K, d, d_reg, d_reg + 2 * n, static_cast<int>(steps.size()), d_best);
+            FTB_CHECK(cudaGetLastError());
+            ++c.launches;
+            FTB_CHECK(cudaMemcpyAsync(best_fixed.data(), d_best, sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+        }
         FTB_CHECK(cudaMemcpyAsync(cut.data(), d_cut, sizeof(float) * cut.size(), cudaMemcpyDeviceToHost, s));
         FTB_CHECK(cudaMemcpyAsync(near_blank.data(), d_nb, sizeof(int) * K, cudaMemcpyDeviceToHost, s));
         FTB_CHECK(cudaStreamSynchronize(s));
@@ -376,7 +408,7 @@ std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const S
         if (n >= 8 && cd.max_frame_fraction > p.max_frame_fraction) flags.push_back("single");
         if (inside > 0 && nmasked > inside / 2) flags.push_back("masked");
         if (n > 0 && near_blank[static_cast<size_t>(k)] > std::max(1, n / 10)) flags.push_back("edge");
-        // detector: needs registration offsets, which registered input frames do not carry
+        if (reg && best_fixed[static_cast<size_t>(k)] >= 0.8 * cd.snr) flags.push_back("detector");
         if (std::hypot(t.bvx, t.bvy) > p.vmax_pxh - 0.5 * dv) flags.push_back("vedge");
         if (std::hypot(t.bvx, t.bvy) < 2.0 * o.fwhm_px / o.span_h) flags.push_back("slow");
         for (size_t i = 0; i < flags.size(); ++i) cd.flags += (i ? "," : "") + flags[i];

@@ -141,14 +141,19 @@ struct ArtArgs {
     int w, h, pitch, n, r;
     double max_frame_fraction;
     char* out;
+    const double* reg_dx;   // registration offsets by frame (null: no detector test)
+    const double* reg_dy;
+    const double* steps;    // detector_flag's grid of offsets
+    int nsteps;
 };
 
-// is_artefact_peak without registration offsets (search.cpp:229-243): the
-// single-frame share of the track's positive signal, then the field-edge test
-// (blank sub-frame or static-sky pixels within r of the track in more than
-// max(1, n/10) frames). One warp per peak: the lanes sample the frames and scan
-// the edge boxes; lane 0 adds the positive signal in frame order, as the
-// reference does.
+// is_artefact_peak (search.cpp:229-243): the single-frame share of the track's
+// positive signal, then the field-edge test (blank sub-frame or static-sky
+// pixels within r of the track in more than max(1, n/10) frames), then, with
+// registration offsets, the detector test (a source fixed on the sensor
+// explains at least 0.8 of the track's S/N). One warp per peak: the lanes
+// sample the frames, scan the edge boxes and share the detector grid; lane 0
+// adds the signal in frame order, as the reference does.
 constexpr int kArtWarps = 4;
 
 __global__ void __launch_bounds__(32 * kArtWarps) artefact_kernel(const ArtArgs a) {
@@ -198,7 +203,29 @@ __global__ void __launch_bounds__(32 * kArtWarps) artefact_kernel(const ArtArgs 
         }
         near_blank += __any_sync(0xffffffffu, blank) ? 1 : 0;
     }
-    if (lane == 0) a.out[k] = (near_blank > max(1, a.n / 10)) ? 1 : 0;
+    const bool edge = near_blank > max(1, a.n / 10);
+    if (edge || !a.reg_dx) {
+        if (lane == 0) a.out[k] = edge ? 1 : 0;
+        return;
+    }
+    // the track's S/N over all frames (track_snr, search.cpp:142-163)
+    double all = 0.0;
+    if (lane == 0) {
+        double sum = 0.0;
+        int count = 0;
+        for (int i = 0; i < a.n; ++i) {
+            const double d = vals[warp][i];
+            if (!isfinite(d)) continue;
+            sum = __dadd_rn(sum, d);
+            ++count;
+        }
+        all = count >= 3 ? __ddiv_rn(sum, __dsqrt_rn(static_cast<double>(count))) : 0.0;
+    }
+    all = __shfl_sync(0xffffffffu, all, 0);
+    const double best = detector_best_fixed(a.filtered, plane, a.w, a.h, a.pitch, a.n, a.t_h, a.reg_dx, a.reg_dy,
+                                            a.steps, a.nsteps, static_cast<double>(pk.x), static_cast<double>(pk.y),
+                                            vx, vy);
+    if (lane == 0) a.out[k] = best >= __dmul_rn(0.8, all) ? 1 : 0;
 }
 
 // Injection increments added in order: one CTA per frame walks its patches in
@@ -368,10 +395,18 @@ NullPeaks split_null_peaks(std::vector<Peak> raster, size_t keep, size_t tested)
     return out;
 }
 
+std::vector<double> detector_steps(double fwhm_px) {
+    std::vector<double> v;
+    const double span = std::max(2.0, 2.0 * fwhm_px);
+    for (double d = -span; d <= span; d += 0.5) v.push_back(d);
+    return v;
+}
+
 std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vector<ArtefactJob>& jobs,
                                                      const std::vector<std::pair<double, double>>& grid,
                                                      const float* d_sub, int w, int h, int n, double fwhm_px,
-                                                     double max_frame_fraction) {
+                                                     double max_frame_fraction, const std::vector<double>& reg_dx,
+                                                     const std::vector<double>& reg_dy) {
     std::vector<std::vector<char>> out(jobs.size());
     size_t total = 0;
     for (size_t k = 0; k < jobs.size(); ++k) {
@@ -383,7 +418,11 @@ std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vect
     // per job: its peaks and times, then one flag per peak; the grid once
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
     std::vector<size_t> off(jobs.size());
-    size_t bytes = al(sizeof(double) * 2 * grid.size());
+    // the grid, then the registration offsets and the detector steps (if any), then the jobs
+    const bool reg = static_cast<int>(reg_dx.size()) == n && static_cast<int>(reg_dy.size()) == n;
+    const std::vector<double> steps = reg ? detector_steps(fwhm_px) : std::vector<double>();
+    const size_t reg_off = al(sizeof(double) * 2 * grid.size());
+    size_t bytes = reg_off + (reg ? al(sizeof(double) * (2 * static_cast<size_t>(n) + steps.size())) : 0);
     for (size_t k = 0; k < jobs.size(); ++k) {
         off[k] = bytes;
         bytes += al(sizeof(PeakRec) * jobs[k].count) + al(sizeof(double) * n) + al(jobs[k].count);
@@ -392,6 +431,12 @@ std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vect
     unsigned char* base = buf.as<unsigned char>();
     std::vector<unsigned char> host(bytes);
     std::memcpy(host.data(), grid.data(), sizeof(double) * 2 * grid.size());
+    if (reg) {
+        double* r = reinterpret_cast<double*>(host.data() + reg_off);
+        std::memcpy(r, reg_dx.data(), sizeof(double) * n);
+        std::memcpy(r + n, reg_dy.data(), sizeof(double) * n);
+        std::memcpy(r + 2 * n, steps.data(), sizeof(double) * steps.size());
+    }
     for (size_t k = 0; k < jobs.size(); ++k) {
         PeakRec* r = reinterpret_cast<PeakRec*>(host.data() + off[k]);
         for (size_t q = 0; q < jobs[k].count; ++q) {
@@ -409,7 +454,14 @@ std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vect
         char* d_out = reinterpret_cast<char*>(b + al(sizeof(PeakRec) * jobs[k].count) + al(sizeof(double) * n));
         ArtArgs a{reinterpret_cast<const PeakRec*>(b), static_cast<int>(jobs[k].count),
                   reinterpret_cast<const double*>(base), jobs[k].d_filtered, d_sub, jobs[k].d_sky, d_t, w, h,
-                  frame_pitch(w), n, r, max_frame_fraction, d_out};
+                  frame_pitch(w), n, r, max_frame_fraction, d_out, nullptr, nullptr, nullptr, 0};
+        if (reg) {
+            const double* d_reg = reinterpret_cast<const double*>(base + reg_off);
+            a.reg_dx = d_reg;
+            a.reg_dy = d_reg + n;
+            a.steps = d_reg + 2 * n;
+            a.nsteps = static_cast<int>(steps.size());
+        }
         artefact_kernel<<<static_cast<unsigned>((jobs[k].count + kArtWarps - 1) / kArtWarps), 32 * kArtWarps, 0, s>>>(a);
         FTB_CHECK(cudaGetLastError());
         ++c.launches;
@@ -471,6 +523,14 @@ void SearchRequest::prepare(const float* frames, const double* mjd, const double
     for (int i = 0; i < n; ++i) o_.t_h.push_back((mjd[order[static_cast<size_t>(i)]] - o_.t_ref_mjd) * 24.0);
     if (exptime)
         for (int i = 0; i < n; ++i) exp_sorted_.push_back(exptime[order[static_cast<size_t>(i)]]);
+    if (!p_.reg_dx.empty() || !p_.reg_dy.empty()) {
+        if (static_cast<int>(p_.reg_dx.size()) != n || static_cast<int>(p_.reg_dy.size()) != n)
+            throw std::runtime_error("search: registration offsets need one (dx, dy) per frame");
+        for (int i = 0; i < n; ++i) {
+            o_.reg_dx.push_back(p_.reg_dx[static_cast<size_t>(order[static_cast<size_t>(i)])]);
+            o_.reg_dy.push_back(p_.reg_dy[static_cast<size_t>(order[static_cast<size_t>(i)])]);
+        }
+    }
 
     raw_ = DevBuf(&c, sizeof(float) * plane_ * n, "raw frames");
     sub_ = DevBuf(&c, sizeof(float) * plane_ * n, "background-subtracted frames");
@@ -661,8 +721,8 @@ void SearchRequest::finish_items(int k0, int k1) {
             jobs.push_back({&q.tested, q.tested.size(), it.filt.as<float>(), it.sky.as<float>(),
                             &orders_[static_cast<size_t>(k)]});
         }
-        const std::vector<std::vector<char>> art = device_artefacts_many(c, jobs, o_.grid, sub_.as<float>(), w, h, n,
-                                                                         o_.fwhm_px, p_.max_frame_fraction);
+        const std::vector<std::vector<char>> art = device_artefacts_many(
+            c, jobs, o_.grid, sub_.as<float>(), w, h, n, o_.fwhm_px, p_.max_frame_fraction, o_.reg_dx, o_.reg_dy);
         // pool_null_peaks (search.cpp:690-693): the screened peaks that are not
         // artefacts, then the rest, in descending S/N as the reference's list
         for (int k = k0; k < kn1; ++k) {

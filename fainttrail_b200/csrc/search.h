@@ -38,6 +38,10 @@ struct SearchParams {
     // 1 check, 2 auto (check; frames that are not registered are an error, as no
     // alignment is done here)
     int align = 0;
+    // registration offsets per frame (detector = registered + offset; the caller's
+    // frame order), from the FITS keywords REGDX / REGDY (types.hpp:61-65); empty:
+    // none, and the detector test of the artefact screen is off (search.cpp:196-225)
+    std::vector<double> reg_dx, reg_dy;
 };
 
 struct Peak {
@@ -140,10 +144,17 @@ struct ArtefactJob {
     const float* d_sky;
     const std::vector<double>* t_h;
 };
+// reg_dx / reg_dy: registration offsets in frame order (empty: no detector test)
 std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vector<ArtefactJob>& jobs,
                                                      const std::vector<std::pair<double, double>>& grid,
                                                      const float* d_sub, int w, int h, int n, double fwhm_px,
-                                                     double max_frame_fraction);
+                                                     double max_frame_fraction, const std::vector<double>& reg_dx,
+                                                     const std::vector<double>& reg_dy);
+
+// detector_flag's grid of offsets (search.cpp:217-220): -span, -span + 0.5, ...
+// while <= span, each step an addition of 0.5 as the reference's loop makes it,
+// span = max(2, 2 fwhm)
+std::vector<double> detector_steps(double fwhm_px);
 
 // An object injected into every frame of a copy (Injection, validate.hpp:18-23).
 struct Injection {
@@ -167,6 +178,7 @@ struct SearchOut {
     int w = 0, h = 0, n = 0;
     double fwhm_px = 0, span_h = 0, t_ref_mjd = 0, dv = 0;
     std::vector<double> t_h, background, sigma;
+    std::vector<double> reg_dx, reg_dy;  // registration offsets in time order (empty: none)
     std::vector<std::pair<double, double>> grid;
     Threshold thr;
     std::vector<double> null_peaks;      // pooled S/N of the null runs (search.hpp:177)

@@ -28,4 +28,50 @@ __device__ __forceinline__ float track_bilinear(const float* img, int w, int h, 
 // x + v t, rounded as the reference's track_pos
 __device__ __forceinline__ double track_coord(double x0, double v, double t) { return __dadd_rn(x0, __dmul_rn(v, t)); }
 
+// detector_flag (search.cpp:196-225) for one straight track, by a warp: the
+// largest S/N of a source fixed on the detector near the track's mean detector
+// position. Lane 0 forms the mean of (track position + registration offset) in
+// frame order; the lanes share the grid of offsets (steps x steps, dy outer),
+// each summing its frames' bilinear values in frame order; the maximum is
+// order-independent. Returns the maximum (0 if no position has 3 frames) to
+// every lane.
+__device__ __forceinline__ double detector_best_fixed(const float* filtered, size_t plane, int w, int h, int pitch,
+                                                      int n, const double* t_h, const double* reg_dx,
+                                                      const double* reg_dy, const double* steps, int nsteps,
+                                                      double bx, double by, double bvx, double bvy) {
+    const int lane = static_cast<int>(threadIdx.x & 31);
+    double mx = 0.0, my = 0.0;
+    if (lane == 0) {
+        for (int i = 0; i < n; ++i) {
+            mx = __dadd_rn(mx, __dadd_rn(track_coord(bx, bvx, t_h[i]), reg_dx[i]));
+            my = __dadd_rn(my, __dadd_rn(track_coord(by, bvy, t_h[i]), reg_dy[i]));
+        }
+        mx = __ddiv_rn(mx, static_cast<double>(n));
+        my = __ddiv_rn(my, static_cast<double>(n));
+    }
+    mx = __shfl_sync(0xffffffffu, mx, 0);
+    my = __shfl_sync(0xffffffffu, my, 0);
+    double best = 0.0;
+    for (int q = lane; q < nsteps * nsteps; q += 32) {
+        const double X = __dadd_rn(mx, steps[q % nsteps]), Y = __dadd_rn(my, steps[q / nsteps]);
+        double sum = 0.0;
+        int count = 0;
+        for (int i = 0; i < n; ++i) {
+            const float v = track_bilinear(filtered + i * plane, w, h, pitch, __dsub_rn(X, reg_dx[i]),
+                                           __dsub_rn(Y, reg_dy[i]));
+            if (!isfinite(v)) continue;
+            sum = __dadd_rn(sum, static_cast<double>(v));
+            ++count;
+        }
+        const double snr = count >= 3 ? __ddiv_rn(sum, __dsqrt_rn(static_cast<double>(count))) : 0.0;
+        best = best < snr ? snr : best;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double other = __shfl_xor_sync(0xffffffffu, best, o);
+        best = best < other ? other : best;
+    }
+    return best;
+}
+
 }  // namespace ftb

@@ -192,6 +192,13 @@ typedef struct ft_b200_search_params {
                               that are not registered are an error (the reference would
                               align them; this backend does not resample frames).
                               The check's outcome: ft_b200_result_registration. */
+    const double* reg_dx; /* per-frame registration offsets (detector = registered +
+                              offset), in the order the frames are passed, from the
+                              FITS keywords REGDX / REGDY (Frame::reg_dx, types.hpp:61-65);
+    */
+    const double* reg_dy; /* with them the artefact screen of the null runs and the
+                              candidates' flags include the detector test
+                              (detector_flag, search.cpp:196-225). NULL (default): none. */
 } ft_b200_search_params;
 
 void ft_b200_search_params_default(ft_b200_search_params* p);

@@ -177,8 +177,10 @@ int ftref_simulate(const ftref_sim* s, float* frames, double* mjd, double* expti
 }
 
 // prepare(): returns an opaque Prepared*.
-void* ftref_prepare(int n, int w, int h, const float* frames, const double* mjd, const double* exptime,
-                    const ft_params* params) {
+// prepare() of frames given as arrays; reg_dx / reg_dy (or NULL): per-frame
+// registration offsets, as load_frames() reads them from REGDX / REGDY.
+void* ftref_prepare_reg(int n, int w, int h, const float* frames, const double* mjd, const double* exptime,
+                        const double* reg_dx, const double* reg_dy, const ft_params* params) {
     try {
         std::vector<Frame> fr(static_cast<std::size_t>(n));
         const std::size_t plane = static_cast<std::size_t>(w) * h;
@@ -187,12 +189,62 @@ void* ftref_prepare(int n, int w, int h, const float* frames, const double* mjd,
             std::memcpy(fr[static_cast<std::size_t>(i)].image.data.data(), frames + i * plane, plane * sizeof(float));
             fr[static_cast<std::size_t>(i)].mjd_mid = mjd[i];
             fr[static_cast<std::size_t>(i)].exptime_s = exptime[i];
+            if (reg_dx && reg_dy) {
+                fr[static_cast<std::size_t>(i)].has_reg_offset = true;
+                fr[static_cast<std::size_t>(i)].reg_dx = reg_dx[i];
+                fr[static_cast<std::size_t>(i)].reg_dy = reg_dy[i];
+            }
         }
         SearchParams sp = to_search_params(params);
         return new Prepared(prepare(std::move(fr), sp));
     } catch (const std::exception& e) {
         g_err = e.what();
         return nullptr;
+    }
+}
+
+void* ftref_prepare(int n, int w, int h, const float* frames, const double* mjd, const double* exptime,
+                    const ft_params* params) {
+    return ftref_prepare_reg(n, w, h, frames, mjd, exptime, nullptr, nullptr, params);
+}
+
+// load_frames() of FITS files (newline-separated paths): with pixels NULL only
+// the sizes; else the pixels (n x h x w), mid-exposure MJD, exposure time and
+// registration offsets (has_reg = 1 when every frame carries REGDX / REGDY).
+int ftref_load_frames(const char* paths_nl, float* pixels, double* mjd, double* exptime, double* reg_dx,
+                      double* reg_dy, int* has_reg, int* w, int* h, int* n) {
+    try {
+        std::vector<std::string> paths;
+        std::string cur;
+        for (const char* c = paths_nl; *c; ++c) {
+            if (*c == '\n') {
+                if (!cur.empty()) paths.push_back(cur);
+                cur.clear();
+            } else {
+                cur += *c;
+            }
+        }
+        if (!cur.empty()) paths.push_back(cur);
+        const std::vector<Frame> fr = load_frames(paths);
+        *n = static_cast<int>(fr.size());
+        *w = fr.empty() ? 0 : fr[0].image.width;
+        *h = fr.empty() ? 0 : fr[0].image.height;
+        if (!pixels) return 0;
+        bool all = true;
+        const std::size_t plane = static_cast<std::size_t>(*w) * *h;
+        for (std::size_t i = 0; i < fr.size(); ++i) {
+            std::memcpy(pixels + i * plane, fr[i].image.data.data(), plane * sizeof(float));
+            mjd[i] = fr[i].mjd_mid;
+            exptime[i] = fr[i].exptime_s;
+            reg_dx[i] = fr[i].reg_dx;
+            reg_dy[i] = fr[i].reg_dy;
+            all = all && fr[i].has_reg_offset;
+        }
+        *has_reg = all ? 1 : 0;
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
     }
 }
 

@@ -192,6 +192,12 @@ class Reference:
         L.ftref_simulate_movers.argtypes = [C.POINTER(SimParams), _f64p, C.c_int, _f32p, _f64p, _f64p]
         L.ftref_prepare.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f64p, _f64p, C.POINTER(FtParams)]
         L.ftref_prepare.restype = C.c_void_p
+        L.ftref_prepare_reg.argtypes = [C.c_int, C.c_int, C.c_int, _f32p, _f64p, _f64p, C.c_void_p, C.c_void_p,
+                                        C.POINTER(FtParams)]
+        L.ftref_prepare_reg.restype = C.c_void_p
+        L.ftref_load_frames.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int)]
         L.ftref_prep_free.argtypes = [C.c_void_p]
         L.ftref_prep_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int)] * 3 + [C.POINTER(C.c_double)] * 3
         L.ftref_prep_vectors.argtypes = [C.c_void_p] + [C.c_void_p] * 5
@@ -364,14 +370,38 @@ class Reference:
                                          C.byref(s2))
         return thr, meth.value.decode(), a.value, k.value, s2.value
 
-    def prepare(self, frames, mjd, exptime, **kw):
+    def prepare(self, frames, mjd, exptime, reg_dx=None, reg_dy=None, **kw):
+        """prepare() (preprocess.cpp:528-585); reg_dx / reg_dy: per-frame
+        registration offsets (Frame::reg_dx, types.hpp:61-65) or None."""
         frames = _f32(frames)
         n, h, w = frames.shape
         p = self.params(**kw)
-        hp = self.L.ftref_prepare(n, w, h, frames, _f64(mjd), _f64(exptime), C.byref(p))
+        rx = ry = None
+        if reg_dx is not None:
+            rx, ry = _f64(reg_dx), _f64(reg_dy)
+        hp = self.L.ftref_prepare_reg(n, w, h, frames, _f64(mjd), _f64(exptime),
+                                      None if rx is None else rx.ctypes.data_as(C.c_void_p),
+                                      None if ry is None else ry.ctypes.data_as(C.c_void_p), C.byref(p))
         if not hp:
             raise RuntimeError(self.err())
         return Prepared(self, hp)
+
+    def load_frames(self, paths):
+        """load_frames() (fits.hpp:86) of FITS files: dict(frames, mjd, exptime,
+        reg_dx, reg_dy) with reg_dx / reg_dy None unless every frame has them."""
+        joined = "\n".join(paths).encode()
+        w, h, n, has = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        if self.L.ftref_load_frames(joined, None, None, None, None, None, C.byref(has), C.byref(w), C.byref(h),
+                                    C.byref(n)):
+            raise RuntimeError(self.err())
+        frames = np.empty((n.value, h.value, w.value), np.float32)
+        mjd, exp, rx, ry = (np.empty(n.value) for _ in range(4))
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        if self.L.ftref_load_frames(joined, ptr(frames), ptr(mjd), ptr(exp), ptr(rx), ptr(ry), C.byref(has),
+                                    C.byref(w), C.byref(h), C.byref(n)):
+            raise RuntimeError(self.err())
+        return dict(frames=frames, mjd=mjd, exptime=exp, reg_dx=rx if has.value else None,
+                    reg_dy=ry if has.value else None)
 
     def completeness(self, frames, mjd, exptime, snr_levels, per_level, min_separation, seed, **kw):
         """The reference's completeness() (validate.cpp:62-165) on raw frames."""
