@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(64) sky_kernel(const SkyArgs a) {
     sky_finish<W>(a, V, S, PF, T, t, m_all, pix, plane);
 }
 
-// The same for n <= N <= 64 with the sorted order from a bitonic network in
+// The same for n <= N <= 128 with the sorted order from a bitonic network in
 // registers instead of counting ranks: the pixel's values (non-finite ones as
 // +inf) are sorted with float min / max, which orders everything but the two
 // zeros; where a -0.0 is present the zero run is rewritten with the zeros in
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(64) sky_kernel(const SkyArgs a) {
 // Each rank's sorted position is then the lower bound of its value in the
 // sorted values plus the number of equal values of lower rank.
 template <int N>
-__global__ void __launch_bounds__(128) sky_net_kernel(const SkyArgs a) {
+__global__ void __launch_bounds__(N <= 64 ? 128 : 64) sky_net_kernel(const SkyArgs a) {
     constexpr int W = (N + 31) / 32;
     extern __shared__ unsigned char sm[];
     const int T = blockDim.x, t = threadIdx.x;
@@ -910,13 +910,13 @@ void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h,
         const int span = c.span_begin("static sky + residuals");
         SkyArgs a{d_sub, sc.residual.as<float>(), d_sky, tb.tab, tb.tab + n, w, h, pitch, n, exclude,
                   std::max(5, static_cast<int>(0.6 * n))};
-        // up to 64 frames: the sorting network; beyond: counted ranks
+        // up to 128 frames: the sorting network; beyond: counted ranks
         const int T = n <= 64 ? 128 : 64;
         const size_t smem = static_cast<size_t>(T) * n * 9;
-        auto kern = n <= 16   ? sky_net_kernel<16>
-                    : n <= 32 ? sky_net_kernel<32>
-                    : n <= 64 ? sky_net_kernel<64>
-                    : n <= 128 ? sky_kernel<4> : sky_kernel<8>;
+        auto kern = n <= 16    ? sky_net_kernel<16>
+                    : n <= 32  ? sky_net_kernel<32>
+                    : n <= 64  ? sky_net_kernel<64>
+                    : n <= 128 ? sky_net_kernel<128> : sky_kernel<8>;
         allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
         kern<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
         FTB_CHECK(cudaGetLastError());

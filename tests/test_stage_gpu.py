@@ -125,7 +125,7 @@ def bits_equal(a, b):
     return np.array_equal(na, nb) and np.array_equal(a.view(np.uint32)[~na], b.view(np.uint32)[~nb])
 
 
-@pytest.mark.parametrize("n,seed", [(9, 1), (20, 2), (31, 3), (40, 4), (64, 5), (65, 6)])
+@pytest.mark.parametrize("n,seed", [(9, 1), (20, 2), (31, 3), (40, 4), (64, 5), (65, 6), (100, 7), (129, 8)])
 def test_ties_and_signed_zeros(device, oracle, n, seed):
     """Small integer values with +0.0 and -0.0 among them: most sorted positions
     are ties, resolved by time rank as the reference's sort of (value, rank)
