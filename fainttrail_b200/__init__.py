@@ -126,6 +126,9 @@ def _declare(L):
     L.ft_b200_search_params_default.argtypes = [C.POINTER(SearchParams)]
     L.ft_b200_search.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p, C.POINTER(SearchParams),
                                  PROGRESS_FN, C.c_void_p, C.POINTER(C.c_void_p)]
+    L.ft_b200_search_tiled.argtypes = [C.c_void_p, _f32p, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
+                                       C.POINTER(SearchParams), C.c_int, PROGRESS_FN, C.c_void_p,
+                                       C.POINTER(C.c_void_p)]
     L.ft_b200_search_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, _f64p, _f64p,
                                      C.POINTER(SearchParams), C.POINTER(C.c_void_p)]
     L.ft_b200_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
@@ -514,6 +517,20 @@ class Device:
                                    None, C.byref(r))
         self.check(rc, "search")
         return self._result(r, w, h, maps, csv_path)
+
+    def search_tiled(self, frames, mjd, exptime, band_rows=0, progress=None, maps=True, **kw):
+        """The tiled search (ft_b200_search_tiled): the frames stay in host
+        memory and go to the device in bands of band_rows rows (0: 1024) with
+        their halos; the result equals search()'s."""
+        frames = np.ascontiguousarray(frames, dtype=np.float32)
+        n, h, w = frames.shape
+        p = self._search_params(self.L, kw)
+        r = C.c_void_p()
+        rc = self.L.ft_b200_search_tiled(self.h, frames, w, h, n, np.ascontiguousarray(mjd, dtype=np.float64),
+                                         np.ascontiguousarray(exptime, dtype=np.float64), C.byref(p), int(band_rows),
+                                         _progress(progress), None, C.byref(r))
+        self.check(rc, "search_tiled")
+        return self._result(r, w, h, maps)
 
     def search_batch(self, frames, mjd, exptime, copies, progress=None, maps=True, **kw):
         """ft_b200_search_batch: the search plus injection copies. `copies` is a

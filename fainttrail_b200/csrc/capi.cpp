@@ -433,6 +433,20 @@ int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height,
     });
 }
 
+int ft_b200_search_tiled(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
+                         const double* exptime, const ft_b200_search_params* params, int band_rows,
+                         ft_b200_progress_fn progress, void* user, ft_b200_result** out) {
+    if (out) *out = nullptr;
+    return guarded(ctx, [&](ftb::Context& c) {
+        if (!frames || !mjd || !out) throw std::runtime_error("search: missing frames, times or result pointer");
+        if (band_rows < 0) throw std::runtime_error("tiled search: band_rows must be 0 (automatic) or positive");
+        auto r = std::make_unique<ft_b200_result>();
+        r->o = ftb::search_tiled_host(c, frames, width, height, nframes, mjd, exptime,
+                                      to_search_params(params, nframes), band_rows, wrap(progress, user));
+        *out = r.release();
+    });
+}
+
 namespace {
 static int search_batch_common(ft_b200_ctx* ctx, const float* frames, bool on_device, int pitch, int width, int height,
                                int nframes, const double* mjd, const double* exptime, const ft_b200_search_params* params,

@@ -38,6 +38,7 @@ struct RefineDev {
     const double* t;
     size_t plane;
     int w, h, pitch, n;
+    int oy, rows;  // the frames hold rows [oy, oy + rows) of the w x h image
 };
 
 // one query per thread: the S/N of a straight track, optionally with the
@@ -54,12 +55,13 @@ __global__ void track_eval_kernel(const TrackQuery* q, int nq, RefineDev d, doub
         if (Q.which == 1 && t >= 0.0) continue;
         if (Q.which == 2 && t < 0.0) continue;
         const double px = track_coord(Q.x, Q.vx, t), py = track_coord(Q.y, Q.vy, t);
-        const float v = track_bilinear(d.filt + i * d.plane, d.w, d.h, d.pitch, px, py);
+        const float v = track_bilinear_band(d.filt + i * d.plane, d.w, d.h, d.pitch, d.oy, d.rows, px, py);
         if (per_frame) {
             per_frame[static_cast<size_t>(k) * d.n + i] = isfinite(v) ? v : CUDART_NAN_F;
             const int xi = static_cast<int>(lround(px)), yi = static_cast<int>(lround(py));
             masked[static_cast<size_t>(k) * d.n + i] =
-                xi >= 0 && yi >= 0 && xi < d.w && yi < d.h && d.mask[static_cast<size_t>(yi) * d.pitch + xi] == 0.0f;
+                xi >= 0 && yi >= 0 && xi < d.w && yi < d.h && yi - d.oy >= 0 && yi - d.oy < d.rows &&
+                d.mask[static_cast<size_t>(yi - d.oy) * d.pitch + xi] == 0.0f;
         }
         if (!isfinite(v)) continue;
         sum = __dadd_rn(sum, static_cast<double>(v));
@@ -83,7 +85,7 @@ __global__ void cutout_kernel(const double4* track, int K, int half, RefineDev d
         const double cx = track_coord(tr.x, tr.z, d.t[i]), cy = track_coord(tr.y, tr.w, d.t[i]);
         const double sx = __dsub_rn(__dadd_rn(cx, static_cast<double>(u)), static_cast<double>(half));
         const double sy = __dsub_rn(__dadd_rn(cy, static_cast<double>(v)), static_cast<double>(half));
-        const float s = track_bilinear(d.res + i * d.plane, d.w, d.h, d.pitch, sx, sy);
+        const float s = track_bilinear_band(d.res + i * d.plane, d.w, d.h, d.pitch, d.oy, d.rows, sx, sy);
         if (!isfinite(s)) continue;
         acc = __fadd_rn(acc, s);
         ++cnt;
@@ -98,8 +100,8 @@ __global__ void detector_kernel(const double4* track, int K, RefineDev d, const 
     const int k = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (k >= K) return;  // the whole warp
     const double4 t = track[k];
-    const double b = detector_best_fixed(d.filt, d.plane, d.w, d.h, d.pitch, d.n, d.t, reg, reg + d.n, steps, nsteps,
-                                         t.x, t.y, t.z, t.w);
+    const double b = detector_best_fixed(d.filt, d.plane, d.w, d.h, d.pitch, d.oy, d.rows, d.n, d.t, reg, reg + d.n,
+                                         steps, nsteps, t.x, t.y, t.z, t.w);
     if ((threadIdx.x & 31) == 0) best[k] = b;
 }
 
@@ -115,9 +117,9 @@ __global__ void edge_kernel(const double4* track, int K, int r, RefineDev d, int
     for (int dy = -r; dy <= r; ++dy)
         for (int dx = -r; dx <= r; ++dx) {
             const int xx = xi + dx, yy = yi + dy;
-            if (xx < 0 || yy < 0 || xx >= d.w || yy >= d.h ||
-                !isfinite(d.sub[i * d.plane + static_cast<size_t>(yy) * d.pitch + xx]) ||
-                !isfinite(d.sky[static_cast<size_t>(yy) * d.pitch + xx])) {
+            if (xx < 0 || yy < 0 || xx >= d.w || yy >= d.h || yy - d.oy < 0 || yy - d.oy >= d.rows ||
+                !isfinite(d.sub[i * d.plane + static_cast<size_t>(yy - d.oy) * d.pitch + xx]) ||
+                !isfinite(d.sky[static_cast<size_t>(yy - d.oy) * d.pitch + xx])) {
                 atomicAdd(near_blank + k, 1);
                 return;
             }
@@ -151,17 +153,18 @@ void finalise_flags(Candidate& c) {  // search.cpp:403-413
 
 }  // namespace
 
-std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const SearchParams& p, const RefineInputs& in) {
-    const std::vector<Peak>& keep = o.selected;
+std::vector<RefinedCandidate> refine_tracks(Context& c, const SearchOut& o, const SearchParams& p,
+                                            const RefineInputs& in, const std::vector<Peak>& keep) {
     const int K = static_cast<int>(keep.size());
-    std::vector<Candidate> out;
-    if (K == 0) return out;
+    std::vector<RefinedCandidate> rc(static_cast<size_t>(K));
+    if (K == 0) return rc;
     const int n = in.n;
     cudaStream_t s = c.stream();
     const double dv = o.dv;
     auto align = [](size_t b) { return (b + 255) / 256 * 256; };
-    RefineDev d{in.d_filt, in.d_res, in.d_sub, in.d_sky, in.d_mask, nullptr, static_cast<size_t>(in.pitch) * in.h,
-                in.w, in.h, in.pitch, n};
+    const int rows = in.band.rows > 0 ? in.band.rows : in.h;
+    RefineDev d{in.d_filt, in.d_res, in.d_sub, in.d_sky, in.d_mask, nullptr, static_cast<size_t>(in.pitch) * rows,
+                in.w, in.h, in.pitch, n, in.band.oy, rows};
 
     // the device times, then batches of track queries
     DevBuf& tb = c.scratch(24, align(sizeof(double) * n), "refine times");
@@ -350,11 +353,6 @@ std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const S
     }
 
     // the candidates (search.cpp:317-395)
-    struct Refined {
-        Candidate c;
-        std::vector<double> contrib;
-    };
-    std::vector<Refined> rc(static_cast<size_t>(K));
     double t2 = 0.0;
     for (double t : o.t_h) t2 += t * t;
     t2 /= std::max(1, n);
@@ -413,9 +411,15 @@ std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const S
         if (std::hypot(t.bvx, t.bvy) < 2.0 * o.fwhm_px / o.span_h) flags.push_back("slow");
         for (size_t i = 0; i < flags.size(); ++i) cd.flags += (i ? "," : "") + flags[i];
     }
+    return rc;
+}
 
+std::vector<Candidate> finish_candidates(const SearchOut& o, std::vector<RefinedCandidate> rc) {
+    const int n = o.n;
+    std::vector<Candidate> out;
     // duplicates and ghosts, flags, false-alarm rates, order, ids (:620-676)
-    std::sort(rc.begin(), rc.end(), [](const Refined& a, const Refined& b) { return a.c.snr > b.c.snr; });
+    std::sort(rc.begin(), rc.end(),
+              [](const RefinedCandidate& a, const RefinedCandidate& b) { return a.c.snr > b.c.snr; });
     const double r_overlap = 1.5 * o.fwhm_px;
     std::vector<bool> drop(rc.size(), false);
     auto pos = [&](const Candidate& cd, int f, double& x, double& y) {
@@ -466,6 +470,10 @@ std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const S
     });
     for (size_t i = 0; i < out.size(); ++i) out[i].id = static_cast<int>(i + 1);
     return out;
+}
+
+std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const SearchParams& p, const RefineInputs& in) {
+    return finish_candidates(o, refine_tracks(c, o, p, in, o.selected));
 }
 
 }  // namespace ftb

@@ -145,6 +145,7 @@ struct ArtArgs {
     const double* reg_dy;
     const double* steps;    // detector_flag's grid of offsets
     int nsteps;
+    int oy, rows;           // the frames are rows [oy, oy + rows) of the image (h rows)
 };
 
 // is_artefact_peak (search.cpp:229-243): the single-frame share of the track's
@@ -163,12 +164,12 @@ __global__ void __launch_bounds__(32 * kArtWarps) artefact_kernel(const ArtArgs 
     if (k >= a.count) return;  // the whole warp
     const PeakRec pk = a.peaks[k];
     const double vx = a.vel[2 * pk.vidx], vy = a.vel[2 * pk.vidx + 1];
-    const size_t plane = static_cast<size_t>(a.pitch) * a.h;
+    const size_t plane = static_cast<size_t>(a.pitch) * a.rows;
     for (int i = lane; i < a.n; i += 32) {
         const double t = a.t_h[i];
         const double px = __dadd_rn(static_cast<double>(pk.x), __dmul_rn(vx, t));
         const double py = __dadd_rn(static_cast<double>(pk.y), __dmul_rn(vy, t));
-        const float v = bilinear(a.filtered + i * plane, a.w, a.h, a.pitch, px, py);
+        const float v = track_bilinear_band(a.filtered + i * plane, a.w, a.h, a.pitch, a.oy, a.rows, px, py);
         vals[warp][i] = isfinite(v) ? static_cast<double>(v) : CUDART_NAN;
     }
     __syncwarp();
@@ -197,9 +198,9 @@ __global__ void __launch_bounds__(32 * kArtWarps) artefact_kernel(const ArtArgs 
         bool blank = false;
         for (int e = lane; e < box && !blank; e += 32) {
             const int xx = xi + e % side - a.r, yy = yi + e / side - a.r;
-            blank = xx < 0 || yy < 0 || xx >= a.w || yy >= a.h ||
-                    !isfinite(a.sub[i * plane + static_cast<size_t>(yy) * a.pitch + xx]) ||
-                    !isfinite(a.sky[static_cast<size_t>(yy) * a.pitch + xx]);
+            blank = xx < 0 || yy < 0 || xx >= a.w || yy >= a.h || yy - a.oy < 0 || yy - a.oy >= a.rows ||
+                    !isfinite(a.sub[i * plane + static_cast<size_t>(yy - a.oy) * a.pitch + xx]) ||
+                    !isfinite(a.sky[static_cast<size_t>(yy - a.oy) * a.pitch + xx]);
         }
         near_blank += __any_sync(0xffffffffu, blank) ? 1 : 0;
     }
@@ -222,9 +223,9 @@ __global__ void __launch_bounds__(32 * kArtWarps) artefact_kernel(const ArtArgs 
         all = count >= 3 ? __ddiv_rn(sum, __dsqrt_rn(static_cast<double>(count))) : 0.0;
     }
     all = __shfl_sync(0xffffffffu, all, 0);
-    const double best = detector_best_fixed(a.filtered, plane, a.w, a.h, a.pitch, a.n, a.t_h, a.reg_dx, a.reg_dy,
-                                            a.steps, a.nsteps, static_cast<double>(pk.x), static_cast<double>(pk.y),
-                                            vx, vy);
+    const double best = detector_best_fixed(a.filtered, plane, a.w, a.h, a.pitch, a.oy, a.rows, a.n, a.t_h,
+                                            a.reg_dx, a.reg_dy, a.steps, a.nsteps, static_cast<double>(pk.x),
+                                            static_cast<double>(pk.y), vx, vy);
     if (lane == 0) a.out[k] = best >= __dmul_rn(0.8, all) ? 1 : 0;
 }
 
@@ -406,7 +407,7 @@ std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vect
                                                      const std::vector<std::pair<double, double>>& grid,
                                                      const float* d_sub, int w, int h, int n, double fwhm_px,
                                                      double max_frame_fraction, const std::vector<double>& reg_dx,
-                                                     const std::vector<double>& reg_dy) {
+                                                     const std::vector<double>& reg_dy, Band band) {
     std::vector<std::vector<char>> out(jobs.size());
     size_t total = 0;
     for (size_t k = 0; k < jobs.size(); ++k) {
@@ -454,7 +455,8 @@ std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vect
         char* d_out = reinterpret_cast<char*>(b + al(sizeof(PeakRec) * jobs[k].count) + al(sizeof(double) * n));
         ArtArgs a{reinterpret_cast<const PeakRec*>(b), static_cast<int>(jobs[k].count),
                   reinterpret_cast<const double*>(base), jobs[k].d_filtered, d_sub, jobs[k].d_sky, d_t, w, h,
-                  frame_pitch(w), n, r, max_frame_fraction, d_out, nullptr, nullptr, nullptr, 0};
+                  frame_pitch(w), n, r, max_frame_fraction, d_out, nullptr, nullptr, nullptr, 0, band.oy,
+                  band.rows > 0 ? band.rows : h};
         if (reg) {
             const double* d_reg = reinterpret_cast<const double*>(base + reg_off);
             a.reg_dx = d_reg;

@@ -144,12 +144,18 @@ struct ArtefactJob {
     const float* d_sky;
     const std::vector<double>* t_h;
 };
-// reg_dx / reg_dy: registration offsets in frame order (empty: no detector test)
+// Rows [oy, oy + rows) of an image whose frames a step holds (rows 0: all).
+struct Band {
+    int oy = 0, rows = 0;
+};
+// reg_dx / reg_dy: registration offsets in frame order (empty: no detector test).
+// band: the device frames (d_sub and the jobs' filtered frames and sky) hold
+// these rows of the w x h image; peaks are in image coordinates.
 std::vector<std::vector<char>> device_artefacts_many(Context& c, const std::vector<ArtefactJob>& jobs,
                                                      const std::vector<std::pair<double, double>>& grid,
                                                      const float* d_sub, int w, int h, int n, double fwhm_px,
                                                      double max_frame_fraction, const std::vector<double>& reg_dx,
-                                                     const std::vector<double>& reg_dy);
+                                                     const std::vector<double>& reg_dy, Band band = {});
 
 // detector_flag's grid of offsets (search.cpp:217-220): -span, -span + 0.5, ...
 // while <= span, each step an addition of 0.5 as the reference's loop makes it,
@@ -203,10 +209,21 @@ struct RefineInputs {
     const float* d_sky;
     const float* d_mask;
     int w, h, pitch, n;
+    Band band;  // the frames hold these rows of the w x h image (rows 0: all)
 };
 // refine() of every selected peak and finish_candidates() (search.cpp:245-400,
 // 620-676): the candidate list, ordered and numbered as the reference's
 std::vector<Candidate> refine_candidates(Context& c, const SearchOut& o, const SearchParams& p, const RefineInputs& in);
+// The two halves: refine() of the peaks `keep` (refine_with_contrib, search.cpp:
+// 245-397; a band's peaks with that band's frames), then finish_candidates over
+// all of them (duplicates, ghosts, flags, false-alarm rates, order, ids).
+struct RefinedCandidate {
+    Candidate c;
+    std::vector<double> contrib;  // per-frame track values
+};
+std::vector<RefinedCandidate> refine_tracks(Context& c, const SearchOut& o, const SearchParams& p,
+                                            const RefineInputs& in, const std::vector<Peak>& keep);
+std::vector<Candidate> finish_candidates(const SearchOut& o, std::vector<RefinedCandidate> rc);
 
 // One search request in phases, so that the passes of several searches (or of
 // one search's null runs and copies) can be stacked in shared launches:
@@ -286,6 +303,12 @@ struct CompletenessOut {
 CompletenessOut completeness_host(Context& c, const float* frames, int w, int h, int n, const double* mjd,
                                   const double* exptime, const SearchParams& p, const std::vector<double>& levels,
                                   int per_level, double min_separation, uint64_t seed);
+
+// The tiled search (search_tiled, tiled.cpp:272-647) of host frames (n x h x w)
+// in full-width bands of band_rows core rows (0: 1024), for sequences larger
+// than HBM: the same result as search_host, bit for bit (tiled.cu).
+SearchOut search_tiled_host(Context& c, const float* frames, int w, int h, int n, const double* mjd,
+                            const double* exptime, const SearchParams& p, int band_rows, const Progress& progress);
 
 SearchOut search_batch_host(Context& c, const float* frames, int w, int h, int n, const double* mjd,
                             const double* exptime, const SearchParams& p,

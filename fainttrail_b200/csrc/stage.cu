@@ -290,6 +290,26 @@ __global__ void sample_kernel(const float* img, size_t plane, int w, int h, int 
     if (k < cap) out[static_cast<size_t>(f) * cap + k] = v;
 }
 
+// sample_kernel for a band of a larger image: the band holds image rows
+// [oy, oy + rows) (row y at img + (y - oy) * pitch); the grid is the whole
+// image's (columns border + i step, rows border + (j0 + j) step for the gh grid
+// rows inside the band's core), so the samples are those the whole image gives
+// in those rows.
+__global__ void sample_band_kernel(const float* img, size_t plane, int pitch, int n, int border, int step, int gw,
+                                   int j0, int gh, int oy, const float* mask, float* out, int cap, int* counts) {
+    const int f = blockIdx.y;
+    const long long g = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= static_cast<long long>(gw) * gh) return;
+    const int x = border + static_cast<int>(g % gw) * step;
+    const int y = border + (j0 + static_cast<int>(g / gw)) * step - oy;
+    const size_t pix = static_cast<size_t>(y) * pitch + x;
+    if (mask && mask[pix] == 0.0f) return;
+    const float v = img[f * plane + pix];
+    if (!finitef(v)) return;
+    const int k = atomicAdd(&counts[f], 1);
+    if (k < cap) out[static_cast<size_t>(f) * cap + k] = v;
+}
+
 __device__ __forceinline__ uint32_t order_key(float v) {
     const uint32_t b = __float_as_uint(v);
     return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
@@ -842,8 +862,9 @@ int sample_grid_points(int w, int h, int border) {
 }
 
 namespace {
-int filter_border(double fwhm_px) { return static_cast<int>(std::ceil(3 * fwhm_px * kFwhmToSigma)) + 1; }
 }  // namespace
+
+int filter_border(double fwhm_px) { return static_cast<int>(std::ceil(3 * fwhm_px * kFwhmToSigma)) + 1; }
 
 StageScratch::StageScratch(Context& c, int w, int h, int n, double fwhm_px) : w_(w), h_(h), n_(n) {
     const int pitch = frame_pitch(w);
@@ -860,6 +881,8 @@ StageScratch::StageScratch(Context& c, int w, int h, int n, double fwhm_px) : w_
 bool StageScratch::fits(int w, int h, int n, double fwhm_px) const {
     return w == w_ && h == h_ && n == n_ && sample_grid_points(w, h, filter_border(fwhm_px)) <= cap;
 }
+
+bool StageScratch::holds(int w, int h, int n) const { return w == w_ && h <= h_ && n == n_; }
 
 // The device tables of a stage in StageScratch::small: filter taps, per-frame
 // sigma, filter sigma, sample counts, cosmic-ray tallies, rank tables.
@@ -1079,6 +1102,164 @@ void prepare_sub(Context& c, StageScratch& sc, float* d_raw, float* d_sub, int w
         ++c.launches;
     c.span_end(span);
     if (h_bg) FTB_CHECK(cudaMemcpyAsync(h_bg, tb.sg, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+}
+
+// ------------------------------------------------------------------ bands (the tiled search)
+
+void stage_sky(Context& c, StageScratch& sc, const float* d_sub, int w, int rows, int n, const double* t_h,
+               int static_exclude, float* d_sky) {
+    if (!sc.holds(w, rows, n)) throw std::runtime_error("stage: scratch sized for another shape");
+    const int pitch = frame_pitch(w);
+    const long long npix = static_cast<long long>(w) * rows;
+    cudaStream_t s = c.stream();
+    const StageTables tb = stage_tables(sc, n);
+    std::vector<int> rank;
+    stage_time_ranks(t_h, n, rank);
+    const int exclude = static_exclude >= 0 ? static_exclude : std::max(1, static_cast<int>(std::lround(n / 8.0)));
+    std::vector<unsigned char> tab(2 * static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) {
+        tab[static_cast<size_t>(i)] = static_cast<unsigned char>(rank[static_cast<size_t>(i)]);
+        tab[static_cast<size_t>(n + rank[static_cast<size_t>(i)])] = static_cast<unsigned char>(i);
+    }
+    FTB_CHECK(cudaMemcpyAsync(tb.tab, tab.data(), tab.size(), cudaMemcpyHostToDevice, s));
+    const int span = c.span_begin("static sky + residuals");
+    SkyArgs a{d_sub, sc.residual.as<float>(), d_sky, tb.tab, tb.tab + n, w, rows, pitch, n, exclude,
+              std::max(5, static_cast<int>(0.6 * n))};
+    const int T = n <= 64 ? 128 : 64;
+    const size_t smem = static_cast<size_t>(T) * n * 9;
+    auto kern = n <= 16    ? sky_net_kernel<16>
+                : n <= 32  ? sky_net_kernel<32>
+                : n <= 64  ? sky_net_kernel<64>
+                : n <= 128 ? sky_net_kernel<128> : sky_kernel<8>;
+    allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
+    kern<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
+    FTB_CHECK(cudaGetLastError());
+    ++c.launches;
+    c.span_end(span);
+}
+
+void sample_band(Context& c, const float* d_img, size_t plane, int pitch, int n, int w, int h, int border, int oy,
+                 int core_y0, int core_y1, const float* d_mask, float* d_samples, int cap, int* d_counts) {
+    const int st = grid_step(w, h, border, 200000);
+    if (st <= 0) return;
+    const int gw = grid_count(border, w - border, st);
+    // the whole image's grid rows border + j st (< h - border) inside the core
+    const int lo = std::max(core_y0, border), hi = std::min(core_y1, h - border);
+    if (hi <= lo) return;
+    const int j0 = (lo - border + st - 1) / st;
+    const int j1 = (hi - border + st - 1) / st;
+    const int gh = j1 - j0;
+    if (gh <= 0 || gw <= 0) return;
+    const long long g = static_cast<long long>(gw) * gh;
+    sample_band_kernel<<<dim3(static_cast<unsigned>((g + 255) / 256), n), 256, 0, c.stream()>>>(
+        d_img, plane, pitch, n, border, st, gw, j0, gh, oy, d_mask, d_samples, cap, d_counts);
+    FTB_CHECK(cudaGetLastError());
+    ++c.launches;
+}
+
+void select_sigma(Context& c, const float* d_samples, int cap, const int* d_counts, int n, double* d_out,
+                  int unit_if_zero) {
+    robust_sigma_cluster_kernel<<<n * kSelCluster, 256, 0, c.stream()>>>(d_samples, cap, d_counts, d_out,
+                                                                          unit_if_zero);
+    FTB_CHECK(cudaGetLastError());
+    ++c.launches;
+}
+
+void select_median(Context& c, const float* d_samples, int cap, const int* d_counts, int n, double* d_out) {
+    median_cluster_kernel<<<n * kSelCluster, 256, 0, c.stream()>>>(d_samples, cap, d_counts, d_out);
+    FTB_CHECK(cudaGetLastError());
+    ++c.launches;
+}
+
+void sample_frames(Context& c, const float* d_frames, size_t plane, int pitch, int n, int w, int h, int border,
+                   float* d_samples, int cap, int* d_counts) {
+    const int st = grid_step(w, h, border, 200000);
+    if (st <= 0) return;
+    const int gw = grid_count(border, w - border, st), gh = grid_count(border, h - border, st);
+    const long long g = static_cast<long long>(gw) * gh;
+    if (g > cap) throw std::runtime_error("sample_frames: sample buffer too small");
+    sample_kernel<<<dim3(static_cast<unsigned>((g + 255) / 256), n), 256, 0, c.stream()>>>(
+        d_frames, plane, w, h, pitch, n, border, st, gw, gh, nullptr, d_samples, cap, d_counts);
+    FTB_CHECK(cudaGetLastError());
+    ++c.launches;
+}
+
+void subtract_grow(Context& c, float* d_raw, float* d_sub, int w, int rows, int n, const double* d_bg) {
+    const int pitch = frame_pitch(w);
+    const size_t plane = static_cast<size_t>(pitch) * rows;
+    const long long npix = static_cast<long long>(w) * rows;
+    const dim3 grid(static_cast<unsigned>((npix + 255) / 256), n);
+    subtract_kernel<<<grid, 256, 0, c.stream()>>>(d_raw, plane, w, rows, pitch, d_bg);
+    FTB_CHECK(cudaGetLastError());
+    grow_kernel<<<grid, 256, 0, c.stream()>>>(d_raw, d_sub, plane, w, rows, pitch, 3);
+    FTB_CHECK(cudaGetLastError());
+    c.launches += 2;
+}
+
+void stage_filter_given(Context& c, StageScratch& sc, int w, int rows, int n, const StageParams& sp,
+                        const double* d_sigma, const double* d_sg, float* d_filtered, float* d_mask) {
+    if (!sc.holds(w, rows, n)) throw std::runtime_error("stage: scratch sized for another shape");
+    const int pitch = frame_pitch(w);
+    const size_t plane = static_cast<size_t>(pitch) * rows;
+    const long long npix = static_cast<long long>(w) * rows;
+    cudaStream_t s = c.stream();
+    const StageTables tb = stage_tables(sc, n);
+    const double psf_sigma = sp.fwhm_px * kFwhmToSigma;
+    const int R = std::max(1, static_cast<int>(std::ceil(3.0 * psf_sigma)));
+    std::vector<float> taps(static_cast<size_t>(2 * R + 1));
+    double k2 = 0.0;
+    for (int i = -R; i <= R; ++i) {
+        const double v = std::exp(-0.5 * i * i / (psf_sigma * psf_sigma));
+        taps[static_cast<size_t>(i + R)] = static_cast<float>(v);
+        k2 += v * v;
+    }
+    if (taps.size() > 512) throw std::runtime_error("stage: PSF too wide");
+    FTB_CHECK(cudaMemcpyAsync(tb.taps, taps.data(), sizeof(float) * taps.size(), cudaMemcpyHostToDevice, s));
+    {
+        const int span = c.span_begin("scatter mask");
+        ScatterArgs a{sc.residual.as<float>(), d_sigma, sc.scatter.as<float>(), w, rows, pitch, n};
+        const int T = 128;
+        const size_t smem = static_cast<size_t>(T) * n * 4;
+        allow_dynamic_smem(reinterpret_cast<const void*>(scatter_kernel), smem);
+        scatter_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
+        FTB_CHECK(cudaGetLastError());
+        const int dil = std::max(1, static_cast<int>(std::lround(0.5 * sp.fwhm_px)));
+        mask_kernel<<<static_cast<unsigned>((npix + 255) / 256), 256, 0, s>>>(sc.scatter.as<float>(), d_mask, w, rows,
+                                                                              pitch, dil, sp.mask_scatter);
+        FTB_CHECK(cudaGetLastError());
+        c.launches += 2;
+        c.span_end(span);
+    }
+    {
+        const int span = c.span_begin("matched filter");
+        FTB_CHECK(cudaMemsetAsync(tb.cr, 0, sizeof(int) * n, s));
+        FilterArgs a;
+        a.residual = sc.residual.as<float>();
+        a.mask = d_mask;
+        a.scatter = sc.scatter.as<float>();
+        a.sigma = d_sigma;
+        a.out = d_filtered;
+        a.cr = tb.cr;
+        a.k = tb.taps;
+        a.norm = static_cast<float>(1.0 / k2);
+        a.wscat = static_cast<float>(sp.weight_scatter);
+        a.hit = static_cast<float>(sp.cr_sigma);
+        a.ratio = static_cast<float>(0.5 * std::exp(-0.5 / (psf_sigma * psf_sigma)));
+        a.clip = static_cast<float>(sp.clip_sigma);
+        a.w = w;
+        a.h = rows;
+        a.pitch = pitch;
+        a.R = R;
+        launch_filter_any(a, n, c.sms(), s);
+        ++c.launches;
+        c.span_end(span);
+    }
+    if (d_sg) {
+        rescale_kernel<<<dim3(static_cast<unsigned>((npix + 255) / 256), n), 256, 0, s>>>(d_filtered, plane, w, rows,
+                                                                                       pitch, d_sg);
+        FTB_CHECK(cudaGetLastError());
+        ++c.launches;
+    }
 }
 
 void frame_sample_stats(Context& c, const float* const* d_frames, int k, int w, int h, int pitch, float* d_samples,

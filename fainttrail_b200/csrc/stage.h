@@ -20,6 +20,7 @@ struct StageParams {
 struct StageScratch {
     StageScratch(Context& c, int w, int h, int n, double fwhm_px);
     bool fits(int w, int h, int n, double fwhm_px) const;
+    bool holds(int w, int h, int n) const;  // a band of at most h rows
     DevBuf residual, scatter, samples, small;
     int cap = 0;  // samples per frame
     int w_ = 0, h_ = 0, n_ = 0;
@@ -53,5 +54,31 @@ void stage_run(Context& c, StageScratch& sc, const float* d_sub, int w, int h, i
 // holds k * cap floats, cap >= sample_grid_points(w, h, 0).
 void frame_sample_stats(Context& c, const float* const* d_frames, int k, int w, int h, int pitch, float* d_samples,
                         int cap, int* d_counts, double* d_stats);
+
+// ---- bands of a larger image (the tiled search): frames of `rows` rows, the
+// per-frame quantities of the whole image given or sampled at its grid.
+int filter_border(double fwhm_px);  // ceil(3 sigma_psf) + 1
+// static sky and residuals (into sc.residual) only
+void stage_sky(Context& c, StageScratch& sc, const float* d_sub, int w, int rows, int n, const double* t_h,
+               int static_exclude, float* d_sky);
+// the samples sample_pixels(…, 200000, mask, border) takes from the w x h image
+// in its rows [core_y0, core_y1), read from a band holding rows [oy, oy + band
+// rows); appended to d_samples (n x cap) and d_counts
+void sample_band(Context& c, const float* d_img, size_t plane, int pitch, int n, int w, int h, int border, int oy,
+                 int core_y0, int core_y1, const float* d_mask, float* d_samples, int cap, int* d_counts);
+// the same for whole frames (n x h x pitch, plane apart)
+void sample_frames(Context& c, const float* d_frames, size_t plane, int pitch, int n, int w, int h, int border,
+                   float* d_samples, int cap, int* d_counts);
+// per-frame robust sigma (unit_if_zero: 1.0 where not > 0, the noise rule) and
+// median of accumulated samples, into device doubles
+void select_sigma(Context& c, const float* d_samples, int cap, const int* d_counts, int n, double* d_out,
+                  int unit_if_zero);
+void select_median(Context& c, const float* d_samples, int cap, const int* d_counts, int n, double* d_out);
+// background subtraction with per-frame backgrounds (device) and blank growth by 3
+void subtract_grow(Context& c, float* d_raw, float* d_sub, int w, int rows, int n, const double* d_bg);
+// scatter, mask and matched filter of sc.residual with the noise given (device);
+// with d_sg, normalised by it, else left unnormalised
+void stage_filter_given(Context& c, StageScratch& sc, int w, int rows, int n, const StageParams& sp,
+                        const double* d_sigma, const double* d_sg, float* d_filtered, float* d_mask);
 
 }  // namespace ftb

@@ -264,6 +264,21 @@ int ft_b200_null_threshold(const double* pooled, long long count, int runs, doub
 int ft_b200_search(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
                    const double* exptime, const ft_b200_search_params* params, ft_b200_progress_fn progress,
                    void* user, ft_b200_result** out);
+
+/* The tiled search (search_tiled, tiled.cpp:272-647; FrameSource tiled.hpp:42-54)
+ * for sequences larger than HBM: the frames (host, as ft_b200_search) stay in
+ * host memory and are uploaded in full-width bands of band_rows core rows (0:
+ * 1024) grown by the reference's halos -- the longest trial shift for the
+ * stacking, the filter and mask reach, the refinement's reach. The background,
+ * residual noise and filter normalisation of every frame are measured on the
+ * whole frame from the untiled search's sample positions, the bands' maps are
+ * assembled before peaks are found, and the null runs' artefact screen and the
+ * refinement run on bands in the whole image's coordinates: the result equals
+ * ft_b200_search's bit for bit (maps, null peaks, threshold, candidates). The
+ * registration check (align) is not run here; cosmic-ray counts are not kept. */
+int ft_b200_search_tiled(ft_b200_ctx* ctx, const float* frames, int width, int height, int nframes, const double* mjd,
+                         const double* exptime, const ft_b200_search_params* params, int band_rows,
+                         ft_b200_progress_fn progress, void* user, ft_b200_result** out);
 /* The same over frames already in device memory: d_frames holds nframes x height
  * rows of `pitch` floats (pitch >= width), is read only, and is copied in time
  * order. Synchronous; no progress callback. */
