@@ -277,6 +277,16 @@ int ft_b200_emulate_stack(const float* frames, int width, int height, int nframe
     }
 }
 
+int ft_b200_set_wait_test(int extra_bytes, long long wait_cycles) {
+    try {
+        ftb::set_wait_test(extra_bytes, wait_cycles);
+        return FT_B200_OK;
+    } catch (const std::exception& e) {
+        g_open_error = e.what();
+        return FT_B200_ERROR;
+    }
+}
+
 int ft_b200_plan_stats(int width, int height, int nframes, const int* dx, const int* dy, int motions, int shape,
                        long long* stats) {
     try {

@@ -121,6 +121,11 @@ bool stack_shape_fits(const StackConfig& c, int n);
 // (used when its windows fit).
 void set_stack_shape(int shape);
 int stack_shape();
+// Test of the bounded staging wait: every stacking launch's barrier expects
+// extra_bytes (> 0) that no copy brings, and its waits give up after
+// wait_cycles clock cycles with the error flag set; 0 restores the normal
+// launches (no extra bytes, a two-second limit).
+void set_wait_test(int extra_bytes, long long wait_cycles);
 
 // Device copy of a plan.
 struct StackPlanDev {

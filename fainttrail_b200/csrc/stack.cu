@@ -194,6 +194,16 @@ inline int roundup(int v, int q) { return (v + q - 1) / q * q; }
 
 namespace {
 std::atomic<int> g_shape{0};
+// a test of the bounded staging wait: extra bytes no copy brings, and the wait's limit
+std::atomic<int> g_wait_extra{0};
+std::atomic<long long> g_wait_cycles{4000000000LL};
+}
+
+void set_wait_test(int extra_bytes, long long wait_cycles) {
+    if (extra_bytes < 0 || extra_bytes > (1 << 20) || (extra_bytes > 0 && wait_cycles < 1000))
+        throw std::runtime_error("wait test: extra bytes in [0, 1 MiB] and a limit of at least 1000 cycles");
+    g_wait_cycles = extra_bytes > 0 ? wait_cycles : 4000000000LL;
+    g_wait_extra = extra_bytes;
 }
 
 void set_stack_shape(int shape) {
@@ -562,6 +572,8 @@ struct StackArgs {
     float* max_snr;
     int* best_v;
     int* err;
+    unsigned extra_tx;      // bytes the staging barrier expects beyond its copies (0; a test of the bounded wait)
+    long long wait_limit;   // clock cycles a staging wait may take
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -600,12 +612,13 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
 
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// Bounded wait on the staging barrier: about two seconds of clock, then the
-// kernel records an error and gives up (the host turns it into an exception).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
+// Bounded wait on the staging barrier: `limit` clock cycles (about two seconds
+// by default), then the kernel records an error and gives up (the host turns it
+// into an exception).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err, long long limit) {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > 4000000000LL) {
+        if (clock64() - t0 > limit) {
             atomicExch(err, 1);
             return false;
         }
@@ -842,7 +855,7 @@ __device__ __forceinline__ bool stage_group(const StackArgs& a, const StackGroup
         const uint32_t tab_bytes = static_cast<uint32_t>(G.tab_bytes);
         if (lane == 0) {
             *block_next = NW;  // blocks 0 .. NW-1 go to the warps in order
-            mbar_expect_tx(bar, static_cast<uint32_t>(G.rows_total * WP * 4) + tab_bytes);
+            mbar_expect_tx(bar, static_cast<uint32_t>(G.rows_total * WP * 4) + tab_bytes + a.extra_tx);
         }
         __syncwarp();
         if (lane == 0) bulk_load(offs, a.slot_off + a.slot_off_base[g], tab_bytes, bar);
@@ -852,7 +865,7 @@ __device__ __forceinline__ bool stage_group(const StackArgs& a, const StackGroup
                 tma_load_3d(win + (wv.row0 + b) * WP, tmap, x0 + wv.dx0, y0 + wv.dy0 + b, i, bar);
         }
     }
-    const bool ok = mbar_wait_bounded(bar, phase, err);
+    const bool ok = mbar_wait_bounded(bar, phase, err, a.wait_limit);
     if (__syncthreads_or(!ok)) return false;
     phase ^= 1u;
     return true;
@@ -1407,6 +1420,8 @@ void launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_desc, si
         a.max_snr = bp.max_snr;
         a.best_v = bp.best_v;
         a.err = d_err;
+        a.extra_tx = static_cast<unsigned>(g_wait_extra.load());
+        a.wait_limit = g_wait_extra.load() > 0 ? g_wait_cycles.load() : 4000000000LL;
         smem = std::max(smem, 256 + keys_bytes + static_cast<size_t>(plan.max_group_bytes));
         if (smem > static_cast<size_t>(plan.cfg.smem_bytes) + 256 + keys_bytes)
             throw std::runtime_error("stack plan exceeds shared memory");

@@ -118,6 +118,14 @@ int ft_b200_emulate_stack(const float* frames, int width, int height, int nframe
 int ft_b200_plan_stats(int width, int height, int nframes, const int* dx, const int* dy, int motions, int shape,
                        long long* stats);
 
+/* Test support for the stacking kernel's bounded waits (no counterpart in
+ * FaintTrail): with extra_bytes > 0 every later stacking launch in the process
+ * makes its staging barrier expect extra_bytes that no copy brings, so each
+ * wait gives up after wait_cycles clock cycles, sets the device error flag and
+ * the kernel returns; the pass then fails with "a device wait timed out" and the
+ * context stays usable. extra_bytes 0 restores normal launches. */
+int ft_b200_set_wait_test(int extra_bytes, long long wait_cycles);
+
 /* Parameters of the preprocessing stage; the defaults are SearchParams'
  * (include/fainttrail/search.hpp:18-90): static_exclude -1 (= max(1, lround(n/8))),
  * clip 8, cosmic-ray level 5, mask scatter 2.5, weight scatter 1.5. fwhm_px is the
