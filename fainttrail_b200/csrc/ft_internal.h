@@ -41,7 +41,8 @@ struct StackGroup {
 // the kernel). A block whose motions, in every frame, share the column shift and
 // lie within kRowSpread rows of one another is described per frame by one
 // 32-bit word: bits 0-15 the window offset of its lowest row, bits 16-23 each
-// slot's row above it (2 bits a slot), bits 24-25 the largest of those.
+// slot's row above it (2 bits a slot), bits 24-25 the largest of those, and,
+// when that is at most 1, bits 26-29 the slots' offsets as a 4-bit pattern.
 constexpr int kMotionBlock = 4;
 constexpr int kRowSpread = 3;
 

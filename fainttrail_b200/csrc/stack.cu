@@ -409,6 +409,8 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
                         smax = std::max(smax, dk);
                     }
                     d |= smax << 24;
+                    if (smax <= 1u)  // each slot's offset as one bit of a 4-bit pattern
+                        for (int k = 0; k < M; ++k) d |= ((d >> (16 + 2 * k)) & 1u) << (26 + k);
                     const size_t e = base + 2 * (static_cast<size_t>(i) * nb + static_cast<size_t>(q));
                     P.slot_off[e] = static_cast<uint16_t>(d & 0xffffu);
                     P.slot_off[e + 1] = static_cast<uint16_t>(d >> 16);
@@ -763,6 +765,18 @@ __device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
     return r;
 }
 
+// The adds of one frame for a block whose motions sit 0 or 1 row above the
+// block's base: bit k of PT is motion k's row offset.
+template <int PT, int H>
+__device__ __forceinline__ void add_pattern(uint64_t (&acc)[4][H], const uint64_t* A) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int dk = (PT >> k) & 1;  // a constant once the loop is unrolled
+#pragma unroll
+        for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q + dk]);
+    }
+}
+
 // One block of 4 motions of a rows_fast group for this thread's P pixels (one
 // column, P rows), frames in ascending order, on an interior tile. In every
 // frame the block's motions read one column of the window at row offsets
@@ -796,6 +810,22 @@ __device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const Stack
 #pragma unroll
         for (int r = 0; r < H; ++r) A[r] = pack2(src[r * WP], src[(r + H) * WP]);
         if (S >= 1u) A[H] = pack2(src[H * WP], src[P * WP]);
+        if (S <= 1u) {
+            // row offsets 0 or 1: one branch on the block's 4-bit pattern, each
+            // case a straight run of adds with fixed register pairs
+            switch ((d >> 26) & 15u) {
+#define FTB_PATTERN_CASE(PT) \
+    case PT:                 \
+        add_pattern<PT, H>(acc, A); \
+        break;
+                FTB_PATTERN_CASE(0) FTB_PATTERN_CASE(1) FTB_PATTERN_CASE(2) FTB_PATTERN_CASE(3)
+                FTB_PATTERN_CASE(4) FTB_PATTERN_CASE(5) FTB_PATTERN_CASE(6) FTB_PATTERN_CASE(7)
+                FTB_PATTERN_CASE(8) FTB_PATTERN_CASE(9) FTB_PATTERN_CASE(10) FTB_PATTERN_CASE(11)
+                FTB_PATTERN_CASE(12) FTB_PATTERN_CASE(13) FTB_PATTERN_CASE(14) FTB_PATTERN_CASE(15)
+#undef FTB_PATTERN_CASE
+            }
+            continue;
+        }
         if (S >= 2u) A[H + 1] = pack2(src[(H + 1) * WP], src[(P + 1) * WP]);
         if (S >= 3u) A[H + 2] = pack2(src[(H + 2) * WP], src[(P + 2) * WP]);
 #pragma unroll

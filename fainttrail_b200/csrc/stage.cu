@@ -65,6 +65,22 @@ __device__ __forceinline__ int sky_toggle(uint32_t (&ex)[W], int p) {
     return 1;
 }
 
+// Position of the k-th (0-based) set bit of x, k < popc(x): a binary search on
+// the population counts of halves.
+__device__ __forceinline__ int nth_set_bit(uint32_t x, int k) {
+    int pos = 0;
+    int c = __popc(x & 0xffffu);
+    if (k >= c) { k -= c; pos += 16; x >>= 16; }
+    c = __popc(x & 0xffu);
+    if (k >= c) { k -= c; pos += 8; x >>= 8; }
+    c = __popc(x & 0xfu);
+    if (k >= c) { k -= c; pos += 4; x >>= 4; }
+    c = __popc(x & 0x3u);
+    if (k >= c) { k -= c; pos += 2; x >>= 2; }
+    if (k >= static_cast<int>(x & 1u)) pos += 1;
+    return pos;
+}
+
 // The static sky and the leave-out residuals of one pixel from its values by
 // time rank (V, +inf where not finite), its m_all finite values in sorted order
 // (S) and each rank's sorted position (PF, 255 where not finite).
@@ -104,8 +120,8 @@ __device__ __forceinline__ void sky_finish(const SkyArgs& a, const float* V, con
                 const uint32_t valid = nb >= 32 ? 0xffffffffu : ((1u << nb) - 1u);
                 const uint32_t keep = ~ex[wd] & valid;
                 const int c = __popc(keep);
-                if (plo < 0 && lo < seen + c) plo = wd * 32 + static_cast<int>(__fns(keep, 0, lo - seen + 1));
-                if (phi < 0 && hi < seen + c) phi = wd * 32 + static_cast<int>(__fns(keep, 0, hi - seen + 1));
+                if (plo < 0 && lo < seen + c) plo = wd * 32 + nth_set_bit(keep, lo - seen);
+                if (phi < 0 && hi < seen + c) phi = wd * 32 + nth_set_bit(keep, hi - seen);
                 seen += c;
             }
             // double add of the two middle values (preprocess.cpp:198)

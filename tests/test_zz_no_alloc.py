@@ -82,7 +82,7 @@ def test_no_alloc_min_count_above_frame_count():
     L = _bind()
     O = Oracle()
     rng = np.random.default_rng(5)
-    n, h, w = 6, 40, 70
+    n, h, w = 6, 40, 72  # a row pitch of 288 bytes: a multiple of 16
     host = rng.standard_normal((n, h, w)).astype(np.float32)
     frames = torch.from_numpy(host).cuda()
     dx = rng.integers(-3, 4, (9, n)).astype(np.int32)
