@@ -63,7 +63,8 @@ struct StackConfig {         // one compiled kernel variant
     int bh = 4;              // TMA box height (rows)
     int mblock = 4;          // motions accumulated together in registers
     int merge = 0;           // 0: best/argmax per thread; 1: one shared maximum per tile (atomicMax)
-    int rows = 0;            // 1: the kernel reads row descriptors (blocks sharing a column)
+    int rows = 0;            // > 0: the kernel reads row descriptors (blocks sharing a column) whose
+                             // row offsets are at most this
     int smem_bytes = 200 * 1024;
 };
 

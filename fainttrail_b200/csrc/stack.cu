@@ -219,10 +219,10 @@ StackConfig stack_shape_config(int shape, int smem_optin) {
     c.bh = 4;
     c.smem_bytes = std::min(smem_optin - 1024, 224 * 1024);
     switch (shape) {
-        case 1: c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 12; c.rows = 1; break;
+        case 1: c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 12; c.rows = kRowSpread; break;
         case 2: c.tile_w = 64; c.wp = 72; c.p = 8; c.ty = 12; break;
-        case 3: c.tile_w = 32; c.wp = 40; c.p = 8; c.ty = 16; c.rows = 1; break;
-        case 4: c.tile_w = 32; c.wp = 40; c.p = 4; c.ty = 16; c.rows = 1; break;
+        case 3: c.tile_w = 32; c.wp = 40; c.p = 8; c.ty = 16; c.rows = kRowSpread; break;
+        case 4: c.tile_w = 32; c.wp = 40; c.p = 4; c.ty = 16; c.rows = kRowSpread; break;
         case 5:  // 32 x 16 with the shared maximum: 16 warps
             c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 16; c.merge = 1;
             c.smem_bytes -= 32 * 16 * 8;  // the keys sit ahead of the windows
@@ -231,7 +231,7 @@ StackConfig stack_shape_config(int shape, int smem_optin) {
             c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 14; c.merge = 1;
             c.smem_bytes -= 32 * 16 * 8;
             break;
-        case 7: c.tile_w = 32; c.wp = 40; c.p = 12; c.ty = 16; c.rows = 1; break;
+        case 7: c.tile_w = 32; c.wp = 40; c.p = 12; c.ty = 16; c.rows = 1; break;  // 128 registers: offsets 0 or 1
         default: throw std::runtime_error("stack: unknown tile shape");
     }
     return c;
@@ -315,6 +315,32 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
         if (real > 1 && (!fits || rows * WP + static_cast<long long>(roundup(M * n, 8)) / 2 > budget)) {
             for (int k = 0; k < M; ++k)
                 if (order[b + k] >= 0) blocks.insert(blocks.end(), {order[b + k], -1, -1, -1});
+        } else if (real > 1 && cfg.rows > 0 && cfg.rows < kRowSpread) {
+            // a kernel that takes smaller row offsets: consecutive runs of the
+            // block whose rows stay within cfg.rows in every frame
+            std::vector<int> run;
+            std::vector<int> lo(static_cast<size_t>(n)), hi(static_cast<size_t>(n));
+            auto close = [&]() {
+                for (int k = 0; k < M; ++k) blocks.push_back(k < static_cast<int>(run.size()) ? run[static_cast<size_t>(k)] : -1);
+                run.clear();
+            };
+            for (int k = 0; k < M; ++k) {
+                const int j = order[b + k];
+                if (j < 0) continue;
+                bool ok = !run.empty();
+                for (int i = 0; i < n && ok; ++i)
+                    ok = std::max(hi[static_cast<size_t>(i)], cdy(j, i)) - std::min(lo[static_cast<size_t>(i)], cdy(j, i)) <=
+                         cfg.rows;
+                if (!ok && !run.empty()) close();
+                if (run.empty())
+                    for (int i = 0; i < n; ++i) lo[static_cast<size_t>(i)] = hi[static_cast<size_t>(i)] = cdy(j, i);
+                for (int i = 0; i < n; ++i) {
+                    lo[static_cast<size_t>(i)] = std::min(lo[static_cast<size_t>(i)], cdy(j, i));
+                    hi[static_cast<size_t>(i)] = std::max(hi[static_cast<size_t>(i)], cdy(j, i));
+                }
+                run.push_back(j);
+            }
+            if (!run.empty()) close();
         } else {
             blocks.insert(blocks.end(), order.begin() + static_cast<long long>(b),
                           order.begin() + static_cast<long long>(b) + M);
@@ -382,7 +408,7 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
                     lo = std::min(lo, cdy(j, i));
                     hi = std::max(hi, cdy(j, i));
                 }
-                fast = fast && hi - lo <= kRowSpread;
+                fast = fast && hi - lo <= cfg.rows;
             }
         g.rows_fast = fast ? 1 : 0;
         g.tab_bytes = fast ? roundup(nb * n * 4, 16) : roundup(g.nslots * n * 2, 16);
@@ -741,39 +767,18 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
     }
 }
 
-// Packed pairs of floats: add.rn.f32x2 / mul.rn.f32x2 are two independent
-// round-to-nearest operations, bit-identical to two scalar ones.
-__device__ __forceinline__ uint64_t pack2(float lo, float hi) {
-    uint64_t r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
-    return r;
-}
-
-__device__ __forceinline__ void unpack2(uint64_t v, float& lo, float& hi) {
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-
-__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
-    uint64_t r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-
-__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
-    uint64_t r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-
+// Pairs of floats: __fadd2_rn / __fmul2_rn are two independent
+// round-to-nearest operations per call, bit-identical to two scalar ones
+// (__fadd_rn / __fmul_rn), issued as one paired instruction on sm_100.
 // The adds of one frame for a block whose motions sit 0 or 1 row above the
 // block's base: bit k of PT is motion k's row offset.
 template <int PT, int H>
-__device__ __forceinline__ void add_pattern(uint64_t (&acc)[4][H], const uint64_t* A) {
+__device__ __forceinline__ void add_pattern(float2 (&acc)[4][H], const float2* A) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const int dk = (PT >> k) & 1;  // a constant once the loop is unrolled
 #pragma unroll
-        for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q + dk]);
+        for (int q = 0; q < H; ++q) acc[k][q] = __fadd2_rn(acc[k][q], A[q + dk]);
     }
 }
 
@@ -786,18 +791,18 @@ __device__ __forceinline__ void add_pattern(uint64_t (&acc)[4][H], const uint64_
 // row q + P/2, and each pair is one add.rn.f32x2: register pair A[r] holds rows
 // (r, r + P/2), so motion k adds A[q + row offset] to its accumulator pair q
 // (rows P/2 .. P/2 + S - 1 are loaded twice, once for each pairing).
-template <int P, int WP>
+template <int P, int WP, int SMAX>
 __device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const StackGroup& G, int s0,
                                                  const float* __restrict__ win, const uint16_t* __restrict__ offs,
                                                  int tb, float inv_n, float (&best)[P], int (&arg)[P]) {
     constexpr int M = 4;
     constexpr int H = P / 2;
     static_assert(P % 2 == 0, "rows are paired");
-    uint64_t acc[M][H];
+    float2 acc[M][H];
 #pragma unroll
     for (int k = 0; k < M; ++k)
 #pragma unroll
-        for (int q = 0; q < H; ++q) acc[k][q] = 0ull;  // (+0.0f, +0.0f)
+        for (int q = 0; q < H; ++q) acc[k][q] = make_float2(0.0f, 0.0f);
     const int nb = G.nslots >> 2;
     const uint32_t* dp = reinterpret_cast<const uint32_t*>(offs) + (s0 >> 2);
     uint32_t dn = dp[0];
@@ -806,10 +811,10 @@ __device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const Stack
         if (i + 1 < a.n) dn = dp[(i + 1) * nb];
         const float* src = win + (d & 0xffffu) + tb;
         const uint32_t S = (d >> 24) & 3u;
-        uint64_t A[H + kRowSpread];
+        float2 A[H + SMAX];
 #pragma unroll
-        for (int r = 0; r < H; ++r) A[r] = pack2(src[r * WP], src[(r + H) * WP]);
-        if (S >= 1u) A[H] = pack2(src[H * WP], src[P * WP]);
+        for (int r = 0; r < H; ++r) A[r] = make_float2(src[r * WP], src[(r + H) * WP]);
+        if (S >= 1u) A[H] = make_float2(src[H * WP], src[P * WP]);
         if (S <= 1u) {
             // row offsets 0 or 1: one branch on the block's 4-bit pattern, each
             // case a straight run of adds with fixed register pairs
@@ -826,35 +831,37 @@ __device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const Stack
             }
             continue;
         }
-        if (S >= 2u) A[H + 1] = pack2(src[(H + 1) * WP], src[(P + 1) * WP]);
-        if (S >= 3u) A[H + 2] = pack2(src[(H + 2) * WP], src[(P + 2) * WP]);
+        if constexpr (SMAX >= 3) {  // row offsets up to 3 (the planner keeps SMAX)
+        if (S >= 2u) A[H + 1] = make_float2(src[(H + 1) * WP], src[(P + 1) * WP]);
+        if (S >= 3u) A[H + 2] = make_float2(src[(H + 2) * WP], src[(P + 2) * WP]);
 #pragma unroll
         for (int k = 0; k < M; ++k) {
             const uint32_t dk = (d >> (16 + 2 * k)) & 3u;
             if (dk == 0u) {
 #pragma unroll
-                for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q]);
+                for (int q = 0; q < H; ++q) acc[k][q] = __fadd2_rn(acc[k][q], A[q]);
             } else if (dk == 1u) {
 #pragma unroll
-                for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q + 1]);
+                for (int q = 0; q < H; ++q) acc[k][q] = __fadd2_rn(acc[k][q], A[q + 1]);
             } else if (dk == 2u) {
 #pragma unroll
-                for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q + 2]);
+                for (int q = 0; q < H; ++q) acc[k][q] = __fadd2_rn(acc[k][q], A[q + 2]);
             } else {
 #pragma unroll
-                for (int q = 0; q < H; ++q) acc[k][q] = add2(acc[k][q], A[q + 3]);
+                for (int q = 0; q < H; ++q) acc[k][q] = __fadd2_rn(acc[k][q], A[q + 3]);
             }
         }
+        }
     }
-    const uint64_t inv2 = pack2(inv_n, inv_n);
+    const float2 inv2 = make_float2(inv_n, inv_n);
 #pragma unroll
     for (int k = 0; k < M; ++k) {
         const int j = a.slot_motion[G.slot0 + s0 + k];
         if (j < 0) continue;
 #pragma unroll
         for (int q = 0; q < H; ++q) {
-            float lo, hi;
-            unpack2(mul2(acc[k][q], inv2), lo, hi);
+            const float2 sn = __fmul2_rn(acc[k][q], inv2);
+            const float lo = sn.x, hi = sn.y;
             if (lo > best[q] || (lo == best[q] && j < arg[q])) {
                 best[q] = lo;
                 arg[q] = j;
@@ -938,7 +945,7 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
         if (G.rows_fast) {
             if (interior) {
                 for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                    motion_quad_rows<P, WP>(a, G, s0, win, offs, tb, inv_n, best, arg);
+                    motion_quad_rows<P, WP, (P == 12 ? 1 : kRowSpread)>(a, G, s0, win, offs, tb, inv_n, best, arg);
             } else {
                 for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
                     motion_quad<P, WP, true, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
@@ -1149,20 +1156,20 @@ __device__ bool stack_tile_atom(const StackArgs& a, const CUtensorMap* tmap, int
 // both columns with one 64-bit shared load, an odd one with two 32-bit loads.
 
 template <int P, int WP>
-__device__ __forceinline__ void load_pairs(uint64_t (&v)[P], const float* __restrict__ src, uint32_t odd) {
+__device__ __forceinline__ void load_pairs(float2 (&v)[P], const float* __restrict__ src, uint32_t odd) {
     if (!odd) {
 #pragma unroll
-        for (int p = 0; p < P; ++p) v[p] = *reinterpret_cast<const uint64_t*>(src + p * WP);
+        for (int p = 0; p < P; ++p) v[p] = *reinterpret_cast<const float2*>(src + p * WP);
     } else {
 #pragma unroll
-        for (int p = 0; p < P; ++p) v[p] = pack2(src[p * WP], src[p * WP + 1]);
+        for (int p = 0; p < P; ++p) v[p] = make_float2(src[p * WP], src[p * WP + 1]);
     }
 }
 
 template <int P>
-__device__ __forceinline__ void add_pairs(uint64_t (&acc)[P], const uint64_t (&v)[P]) {
+__device__ __forceinline__ void add_pairs(float2 (&acc)[P], const float2 (&v)[P]) {
 #pragma unroll
-    for (int p = 0; p < P; ++p) acc[p] = add2(acc[p], v[p]);
+    for (int p = 0; p < P; ++p) acc[p] = __fadd2_rn(acc[p], v[p]);
 }
 
 // motion_quad for paired columns: x is the thread's first column
@@ -1173,11 +1180,11 @@ __device__ __forceinline__ void motion_quad2(const StackArgs& a, const StackGrou
                                              int (&arg)[P][2]) {
     constexpr int M = 4;
     constexpr int PW = (P + 3) / 4;
-    uint64_t acc[M][P];
+    float2 acc[M][P];
 #pragma unroll
     for (int k = 0; k < M; ++k)
 #pragma unroll
-        for (int p = 0; p < P; ++p) acc[k][p] = 0ull;  // (+0.0f, +0.0f)
+        for (int p = 0; p < P; ++p) acc[k][p] = make_float2(0.0f, 0.0f);
     int cfull[M] = {0, 0, 0, 0};
     uint32_t cpart[M][2][PW];
 #pragma unroll
@@ -1192,7 +1199,7 @@ __device__ __forceinline__ void motion_quad2(const StackArgs& a, const StackGrou
         const uint2 q = qn;
         if (i + 1 < a.n) qn = *reinterpret_cast<const uint2*>(op + (i + 1) * G.nslots);
         const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
-        uint64_t v[P];
+        float2 v[P];
         load_pairs<P, WP>(v, win + o0 + tb, o0 & 1u);
         add_pairs<P>(acc[0], v);
         if (o1 != o0) load_pairs<P, WP>(v, win + o1 + tb, o1 & 1u);
@@ -1221,7 +1228,7 @@ __device__ __forceinline__ void motion_quad2(const StackArgs& a, const StackGrou
             }
         }
     }
-    const uint64_t inv2 = pack2(inv_n, inv_n);
+    const float2 inv2 = make_float2(inv_n, inv_n);
 #pragma unroll
     for (int k = 0; k < M; ++k) {
         const int j = a.slot_motion[G.slot0 + s0 + k];
@@ -1238,7 +1245,9 @@ __device__ __forceinline__ void motion_quad2(const StackArgs& a, const StackGrou
                     ok[c] = cc >= a.min_count;
                     f[c] = a.inv_sqrt[ok[c] ? cc : 0];
                 }
-                unpack2(mul2(acc[k][p], pack2(f[0], f[1])), s[0], s[1]);
+                const float2 sn = __fmul2_rn(acc[k][p], make_float2(f[0], f[1]));
+                s[0] = sn.x;
+                s[1] = sn.y;
 #pragma unroll
                 for (int c = 0; c < 2; ++c)
                     if (ok[c] && (s[c] > best[p][c] || (s[c] == best[p][c] && j < arg[p][c]))) {
@@ -1246,7 +1255,9 @@ __device__ __forceinline__ void motion_quad2(const StackArgs& a, const StackGrou
                         arg[p][c] = j;
                     }
             } else {
-                unpack2(mul2(acc[k][p], inv2), s[0], s[1]);
+                const float2 sn = __fmul2_rn(acc[k][p], inv2);
+                s[0] = sn.x;
+                s[1] = sn.y;
 #pragma unroll
                 for (int c = 0; c < 2; ++c)
                     if (s[c] > best[p][c] || (s[c] == best[p][c] && j < arg[p][c])) {

@@ -481,6 +481,65 @@ __global__ void __launch_bounds__(128) scatter_kernel(const ScatterArgs a) {
     a.scatter[pix] = __double2float_rn(1.4826 * m);
 }
 
+// The same for n <= N <= 128 by a bitonic network in registers over the values'
+// bit patterns (the values are >= +0.0 or +inf, so their patterns order like the
+// values; absent frames are padded with 0xffffffff, above every pattern): the
+// middle pair is then read from the sorted registers.
+template <int N>
+__global__ void __launch_bounds__(N <= 64 ? 128 : 64) scatter_net_kernel(const ScatterArgs a) {
+    const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int x = static_cast<int>(q % a.w), y = static_cast<int>(q / a.w);
+    if (y >= a.h) return;
+    const size_t plane = static_cast<size_t>(a.pitch) * a.h;
+    const size_t pix = static_cast<size_t>(y) * a.pitch + x;
+    uint32_t sv[N];
+    int c = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        uint32_t key = 0xffffffffu;
+        if (i < a.n) {
+            const float v = a.residual[i * plane + pix];
+            if (finitef(v)) {
+                key = __float_as_uint(__double2float_rn(__ddiv_rn(static_cast<double>(fabsf(v)), a.sigma[i])));
+                ++c;
+            }
+        }
+        sv[i] = key;
+    }
+    if (c < a.n / 2) {
+        a.scatter[pix] = 1e9f;
+        return;
+    }
+#pragma unroll
+    for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1)
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int l = i ^ j;
+                if (l > i) {
+                    const uint32_t lo = min(sv[i], sv[l]), hi = max(sv[i], sv[l]);
+                    if ((i & k) == 0) {
+                        sv[i] = lo;
+                        sv[l] = hi;
+                    } else {
+                        sv[i] = hi;
+                        sv[l] = lo;
+                    }
+                }
+            }
+    const int mid = c / 2;
+    uint32_t vmid = 0, vlow = 0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        vmid = i == mid ? sv[i] : vmid;
+        vlow = i == mid - 1 ? sv[i] : vlow;
+    }
+    double m = __uint_as_float(vmid);
+    if (c % 2 == 0) m = 0.5 * (m + __uint_as_float(vlow));
+    a.scatter[pix] = __double2float_rn(1.4826 * m);
+}
+
 __global__ void mask_kernel(const float* scatter, float* mask, int w, int h, int pitch, int dil, double limit) {
     const long long q = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int x = static_cast<int>(q % w), y = static_cast<int>(q / w);
@@ -630,6 +689,23 @@ __global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
     }
     __syncthreads();
     if (threadIdx.x == 0 && cr_tile) atomicAdd(&a.cr[f], cr_tile);
+}
+
+// the temporal scatter: the sorting network up to 128 frames, counting beyond
+void launch_scatter(const ScatterArgs& a, int n, long long npix, cudaStream_t s) {
+    if (n <= 128) {
+        const int T = n <= 64 ? 128 : 64;
+        auto kern = n <= 16 ? scatter_net_kernel<16>
+                    : n <= 32 ? scatter_net_kernel<32>
+                    : n <= 64 ? scatter_net_kernel<64> : scatter_net_kernel<128>;
+        kern<<<static_cast<unsigned>((npix + T - 1) / T), T, 0, s>>>(a);
+    } else {
+        const int T = 128;
+        const size_t smem = static_cast<size_t>(T) * n * 4;
+        allow_dynamic_smem(reinterpret_cast<const void*>(scatter_kernel), smem);
+        scatter_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
+    }
+    FTB_CHECK(cudaGetLastError());
 }
 
 // 4-byte asynchronous copy global -> shared; a source outside the image copies
@@ -1012,11 +1088,7 @@ void stage_filter(Context& c, StageScratch& sc, int w, int h, int n, const Stage
     {
         const int span = c.span_begin("scatter mask");
         ScatterArgs a{sc.residual.as<float>(), d_sigma, sc.scatter.as<float>(), w, h, pitch, n};
-        const int T = 128;
-        const size_t smem = static_cast<size_t>(T) * n * 4;
-        allow_dynamic_smem(reinterpret_cast<const void*>(scatter_kernel), smem);
-        scatter_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
-        FTB_CHECK(cudaGetLastError());
+        launch_scatter(a, n, npix, s);
         ++c.launches;
         const int dil = std::max(1, static_cast<int>(std::lround(0.5 * sp.fwhm_px)));
         mask_kernel<<<static_cast<unsigned>((npix + 255) / 256), 256, 0, s>>>(sc.scatter.as<float>(), d_mask, w, h,
@@ -1234,11 +1306,7 @@ void stage_filter_given(Context& c, StageScratch& sc, int w, int rows, int n, co
     {
         const int span = c.span_begin("scatter mask");
         ScatterArgs a{sc.residual.as<float>(), d_sigma, sc.scatter.as<float>(), w, rows, pitch, n};
-        const int T = 128;
-        const size_t smem = static_cast<size_t>(T) * n * 4;
-        allow_dynamic_smem(reinterpret_cast<const void*>(scatter_kernel), smem);
-        scatter_kernel<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
-        FTB_CHECK(cudaGetLastError());
+        launch_scatter(a, n, npix, s);
         const int dil = std::max(1, static_cast<int>(std::lround(0.5 * sp.fwhm_px)));
         mask_kernel<<<static_cast<unsigned>((npix + 255) / 256), 256, 0, s>>>(sc.scatter.as<float>(), d_mask, w, rows,
                                                                               pitch, dil, sp.mask_scatter);
