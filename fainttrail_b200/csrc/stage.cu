@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(64) sky_kernel(const SkyArgs a) {
 // Each rank's sorted position is then the lower bound of its value in the
 // sorted values plus the number of equal values of lower rank.
 template <int N>
-__global__ void __launch_bounds__(N <= 64 ? 128 : 64) sky_net_kernel(const SkyArgs a) {
+__global__ void __launch_bounds__(64) sky_net_kernel(const SkyArgs a) {
     constexpr int W = (N + 31) / 32;
     extern __shared__ unsigned char sm[];
     const int T = blockDim.x, t = threadIdx.x;
@@ -691,13 +691,23 @@ __global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
     if (threadIdx.x == 0 && cr_tile) atomicAdd(&a.cr[f], cr_tile);
 }
 
+// the static sky: counted ranks up to 64 frames (measured faster there: 554
+// against 375 GB/s at 40 frames), the sorting network up to 128 (where the
+// counting grows with n^2), counted ranks beyond
+void launch_sky(const SkyArgs& a, int n, long long npix, cudaStream_t s) {
+    const int T = 64;
+    const size_t smem = static_cast<size_t>(T) * n * 9;
+    auto kern = n <= 32 ? sky_kernel<1> : n <= 64 ? sky_kernel<2> : n <= 128 ? sky_net_kernel<128> : sky_kernel<8>;
+    allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
+    kern<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
+    FTB_CHECK(cudaGetLastError());
+}
+
 // the temporal scatter: the sorting network up to 128 frames, counting beyond
 void launch_scatter(const ScatterArgs& a, int n, long long npix, cudaStream_t s) {
     if (n <= 128) {
         const int T = n <= 64 ? 128 : 64;
-        auto kern = n <= 16 ? scatter_net_kernel<16>
-                    : n <= 32 ? scatter_net_kernel<32>
-                    : n <= 64 ? scatter_net_kernel<64> : scatter_net_kernel<128>;
+        auto kern = n <= 32 ? scatter_net_kernel<32> : n <= 64 ? scatter_net_kernel<64> : scatter_net_kernel<128>;
         kern<<<static_cast<unsigned>((npix + T - 1) / T), T, 0, s>>>(a);
     } else {
         const int T = 128;
@@ -1025,16 +1035,7 @@ void stage_noise(Context& c, StageScratch& sc, const float* d_sub, int w, int h,
         const int span = c.span_begin("static sky + residuals");
         SkyArgs a{d_sub, sc.residual.as<float>(), d_sky, tb.tab, tb.tab + n, w, h, pitch, n, exclude,
                   std::max(5, static_cast<int>(0.6 * n))};
-        // up to 128 frames: the sorting network; beyond: counted ranks
-        const int T = n <= 64 ? 128 : 64;
-        const size_t smem = static_cast<size_t>(T) * n * 9;
-        auto kern = n <= 16    ? sky_net_kernel<16>
-                    : n <= 32  ? sky_net_kernel<32>
-                    : n <= 64  ? sky_net_kernel<64>
-                    : n <= 128 ? sky_net_kernel<128> : sky_kernel<8>;
-        allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
-        kern<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
-        FTB_CHECK(cudaGetLastError());
+        launch_sky(a, n, npix, s);
         ++c.launches;
         c.span_end(span);
     }
@@ -1213,15 +1214,7 @@ void stage_sky(Context& c, StageScratch& sc, const float* d_sub, int w, int rows
     const int span = c.span_begin("static sky + residuals");
     SkyArgs a{d_sub, sc.residual.as<float>(), d_sky, tb.tab, tb.tab + n, w, rows, pitch, n, exclude,
               std::max(5, static_cast<int>(0.6 * n))};
-    const int T = n <= 64 ? 128 : 64;
-    const size_t smem = static_cast<size_t>(T) * n * 9;
-    auto kern = n <= 16    ? sky_net_kernel<16>
-                : n <= 32  ? sky_net_kernel<32>
-                : n <= 64  ? sky_net_kernel<64>
-                : n <= 128 ? sky_net_kernel<128> : sky_kernel<8>;
-    allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
-    kern<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
-    FTB_CHECK(cudaGetLastError());
+    launch_sky(a, n, npix, s);
     ++c.launches;
     c.span_end(span);
 }
