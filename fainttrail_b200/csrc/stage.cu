@@ -746,11 +746,13 @@ __global__ void __launch_bounds__(256) filter_frames_kernel(const FilterArgs a, 
     float* Tt = fs + 4 * ZN;                // TR x TWc horizontal pass
     unsigned char* F = reinterpret_cast<unsigned char*>(Tt + TR * TWc);  // ZN cosmic-ray centre flags
     __shared__ int cr_tile;
-    float kr[KN], kn[KN];
+    static_assert(TWc % 4 == 0 && THc % 4 == 0, "tile in column quads and row quads");
+    float2 kk[KN], kp[KN];  // the taps, and the taps times the norm, both halves equal
 #pragma unroll
     for (int j = 0; j < KN; ++j) {
-        kr[j] = a.k[j];
-        kn[j] = __fmul_rn(kr[j], a.norm);
+        const float kr = a.k[j], kn = __fmul_rn(kr, a.norm);
+        kk[j] = make_float2(kr, kr);
+        kp[j] = make_float2(kn, kn);
     }
     const int x0 = blockIdx.x * TWc, y0 = blockIdx.y * THc;
     const int fa = blockIdx.z * fpc, fb = min(n, fa + fpc);
@@ -831,26 +833,58 @@ __global__ void __launch_bounds__(256) filter_frames_kernel(const FilterArgs a, 
             Z[e] = zc < -a.clip ? -a.clip : (a.clip < zc ? a.clip : zc);
         }
         __syncthreads();
-        // horizontal pass over rows y0-R .. y0+THc+R-1, the tile's columns
-        for (int e = tid; e < TR * TWc; e += blockDim.x) {
-            const int c = e % TWc, r = e / TWc;
-            const float* row = Z + (r + 2) * ZW + (c + 2);
-            float acc = 0.0f;
+        // horizontal pass over rows y0-R .. y0+THc+R-1, the tile's columns: rows
+        // in pairs (r, r + 1) and CQ adjacent columns per item; the pair's values
+        // at a column are one float2, so each tap is one __fmul2_rn and one
+        // __fadd2_rn for two outputs (each the reference's row[j] * k[j] added in
+        // tap order), and the CQ columns share the loaded row segments
+        {
+            constexpr int CQ = 4, NV = CQ + KN - 1, ITEMS = (TR / 2) * (TWc / CQ);
+            for (int it = tid; it < ITEMS; it += blockDim.x) {
+                const int c = (it % (TWc / CQ)) * CQ, r = 2 * (it / (TWc / CQ));
+                const float* r0 = Z + (r + 2) * ZW + (c + 2);
+                float2 v[NV];
 #pragma unroll
-            for (int j = 0; j < KN; ++j) acc = __fadd_rn(acc, __fmul_rn(row[j], kr[j]));
-            const int gy = y0 - R + r;
-            Tt[e] = (gy >= 0 && gy < a.h) ? acc : 0.0f;
+                for (int x = 0; x < NV; ++x) v[x] = make_float2(r0[x], r0[x + ZW]);
+                const bool in0 = y0 - R + r >= 0 && y0 - R + r < a.h, in1 = y0 - R + r + 1 >= 0 && y0 - R + r + 1 < a.h;
+#pragma unroll
+                for (int q = 0; q < CQ; ++q) {
+                    float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+                    for (int j = 0; j < KN; ++j) acc = __fadd2_rn(acc, __fmul2_rn(v[q + j], kk[j]));
+                    Tt[r * TWc + c + q] = in0 ? acc.x : 0.0f;
+                    Tt[(r + 1) * TWc + c + q] = in1 ? acc.y : 0.0f;
+                }
+            }
         }
         __syncthreads();
-        float* out = a.out + f * plane;
-        for (int e = tid; e < TWc * THc; e += blockDim.x) {
-            const int c = e % TWc, r = e / TWc;
-            const int gx = x0 + c, gy = y0 + r;
-            if (gx >= a.w || gy >= a.h) continue;
-            float acc = 0.0f;
+        // vertical pass: two adjacent columns (one 8-byte load of the horizontal
+        // pass) and RQ rows per item, the loaded column pairs shared by the rows
+        {
+            constexpr int RQ = 4, NV = RQ + KN - 1, ITEMS = (THc / RQ) * (TWc / 2);
+            float* out = a.out + f * plane;
+            for (int it = tid; it < ITEMS; it += blockDim.x) {
+                const int c = 2 * (it % (TWc / 2)), r = (it / (TWc / 2)) * RQ;
+                const int gx = x0 + c;
+                if (gx >= a.w) continue;
+                float2 tv[NV];
 #pragma unroll
-            for (int j = 0; j < KN; ++j) acc = __fadd_rn(acc, __fmul_rn(kn[j], Tt[(r + j) * TWc + c]));
-            out[static_cast<size_t>(gy) * a.pitch + gx] = acc;
+                for (int x = 0; x < NV; ++x) tv[x] = *reinterpret_cast<const float2*>(Tt + (r + x) * TWc + c);
+#pragma unroll
+                for (int q = 0; q < RQ; ++q) {
+                    const int gy = y0 + r + q;
+                    if (gy >= a.h) break;
+                    float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+                    for (int j = 0; j < KN; ++j) acc = __fadd2_rn(acc, __fmul2_rn(kp[j], tv[q + j]));
+                    float* o = out + static_cast<size_t>(gy) * a.pitch + gx;
+                    if (gx + 1 < a.w) {
+                        *reinterpret_cast<float2*>(o) = acc;
+                    } else {
+                        o[0] = acc.x;
+                    }
+                }
+            }
         }
         if (tid == 0 && cr_tile) atomicAdd(&a.cr[f], cr_tile);
     }
