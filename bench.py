@@ -34,7 +34,10 @@ the same requests run one after another), `reference_cuda` (the reference's own
 CUDA backend built for sm_100a on one pass of the full-frame frames, beside this
 backend's pass of the same frames, compared bit for bit) and
 `parity_vs_reference` (the device search on the crop the CPU baseline times,
-compared with the reference's search() of that crop). --no-extras skips them.
+compared with the reference's search() of that crop) and `stage` (the
+preprocessing stage alone on 2048^2 frames at 40 and 120 frames: the static-sky
+and matched-filter kernels against the HBM roofline). --no-extras skips them
+(--stage-only keeps the stage part).
 
 --impl reference times the reference's own CPU implementation (FaintTrail
 0.9.1 built from its sources, oracle/_ref) on the host's cores with all
@@ -58,7 +61,7 @@ sys.path.insert(0, ROOT)
 METRIC = "pixel·frame·motion/s"
 SHAPES = {0: "by frame count", 1: "32x16, 12 warps", 2: "64x8 paired columns, 12 warps", 3: "32x8, 16 warps",
           4: "32x4, 16 warps", 5: "32x16 shared maximum, 16 warps", 6: "32x16 shared maximum, 14 warps",
-          7: "32x12, 16 warps"}
+          7: "32x12, 16 warps", 8: "32x20 shared maximum, 16 warps"}
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -73,7 +76,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tile-shape", type=int, default=0, help="stack kernel tile shape (0: autotuned)")
     ap.add_argument("--workers", type=int, default=2, help="serving: rounds in flight at once")
-    ap.add_argument("--no-extras", action="store_true", help="skip the batched, serving and reference-CUDA parts")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched, serving, stage and reference-CUDA parts")
+    ap.add_argument("--stage-only", action="store_true", help="with --no-extras: still time the stage at 40 / 120 frames")
+    ap.add_argument("--once", action="store_true",
+                    help="one search of the workload without warm-up (for large-sensor with its 32 null runs); "
+                         "prints its time, rate and stage spans, not the benchmark line")
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-max-adds", type=float, default=5.0e13)
     return ap.parse_args()
@@ -314,6 +322,63 @@ def batched_measure(dev, local_rank):
             "clocks": clk}
 
 
+def stage_measure(dev, local_rank, side=2048, counts=(40, 120), reps=3):
+    """The preprocessing stage alone (ft_b200_stage_dev) on side x side frames at
+    each frame count: sky-like noise with a few NaN pixels, 30 s cadence, FWHM 6
+    px. Per kernel span: CUDA-event seconds (best of `reps` after a warm-up)
+    and algorithmic bytes over that time against the measured HBM peak."""
+    import torch
+    peaks, _ = measured_peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    out = {}
+    for n in counts:
+        g = torch.Generator(device=f"cuda:{local_rank}").manual_seed(5 + n)
+        sub = torch.randn((n, side, side), generator=g, device=f"cuda:{local_rank}", dtype=torch.float32) * 8.0
+        sub[:, ::97, ::89] = float("nan")
+        filt = torch.empty_like(sub)
+        t_h = (np.arange(n) - 0.5 * (n - 1)) * 30.0 / 3600.0
+        best = {}
+        for k in range(reps + 1):
+            dev.stage_dev(sub.data_ptr(), side, side, side, n, t_h, 6.0, d_filtered=filt.data_ptr())
+            if k == 0:
+                continue
+            for name, v in dev.timings():
+                best[name] = min(best.get(name, float("inf")), v)
+        torch.cuda.synchronize()
+        sky_b = (8.0 * n + 4.0) * side * side
+        filt_b = (8.0 * n + 8.0) * side * side
+        ent = {"frames": n, "side": side, "seconds": {k: v for k, v in best.items()}}
+        for key, name, b in (("sky", "static sky + residuals", sky_b), ("filter", "matched filter", filt_b)):
+            if name in best:
+                gbs = b / best[name] / 1e9
+                ent[key] = {"achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "bytes_per_launch": b}
+        out[f"n{n}"] = ent
+        del sub, filt
+        torch.cuda.empty_cache()
+    return out
+
+
+def once_measure(args, dev, wl, frames, mjd, exptime, params, local_rank):
+    """One search (device-resident frames, all null runs) with no warm-up: the
+    rate over its device time, the stack kernel's rate, the stage spans and the
+    clocks. Includes the tile-shape autotuner's first probes."""
+    n, h, w = frames.shape
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    r = dev.search_dev(frames.data_ptr(), w, h, w, n, mjd, exptime, maps=False, **params)
+    tm = dict(dev.timings())
+    clk = clocks.stop()
+    m = r["n_velocities"]
+    passes = 1 + wl.null_runs
+    adds = float(m) * n * w * h * passes
+    print(json.dumps({"once": workload_desc(wl, m), "seconds": tm["total"], "value": adds / tm["total"],
+                      "unit": METRIC, "stack_kernel": {"seconds": tm["kernel"], "adds_per_s": adds / tm["kernel"]},
+                      "threshold_snr": r["threshold"], "threshold_method": r["method"],
+                      "candidates": len(r["candidates"]), "spans": tm, "clocks": clk,
+                      "gpu_launches": dev.launches()}), flush=True)
+    dev.close()
+
+
 # --------------------------------------------------------------------------- arms
 def reference_arm(args):
     rank, _, world = env_rank()
@@ -366,6 +431,8 @@ def b200_arm(args):
     dev = ftb.Device(local_rank)
     copies = synthetic.injection_copies(wl, frames.shape, seed=11 + rank)
     batched = len(copies) > 0
+    if args.once:
+        return once_measure(args, dev, wl, frames, mjd, exptime, params, local_rank)
 
     def step(**over):
         kw = dict(params, **over)
@@ -482,6 +549,8 @@ def b200_arm(args):
         torch.cuda.empty_cache()
         extras["batched"] = batched_measure(dev, local_rank)
         extras["serving"] = serving_measure(args, local_rank)
+    if world == 1 and (args.stage_only or not args.no_extras) and not batched:
+        extras["stage"] = stage_measure(dev, local_rank)
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                "warmup": max(3, args.warmup), "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,

@@ -305,7 +305,8 @@ def emulate_stack(frames, dx, dy, min_count, shape=0):
 def set_tile_shape(shape):
     """ft_b200_set_tile_shape: 0 automatic, 1 = 32 x 16, 2 = 64 x 8 paired
     columns, 3 = 32 x 8, 4 = 32 x 4, 5 / 6 = 32 x 16 with one shared maximum per
-    tile (16 / 14 warps), 7 = 32 x 12 (16 warps); process-wide."""
+    tile (16 / 14 warps), 7 = 32 x 12 (16 warps), 8 = 32 x 20 with the shared
+    maximum (16 warps); process-wide."""
     L = lib()
     L.ft_b200_set_tile_shape.argtypes = [C.c_int]
     if L.ft_b200_set_tile_shape(int(shape)) != FT_B200_OK:

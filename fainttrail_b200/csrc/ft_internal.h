@@ -42,9 +42,14 @@ struct StackGroup {
 // lie within kRowSpread rows of one another is described per frame by one
 // 32-bit word: bits 0-15 the window offset of its lowest row, bits 16-23 each
 // slot's row above it (2 bits a slot), bits 24-25 the largest of those, and,
-// when that is at most 1, bits 26-29 the slots' offsets as a 4-bit pattern.
+// when that is at most 1, bits 26-29 the slots' offsets as a 4-bit pattern;
+// bits 30-31 are zero, so a word below 2^24 has every slot on the lowest row.
 constexpr int kMotionBlock = 4;
 constexpr int kRowSpread = 3;
+// The largest row offset a tile shape's kernel takes in a row-descriptor block:
+// 1 for the shapes with fewer registers a thread (the 12-row tile and the shared
+// maximum), kRowSpread otherwise. The planner cuts blocks to it.
+__host__ __device__ constexpr int shape_row_spread(int p, int merge) { return (p == 12 || merge) ? 1 : kRowSpread; }
 
 struct StackWin {            // one frame's window for a group
     int dx0 = 0;             // window x origin relative to the tile (a multiple of 4)
@@ -115,8 +120,8 @@ void allow_dynamic_smem(const void* func, size_t bytes);
 // Compiled stack kernel shapes: 1 = 32 x 16 tiles (12 warps), 2 = 64 x 8 tiles with
 // paired columns (12 warps), 3 = 32 x 8 (16 warps), 4 = 32 x 4 (16 warps),
 // 5 = 32 x 16 with one shared maximum per tile (16 warps), 6 = the same with 14 warps,
-// 7 = 32 x 12 (16 warps).
-constexpr int kStackShapes = 7;
+// 7 = 32 x 12 (16 warps), 8 = 32 x 20 with the shared maximum (16 warps).
+constexpr int kStackShapes = 8;
 StackConfig stack_shape_config(int shape, int device_smem_optin);
 bool stack_shape_fits(const StackConfig& c, int n);
 // A process-wide choice for choose_stack_config: 0 = by frame count, else a shape

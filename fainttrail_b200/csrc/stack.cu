@@ -219,19 +219,23 @@ StackConfig stack_shape_config(int shape, int smem_optin) {
     c.bh = 4;
     c.smem_bytes = std::min(smem_optin - 1024, 224 * 1024);
     switch (shape) {
-        case 1: c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 12; c.rows = kRowSpread; break;
+        case 1: c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 12; c.rows = shape_row_spread(16, 0); break;
         case 2: c.tile_w = 64; c.wp = 72; c.p = 8; c.ty = 12; break;
-        case 3: c.tile_w = 32; c.wp = 40; c.p = 8; c.ty = 16; c.rows = kRowSpread; break;
-        case 4: c.tile_w = 32; c.wp = 40; c.p = 4; c.ty = 16; c.rows = kRowSpread; break;
+        case 3: c.tile_w = 32; c.wp = 40; c.p = 8; c.ty = 16; c.rows = shape_row_spread(8, 0); break;
+        case 4: c.tile_w = 32; c.wp = 40; c.p = 4; c.ty = 16; c.rows = shape_row_spread(4, 0); break;
         case 5:  // 32 x 16 with the shared maximum: 16 warps
-            c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 16; c.merge = 1;
+            c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 16; c.merge = 1; c.rows = shape_row_spread(16, 1);
             c.smem_bytes -= 32 * 16 * 8;  // the keys sit ahead of the windows
             break;
         case 6:  // the same with 14 warps (146 registers a thread)
-            c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 14; c.merge = 1;
+            c.tile_w = 32; c.wp = 40; c.p = 16; c.ty = 14; c.merge = 1; c.rows = shape_row_spread(16, 1);
             c.smem_bytes -= 32 * 16 * 8;
             break;
-        case 7: c.tile_w = 32; c.wp = 40; c.p = 12; c.ty = 16; c.rows = 1; break;  // 128 registers: offsets 0 or 1
+        case 7: c.tile_w = 32; c.wp = 40; c.p = 12; c.ty = 16; c.rows = shape_row_spread(12, 0); break;
+        case 8:  // 32 x 20 with the shared maximum: 16 warps
+            c.tile_w = 32; c.wp = 40; c.p = 20; c.ty = 16; c.merge = 1; c.rows = shape_row_spread(20, 1);
+            c.smem_bytes -= 32 * 20 * 8;
+            break;
         default: throw std::runtime_error("stack: unknown tile shape");
     }
     return c;
@@ -347,6 +351,11 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
         }
     }
     const int nblk = static_cast<int>(blocks.size()) / M;
+    // each block's motions in ascending index, pads last: the kernel's in-block
+    // maximum then keeps the first of equal S/N with a strict comparison
+    for (int b = 0; b < nblk; ++b)
+        std::sort(blocks.begin() + static_cast<long long>(b) * M, blocks.begin() + static_cast<long long>(b + 1) * M,
+                  [](int a, int c) { return a >= 0 && (c < 0 || a < c); });
     // slot k of block b, pads standing for the block's last motion (their
     // windows and offsets repeat it; their slot_motion is -1)
     auto slot = [&](int b, int k) {
@@ -411,7 +420,9 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
                 fast = fast && hi - lo <= cfg.rows;
             }
         g.rows_fast = fast ? 1 : 0;
-        g.tab_bytes = fast ? roundup(nb * n * 4, 16) : roundup(g.nslots * n * 2, 16);
+        // a row descriptor table holds one more frame of zeros: the kernel loads
+        // frame i + 1's words while it adds frame i's
+        g.tab_bytes = fast ? roundup(nb * (n + 1) * 4, 16) : roundup(g.nslots * n * 2, 16);
         P.max_rows = std::max(P.max_rows, row);
         P.max_group_bytes = std::max(P.max_group_bytes, static_cast<long long>(row) * WP * 4 + g.tab_bytes);
         P.max_slots = std::max(P.max_slots, g.nslots);
@@ -696,6 +707,27 @@ __device__ __forceinline__ uint2 block_offsets(const uint16_t* __restrict__ offs
     }
 }
 
+// The maximum of one block's motions at one pixel. A block's slots hold its
+// motions in ascending index with pads repeating the last one, so a strict
+// comparison keeps the first of equal S/N and a pad (equal to the slot before
+// it) never wins; starting from -inf with no motion, NaN and -inf never enter.
+__device__ __forceinline__ void block_max(float s, int j, float& b, int& bj) {
+    if (s > b) {
+        b = s;
+        bj = j;
+    }
+}
+
+// The block's maximum into the running one: larger S/N, and of equal S/N the
+// smaller motion index (backend_cpu.cpp:77-204). A block maximum of -inf has no
+// motion (-1) and then changes nothing: a running -inf also has none.
+__device__ __forceinline__ void merge_max(float b, int bj, float& best, int& arg) {
+    if (b > best || (b == best && bj < arg)) {
+        best = b;
+        arg = bj;
+    }
+}
+
 template <int P, int WP, bool BORDER, bool ROWS>
 __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup& G, int s0,
                                             const float* __restrict__ win, const uint16_t* __restrict__ offs, int tb,
@@ -715,10 +747,11 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
         for (int w = 0; w < PW; ++w) cpart[k][w] = 0;
     // the next frame's four offsets are loaded one frame ahead, so the reuse
     // tests below do not wait on a shared-memory load
+    const int n = a.n;  // loop bounds and table strides in registers, not reloaded from the pass arguments
     uint2 qn = block_offsets<ROWS, WP>(offs, G, s0, 0);
-    for (int i = 0; i < a.n; ++i) {
+    for (int i = 0; i < n; ++i) {
         const uint2 q = qn;
-        if (i + 1 < a.n) qn = block_offsets<ROWS, WP>(offs, G, s0, i + 1);
+        if (i + 1 < n) qn = block_offsets<ROWS, WP>(offs, G, s0, i + 1);
         const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
         float v[P];
         load_column<P, WP>(v, win + o0 + tb);
@@ -732,7 +765,7 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
         if constexpr (BORDER) {
 #pragma unroll
             for (int k = 0; k < M; ++k) {
-                const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * a.n + i];
+                const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * n + i];
                 const bool whole = x0 + sh.x >= 0 && x0 + 31 + sh.x < a.w && y0 + sh.y >= 0 && y0 + P - 1 + sh.y < a.h;
                 if (whole) {
                     ++cfull[k];
@@ -745,6 +778,20 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
                 }
             }
         }
+    }
+    if constexpr (!BORDER) {
+        int jk[M];
+#pragma unroll
+        for (int k = 0; k < M; ++k) jk[k] = a.slot_motion[G.slot0 + s0 + k];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            float b = -CUDART_INF_F;
+            int bj = -1;
+#pragma unroll
+            for (int k = 0; k < M; ++k) block_max(__fmul_rn(acc[k][p], inv_n), jk[k], b, bj);
+            merge_max(b, bj, best[p], arg[p]);
+        }
+        return;
     }
 #pragma unroll
     for (int k = 0; k < M; ++k) {
@@ -765,6 +812,26 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
             }
         }
     }
+}
+
+// ---- one shared maximum per tile: instead of a best/argmax pair per pixel in
+// every thread, the CTA's warps merge into one array of 64-bit keys in shared
+// memory with atomicMax. key = (order-preserving bits of S/N) << 32 | ~index,
+// so a larger S/N wins and equal S/N goes to the lower motion index -- the
+// reference's rule. S/N is never -0.0 (sums start at +0.0f and round to
+// nearest) and -inf / NaN never enter, as in the register rule. Frees 2P
+// registers per thread, so 16-row tiles run 16 warps.
+
+__device__ __forceinline__ unsigned long long snr_key(float s, int j) {
+    const uint32_t b = __float_as_uint(s);
+    const uint32_t o = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+    return (static_cast<unsigned long long>(o) << 32) | static_cast<uint32_t>(~j);
+}
+
+__device__ __forceinline__ void snr_unkey(unsigned long long k, float& s, int& j) {
+    const uint32_t o = static_cast<uint32_t>(k >> 32);
+    s = __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+    j = static_cast<int>(~static_cast<uint32_t>(k));
 }
 
 // Pairs of floats: __fadd2_rn / __fmul2_rn are two independent
@@ -792,28 +859,39 @@ __device__ __forceinline__ void add_pattern(float2 (&acc)[4][H], const float2* A
 // (r, r + P/2), so motion k adds A[q + row offset] to its accumulator pair q
 // (rows P/2 .. P/2 + S - 1 are loaded twice, once for each pairing).
 template <int P, int WP, int SMAX>
-__device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const StackGroup& G, int s0,
-                                                 const float* __restrict__ win, const uint16_t* __restrict__ offs,
-                                                 int tb, float inv_n, float (&best)[P], int (&arg)[P]) {
+__device__ __forceinline__ void rows_accumulate(const StackArgs& a, const StackGroup& G, int s0,
+                                                const float* __restrict__ win, const uint16_t* __restrict__ offs,
+                                                int tb, float2 (&acc)[4][P / 2]) {
     constexpr int M = 4;
     constexpr int H = P / 2;
     static_assert(P % 2 == 0, "rows are paired");
-    float2 acc[M][H];
 #pragma unroll
     for (int k = 0; k < M; ++k)
 #pragma unroll
         for (int q = 0; q < H; ++q) acc[k][q] = make_float2(0.0f, 0.0f);
-    const int nb = G.nslots >> 2;
+    const int n = a.n, nb = G.nslots >> 2;
     const uint32_t* dp = reinterpret_cast<const uint32_t*>(offs) + (s0 >> 2);
-    uint32_t dn = dp[0];
-    for (int i = 0; i < a.n; ++i) {
+    // the descriptor is the same word in every lane; the broadcast from lane 0
+    // lets the compiler treat it, and the branches on it, as warp-uniform
+    uint32_t dn = __shfl_sync(0xffffffffu, dp[0], 0);
+    for (int i = 0; i < n; ++i) {
         const uint32_t d = dn;
-        if (i + 1 < a.n) dn = dp[(i + 1) * nb];
+        // the table's extra frame makes the last prefetch a zero word
+        dn = __shfl_sync(0xffffffffu, dp[(i + 1) * nb], 0);
         const float* src = win + (d & 0xffffu) + tb;
-        const uint32_t S = (d >> 24) & 3u;
         float2 A[H + SMAX];
 #pragma unroll
         for (int r = 0; r < H; ++r) A[r] = make_float2(src[r * WP], src[(r + H) * WP]);
+        if (d < (1u << 24)) {
+            // every motion on the base row (no row offset, pattern 0): the most
+            // common frame of a block, tested first
+#pragma unroll
+            for (int k = 0; k < M; ++k)
+#pragma unroll
+                for (int q = 0; q < H; ++q) acc[k][q] = __fadd2_rn(acc[k][q], A[q]);
+            continue;
+        }
+        const uint32_t S = (d >> 24) & 3u;
         if (S >= 1u) A[H] = make_float2(src[H * WP], src[P * WP]);
         if (S <= 1u) {
             // row offsets 0 or 1: one branch on the block's 4-bit pattern, each
@@ -853,24 +931,64 @@ __device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const Stack
         }
         }
     }
+}
+
+// The block's maxima at row pairs (q, q + P/2) from the row-paired sums.
+template <int P>
+__device__ __forceinline__ void rows_block_max(const float2 (&acc)[4][P / 2], const int (&jk)[4], float inv_n, int q,
+                                               float& bl, int& al, float& bh, int& ah) {
     const float2 inv2 = make_float2(inv_n, inv_n);
+    bl = bh = -CUDART_INF_F;
+    al = ah = -1;
 #pragma unroll
-    for (int k = 0; k < M; ++k) {
-        const int j = a.slot_motion[G.slot0 + s0 + k];
-        if (j < 0) continue;
+    for (int k = 0; k < 4; ++k) {
+        const float2 sn = __fmul2_rn(acc[k][q], inv2);
+        block_max(sn.x, jk[k], bl, al);
+        block_max(sn.y, jk[k], bh, ah);
+    }
+}
+
+// rows_accumulate for one block, its maxima into this thread's running ones.
+template <int P, int WP, int SMAX>
+__device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const StackGroup& G, int s0,
+                                                 const float* __restrict__ win, const uint16_t* __restrict__ offs,
+                                                 int tb, float inv_n, float (&best)[P], int (&arg)[P]) {
+    constexpr int H = P / 2;
+    float2 acc[4][H];
+    rows_accumulate<P, WP, SMAX>(a, G, s0, win, offs, tb, acc);
+    int jk[4];
 #pragma unroll
-        for (int q = 0; q < H; ++q) {
-            const float2 sn = __fmul2_rn(acc[k][q], inv2);
-            const float lo = sn.x, hi = sn.y;
-            if (lo > best[q] || (lo == best[q] && j < arg[q])) {
-                best[q] = lo;
-                arg[q] = j;
-            }
-            if (hi > best[q + H] || (hi == best[q + H] && j < arg[q + H])) {
-                best[q + H] = hi;
-                arg[q + H] = j;
-            }
-        }
+    for (int k = 0; k < 4; ++k) jk[k] = a.slot_motion[G.slot0 + s0 + k];
+#pragma unroll
+    for (int q = 0; q < H; ++q) {
+        float bl, bh;
+        int al, ah;
+        rows_block_max<P>(acc, jk, inv_n, q, bl, al, bh, ah);
+        merge_max(bl, al, best[q], arg[q]);
+        merge_max(bh, ah, best[q + H], arg[q + H]);
+    }
+}
+
+// rows_accumulate for one block, its maxima into the tile's shared keys (one
+// atomic per pixel that has a motion: a block maximum above -inf).
+template <int P, int WP, int SMAX>
+__device__ __forceinline__ void motion_quad_rows_atom(const StackArgs& a, const StackGroup& G, int s0,
+                                                      const float* __restrict__ win,
+                                                      const uint16_t* __restrict__ offs, int tb, float inv_n,
+                                                      unsigned long long* keys) {
+    constexpr int H = P / 2;
+    float2 acc[4][H];
+    rows_accumulate<P, WP, SMAX>(a, G, s0, win, offs, tb, acc);
+    int jk[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) jk[k] = a.slot_motion[G.slot0 + s0 + k];
+#pragma unroll
+    for (int q = 0; q < H; ++q) {
+        float bl, bh;
+        int al, ah;
+        rows_block_max<P>(acc, jk, inv_n, q, bl, al, bh, ah);
+        if (al >= 0) atomicMax(keys + q * 32 + tb, snr_key(bl, al));
+        if (ah >= 0) atomicMax(keys + (q + H) * 32 + tb, snr_key(bh, ah));
     }
 }
 
@@ -945,7 +1063,7 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
         if (G.rows_fast) {
             if (interior) {
                 for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                    motion_quad_rows<P, WP, (P == 12 ? 1 : kRowSpread)>(a, G, s0, win, offs, tb, inv_n, best, arg);
+                    motion_quad_rows<P, WP, shape_row_spread(P, 0)>(a, G, s0, win, offs, tb, inv_n, best, arg);
             } else {
                 for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
                     motion_quad<P, WP, true, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
@@ -999,27 +1117,7 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
     return true;
 }
 
-// ---- one shared maximum per tile: instead of a best/argmax pair per pixel in
-// every thread, the CTA's warps merge into one array of 64-bit keys in shared
-// memory with atomicMax. key = (order-preserving bits of S/N) << 32 | ~index,
-// so a larger S/N wins and equal S/N goes to the lower motion index -- the
-// reference's rule. S/N is never -0.0 (sums start at +0.0f and round to
-// nearest) and -inf / NaN never enter, as in the register rule. Frees 2P
-// registers per thread, so 16-row tiles run 16 warps.
-
-__device__ __forceinline__ unsigned long long snr_key(float s, int j) {
-    const uint32_t b = __float_as_uint(s);
-    const uint32_t o = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-    return (static_cast<unsigned long long>(o) << 32) | static_cast<uint32_t>(~j);
-}
-
-__device__ __forceinline__ void snr_unkey(unsigned long long k, float& s, int& j) {
-    const uint32_t o = static_cast<uint32_t>(k >> 32);
-    s = __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
-    j = static_cast<int>(~static_cast<uint32_t>(k));
-}
-
-template <int P, int WP, bool BORDER>
+template <int P, int WP, bool BORDER, bool ROWS>
 __device__ __forceinline__ void motion_quad_atom(const StackArgs& a, const StackGroup& G, int s0,
                                                  const float* __restrict__ win, const uint16_t* __restrict__ offs,
                                                  int tb, int x, int x0, int y0, float inv_n, unsigned long long* keys) {
@@ -1036,11 +1134,11 @@ __device__ __forceinline__ void motion_quad_atom(const StackArgs& a, const Stack
     for (int k = 0; k < M; ++k)
 #pragma unroll
         for (int w = 0; w < PW; ++w) cpart[k][w] = 0;
-    const uint16_t* op = offs + s0;
-    uint2 qn = *reinterpret_cast<const uint2*>(op);
-    for (int i = 0; i < a.n; ++i) {
+    const int n = a.n;
+    uint2 qn = block_offsets<ROWS, WP>(offs, G, s0, 0);
+    for (int i = 0; i < n; ++i) {
         const uint2 q = qn;
-        if (i + 1 < a.n) qn = *reinterpret_cast<const uint2*>(op + (i + 1) * G.nslots);
+        if (i + 1 < n) qn = block_offsets<ROWS, WP>(offs, G, s0, i + 1);
         const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
         float v[P];
         load_column<P, WP>(v, win + o0 + tb);
@@ -1054,7 +1152,7 @@ __device__ __forceinline__ void motion_quad_atom(const StackArgs& a, const Stack
         if constexpr (BORDER) {
 #pragma unroll
             for (int k = 0; k < M; ++k) {
-                const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * a.n + i];
+                const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * n + i];
                 const bool whole = x0 + sh.x >= 0 && x0 + 31 + sh.x < a.w && y0 + sh.y >= 0 && y0 + P - 1 + sh.y < a.h;
                 if (whole) {
                     ++cfull[k];
@@ -1121,12 +1219,20 @@ __device__ bool stack_tile_atom(const StackArgs& a, const CUtensorMap* tmap, int
         if (!stage_group<NW, WP, BH>(a, G, g, tmap, x0, y0, bar, win, offs, block_next, err, phase)) return false;
         const bool interior = full && x0 + G.gdxmin >= 0 && x0 + 31 + G.gdxmax < a.w && y0 + G.gdymin >= 0 &&
                               y0 + P - 1 + G.gdymax < a.h;
-        if (interior) {
+        if (G.rows_fast) {
+            if (interior) {
+                for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
+                    motion_quad_rows_atom<P, WP, shape_row_spread(P, 1)>(a, G, s0, win, offs, tb, inv_n, keys);
+            } else {
+                for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
+                    motion_quad_atom<P, WP, true, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
+            }
+        } else if (interior) {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                motion_quad_atom<P, WP, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
+                motion_quad_atom<P, WP, false, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
         } else {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                motion_quad_atom<P, WP, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
+                motion_quad_atom<P, WP, true, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
         }
     }
     __syncthreads();
@@ -1195,9 +1301,10 @@ __device__ __forceinline__ void motion_quad2(const StackArgs& a, const StackGrou
             for (int w = 0; w < PW; ++w) cpart[k][c][w] = 0;
     const uint16_t* op = offs + s0;
     uint2 qn = *reinterpret_cast<const uint2*>(op);
-    for (int i = 0; i < a.n; ++i) {
+    const int n = a.n;
+    for (int i = 0; i < n; ++i) {
         const uint2 q = qn;
-        if (i + 1 < a.n) qn = *reinterpret_cast<const uint2*>(op + (i + 1) * G.nslots);
+        if (i + 1 < n) qn = *reinterpret_cast<const uint2*>(op + (i + 1) * G.nslots);
         const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
         float2 v[P];
         load_pairs<P, WP>(v, win + o0 + tb, o0 & 1u);
@@ -1211,7 +1318,7 @@ __device__ __forceinline__ void motion_quad2(const StackArgs& a, const StackGrou
         if constexpr (BORDER) {
 #pragma unroll
             for (int k = 0; k < M; ++k) {
-                const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * a.n + i];
+                const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0 + k) * n + i];
                 const bool whole = x0 + sh.x >= 0 && x0 + 63 + sh.x < a.w && y0 + sh.y >= 0 && y0 + P - 1 + sh.y < a.h;
                 if (whole) {
                     ++cfull[k];
@@ -1503,6 +1610,8 @@ void stack_launch_batch(const std::vector<BatchPass>& batch, unsigned char* d_de
         launch_batch<14, 16, 40, 4, 32, 1>(batch, d_desc, desc_bytes, d_err, sms, s);
     else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 12 && c.merge == 0)
         launch_batch<16, 12, 40, 4, 32, 0>(batch, d_desc, desc_bytes, d_err, sms, s);
+    else if (c.tile_w == 32 && c.wp == 40 && c.ty == 16 && c.p == 20 && c.merge == 1)
+        launch_batch<16, 20, 40, 4, 32, 1>(batch, d_desc, desc_bytes, d_err, sms, s);
 
     else
         throw std::runtime_error("stack: unsupported tile shape");

@@ -747,12 +747,11 @@ __global__ void __launch_bounds__(256) filter_frames_kernel(const FilterArgs a, 
     unsigned char* F = reinterpret_cast<unsigned char*>(Tt + TR * TWc);  // ZN cosmic-ray centre flags
     __shared__ int cr_tile;
     static_assert(TWc % 4 == 0 && THc % 4 == 0, "tile in column quads and row quads");
-    float2 kk[KN], kp[KN];  // the taps, and the taps times the norm, both halves equal
+    float kk[KN], kp[KN];  // the taps, and the taps times the norm (the reference's float product)
 #pragma unroll
     for (int j = 0; j < KN; ++j) {
-        const float kr = a.k[j], kn = __fmul_rn(kr, a.norm);
-        kk[j] = make_float2(kr, kr);
-        kp[j] = make_float2(kn, kn);
+        kk[j] = a.k[j];
+        kp[j] = __fmul_rn(kk[j], a.norm);
     }
     const int x0 = blockIdx.x * TWc, y0 = blockIdx.y * THc;
     const int fa = blockIdx.z * fpc, fb = min(n, fa + fpc);
@@ -834,10 +833,14 @@ __global__ void __launch_bounds__(256) filter_frames_kernel(const FilterArgs a, 
         }
         __syncthreads();
         // horizontal pass over rows y0-R .. y0+THc+R-1, the tile's columns: rows
-        // in pairs (r, r + 1) and CQ adjacent columns per item; the pair's values
-        // at a column are one float2, so each tap is one __fmul2_rn and one
-        // __fadd2_rn for two outputs (each the reference's row[j] * k[j] added in
-        // tap order), and the CQ columns share the loaded row segments
+        // in pairs (r, r + 1) and CQ adjacent columns per item; the pair's two
+        // products of a tap are scalar round-to-nearest multiplies and their adds
+        // into the pair's sums one __fadd2_rn (each output the reference's row[j]
+        // * k[j] added in tap order), and the CQ columns share the loaded row
+        // segments. The products stay scalar: a paired multiply followed by a
+        // paired add was contracted into a fused multiply-add by the compiler
+        // (even from inline PTX mul.rn.f32x2, and with --fmad=false), which rounds
+        // once and differs from the reference in the last bits.
         {
             constexpr int CQ = 4, NV = CQ + KN - 1, ITEMS = (TR / 2) * (TWc / CQ);
             for (int it = tid; it < ITEMS; it += blockDim.x) {
@@ -851,7 +854,8 @@ __global__ void __launch_bounds__(256) filter_frames_kernel(const FilterArgs a, 
                 for (int q = 0; q < CQ; ++q) {
                     float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
-                    for (int j = 0; j < KN; ++j) acc = __fadd2_rn(acc, __fmul2_rn(v[q + j], kk[j]));
+                    for (int j = 0; j < KN; ++j)
+                        acc = __fadd2_rn(acc, make_float2(__fmul_rn(v[q + j].x, kk[j]), __fmul_rn(v[q + j].y, kk[j])));
                     Tt[r * TWc + c + q] = in0 ? acc.x : 0.0f;
                     Tt[(r + 1) * TWc + c + q] = in1 ? acc.y : 0.0f;
                 }
@@ -876,7 +880,8 @@ __global__ void __launch_bounds__(256) filter_frames_kernel(const FilterArgs a, 
                     if (gy >= a.h) break;
                     float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
-                    for (int j = 0; j < KN; ++j) acc = __fadd2_rn(acc, __fmul2_rn(kp[j], tv[q + j]));
+                    for (int j = 0; j < KN; ++j)
+                        acc = __fadd2_rn(acc, make_float2(__fmul_rn(kp[j], tv[q + j].x), __fmul_rn(kp[j], tv[q + j].y)));
                     float* o = out + static_cast<size_t>(gy) * a.pitch + gx;
                     if (gx + 1 < a.w) {
                         *reinterpret_cast<float2*>(o) = acc;

@@ -416,7 +416,8 @@ int ft_b200_result_registration(const ft_b200_result* r, ft_b200_drift_check* ou
  * (the default: the autotuned choice where one is cached for the pass's frame
  * count, else the first shape whose windows fit), 1 = 32 x 16 output tiles,
  * 2 = 64 x 8 tiles with paired columns, 3 = 32 x 8, 4 = 32 x 4, 5 and 6 = 32 x 16
- * with one shared maximum per tile (16 and 14 warps), 7 = 32 x 12. A fixed shape
+ * with one shared maximum per tile (16 and 14 warps), 7 = 32 x 12, 8 = 32 x 20
+ * with the shared maximum (16 warps). A fixed shape
  * whose frame windows do not fit shared memory falls back to automatic. Results
  * do not depend on the shape. No counterpart in the reference (its CUDA kernel
  * has one shape, backend_cuda.cu:55-72). */

@@ -60,11 +60,11 @@ def test_host_only_entries_without_a_gpu():
     import fainttrail_b200 as ftb
     L = ftb.lib()
     assert ftb.tile_shape() == 0
-    for shape in range(0, 8):
+    for shape in range(0, 9):
         ftb.set_tile_shape(shape)
         assert ftb.tile_shape() == shape
     ftb.set_tile_shape(0)
-    for bad in (-1, 8, 99):
+    for bad in (-1, 9, 99):
         with pytest.raises(ValueError, match="tile shape"):
             ftb.set_tile_shape(bad)
     assert ftb.tile_shape() == 0

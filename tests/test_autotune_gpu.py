@@ -27,7 +27,7 @@ def test_autotuned_pass_equals_fixed_shapes(device):
         ftb.set_tile_shape(0)
     tuned = ftb.tuned_shapes()
     m = out[0]["n_velocities"]
-    assert tuned.get((n, m, w, h)) in range(1, 8)  # a compiled shape that fits
+    assert tuned.get((n, m, w, h)) in range(1, 9)  # a compiled shape that fits
     for shape in (1, 2):
         assert np.array_equal(out[shape]["max_snr"], out[0]["max_snr"])
         assert np.array_equal(out[shape]["best_v"], out[0]["best_v"])

@@ -5,6 +5,8 @@ the benchmark configurations, on the same seeded synthetic frames.
   0.2-1.1 px/min on a half-pixel grid (5,468 trial motions), 8 null runs.
 * The full-frame 4096^2 sequence (40 frames, 30 s cadence, 19,328 motions)
   cropped to the 512 x 512 window the CPU baseline times, with its 3 null runs.
+* The large-sensor sequence (60 x 9576 x 6388) cut to a 256 x 256 crop with 2
+  null runs, through the tiled path in 64-row bands.
 * The batched calibration sequence (30 frames, 2048^2) cut to a 512 x 512 crop
   with 8 null runs and 2 injection copies of 50 objects each, against the
   reference's inject() + prepare() + search() per copy (validate.cpp:88-126).
@@ -39,10 +41,10 @@ def _frames(name, seed, crop=None):
     return wl, host, mjd, exptime
 
 
-def _compare_search(R, device, frames, mjd, exptime, params, min_peaks=1):
+def _compare_search(R, device, frames, mjd, exptime, params, min_peaks=1, search=None):
     prep = R.prepare(frames, mjd, exptime, fwhm_px=params["fwhm_px"], null_runs=params["null_runs"])
     ref = prep.search(backend="cpu", **params)
-    got = device.search(frames, mjd, exptime, **params)
+    got = (search or device.search)(frames, mjd, exptime, **params)
     assert got["fwhm"] == prep.fwhm and got["n_velocities"] == ref["n_velocities"]
     assert got["threshold"] == ref["threshold"] and got["method"] == ref["method"]
     assert (got["null_a"], got["null_k"], got["null_inv_s2"]) == (ref["null_a"], ref["null_k"], ref["null_inv_s2"])
@@ -82,6 +84,17 @@ def test_fullframe_4k_crop(device, reference):
     wl, frames, mjd, exptime = _frames("fullframe-4k", 7, crop=512)
     got, _ = _compare_search(reference, device, frames, mjd, exptime, wl.search_params(), min_peaks=100)
     assert got["n_velocities"] == 19328
+
+
+def test_large_sensor_crop_tiled(device, reference):
+    """The large-sensor sequence (60 x 9576 x 6388 frames, 30 s cadence, rates
+    0.05-3 px/min: 98,948 trial motions), a 256 x 256 crop with 2 null runs,
+    searched by the tiled path (ft_b200_search_tiled) in 64-row bands."""
+    wl, frames, mjd, exptime = _frames("large-sensor", 7, crop=256)
+    params = dict(wl.search_params(), null_runs=2)
+    got, _ = _compare_search(reference, device, frames, mjd, exptime, params, min_peaks=10,
+                             search=lambda f, m, e, **kw: device.search_tiled(f, m, e, band_rows=64, **kw))
+    assert got["n_velocities"] == 98948
 
 
 def test_batched_2k_crop_with_injection_copies(device, reference, oracle):

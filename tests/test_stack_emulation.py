@@ -13,7 +13,7 @@ import pytest
 import fainttrail_b200 as ftb
 from conftest import golden
 
-SHAPES = range(1, 8)
+SHAPES = range(1, 9)
 
 
 def same(a, b):

@@ -19,8 +19,9 @@ def run(backend, frames, **kw):
     return r.max_snr, r.best_v
 
 
-@pytest.fixture(params=[0, 1, 2, 3, 4, 5, 6, 7],
-                ids=["auto", "32x16", "64x8pair", "32x8", "32x4", "32x16shared16w", "32x16shared14w", "32x12"])
+@pytest.fixture(params=[0, 1, 2, 3, 4, 5, 6, 7, 8],
+                ids=["auto", "32x16", "64x8pair", "32x8", "32x4", "32x16shared16w", "32x16shared14w", "32x12",
+                     "32x20shared16w"])
 def shape(request):
     """Every compiled tile shape (a shape whose windows do not fit falls back)."""
     ftb.set_tile_shape(request.param)
