@@ -18,7 +18,16 @@ namespace ftb {
 
 DevBuf::DevBuf(Context* c, size_t bytes, const char* what) : ctx_(c), bytes_(bytes) {
     c->charge(bytes, what);
-    const cudaError_t e = cudaMallocAsync(&p_, std::max<size_t>(bytes, 1), c->stream());
+    p_ = c->take_cached(bytes);
+    if (p_) return;
+    cudaError_t e = cudaMallocAsync(&p_, std::max<size_t>(bytes, 1), c->stream());
+    if (e != cudaSuccess) {
+        // the cached blocks back to the device, then once more
+        cudaGetLastError();
+        c->drop_cache();
+        cudaStreamSynchronize(c->stream());
+        e = cudaMallocAsync(&p_, std::max<size_t>(bytes, 1), c->stream());
+    }
     if (e != cudaSuccess) {
         c->release(bytes);
         p_ = nullptr;
@@ -30,12 +39,38 @@ DevBuf::DevBuf(Context* c, size_t bytes, const char* what) : ctx_(c), bytes_(byt
 
 void DevBuf::reset() {
     if (p_) {
-        cudaFreeAsync(p_, ctx_->stream());
+        if (!ctx_->put_cached(p_, bytes_)) cudaFreeAsync(p_, ctx_->stream());
         ctx_->release(bytes_);
     }
     p_ = nullptr;
     bytes_ = 0;
     ctx_ = nullptr;
+}
+
+void* Context::take_cached(size_t bytes) {
+    std::lock_guard<std::mutex> lk(cache_mu_);
+    auto it = cache_.find(bytes);
+    if (it == cache_.end()) return nullptr;
+    void* p = it->second;
+    cache_.erase(it);
+    cached_ -= bytes;
+    return p;
+}
+
+bool Context::put_cached(void* p, size_t bytes) {
+    std::lock_guard<std::mutex> lk(cache_mu_);
+    if (bytes < (size_t{1} << 20) || acct_.use_count() > 1) return false;  // small blocks: the pool
+    if (cached_ + bytes > kCacheBytes || acct_->used.load() + cached_ + bytes > acct_->budget) return false;
+    cache_.emplace(bytes, p);
+    cached_ += bytes;
+    return true;
+}
+
+void Context::drop_cache() {
+    std::lock_guard<std::mutex> lk(cache_mu_);
+    for (auto& kv : cache_) cudaFreeAsync(kv.second, stream_);
+    cache_.clear();
+    cached_ = 0;
 }
 
 Context::Context(int device, double budget_bytes) {
@@ -146,6 +181,7 @@ void Context::timing_resolve() {
 Context::~Context() {
     cudaSetDevice(device_);
     scratch_.clear();
+    drop_cache();
     for (cudaEvent_t e : events_) cudaEventDestroy(e);
     if (stream_) cudaStreamSynchronize(stream_);
     if (d_err_) cudaFree(d_err_);
@@ -449,7 +485,63 @@ void clear_tuned_shapes() {
 
 // ------------------------------------------------------------------ batched passes
 
-void stack_passes_device(Context& c, std::vector<PassJob>& jobs) {
+namespace {
+
+// The configuration a pass takes when no probe has to run first: a fixed
+// shape, the autotuner's cached choice, or the frame-count rule for a pass too
+// small to tune. False when the autotuner still has to time the pass's kind.
+bool known_config(const Context& c, const PassJob& j, StackConfig& cfg) {
+    int shape = 0;
+    if (stack_shape() == 0 && static_cast<double>(j.m) * j.n * j.w * j.h >= kTuneMinAdds) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(std::make_tuple(j.n, j.m, j.w, j.h));
+        if (it == g_tuned.end()) return false;
+        shape = it->second;
+    }
+    cfg = shape > 0 ? stack_shape_config(shape, c.smem_optin()) : choose_stack_config(j.w, j.h, j.n, c.smem_optin());
+    return true;
+}
+
+bool same_config(const StackConfig& a, const StackConfig& b) {
+    return a.ty == b.ty && a.p == b.p && a.tile_w == b.tile_w && a.wp == b.wp && a.merge == b.merge &&
+           a.rows == b.rows && a.smem_bytes == b.smem_bytes;
+}
+
+}  // namespace
+
+PlanAhead plan_ahead(Context& c, std::vector<PassJob> tables) {
+    PlanAhead out;
+    out.plans.resize(tables.size());
+    auto jobs = std::make_shared<std::vector<PassJob>>(std::move(tables));
+    auto cfgs = std::make_shared<std::vector<StackConfig>>(jobs->size());
+    auto promises = std::make_shared<std::vector<std::promise<StackPlan>>>();
+    std::vector<size_t> todo;
+    for (size_t k = 0; k < jobs->size(); ++k)
+        if ((*jobs)[k].min_count <= (*jobs)[k].n && known_config(c, (*jobs)[k], (*cfgs)[k])) todo.push_back(k);
+    promises->resize(todo.size());
+    for (size_t q = 0; q < todo.size(); ++q) out.plans[todo[q]] = (*promises)[q].get_future().share();
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t workers = std::min<size_t>(hw, todo.size());
+    for (size_t wkr = 0; wkr < workers; ++wkr)
+        std::thread([jobs, cfgs, promises, todo, wkr, workers] {
+            for (size_t q = wkr; q < todo.size(); q += workers) {
+                const PassJob& j = (*jobs)[todo[q]];
+                try {
+                    StackPlan plan = make_stack_plan(j.w, j.h, j.n, j.dx.data(), j.dy.data(), j.m, j.min_count,
+                                                     motion_order(j.dx.data(), j.dy.data(), j.m, j.n, 4.0, 4.0),
+                                                     (*cfgs)[todo[q]]);
+                    plan.pitch = j.pitch;
+                    (*promises)[q].set_value(std::move(plan));
+                } catch (...) {
+                    (*promises)[q].set_exception(std::current_exception());
+                }
+            }
+        }).detach();
+    out.cfgs = *cfgs;
+    return out;
+}
+
+void stack_passes_device(Context& c, std::vector<PassJob>& jobs, PlanAhead* ahead) {
     if (jobs.empty()) return;
     // a pass whose min_count exceeds its frame count (a search's min_coverage
     // above 1) defines no S/N anywhere: its maps are filled, not stacked
@@ -482,6 +574,13 @@ void stack_passes_device(Context& c, std::vector<PassJob>& jobs) {
                     const PassJob& j = jobs[k];
                     const StackConfig cfg = shapes_for[k] > 0 ? stack_shape_config(shapes_for[k], c.smem_optin())
                                                               : choose_stack_config(j.w, j.h, j.n, c.smem_optin());
+                    // a plan made ahead for the same configuration (the tables are the job's)
+                    if (ahead && k < ahead->plans.size() && ahead->plans[k].valid() &&
+                        same_config(ahead->cfgs[k], cfg)) {
+                        plans[k] = ahead->plans[k].get();
+                        plans[k].pitch = j.pitch;
+                        continue;
+                    }
                     plans[k] = make_stack_plan(j.w, j.h, j.n, j.dx.data(), j.dy.data(), j.m, j.min_count,
                                                motion_order(j.dx.data(), j.dy.data(), j.m, j.n, 4.0, 4.0), cfg);
                     plans[k].pitch = j.pitch;
@@ -493,7 +592,7 @@ void stack_passes_device(Context& c, std::vector<PassJob>& jobs) {
     for (auto& t : pool) t.join();
     for (auto& e : errs)
         if (e) std::rethrow_exception(e);
-    c.host_time("setup", wall_seconds() - t0);
+    c.host_time("plans", wall_seconds() - t0);
     std::vector<StackPlanDev> devs(jobs.size());
     try {
         for (size_t k = 0; k < jobs.size(); ++k) devs[k].upload(plans[k], c.stream());

@@ -7,8 +7,11 @@
 #include <array>
 #include <atomic>
 #include <functional>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <future>
 #include <vector>
 
 #include "ft_internal.h"
@@ -86,6 +89,17 @@ public:
     // reusable device buffers, grown on demand
     DevBuf& scratch(int slot, size_t bytes, const char* what);
 
+    // Blocks freed by this context's DevBufs, kept by size for the next
+    // allocation of the same size (in order on the context's stream), so that
+    // repeated searches of one shape allocate nothing; at most kCacheBytes, and
+    // no more than the budget leaves beside what is charged, are kept, all of
+    // them are returned when an allocation fails, and a context whose budget
+    // account is shared with others (the server's workers) keeps none.
+    void* take_cached(size_t bytes);
+    bool put_cached(void* p, size_t bytes);  // false: not kept (the caller frees it)
+    void drop_cache();
+    static constexpr size_t kCacheBytes = size_t{48} << 30;
+
     // stage timings of the last call: CUDA-event spans on the stream, or host time
     void timing_reset();
     int span_begin(const std::string& name);   // records a start event
@@ -107,6 +121,9 @@ private:
     void init(int device);
     int* d_err_ = nullptr;
     std::vector<DevBuf> scratch_;
+    std::mutex cache_mu_;
+    std::multimap<size_t, void*> cache_;
+    size_t cached_ = 0;
     struct Span {
         std::string name;
         int a = -1, b = -1;
@@ -144,9 +161,20 @@ struct PassJob {
     int* d_bv = nullptr;
 };
 
-// Several passes, possibly of different shapes: plans built on host threads,
-// then one persistent launch per kernel shape; returns when all are complete.
-void stack_passes_device(Context& c, std::vector<PassJob>& jobs);
+// Plans built ahead on host threads: a pass's plan depends only on its shift
+// table, sizes and tile shape, so it can be made while the GPU still runs the
+// work queued before the stacking (the null runs' preprocessing). A pass whose
+// shape is not yet known (the autotuner has not timed its kind) gets none.
+struct PlanAhead {
+    std::vector<std::shared_future<StackPlan>> plans;  // per job; invalid: none
+    std::vector<StackConfig> cfgs;                     // the configuration each plan is made for
+};
+PlanAhead plan_ahead(Context& c, std::vector<PassJob> tables);
+
+// Several passes, possibly of different shapes: plans built on host threads (or
+// taken from `ahead`, in the same job order), then one persistent launch per
+// kernel shape; returns when all are complete.
+void stack_passes_device(Context& c, std::vector<PassJob>& jobs, PlanAhead* ahead = nullptr);
 
 // The tile-shape autotuner's cache: ((frames, motions, width, height), shape).
 std::vector<std::pair<std::array<int, 4>, int>> tuned_shapes();

@@ -646,13 +646,37 @@ PassJob SearchRequest::job(const float* frames, const std::vector<double>& t, fl
     return j;
 }
 
+std::vector<PassJob> SearchRequest::pass_tables(int k0, int k1) const {
+    std::vector<PassJob> jobs;
+    if (!real_queued_) jobs.push_back(job(nullptr, o_.t_h, nullptr, nullptr));
+    for (int k = k0; k < k1; ++k)
+        jobs.push_back(job(nullptr, k < runs_ ? orders_[static_cast<size_t>(k)] : o_.t_h, nullptr, nullptr));
+    return jobs;
+}
+
 void SearchRequest::stage_items(int k0, int k1, const std::vector<std::vector<Injection>>& copies,
-                                std::vector<PassJob>& jobs) {
+                                std::vector<PassJob>& jobs, size_t at) {
     Context& c = c_;
     const int w = o_.w, h = o_.h, n = o_.n;
     const bool add_real = !real_queued_;
+    // jobs[at ..] holds pass_tables(k0, k1) (the shift tables, made ahead), or
+    // at is kAppend and the jobs are appended with their tables
+    const bool tabled = at != kAppend;
+    if (tabled && jobs.size() < at + static_cast<size_t>(k1 - k0 + (add_real ? 1 : 0)))
+        throw std::runtime_error("search: pass tables do not match the batch");
+    size_t next = at;
+    auto put = [&](float* filt, const std::vector<double>& t, float* d_max, int* d_bv) {
+        if (tabled) {
+            PassJob& j = jobs[next++];
+            j.d_frames = filt;
+            j.d_max = d_max;
+            j.d_bv = d_bv;
+        } else {
+            jobs.push_back(job(filt, t, d_max, d_bv));
+        }
+    };
     if (add_real) {
-        jobs.push_back(job(filt_.as<float>(), o_.t_h, max_.as<float>(), bv_.as<int>()));
+        put(filt_.as<float>(), o_.t_h, max_.as<float>(), bv_.as<int>());
         real_queued_ = true;
     }
     for (int k = k0; k < k1; ++k) {
@@ -666,7 +690,7 @@ void SearchRequest::stage_items(int k0, int k1, const std::vector<std::vector<In
             it.mask = DevBuf(&c, sizeof(float) * plane_, "null mask");
             stage_run(c, *sc_, sub_.as<float>(), w, h, n, orders_[static_cast<size_t>(k)].data(), sp_,
                       it.filt.as<float>(), it.sky.as<float>(), it.mask.as<float>(), nullptr, nullptr);
-            jobs.push_back(job(it.filt.as<float>(), orders_[static_cast<size_t>(k)], it.max.as<float>(), it.bv.as<int>()));
+            put(it.filt.as<float>(), orders_[static_cast<size_t>(k)], it.max.as<float>(), it.bv.as<int>());
         } else {
             // an injection copy: raw frames + objects, prepared again with the same PSF width
             const int j = k - runs_;
@@ -686,7 +710,7 @@ void SearchRequest::stage_items(int k0, int k1, const std::vector<std::vector<In
                       it.sky.as<float>(), it.mask.as<float>(), it.sigma.data(), nullptr);
             FTB_CHECK(cudaMemcpyAsync(it.res.as<float>(), sc_->residual.as<float>(), sizeof(float) * plane_ * n,
                                       cudaMemcpyDeviceToDevice, c.stream()));
-            jobs.push_back(job(it.filt.as<float>(), o_.t_h, it.max.as<float>(), it.bv.as<int>()));
+            put(it.filt.as<float>(), o_.t_h, it.max.as<float>(), it.bv.as<int>());
         }
         items_.emplace(k, std::move(it));
     }
@@ -864,9 +888,12 @@ SearchOut search_batch_host(Context& c, const float* frames, int w, int h, int n
     const double share = 0.9 / (1 + items);
     for (const auto& [k0, k1] : batches) {
         report(0.1 + 0.9 * share * (k0 + 1), "null");
-        std::vector<PassJob> jobs;
-        r.stage_items(k0, k1, copies, jobs);
-        stack_passes_device(c, jobs);
+        // the passes' plans are made on host threads while the GPU runs the
+        // batch's preprocessing
+        std::vector<PassJob> jobs = r.pass_tables(k0, k1);
+        PlanAhead ahead = plan_ahead(c, jobs);
+        r.stage_items(k0, k1, copies, jobs, 0);
+        stack_passes_device(c, jobs, &ahead);
         const int pk = c.span_begin("peaks");
         r.finish_items(k0, k1);
         c.span_end(pk);

@@ -240,7 +240,15 @@ public:
     size_t item_bytes() const;                        // device bytes one null run or copy holds in flight
     void expect_copies(bool on) { copies_ = on; }     // copies hold their own frames until their refinement
     static size_t base_bytes(int w, int h, int n);    // device bytes of a prepared request
-    void stage_items(int k0, int k1, const std::vector<std::vector<Injection>>& copies, std::vector<PassJob>& jobs);
+    // The shift tables of the passes stage_items(k0, k1) queues, in its order
+    // (frame and map pointers unset), for planning ahead.
+    std::vector<PassJob> pass_tables(int k0, int k1) const;
+    // Queues the preprocessing of items [k0, k1) (and the real pass, the first
+    // time) and fills the frame and map pointers of jobs[at ..], which hold
+    // pass_tables(k0, k1); with at = kAppend the jobs are appended, tables made.
+    static constexpr size_t kAppend = ~size_t{0};
+    void stage_items(int k0, int k1, const std::vector<std::vector<Injection>>& copies, std::vector<PassJob>& jobs,
+                     size_t at = kAppend);
     void finish_items(int k0, int k1);
     SearchOut finalize(std::vector<SearchOut>* copies_out);
 

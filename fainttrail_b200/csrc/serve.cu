@@ -272,16 +272,27 @@ void Server::loop(Context& c) {
         }
         int requests_in_step = 0;
         try {
+            // every request's shift tables first, their plans made on host
+            // threads while the GPU runs the step's preprocessing
+            std::vector<size_t> at(active.size(), SearchRequest::kAppend);
             for (size_t k = 0; k < active.size(); ++k) {
                 Active& a = active[k];
                 if (!a.s || a.r->failed) continue;
                 if (take[k] == 0 && a.real_staged) continue;
-                a.s->stage_items(a.next, a.next + take[k], {}, jobs);
+                at[k] = jobs.size();
+                std::vector<PassJob> t = a.s->pass_tables(a.next, a.next + take[k]);
+                for (auto& j : t) jobs.push_back(std::move(j));
+            }
+            PlanAhead ahead = plan_ahead(c, jobs);
+            for (size_t k = 0; k < active.size(); ++k) {
+                if (at[k] == SearchRequest::kAppend) continue;
+                Active& a = active[k];
+                a.s->stage_items(a.next, a.next + take[k], {}, jobs, at[k]);
                 ranges.push_back({static_cast<int>(k), a.next, a.next + take[k]});
                 a.real_staged = true;
                 ++requests_in_step;
             }
-            if (!jobs.empty()) stack_passes_device(c, jobs);
+            if (!jobs.empty()) stack_passes_device(c, jobs, &ahead);
             for (const auto& rg : ranges) {
                 Active& a = active[static_cast<size_t>(rg[0])];
                 a.s->finish_items(rg[1], rg[2]);

@@ -316,7 +316,9 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
             if (hx - floor4(lx) + TW > WP) fits = false;
             rows += roundup(TH + hy - ly, BH);
         }
-        if (real > 1 && (!fits || rows * WP + static_cast<long long>(roundup(M * n, 8)) / 2 > budget)) {
+        const long long table1 = std::max(static_cast<long long>(roundup(M * n, 8)) / 2,
+                                          static_cast<long long>(roundup((n + 1) * 4, 16)) / 4);
+        if (real > 1 && (!fits || rows * WP + table1 > budget)) {
             for (int k = 0; k < M; ++k)
                 if (order[b + k] >= 0) blocks.insert(blocks.end(), {order[b + k], -1, -1, -1});
         } else if (real > 1 && cfg.rows > 0 && cfg.rows < kRowSpread) {
@@ -372,7 +374,12 @@ StackPlan make_stack_plan(int w, int h, int n, const int* dx, const int* dy, int
 
     // offset table of a group of `nb` blocks, in floats (the 16-bit slot table,
     // the larger of the two forms)
-    auto table_floats = [&](int nb) { return static_cast<long long>(roundup(nb * M * n, 8)) / 2; };
+    // the larger of the two table forms: 16-bit slot offsets, or row descriptors
+    // with their frame of zeros
+    auto table_floats = [&](int nb) {
+        return std::max(static_cast<long long>(roundup(nb * M * n, 8)) / 2,
+                        static_cast<long long>(roundup(nb * (n + 1) * 4, 16)) / 4);
+    };
     auto flush = [&]() {
         StackGroup g;
         g.slot0 = static_cast<int>(P.slot_motion.size());
