@@ -856,19 +856,39 @@ __device__ __forceinline__ void add_pattern(float2 (&acc)[4][H], const float2* A
     }
 }
 
+// Coverage of a border tile's pixels by a block's motions: cx counts the frames
+// whose rows cover the whole tile for every motion and whose column covers
+// this thread's pixels; cpart[k] holds, one byte a row, the frames that cover
+// row p of motion k's pixels otherwise. A pixel's frame count is cx plus its
+// byte (frames never exceed 255).
+template <int P>
+struct BorderCount {
+    static constexpr int PW = (P + 3) / 4;
+    int cx = 0;
+    uint32_t cpart[4][PW] = {};
+    __device__ __forceinline__ int count(int k, int p) const {
+        return cx + static_cast<int>((cpart[k][p >> 2] >> (8 * (p & 3))) & 0xffu);
+    }
+};
+
 // One block of 4 motions of a rows_fast group for this thread's P pixels (one
-// column, P rows), frames in ascending order, on an interior tile. In every
-// frame the block's motions read one column of the window at row offsets
-// 0..3 above the descriptor's base, so the thread loads that column once
-// (P + S rows, S = the largest row offset) and every motion adds its P rows
-// from registers. Rows are paired across the two halves of the tile, row q with
-// row q + P/2, and each pair is one add.rn.f32x2: register pair A[r] holds rows
-// (r, r + P/2), so motion k adds A[q + row offset] to its accumulator pair q
-// (rows P/2 .. P/2 + S - 1 are loaded twice, once for each pairing).
-template <int P, int WP, int SMAX>
+// column, P rows), frames in ascending order. In every frame the block's
+// motions read one column of the window at row offsets 0..3 above the
+// descriptor's base, so the thread loads that column once (P + S rows, S = the
+// largest row offset) and every motion adds its P rows from registers. Rows are
+// paired across the two halves of the tile, row q with row q + P/2, and each
+// pair is one add.rn.f32x2: register pair A[r] holds rows (r, r + P/2), so
+// motion k adds A[q + row offset] to its accumulator pair q (rows P/2 .. P/2 +
+// S - 1 are loaded twice, once for each pairing). Outside the frame the windows
+// hold +0.0f (the copies' zero fill), which adds nothing to a sum that starts
+// at +0.0f, so the sums of a border tile are the reference's truncated sums;
+// with COUNT the frames covering each pixel are counted as well, from the
+// block's first slot's shift and the descriptor's row offsets.
+template <int P, int WP, int SMAX, bool COUNT>
 __device__ __forceinline__ void rows_accumulate(const StackArgs& a, const StackGroup& G, int s0,
                                                 const float* __restrict__ win, const uint16_t* __restrict__ offs,
-                                                int tb, float2 (&acc)[4][P / 2]) {
+                                                int tb, float2 (&acc)[4][P / 2], int x, int y0,
+                                                BorderCount<P>& cov) {
     constexpr int M = 4;
     constexpr int H = P / 2;
     static_assert(P % 2 == 0, "rows are paired");
@@ -889,6 +909,26 @@ __device__ __forceinline__ void rows_accumulate(const StackArgs& a, const StackG
         float2 A[H + SMAX];
 #pragma unroll
         for (int r = 0; r < H; ++r) A[r] = make_float2(src[r * WP], src[(r + H) * WP]);
+        if constexpr (COUNT) {
+            const short2 sh = a.slot_shift[static_cast<size_t>(G.slot0 + s0) * n + i];
+            const int dylow = sh.y - static_cast<int>((d >> 16) & 3u), smax = static_cast<int>((d >> 24) & 3u);
+            const bool inx = static_cast<unsigned>(x + sh.x) < static_cast<unsigned>(a.w);
+            if (y0 + dylow >= 0 && y0 + P - 1 + dylow + smax < a.h) {
+                cov.cx += inx ? 1 : 0;
+            } else if (inx) {
+#pragma unroll
+                for (int k = 0; k < M; ++k) {
+                    const int dy = dylow + static_cast<int>((d >> (16 + 2 * k)) & 3u);
+                    const int lo = max(0, -(y0 + dy)), hi = min(P - 1, a.h - 1 - (y0 + dy));
+                    if (lo > hi) continue;
+                    // rows lo..hi as bits, then each row's bit as one byte of its word
+                    const uint32_t m = (0xffffffffu >> (31 - hi)) & (0xffffffffu << lo);
+#pragma unroll
+                    for (int w = 0; w < BorderCount<P>::PW; ++w)
+                        cov.cpart[k][w] += (((m >> (4 * w)) & 15u) * 0x00204081u) & 0x01010101u;
+                }
+            }
+        }
         if (d < (1u << 24)) {
             // every motion on the base row (no row offset, pattern 0): the most
             // common frame of a block, tested first
@@ -962,7 +1002,8 @@ __device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const Stack
                                                  int tb, float inv_n, float (&best)[P], int (&arg)[P]) {
     constexpr int H = P / 2;
     float2 acc[4][H];
-    rows_accumulate<P, WP, SMAX>(a, G, s0, win, offs, tb, acc);
+    BorderCount<P> cov;
+    rows_accumulate<P, WP, SMAX, false>(a, G, s0, win, offs, tb, acc, 0, 0, cov);
     int jk[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) jk[k] = a.slot_motion[G.slot0 + s0 + k];
@@ -976,6 +1017,47 @@ __device__ __forceinline__ void motion_quad_rows(const StackArgs& a, const Stack
     }
 }
 
+// The block's maximum at pixel row p of a border tile: each motion's sum times
+// 1 / sqrt(frames covering the pixel), motions covered by fewer than min_count
+// frames left out (backend_cpu.cpp:77-204).
+template <int P>
+__device__ __forceinline__ void border_block_max(const StackArgs& a, const float2 (&acc)[4][P / 2],
+                                                 const BorderCount<P>& cov, const int (&jk)[4], int p, float& b,
+                                                 int& bj) {
+    constexpr int H = P / 2;
+    b = -CUDART_INF_F;
+    bj = -1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int c = cov.count(k, p);
+        if (c < a.min_count) continue;
+        const float sum = p < H ? acc[k][p].x : acc[k][p - H].y;
+        block_max(__fmul_rn(sum, a.inv_sqrt[c]), jk[k], b, bj);
+    }
+}
+
+// The same block on a border tile: sums by the row-descriptor path, the frames
+// covering each pixel counted beside them.
+template <int P, int WP, int SMAX>
+__device__ __forceinline__ void motion_quad_rows_border(const StackArgs& a, const StackGroup& G, int s0,
+                                                        const float* __restrict__ win,
+                                                        const uint16_t* __restrict__ offs, int tb, int x, int y0,
+                                                        float (&best)[P], int (&arg)[P]) {
+    float2 acc[4][P / 2];
+    BorderCount<P> cov;
+    rows_accumulate<P, WP, SMAX, true>(a, G, s0, win, offs, tb, acc, x, y0, cov);
+    int jk[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) jk[k] = a.slot_motion[G.slot0 + s0 + k];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        float b;
+        int bj;
+        border_block_max<P>(a, acc, cov, jk, p, b, bj);
+        merge_max(b, bj, best[p], arg[p]);
+    }
+}
+
 // rows_accumulate for one block, its maxima into the tile's shared keys (one
 // atomic per pixel that has a motion: a block maximum above -inf).
 template <int P, int WP, int SMAX>
@@ -985,7 +1067,8 @@ __device__ __forceinline__ void motion_quad_rows_atom(const StackArgs& a, const 
                                                       unsigned long long* keys) {
     constexpr int H = P / 2;
     float2 acc[4][H];
-    rows_accumulate<P, WP, SMAX>(a, G, s0, win, offs, tb, acc);
+    BorderCount<P> cov;
+    rows_accumulate<P, WP, SMAX, false>(a, G, s0, win, offs, tb, acc, 0, 0, cov);
     int jk[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) jk[k] = a.slot_motion[G.slot0 + s0 + k];
@@ -996,6 +1079,27 @@ __device__ __forceinline__ void motion_quad_rows_atom(const StackArgs& a, const 
         rows_block_max<P>(acc, jk, inv_n, q, bl, al, bh, ah);
         if (al >= 0) atomicMax(keys + q * 32 + tb, snr_key(bl, al));
         if (ah >= 0) atomicMax(keys + (q + H) * 32 + tb, snr_key(bh, ah));
+    }
+}
+
+// The same on a border tile, into the shared keys.
+template <int P, int WP, int SMAX>
+__device__ __forceinline__ void motion_quad_rows_border_atom(const StackArgs& a, const StackGroup& G, int s0,
+                                                             const float* __restrict__ win,
+                                                             const uint16_t* __restrict__ offs, int tb, int x, int y0,
+                                                             unsigned long long* keys) {
+    float2 acc[4][P / 2];
+    BorderCount<P> cov;
+    rows_accumulate<P, WP, SMAX, true>(a, G, s0, win, offs, tb, acc, x, y0, cov);
+    int jk[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) jk[k] = a.slot_motion[G.slot0 + s0 + k];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        float b;
+        int bj;
+        border_block_max<P>(a, acc, cov, jk, p, b, bj);
+        if (bj >= 0) atomicMax(keys + p * 32 + tb, snr_key(b, bj));
     }
 }
 
@@ -1073,7 +1177,7 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
                     motion_quad_rows<P, WP, shape_row_spread(P, 0)>(a, G, s0, win, offs, tb, inv_n, best, arg);
             } else {
                 for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                    motion_quad<P, WP, true, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+                    motion_quad_rows_border<P, WP, shape_row_spread(P, 0)>(a, G, s0, win, offs, tb, x, y0, best, arg);
             }
         } else if (interior) {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
@@ -1232,7 +1336,7 @@ __device__ bool stack_tile_atom(const StackArgs& a, const CUtensorMap* tmap, int
                     motion_quad_rows_atom<P, WP, shape_row_spread(P, 1)>(a, G, s0, win, offs, tb, inv_n, keys);
             } else {
                 for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                    motion_quad_atom<P, WP, true, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
+                    motion_quad_rows_border_atom<P, WP, shape_row_spread(P, 1)>(a, G, s0, win, offs, tb, x, y0, keys);
             }
         } else if (interior) {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
