@@ -597,7 +597,7 @@ void stack_passes_device(Context& c, std::vector<PassJob>& jobs, PlanAhead* ahea
     try {
         for (size_t k = 0; k < jobs.size(); ++k) devs[k].upload(plans[k], c.stream());
         // one persistent launch per kernel shape
-        auto key = [](const StackConfig& q) { return std::make_pair(q.ty * 1000 + q.p, q.tile_w); };
+        auto key = [](const StackConfig& q) { return std::make_pair((q.ty * 1000 + q.p) * 2 + q.merge, q.tile_w); };
         std::vector<std::pair<int, int>> shapes;
         for (const auto& p : plans)
             if (std::find(shapes.begin(), shapes.end(), key(p.cfg)) == shapes.end()) shapes.push_back(key(p.cfg));
