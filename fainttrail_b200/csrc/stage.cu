@@ -81,6 +81,82 @@ __device__ __forceinline__ int nth_set_bit(uint32_t x, int k) {
     return pos;
 }
 
+// Position of the k-th (0-based) set bit of a 64-bit x, k < popc(x): the
+// half that holds it by one population count, then nth_set_bit.
+__device__ __forceinline__ int nth_set_bit64(uint64_t x, int k) {
+    const uint32_t lo = static_cast<uint32_t>(x);
+    const int c = __popc(lo);
+    const bool up = k >= c;
+    return (up ? 32 : 0) + nth_set_bit(up ? static_cast<uint32_t>(x >> 32) : lo, up ? k - c : k);
+}
+
+// sky_finish for at most 64 W64 frames: the kept sorted positions (set:
+// outside the exclusion window) in W64 64-bit words (1 or 2), the lo-th by
+// population counts (nth_set_bit64 within its word) and the hi-th, when it
+// differs, as the next set bit above it.
+template <int W64>
+__device__ __forceinline__ void sky_finish_words(const SkyArgs& a, const float* V, const float* S,
+                                                 const unsigned char* PF, int T, int t, int m_all, size_t pix,
+                                                 size_t plane) {
+    static_assert(W64 == 1 || W64 == 2, "one or two words");
+    const int n = a.n, e = a.exclude;
+    // global median: the two middle floats are added in float (preprocess.cpp:171)
+    const float mid_sum = __fadd_rn(S[((m_all - 1) / 2) * T + t], S[(m_all / 2) * T + t]);
+    const double global = 0.5 * static_cast<double>(mid_sum);
+    a.sky[pix] = __double2float_rn(global);
+    uint64_t k0 = m_all >= 64 ? ~0ull : (1ull << m_all) - 1ull;
+    uint64_t k1 = W64 == 1 || m_all <= 64 ? 0ull : (m_all >= 128 ? ~0ull : (1ull << (m_all - 64)) - 1ull);
+    int m = m_all;
+    // flips position p (255: a non-finite value, none); d: the change in m
+    auto flip = [&](int p, int d) {
+        if (p == 255) return;
+        const uint64_t b = 1ull << (p & 63);
+        if (W64 == 1 || p < 64)
+            k0 ^= b;
+        else
+            k1 ^= b;
+        m += d;
+    };
+    if (e > 0)
+        for (int r = 0; r <= min(e, n - 1); ++r) flip(PF[r * T + t], -1);  // rank 0's window
+    for (int r = 0; r < n; ++r) {
+        if (e > 0 && r > 0) {
+            if (r - 1 - e >= 0) flip(PF[(r - 1 - e) * T + t], 1);  // leaves the window: kept again
+            if (r + e < n) flip(PF[(r + e) * T + t], -1);          // enters: excluded
+        }
+        const float v = V[r * T + t];
+        float* out = a.residual + a.frame_of[r] * plane + pix;
+        if (v == CUDART_INF_F) {
+            *out = CUDART_NAN_F;
+            continue;
+        }
+        double st = global;
+        if (e > 0 && m >= 5) {
+            const int lo = (m - 1) / 2, hi = m / 2;
+            int plo, phi;
+            if (W64 == 1) {
+                plo = nth_set_bit64(k0, lo);
+                phi = hi == lo ? plo : plo + __ffsll(static_cast<long long>(k0 >> (plo + 1)));
+            } else {
+                const int c0 = __popcll(k0);
+                plo = lo < c0 ? nth_set_bit64(k0, lo) : 64 + nth_set_bit64(k1, lo - c0);
+                if (hi == lo) {
+                    phi = plo;
+                } else if (hi < c0) {  // the next kept position is in the first word
+                    phi = plo + __ffsll(static_cast<long long>(k0 >> (plo + 1)));
+                } else if (lo < c0) {  // plo is the first word's last: the second word's first
+                    phi = 63 + __ffsll(static_cast<long long>(k1));
+                } else {
+                    phi = plo + __ffsll(static_cast<long long>(k1 >> (plo - 63)));
+                }
+            }
+            // double add of the two middle values (preprocess.cpp:198)
+            st = 0.5 * (static_cast<double>(S[plo * T + t]) + static_cast<double>(S[phi * T + t]));
+        }
+        *out = __double2float_rn(static_cast<double>(v) - st);
+    }
+}
+
 // The static sky and the leave-out residuals of one pixel from its values by
 // time rank (V, +inf where not finite), its m_all finite values in sorted order
 // (S) and each rank's sorted position (PF, 255 where not finite).
@@ -189,7 +265,10 @@ __global__ void __launch_bounds__(64) sky_kernel(const SkyArgs a) {
             PF[(e0 + b) * T + t] = fin ? static_cast<unsigned char>(pos[b]) : 255;
         }
     }
-    sky_finish<W>(a, V, S, PF, T, t, m_all, pix, plane);
+    if constexpr (W <= 2)
+        sky_finish_words<1>(a, V, S, PF, T, t, m_all, pix, plane);
+    else
+        sky_finish<W>(a, V, S, PF, T, t, m_all, pix, plane);
 }
 
 // The same for n <= N <= 128 with the sorted order from a bitonic network in
@@ -284,7 +363,10 @@ __global__ void __launch_bounds__(64) sky_net_kernel(const SkyArgs a) {
             for (int f = 0; f < r; ++f) p += V[f * T + t] == v;
         PF[r * T + t] = static_cast<unsigned char>(p);
     }
-    sky_finish<W>(a, V, S, PF, T, t, m_all, pix, plane);
+    if constexpr (N <= 128)
+        sky_finish_words<(N + 63) / 64>(a, V, S, PF, T, t, m_all, pix, plane);
+    else
+        sky_finish<W>(a, V, S, PF, T, t, m_all, pix, plane);
 }
 
 // ------------------------------------------------------------------ samples + exact medians
@@ -697,7 +779,7 @@ __global__ void __launch_bounds__(256) filter_kernel(const FilterArgs a) {
 void launch_sky(const SkyArgs& a, int n, long long npix, cudaStream_t s) {
     const int T = 64;
     const size_t smem = static_cast<size_t>(T) * n * 9;
-    auto kern = n <= 32 ? sky_kernel<1> : n <= 64 ? sky_kernel<2> : n <= 128 ? sky_net_kernel<128> : sky_kernel<8>;
+    auto kern = n <= 64 ? sky_kernel<2> : n <= 128 ? sky_net_kernel<128> : sky_kernel<8>;
     allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     kern<<<static_cast<unsigned>((npix + T - 1) / T), T, smem, s>>>(a);
     FTB_CHECK(cudaGetLastError());
