@@ -866,7 +866,8 @@ __global__ void __launch_bounds__(256) filter_frames_kernel(const FilterArgs a, 
         if (f + 1 < fb) issue(((f - fa) & 1) ? Rb0 : Rb1, f + 1);
         if (tid == 0) cr_tile = 0;
         const float inv = __double2float_rn(__ddiv_rn(1.0, a.sigma[f]));
-        for (int e = tid; e < ZN; e += blockDim.x) {
+        // z of element e: (v / sigma) / weight, 0 where masked, outside or not finite
+        auto zval = [&](int e) {
             const float v = cur[e], ev = E[e];
             float z = 0.0f;
             if (ev == ev && finitef(v)) {
@@ -874,24 +875,25 @@ __global__ void __launch_bounds__(256) filter_frames_kernel(const FilterArgs a, 
                 // (v / sigma) / e, e = scatter above weight_scatter, else 1 (an exact division)
                 z = ev != 1.0f ? __fdiv_rn(vm, ev) : vm;
             }
-            Z[e] = z;
-        }
-        __syncthreads();
-        // cosmic-ray centres (preprocess.cpp:433-447): inside [1, w-2] x [1, h-2]
+            return z;
+        };
+        // z over the tile + R + 2, and in the same pass the cosmic-ray centres
+        // (preprocess.cpp:433-447, inside [1, w-2] x [1, h-2]): a z at or above
+        // the hit level takes its four neighbours' z from the residual tile
+        // (the same arithmetic as their own entries)
         for (int e = tid; e < ZN; e += blockDim.x) {
+            const float v = zval(e);
+            Z[e] = v;
             const int lx = e % ZW, ly = e / ZW;
             const int gx = x0 - H + lx, gy = y0 - H + ly;
             unsigned char flag = 0;
-            if (lx >= 1 && ly >= 1 && lx < ZW - 1 && ly < ZH - 1 && gx >= 1 && gy >= 1 && gx < a.w - 1 &&
-                gy < a.h - 1) {
-                const float v = Z[e];
-                if (v >= a.hit) {
-                    const float s4 = __fadd_rn(__fadd_rn(__fadd_rn(Z[e - 1], Z[e + 1]), Z[e - ZW]), Z[e + ZW]);
-                    const float n4 = __fmul_rn(0.25f, s4);
-                    if (!(n4 >= __fmul_rn(a.ratio, v))) {
-                        flag = 1;
-                        if (gx >= x0 && gx < x0 + TWc && gy >= y0 && gy < y0 + THc) atomicAdd(&cr_tile, 1);
-                    }
+            if (v >= a.hit && lx >= 1 && ly >= 1 && lx < ZW - 1 && ly < ZH - 1 && gx >= 1 && gy >= 1 &&
+                gx < a.w - 1 && gy < a.h - 1) {
+                const float s4 = __fadd_rn(__fadd_rn(__fadd_rn(zval(e - 1), zval(e + 1)), zval(e - ZW)), zval(e + ZW));
+                const float n4 = __fmul_rn(0.25f, s4);
+                if (!(n4 >= __fmul_rn(a.ratio, v))) {
+                    flag = 1;
+                    if (gx >= x0 && gx < x0 + TWc && gy >= y0 && gy < y0 + THc) atomicAdd(&cr_tile, 1);
                 }
             }
             F[e] = flag;
