@@ -34,7 +34,10 @@ const char* ft_b200_version(void);
 
 /* Open device `device` (-1: FAINTTRAIL_CUDA_DEVICE or 0, as the reference CUDA
  * backend resolves it, backend_cuda.cu:74-78). hbm_budget_bytes caps the device
- * memory the context allocates (0 = 90 % of the free memory). */
+ * memory the context allocates (0 = 90 % of the free memory). Blocks a call frees
+ * stay with the context for the next call's allocations of the same sizes (at
+ * most 48 GB, within the budget) until ft_b200_close, so the device memory in use
+ * does not drop between calls; an allocation that fails returns them first. */
 int ft_b200_open(int device, double hbm_budget_bytes, ft_b200_ctx** out);
 void ft_b200_close(ft_b200_ctx* ctx);
 /* Last error message of the context (ft_last_error, fainttrail.h:106); with a
