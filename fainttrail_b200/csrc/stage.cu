@@ -247,10 +247,21 @@ __global__ void __launch_bounds__(64) sky_kernel(const SkyArgs a) {
             for (int b = 0; b < B; ++b) pos[b] += vf <= ve[b];
         }
         const int e1 = min(e0 + B, n);
-        for (int f = e0; f < e1; ++f) {
-            const float vf = V[f * T + t];
+        if (e1 - e0 == B) {
+            // a full block against itself: rank e0 + c before rank e0 + b sorts an
+            // equal value first, so the comparison is fixed per (c, b) pair
 #pragma unroll
-            for (int b = 0; b < B; ++b) pos[b] += vf < ve[b] || (vf == ve[b] && f < e0 + b);
+            for (int c = 0; c < B; ++c) {
+                const float vf = V[(e0 + c) * T + t];
+#pragma unroll
+                for (int b = 0; b < B; ++b) pos[b] += c < b ? vf <= ve[b] : vf < ve[b];
+            }
+        } else {
+            for (int f = e0; f < e1; ++f) {
+                const float vf = V[f * T + t];
+#pragma unroll
+                for (int b = 0; b < B; ++b) pos[b] += vf < ve[b] || (vf == ve[b] && f < e0 + b);
+            }
         }
         for (int f = e1; f < n; ++f) {  // higher ranks: only smaller values
             const float vf = V[f * T + t];
