@@ -691,27 +691,10 @@ __device__ __forceinline__ void add_column(float (&acc)[P], const float (&v)[P])
     for (int p = 0; p < P; ++p) acc[p] = __fadd_rn(acc[p], v[p]);
 }
 
-// One block of 4 consecutive motions of a group for this thread's P pixels
-// (one column, P rows), frames in ascending order. A motion whose window offset
-// for frame i equals the previous motion's adds the P values already in
-// registers instead of loading them again; the offsets are the same for the
-// whole CTA, so these branches are warp-uniform.
-// BORDER: coverage counts. A frame that covers the whole tile for a motion (the
-// common case; a warp-uniform test) adds 1 to the motion's count, a frame that
-// covers part of it is counted per pixel (8-bit counters, 4 per register).
-// ROWS: the group's table holds row descriptors ([frame][block] 32-bit words)
-// instead of 16-bit slot offsets; the four offsets follow from the descriptor.
-template <bool ROWS, int WP>
+// The four slot offsets of a block for frame i, from the group's [frame][slot]
+// table of 16-bit window offsets.
 __device__ __forceinline__ uint2 block_offsets(const uint16_t* __restrict__ offs, const StackGroup& G, int s0, int i) {
-    if constexpr (ROWS) {
-        const uint32_t d = reinterpret_cast<const uint32_t*>(offs)[i * (G.nslots >> 2) + (s0 >> 2)];
-        const uint32_t o = d & 0xffffu;
-        const uint32_t o0 = o + ((d >> 16) & 3u) * WP, o1 = o + ((d >> 18) & 3u) * WP;
-        const uint32_t o2 = o + ((d >> 20) & 3u) * WP, o3 = o + ((d >> 22) & 3u) * WP;
-        return make_uint2(o0 | (o1 << 16), o2 | (o3 << 16));
-    } else {
-        return *reinterpret_cast<const uint2*>(offs + i * G.nslots + s0);
-    }
+    return *reinterpret_cast<const uint2*>(offs + i * G.nslots + s0);
 }
 
 // The maximum of one block's motions at one pixel. A block's slots hold its
@@ -735,7 +718,15 @@ __device__ __forceinline__ void merge_max(float b, int bj, float& best, int& arg
     }
 }
 
-template <int P, int WP, bool BORDER, bool ROWS>
+// One block of 4 consecutive motions of a group for this thread's P pixels
+// (one column, P rows), frames in ascending order. A motion whose window offset
+// for frame i equals the previous motion's adds the P values already in
+// registers instead of loading them again; the offsets are the same for the
+// whole CTA, so these branches are warp-uniform.
+// BORDER: coverage counts. A frame that covers the whole tile for a motion (the
+// common case; a warp-uniform test) adds 1 to the motion's count, a frame that
+// covers part of it is counted per pixel (8-bit counters, 4 per register).
+template <int P, int WP, bool BORDER>
 __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup& G, int s0,
                                             const float* __restrict__ win, const uint16_t* __restrict__ offs, int tb,
                                             int x, int x0, int y0, float inv_n, float (&best)[P], int (&arg)[P]) {
@@ -755,10 +746,10 @@ __device__ __forceinline__ void motion_quad(const StackArgs& a, const StackGroup
     // the next frame's four offsets are loaded one frame ahead, so the reuse
     // tests below do not wait on a shared-memory load
     const int n = a.n;  // loop bounds and table strides in registers, not reloaded from the pass arguments
-    uint2 qn = block_offsets<ROWS, WP>(offs, G, s0, 0);
+    uint2 qn = block_offsets(offs, G, s0, 0);
     for (int i = 0; i < n; ++i) {
         const uint2 q = qn;
-        if (i + 1 < n) qn = block_offsets<ROWS, WP>(offs, G, s0, i + 1);
+        if (i + 1 < n) qn = block_offsets(offs, G, s0, i + 1);
         const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
         float v[P];
         load_column<P, WP>(v, win + o0 + tb);
@@ -1181,10 +1172,10 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
             }
         } else if (interior) {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                motion_quad<P, WP, false, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+                motion_quad<P, WP, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
         } else {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                motion_quad<P, WP, true, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
+                motion_quad<P, WP, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, best, arg);
         }
     }
     // merge the warps' maxima (and, for a continued pass, the stored running ones)
@@ -1228,7 +1219,7 @@ __device__ bool stack_tile(const StackArgs& a, const CUtensorMap* tmap, int x0, 
     return true;
 }
 
-template <int P, int WP, bool BORDER, bool ROWS>
+template <int P, int WP, bool BORDER>
 __device__ __forceinline__ void motion_quad_atom(const StackArgs& a, const StackGroup& G, int s0,
                                                  const float* __restrict__ win, const uint16_t* __restrict__ offs,
                                                  int tb, int x, int x0, int y0, float inv_n, unsigned long long* keys) {
@@ -1246,10 +1237,10 @@ __device__ __forceinline__ void motion_quad_atom(const StackArgs& a, const Stack
 #pragma unroll
         for (int w = 0; w < PW; ++w) cpart[k][w] = 0;
     const int n = a.n;
-    uint2 qn = block_offsets<ROWS, WP>(offs, G, s0, 0);
+    uint2 qn = block_offsets(offs, G, s0, 0);
     for (int i = 0; i < n; ++i) {
         const uint2 q = qn;
-        if (i + 1 < n) qn = block_offsets<ROWS, WP>(offs, G, s0, i + 1);
+        if (i + 1 < n) qn = block_offsets(offs, G, s0, i + 1);
         const uint32_t o0 = q.x & 0xffffu, o1 = q.x >> 16, o2 = q.y & 0xffffu, o3 = q.y >> 16;
         float v[P];
         load_column<P, WP>(v, win + o0 + tb);
@@ -1340,10 +1331,10 @@ __device__ bool stack_tile_atom(const StackArgs& a, const CUtensorMap* tmap, int
             }
         } else if (interior) {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                motion_quad_atom<P, WP, false, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
+                motion_quad_atom<P, WP, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
         } else {
             for (int s0 = warp * M; s0 < G.nslots; s0 = next_block(block_next) * M)
-                motion_quad_atom<P, WP, true, false>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
+                motion_quad_atom<P, WP, true>(a, G, s0, win, offs, tb, x, x0, y0, inv_n, keys);
         }
     }
     __syncthreads();
