@@ -39,6 +39,10 @@ preprocessing stage alone on 2048^2 frames at 40 and 120 frames: the static-sky
 and matched-filter kernels against the HBM roofline). --no-extras skips them
 (--stage-only keeps the stage part).
 
+--workload large-sensor --once: one search of 60 x 9576 x 6388 frames with its
+32 null runs (about 12 minutes), no warm-up; prints that search's time, rate,
+stack-kernel rate, threshold and spans instead of the benchmark line.
+
 --impl reference times the reference's own CPU implementation (FaintTrail
 0.9.1 built from its sources, oracle/_ref) on the host's cores with all
 threads, each step a bounded crop of the same workload (all frames, the full
